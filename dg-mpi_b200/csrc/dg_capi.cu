@@ -1,0 +1,722 @@
+// dg_capi.cu -- the C ABI of include/dg_b200.h: context management, table
+// upload, the graph-captured RK4 loop, layout transposes and the FP64
+// reductions (L2 error, kinetic energy).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/dg_b200.h"
+#include "../host/case.h"
+#include "../host/mesh.h"
+#include "../host/numerics.h"
+#include "dg_stage.cuh"
+
+using dgk::GeoDev;
+using dgk::StageArgs;
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// per-order launch configuration of the stage kernel: elements per CTA and
+// threads per CTA (shared memory = E * per-element working set)
+template <int P> struct Cfg;
+template <> struct Cfg<0> { static constexpr int E = 32, NT = 128; };
+template <> struct Cfg<1> { static constexpr int E = 8, NT = 128; };
+template <> struct Cfg<2> { static constexpr int E = 6, NT = 96; };
+template <> struct Cfg<3> { static constexpr int E = 4, NT = 128; };
+template <> struct Cfg<4> { static constexpr int E = 3, NT = 128; };
+template <> struct Cfg<5> { static constexpr int E = 3, NT = 160; };
+
+// tables of the IC / error rule (2*max(p,1)+2 points) and of the volume rule
+constexpr int kMaxMe = 12;
+__constant__ double cBe[dgk::kMaxP + 1][kMaxMe * (dgk::kMaxP + 1)];
+__constant__ double cWe[dgk::kMaxP + 1][kMaxMe];
+__constant__ double cXe[dgk::kMaxP + 1][kMaxMe];
+__constant__ double cXq[dgk::kMaxP + 1][dgk::kMaxP + 2];
+
+std::mutex g_table_mutex;
+bool g_tables_loaded[64] = {};
+thread_local std::string g_create_error;
+
+}  // namespace
+
+struct dg_ctx {
+    int device = 0, p = 0, nb = 0, ne = 0, flux = 0, precision = 0;
+    double gamma = 1.4, R = 287.05;
+    cudaStream_t stream = nullptr;
+    double *d_U0 = nullptr, *d_Ua = nullptr, *d_Ub = nullptr, *d_acc = nullptr, *d_out = nullptr;
+    int2* d_conn = nullptr;
+    int* d_geo_class = nullptr;
+    GeoDev* d_geo = nullptr;
+    uint8_t* d_cmap = nullptr;
+    double* d_X0 = nullptr;
+    double* d_partials = nullptr;
+    unsigned* d_status = nullptr;
+    int stage_grid = 0, red_grid = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    double graph_dt = 0.0;
+    dgh::PreparedMesh pm;
+    dgh::Tables1D tab;
+    unsigned status_accum = 0;
+    std::string err;
+};
+
+namespace {
+
+int fail(dg_ctx* c, int code, const std::string& msg)
+{
+    if (c) c->err = msg;
+    else g_create_error = msg;
+    return code;
+}
+
+#define DG_CUDA(c, call)                                                                         \
+    do {                                                                                         \
+        cudaError_t e_ = (call);                                                                 \
+        if (e_ != cudaSuccess)                                                                   \
+            return fail((c), DG_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));   \
+    } while (0)
+
+int load_constant_tables(dg_ctx* c)
+{
+    std::lock_guard<std::mutex> lk(g_table_mutex);
+    if (c->device >= 0 && c->device < 64 && g_tables_loaded[c->device]) return DG_OK;
+    double B[dgk::kMaxP + 1][dgk::kTabB] = {}, Dm[dgk::kMaxP + 1][dgk::kTabB] = {};
+    double W[dgk::kMaxP + 1][dgk::kMaxP + 2] = {}, Mi[dgk::kMaxP + 1][(dgk::kMaxP + 1) * (dgk::kMaxP + 1)] = {};
+    double Be[dgk::kMaxP + 1][kMaxMe * (dgk::kMaxP + 1)] = {}, We[dgk::kMaxP + 1][kMaxMe] = {};
+    double Xe[dgk::kMaxP + 1][kMaxMe] = {}, Xq[dgk::kMaxP + 1][dgk::kMaxP + 2] = {};
+    for (int p = 0; p <= dgk::kMaxP; ++p) {
+        const dgh::Tables1D t = dgh::make_tables(p);
+        std::copy(t.B.begin(), t.B.end(), B[p]);
+        std::copy(t.D.begin(), t.D.end(), Dm[p]);
+        std::copy(t.wq.begin(), t.wq.end(), W[p]);
+        std::copy(t.xq.begin(), t.xq.end(), Xq[p]);
+        std::copy(t.Minv.begin(), t.Minv.end(), Mi[p]);
+        std::copy(t.Be.begin(), t.Be.end(), Be[p]);
+        std::copy(t.we.begin(), t.we.end(), We[p]);
+        std::copy(t.xe.begin(), t.xe.end(), Xe[p]);
+    }
+    DG_CUDA(c, cudaMemcpyToSymbol(dgk::cB, B, sizeof(B)));
+    DG_CUDA(c, cudaMemcpyToSymbol(dgk::cD, Dm, sizeof(Dm)));
+    DG_CUDA(c, cudaMemcpyToSymbol(dgk::cW, W, sizeof(W)));
+    DG_CUDA(c, cudaMemcpyToSymbol(dgk::cMinv, Mi, sizeof(Mi)));
+    DG_CUDA(c, cudaMemcpyToSymbol(cBe, Be, sizeof(Be)));
+    DG_CUDA(c, cudaMemcpyToSymbol(cWe, We, sizeof(We)));
+    DG_CUDA(c, cudaMemcpyToSymbol(cXe, Xe, sizeof(Xe)));
+    DG_CUDA(c, cudaMemcpyToSymbol(cXq, Xq, sizeof(Xq)));
+    if (c->device >= 0 && c->device < 64) g_tables_loaded[c->device] = true;
+    return DG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// stage launches
+
+template <int P>
+int launch_stage_p(dg_ctx* c, const StageArgs& a)
+{
+    constexpr int E = Cfg<P>::E, NT = Cfg<P>::NT;
+    constexpr size_t smem = dgk::stage_smem_bytes<P, E>();
+    static_assert(smem <= 227 * 1024, "stage kernel shared memory exceeds 227 KB");
+    auto kern = dgk::stage_kernel<P, E, NT>;
+    if (c->stage_grid == 0) {
+        DG_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int dev_sms = 0, per_sm = 0;
+        DG_CUDA(c, cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, c->device));
+        DG_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem));
+        if (per_sm < 1) return fail(c, DG_ERR_UNSUPPORTED, "stage kernel does not fit on an SM");
+        const int batches = (c->ne + E - 1) / E;
+        c->stage_grid = std::max(1, std::min(batches, dev_sms * per_sm));
+    }
+    kern<<<c->stage_grid, NT, smem, c->stream>>>(a);
+    DG_CUDA(c, cudaGetLastError());
+    return DG_OK;
+}
+
+int launch_stage(dg_ctx* c, int mode, const double* Us, const double* U0, double* out, double dt)
+{
+    StageArgs a{};
+    a.Us = Us;
+    a.U0 = U0;
+    a.acc = c->d_acc;
+    a.out = out;
+    a.conn = c->d_conn;
+    a.geo_class = c->d_geo_class;
+    a.geo = c->d_geo;
+    a.cmap = c->d_cmap;
+    a.status = c->d_status;
+    a.ne = c->ne;
+    a.flux = c->flux;
+    a.mode = mode;
+    a.gamma = c->gamma;
+    a.dt = dt;
+    switch (c->p) {
+        case 0: return launch_stage_p<0>(c, a);
+        case 1: return launch_stage_p<1>(c, a);
+        case 2: return launch_stage_p<2>(c, a);
+        case 3: return launch_stage_p<3>(c, a);
+        case 4: return launch_stage_p<4>(c, a);
+        case 5: return launch_stage_p<5>(c, a);
+        default: return fail(c, DG_ERR_UNSUPPORTED, "order out of range");
+    }
+}
+
+// ---------------------------------------------------------------------------
+// layout transposes between the host layout [ne][nb][5] and the device
+// layout [ne][5][nb]
+
+__global__ void to_device_layout(const double* __restrict__ src, double* __restrict__ dst, long long n, int nb)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const long long e = i / (5LL * nb);
+        const int r = (int)(i - e * 5LL * nb), v = r / nb, b = r - v * nb;
+        dst[i] = src[(e * nb + b) * 5 + v];
+    }
+}
+
+__global__ void to_host_layout(const double* __restrict__ src, double* __restrict__ dst, long long n, int nb)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const long long e = i / (5LL * nb);
+        const int r = (int)(i - e * 5LL * nb), b = r / 5, v = r - b * 5;
+        dst[i] = src[(e * 5 + v) * nb + b];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// reductions: one CTA per element (grid-stride), threads over points; per-CTA
+// partial sums land in a scratch array that the host adds in a fixed order.
+
+struct ReduceArgs {
+    const double* U;        // device state [ne][5][nb]
+    const int* geo_class;
+    const GeoDev* geo;
+    const double* X0;       // [ne][3]
+    const double* J;        // [nclasses][9]
+    double* partials;       // [gridDim.x][5]
+    int ne, ic_type, kind;  // kind 0: L2 error, 1: kinetic energy
+    double gamma, R, t;
+    double data[16];
+};
+
+template <int P>
+__global__ void __launch_bounds__(256) reduce_kernel(ReduceArgs a)
+{
+    constexpr int N = P + 1, NB = N * N * N;
+    __shared__ double sU[5 * NB];
+    __shared__ double red[5][256];
+    const int me = a.kind == 0 ? (P > 1 ? 2 * P + 2 : 4) : P + 2;
+    const double* Bq = a.kind == 0 ? cBe[P] : dgk::cB[P];
+    const double* Wq = a.kind == 0 ? cWe[P] : dgk::cW[P];
+    const double* Xq = a.kind == 0 ? cXe[P] : cXq[P];
+    double acc[5] = {0, 0, 0, 0, 0};
+    for (int e = blockIdx.x; e < a.ne; e += gridDim.x) {
+        __syncthreads();
+        for (int i = threadIdx.x; i < 5 * NB; i += blockDim.x) sU[i] = a.U[(size_t)e * 5 * NB + i];
+        __syncthreads();
+        const int cls = a.geo_class[e];
+        const double* J = a.J + cls * 9;
+        const double djac = 1.0 / a.geo[cls].inv_djac;
+        for (int q = threadIdx.x; q < me * me * me; q += blockDim.x) {
+            const int i = q % me, j = (q / me) % me, k = q / (me * me);
+            double Uq[5];
+#pragma unroll
+            for (int v = 0; v < 5; ++v) {
+                double sz = 0.0;
+                for (int bz = 0; bz < N; ++bz) {
+                    double sy = 0.0;
+                    for (int by = 0; by < N; ++by) {
+                        double sx = 0.0;
+#pragma unroll
+                        for (int bx = 0; bx < N; ++bx) sx += Bq[i * N + bx] * sU[v * NB + (bz * N + by) * N + bx];
+                        sy += Bq[j * N + by] * sx;
+                    }
+                    sz += Bq[k * N + bz] * sy;
+                }
+                Uq[v] = sz;
+            }
+            const double w = (Wq[i] * Wq[j]) * Wq[k] * djac;
+            if (a.kind == 0) {
+                const double xi[3] = {Xq[i] + 1.0, Xq[j] + 1.0, Xq[k] + 1.0};
+                double x[3], Ue[5];
+                for (int d = 0; d < 3; ++d)
+                    x[d] = a.X0[(size_t)e * 3 + d] + J[d * 3 + 0] * xi[0] + J[d * 3 + 1] * xi[1] + J[d * 3 + 2] * xi[2];
+                dgp::initial_state(a.ic_type, a.data, a.gamma, a.R, x, a.t, Ue);
+#pragma unroll
+                for (int v = 0; v < 5; ++v) {
+                    const double d = Uq[v] - Ue[v];
+                    acc[v] += d * d * w;
+                }
+            } else {
+                acc[0] += 0.5 * (Uq[1] * Uq[1] + Uq[2] * Uq[2] + Uq[3] * Uq[3]) / Uq[0] * w;
+            }
+        }
+    }
+    __syncthreads();
+    for (int v = 0; v < 5; ++v) red[v][threadIdx.x] = acc[v];
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s)
+            for (int v = 0; v < 5; ++v) red[v][threadIdx.x] += red[v][threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int v = 0; v < 5; ++v) a.partials[blockIdx.x * 5 + v] = red[v][0];
+}
+
+int run_reduce(dg_ctx* c, int kind, int ic_type, const double* data, int ndata, double t, double* out5)
+{
+    ReduceArgs a{};
+    a.U = c->d_U0;
+    a.geo_class = c->d_geo_class;
+    a.geo = c->d_geo;
+    a.X0 = c->d_X0;
+    a.partials = c->d_partials;
+    a.ne = c->ne;
+    a.ic_type = ic_type;
+    a.kind = kind;
+    a.gamma = c->gamma;
+    a.R = c->R;
+    a.t = t;
+    for (int i = 0; i < ndata && i < 16; ++i) a.data[i] = data[i];
+    // per-class Jacobians, kept on the device after the classes
+    a.J = reinterpret_cast<const double*>(c->d_geo + c->pm.classes.size());
+    switch (c->p) {
+        case 0: reduce_kernel<0><<<c->red_grid, 256, 0, c->stream>>>(a); break;
+        case 1: reduce_kernel<1><<<c->red_grid, 256, 0, c->stream>>>(a); break;
+        case 2: reduce_kernel<2><<<c->red_grid, 256, 0, c->stream>>>(a); break;
+        case 3: reduce_kernel<3><<<c->red_grid, 256, 0, c->stream>>>(a); break;
+        case 4: reduce_kernel<4><<<c->red_grid, 256, 0, c->stream>>>(a); break;
+        case 5: reduce_kernel<5><<<c->red_grid, 256, 0, c->stream>>>(a); break;
+        default: return fail(c, DG_ERR_UNSUPPORTED, "order out of range");
+    }
+    DG_CUDA(c, cudaGetLastError());
+    std::vector<double> part(static_cast<size_t>(c->red_grid) * 5);
+    DG_CUDA(c, cudaMemcpyAsync(part.data(), c->d_partials, part.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    DG_CUDA(c, cudaStreamSynchronize(c->stream));
+    for (int v = 0; v < 5; ++v) out5[v] = 0.0;
+    for (int b = 0; b < c->red_grid; ++b)
+        for (int v = 0; v < 5; ++v) out5[v] += part[static_cast<size_t>(b) * 5 + v];
+    return DG_OK;
+}
+
+int check_status(dg_ctx* c)
+{
+    unsigned st = 0;
+    DG_CUDA(c, cudaMemcpyAsync(&st, c->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
+    DG_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (st) {
+        c->status_accum |= st;
+        DG_CUDA(c, cudaMemsetAsync(c->d_status, 0, sizeof(unsigned), c->stream));
+        DG_CUDA(c, cudaStreamSynchronize(c->stream));
+        char buf[160];
+        snprintf(buf, sizeof(buf), "non-physical state detected on the device (status 0x%x)", st);
+        return fail(c, DG_ERR_NONPHYSICAL, buf);
+    }
+    return DG_OK;
+}
+
+int upload_state_host_layout(dg_ctx* c, const double* Uc, double* dst)
+{
+    const size_t n = static_cast<size_t>(c->ne) * c->nb * 5;
+    DG_CUDA(c, cudaMemcpyAsync(c->d_out, Uc, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    to_device_layout<<<1024, 256, 0, c->stream>>>(c->d_out, dst, (long long)n, c->nb);
+    DG_CUDA(c, cudaGetLastError());
+    DG_CUDA(c, cudaStreamSynchronize(c->stream));
+    return DG_OK;
+}
+
+int download_host_layout(dg_ctx* c, const double* src, double* Uc)
+{
+    const size_t n = static_cast<size_t>(c->ne) * c->nb * 5;
+    to_host_layout<<<1024, 256, 0, c->stream>>>(src, c->d_acc == src ? c->d_out : c->d_Ub, (long long)n, c->nb);
+    DG_CUDA(c, cudaGetLastError());
+    DG_CUDA(c, cudaMemcpyAsync(Uc, c->d_acc == src ? c->d_out : c->d_Ub, n * sizeof(double), cudaMemcpyDeviceToHost,
+                               c->stream));
+    DG_CUDA(c, cudaStreamSynchronize(c->stream));
+    return DG_OK;
+}
+
+void release(dg_ctx* c)
+{
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+    if (c->graph) cudaGraphDestroy(c->graph);
+    cudaFree(c->d_U0); cudaFree(c->d_Ua); cudaFree(c->d_Ub); cudaFree(c->d_acc); cudaFree(c->d_out);
+    cudaFree(c->d_conn); cudaFree(c->d_geo_class); cudaFree(c->d_geo); cudaFree(c->d_cmap);
+    cudaFree(c->d_X0); cudaFree(c->d_partials); cudaFree(c->d_status);
+    if (c->stream) cudaStreamDestroy(c->stream);
+}
+
+}  // namespace
+
+// ===========================================================================
+extern "C" {
+
+int dg_create(const dg_case_desc* cd, const dg_mesh_desc* md, dg_ctx** out)
+{
+    g_create_error.clear();
+    if (!cd || !md || !out) return fail(nullptr, DG_ERR_ARG, "dg_create: null argument");
+    *out = nullptr;
+    if (cd->order < 0 || cd->order > dgk::kMaxP) return fail(nullptr, DG_ERR_UNSUPPORTED, "order must be 0..5");
+    if (cd->flux != DG_FLUX_LAX_FRIEDRICHS && cd->flux != DG_FLUX_HLLC) return fail(nullptr, DG_ERR_ARG, "unknown flux");
+    if (!(cd->gamma > 1.0)) return fail(nullptr, DG_ERR_ARG, "gamma must exceed 1");
+    if (cd->precision != DG_PREC_FP64)
+        return fail(nullptr, DG_ERR_UNSUPPORTED, "only the FP64 residual is built into this library");
+
+    dg_ctx* c = new (std::nothrow) dg_ctx();
+    if (!c) return fail(nullptr, DG_ERR_NOMEM, "host allocation failed");
+    c->device = cd->device;
+    c->p = cd->order;
+    c->nb = (c->p + 1) * (c->p + 1) * (c->p + 1);
+    c->flux = cd->flux;
+    c->gamma = cd->gamma;
+    c->R = cd->gas_constant;
+    c->precision = cd->precision;
+
+    dgh::MeshView mv;
+    mv.nnode = md->nnode;
+    mv.nelem = md->nelem;
+    mv.nface = md->nface;
+    mv.rank = md->rank;
+    mv.coords = md->node_coords;
+    mv.e2n = md->elem_to_node_ids;
+    mv.faces = md->interior_faces;
+    std::string perr;
+    try {
+        perr = dgh::prepare_mesh(mv, c->p + 2, c->pm);
+        c->tab = dgh::make_tables(c->p);
+    } catch (const std::exception& ex) {
+        perr = std::string("mesh preparation failed: ") + ex.what();
+    }
+    if (!perr.empty()) {
+        delete c;
+        const bool unsup = perr.rfind("unsupported:", 0) == 0;
+        return fail(nullptr, unsup ? DG_ERR_UNSUPPORTED : DG_ERR_ARG, perr);
+    }
+    c->ne = c->pm.ne;
+
+    // the mesh is valid; now the device
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        delete c;
+        return fail(nullptr, DG_ERR_CUDA, "no CUDA device available");
+    }
+    if (cd->device < 0 || cd->device >= ndev) {
+        delete c;
+        return fail(nullptr, DG_ERR_ARG, "device ordinal out of range");
+    }
+
+    int rc = DG_OK;
+    auto bail = [&](int code) {
+        g_create_error = c->err;
+        release(c);
+        delete c;
+        return code;
+    };
+    if (cudaSetDevice(c->device) != cudaSuccess) {
+        c->err = "cudaSetDevice failed";
+        return bail(DG_ERR_CUDA);
+    }
+    if ((rc = load_constant_tables(c)) != DG_OK) return bail(rc);
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        c->err = "cudaStreamCreate failed";
+        return bail(DG_ERR_CUDA);
+    }
+    const size_t nstate = static_cast<size_t>(c->ne) * c->nb * 5;
+    const size_t ncls = c->pm.classes.size();
+    int dev_sms = 0;
+    cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, c->device);
+    c->red_grid = std::max(1, std::min(c->ne, 4 * dev_sms));
+    struct Alloc { void** p; size_t bytes; } allocs[] = {
+        {(void**)&c->d_U0, nstate * sizeof(double)},
+        {(void**)&c->d_Ua, nstate * sizeof(double)},
+        {(void**)&c->d_Ub, nstate * sizeof(double)},
+        {(void**)&c->d_acc, nstate * sizeof(double)},
+        {(void**)&c->d_out, nstate * sizeof(double)},
+        {(void**)&c->d_conn, static_cast<size_t>(c->ne) * 6 * sizeof(int2)},
+        {(void**)&c->d_geo_class, static_cast<size_t>(c->ne) * sizeof(int)},
+        {(void**)&c->d_geo, ncls * (sizeof(GeoDev) + 9 * sizeof(double))},
+        {(void**)&c->d_cmap, std::max<size_t>(1, c->pm.cmap.size())},
+        {(void**)&c->d_X0, static_cast<size_t>(c->ne) * 3 * sizeof(double)},
+        {(void**)&c->d_partials, static_cast<size_t>(c->red_grid) * 5 * sizeof(double)},
+        {(void**)&c->d_status, sizeof(unsigned)},
+    };
+    for (auto& al : allocs) {
+        if (cudaMalloc(al.p, al.bytes) != cudaSuccess) {
+            cudaGetLastError();
+            c->err = "device allocation of " + std::to_string(al.bytes) + " bytes failed";
+            return bail(DG_ERR_NOMEM);
+        }
+    }
+    // geometry classes, followed by their Jacobians (used by the reductions)
+    std::vector<unsigned char> geo_blob(ncls * (sizeof(GeoDev) + 9 * sizeof(double)));
+    for (size_t k = 0; k < ncls; ++k) {
+        GeoDev g{};
+        const auto& src = c->pm.classes[k];
+        std::memcpy(g.JD, src.JD, sizeof(g.JD));
+        g.inv_djac = src.inv_djac;
+        std::memcpy(g.N, src.N, sizeof(g.N));
+        std::memcpy(geo_blob.data() + k * sizeof(GeoDev), &g, sizeof(GeoDev));
+        std::memcpy(geo_blob.data() + ncls * sizeof(GeoDev) + k * 9 * sizeof(double), src.J, 9 * sizeof(double));
+    }
+    std::vector<int2> conn(static_cast<size_t>(c->ne) * 6);
+    for (size_t i = 0; i < conn.size(); ++i) conn[i] = make_int2(c->pm.conn[i * 2], c->pm.conn[i * 2 + 1]);
+    bool ok = cudaMemcpy(c->d_geo, geo_blob.data(), geo_blob.size(), cudaMemcpyHostToDevice) == cudaSuccess &&
+              cudaMemcpy(c->d_conn, conn.data(), conn.size() * sizeof(int2), cudaMemcpyHostToDevice) == cudaSuccess &&
+              cudaMemcpy(c->d_geo_class, c->pm.geo_class.data(), c->ne * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess &&
+              cudaMemcpy(c->d_X0, c->pm.X0.data(), c->pm.X0.size() * sizeof(double), cudaMemcpyHostToDevice) == cudaSuccess &&
+              (c->pm.cmap.empty() || cudaMemcpy(c->d_cmap, c->pm.cmap.data(), c->pm.cmap.size(), cudaMemcpyHostToDevice) == cudaSuccess) &&
+              cudaMemset(c->d_status, 0, sizeof(unsigned)) == cudaSuccess &&
+              cudaMemset(c->d_U0, 0, nstate * sizeof(double)) == cudaSuccess &&
+              cudaMemset(c->d_acc, 0, nstate * sizeof(double)) == cudaSuccess;
+    if (!ok) {
+        c->err = std::string("table upload failed: ") + cudaGetErrorString(cudaGetLastError());
+        return bail(DG_ERR_CUDA);
+    }
+    *out = c;
+    return DG_OK;
+}
+
+void dg_destroy(dg_ctx* ctx)
+{
+    if (!ctx) return;
+    release(ctx);
+    delete ctx;
+}
+
+const char* dg_last_error(const dg_ctx* ctx)
+{
+    if (!ctx) return g_create_error.c_str();
+    return ctx->err.c_str();
+}
+
+int dg_num_basis(const dg_ctx* ctx) { return ctx ? ctx->nb : 0; }
+int dg_num_elements(const dg_ctx* ctx) { return ctx ? ctx->ne : 0; }
+
+int dg_set_state(dg_ctx* c, const double* Uc)
+{
+    if (!c || !Uc) return fail(c, DG_ERR_ARG, "dg_set_state: null argument");
+    DG_CUDA(c, cudaSetDevice(c->device));
+    return upload_state_host_layout(c, Uc, c->d_U0);
+}
+
+int dg_get_state(dg_ctx* c, double* Uc)
+{
+    if (!c || !Uc) return fail(c, DG_ERR_ARG, "dg_get_state: null argument");
+    DG_CUDA(c, cudaSetDevice(c->device));
+    return download_host_layout(c, c->d_U0, Uc);
+}
+
+int dg_residual(dg_ctx* c, double* res)
+{
+    if (!c || !res) return fail(c, DG_ERR_ARG, "dg_residual: null argument");
+    DG_CUDA(c, cudaSetDevice(c->device));
+    int rc = launch_stage(c, dgk::kModeResidual, c->d_U0, c->d_U0, c->d_acc, 0.0);
+    if (rc) return rc;
+    rc = download_host_layout(c, c->d_acc, res);
+    if (rc) return rc;
+    return check_status(c);
+}
+
+int dg_mass_inverse_residual(dg_ctx* c, double dt, double* dU)
+{
+    if (!c || !dU) return fail(c, DG_ERR_ARG, "dg_mass_inverse_residual: null argument");
+    DG_CUDA(c, cudaSetDevice(c->device));
+    int rc = launch_stage(c, dgk::kModeMassInv, c->d_U0, c->d_U0, c->d_acc, dt);
+    if (rc) return rc;
+    rc = download_host_layout(c, c->d_acc, dU);
+    if (rc) return rc;
+    return check_status(c);
+}
+
+int dg_rk4_steps(dg_ctx* c, double dt, int nsteps)
+{
+    if (!c || nsteps < 0) return fail(c, DG_ERR_ARG, "dg_rk4_steps: bad argument");
+    if (nsteps == 0) return DG_OK;
+    DG_CUDA(c, cudaSetDevice(c->device));
+    if (!c->graph_exec || c->graph_dt != dt) {
+        if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }
+        if (c->graph) { cudaGraphDestroy(c->graph); c->graph = nullptr; }
+        // first launches outside capture set the kernel attributes and grid
+        if (c->stage_grid == 0) {
+            int rc = launch_stage(c, dgk::kModeMassInv, c->d_U0, c->d_U0, c->d_out, 0.0);
+            if (rc) return rc;
+            DG_CUDA(c, cudaStreamSynchronize(c->stream));
+        }
+        DG_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        int rc = launch_stage(c, dgk::kModeRK1, c->d_U0, c->d_U0, c->d_Ua, dt);
+        if (!rc) rc = launch_stage(c, dgk::kModeRK2, c->d_Ua, c->d_U0, c->d_Ub, dt);
+        if (!rc) rc = launch_stage(c, dgk::kModeRK3, c->d_Ub, c->d_U0, c->d_Ua, dt);
+        if (!rc) rc = launch_stage(c, dgk::kModeRK4, c->d_Ua, c->d_U0, c->d_U0, dt);
+        cudaGraph_t g = nullptr;
+        cudaError_t ce = cudaStreamEndCapture(c->stream, &g);
+        if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+        if (ce != cudaSuccess) return fail(c, DG_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+        c->graph = g;
+        DG_CUDA(c, cudaGraphInstantiate(&c->graph_exec, c->graph, 0));
+        c->graph_dt = dt;
+    }
+    for (int s = 0; s < nsteps; ++s) DG_CUDA(c, cudaGraphLaunch(c->graph_exec, c->stream));
+    DG_CUDA(c, cudaStreamSynchronize(c->stream));
+    return check_status(c);
+}
+
+int dg_fe_steps(dg_ctx* c, double dt, int nsteps)
+{
+    if (!c || nsteps < 0) return fail(c, DG_ERR_ARG, "dg_fe_steps: bad argument");
+    DG_CUDA(c, cudaSetDevice(c->device));
+    for (int s = 0; s < nsteps; ++s) {
+        int rc = launch_stage(c, dgk::kModeFE, c->d_U0, c->d_U0, c->d_Ua, dt);
+        if (rc) return rc;
+        std::swap(c->d_U0, c->d_Ua);
+    }
+    // the RK4 graph captured the old buffer addresses
+    if (nsteps > 0 && c->graph_exec) {
+        cudaGraphExecDestroy(c->graph_exec);
+        cudaGraphDestroy(c->graph);
+        c->graph_exec = nullptr;
+        c->graph = nullptr;
+    }
+    DG_CUDA(c, cudaStreamSynchronize(c->stream));
+    return check_status(c);
+}
+
+int dg_project_ic(dg_ctx* c, int ic_type, const double* data, int ndata, double t, double* Uc)
+{
+    if (!c) return fail(c, DG_ERR_ARG, "dg_project_ic: null context");
+    if (ic_type < DG_IC_UNIFORM || ic_type > DG_IC_TAYLOR_GREEN) return fail(c, DG_ERR_ARG, "unknown initial condition");
+    double d[16] = {0};
+    for (int i = 0; i < ndata && i < 16; ++i) d[i] = data[i];
+    const int need[] = {5, 0, 0, 9, 1};
+    if (ndata < need[ic_type]) return fail(c, DG_ERR_ARG, "initial condition needs more data values");
+    std::vector<double> U(static_cast<size_t>(c->ne) * c->nb * 5);
+    dgh::project_initial_condition(c->pm, c->tab, ic_type, d, c->gamma, c->R, t, U.data());
+    if (Uc) std::memcpy(Uc, U.data(), U.size() * sizeof(double));
+    DG_CUDA(c, cudaSetDevice(c->device));
+    return upload_state_host_layout(c, U.data(), c->d_U0);
+}
+
+int dg_l2_error(dg_ctx* c, int ic_type, const double* data, int ndata, double t, double* err)
+{
+    if (!c || !err) return fail(c, DG_ERR_ARG, "dg_l2_error: null argument");
+    if (ic_type < DG_IC_UNIFORM || ic_type > DG_IC_TAYLOR_GREEN) return fail(c, DG_ERR_ARG, "unknown exact solution");
+    DG_CUDA(c, cudaSetDevice(c->device));
+    double sums[5];
+    int rc = run_reduce(c, 0, ic_type, data, ndata, t, sums);
+    if (rc) return rc;
+    for (int v = 0; v < 5; ++v) err[v] = std::sqrt(sums[v] / c->pm.volume);
+    return DG_OK;
+}
+
+int dg_kinetic_energy(dg_ctx* c, double* ke)
+{
+    if (!c || !ke) return fail(c, DG_ERR_ARG, "dg_kinetic_energy: null argument");
+    DG_CUDA(c, cudaSetDevice(c->device));
+    double sums[5];
+    int rc = run_reduce(c, 1, 0, nullptr, 0, 0.0, sums);
+    if (rc) return rc;
+    *ke = sums[0] / c->pm.volume;
+    return DG_OK;
+}
+
+int dg_total_volume(const dg_ctx* c, double* vol)
+{
+    if (!c || !vol) return DG_ERR_ARG;
+    *vol = c->pm.volume;
+    return DG_OK;
+}
+
+int dg_status(dg_ctx* c, unsigned* flags)
+{
+    if (!c || !flags) return fail(c, DG_ERR_ARG, "dg_status: null argument");
+    unsigned st = 0;
+    DG_CUDA(c, cudaSetDevice(c->device));
+    DG_CUDA(c, cudaMemcpy(&st, c->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    DG_CUDA(c, cudaMemset(c->d_status, 0, sizeof(unsigned)));
+    *flags = st | c->status_accum;
+    c->status_accum = 0;
+    return DG_OK;
+}
+
+int dg_sync(dg_ctx* c)
+{
+    if (!c) return DG_ERR_ARG;
+    DG_CUDA(c, cudaSetDevice(c->device));
+    DG_CUDA(c, cudaStreamSynchronize(c->stream));
+    return DG_OK;
+}
+
+void* dg_device_state(dg_ctx* c) { return c ? c->d_U0 : nullptr; }
+
+int dg_mesh_periodic_box(const int n[3], const double x0[3], const double len[3], unsigned rotate_seed,
+                         int* nnode, double* node_coords, int* nelem, unsigned* elem_to_node_ids, int* nface,
+                         unsigned* interior_faces)
+{
+    if (!n || !x0 || !len || !nnode || !nelem || !nface) return DG_ERR_ARG;
+    if (n[0] < 1 || n[1] < 1 || n[2] < 1) return DG_ERR_ARG;
+    const long long ne = 1LL * n[0] * n[1] * n[2];
+    if (ne > (1LL << 30)) return DG_ERR_ARG;
+    *nnode = (n[0] + 1) * (n[1] + 1) * (n[2] + 1);
+    *nelem = static_cast<int>(ne);
+    *nface = static_cast<int>(3 * ne);
+    if (!node_coords && !elem_to_node_ids && !interior_faces) return DG_OK;
+    if (!node_coords || !elem_to_node_ids || !interior_faces) return DG_ERR_ARG;
+    try {
+        dgh::BoxMesh b = dgh::make_periodic_box(n, x0, len, rotate_seed);
+        std::memcpy(node_coords, b.coords.data(), b.coords.size() * sizeof(double));
+        std::memcpy(elem_to_node_ids, b.e2n.data(), b.e2n.size() * sizeof(unsigned));
+        std::memcpy(interior_faces, b.faces.data(), b.faces.size() * sizeof(unsigned));
+    } catch (const std::exception&) {
+        return DG_ERR_ARG;
+    }
+    return DG_OK;
+}
+
+int dg_gauss_legendre(int n, double* x, double* w)
+{
+    if (n < 1 || n > 64 || !x || !w) return DG_ERR_ARG;
+    std::vector<double> xv, wv;
+    dgh::gauss_legendre(n, xv, wv);
+    std::copy(xv.begin(), xv.end(), x);
+    std::copy(wv.begin(), wv.end(), w);
+    return DG_OK;
+}
+
+int dg_face_orientation_order(int orient, int npts, int* order)
+{
+    if (orient < 0 || orient > 7 || npts < 1 || !order) return DG_ERR_ARG;
+    std::vector<int> o;
+    dgh::face_orientation_order(orient, npts, o);
+    std::copy(o.begin(), o.end(), order);
+    return DG_OK;
+}
+
+int dg_basis_tables(int p, double* B, double* D, double* Minv)
+{
+    if (p < 0 || p > 8) return DG_ERR_ARG;
+    const dgh::Tables1D t = dgh::make_tables(p);
+    if (B) std::copy(t.B.begin(), t.B.end(), B);
+    if (D) std::copy(t.D.begin(), t.D.end(), D);
+    if (Minv) std::copy(t.Minv.begin(), t.Minv.end(), Minv);
+    return DG_OK;
+}
+
+int dg_cfl_time_step(dg_ctx* c, const double* Uc, double cfl, double* dt)
+{
+    if (!c || !Uc || !dt || !(cfl > 0.0)) return fail(c, DG_ERR_ARG, "dg_cfl_time_step: bad argument");
+    const double v = dgh::cfl_time_step(c->pm, c->p, c->gamma, Uc, cfl);
+    if (!(v > 0.0)) return fail(c, DG_ERR_NONPHYSICAL, "state has non-positive density or pressure");
+    *dt = v;
+    return DG_OK;
+}
+
+}  // extern "C"

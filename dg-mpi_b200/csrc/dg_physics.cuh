@@ -1,0 +1,202 @@
+// dg_physics.cuh -- pointwise 3D Euler physics shared by the host C++ side and
+// the CUDA kernels: pressure, wave speed, interior flux, Lax-Friedrichs and
+// HLLC numerical fluxes, initial conditions / exact solutions.  Operation
+// order follows the reference's functions so that a face flux computed here
+// rounds like the reference's; citations are relative to the reference root.
+#pragma once
+#include <math.h>
+
+#ifdef __CUDACC__
+#define DG_HD __host__ __device__ __forceinline__
+#else
+#define DG_HD inline
+#endif
+
+namespace dgp {
+
+constexpr double kPi = 3.14159265358979323846;
+
+// EulerFcnType::get_pressure<3>, src/physics/euler/functions.cpp:10-23
+DG_HD double pressure(double gamma, const double* U)
+{
+    const double rKE = (U[1] * U[1] + U[2] * U[2] + U[3] * U[3]) / U[0];
+    return (gamma - 1.0) * (U[4] - 0.5 * rKE);
+}
+
+// EulerFcnType::get_maxwavespeed<3>, functions.cpp:25-40
+DG_HD double max_wave_speed(double gamma, const double* U)
+{
+    const double rho1 = 1. / U[0];
+    const double sqrtrKE = sqrt(U[1] * U[1] + U[2] * U[2] + U[3] * U[3]) * rho1;
+    return sqrtrKE + sqrt(gamma * pressure(gamma, U) * rho1);
+}
+
+// EulerFcnType::conv_flux_interior<3>, functions.cpp:64-91; F[j*5+s]
+DG_HD void interior_flux(double gamma, const double* U, double* F)
+{
+    const double r1 = 1. / U[0];
+    const double ru = U[1], rv = U[2], rw = U[3], rE = U[4];
+    const double P = pressure(gamma, U);
+    F[0] = ru;
+    F[1] = ru * ru * r1 + P;
+    F[2] = ru * rv * r1;
+    F[3] = ru * rw * r1;
+    F[4] = (rE + P) * ru * r1;
+    F[5] = rv;
+    F[6] = rv * ru * r1;
+    F[7] = rv * rv * r1 + P;
+    F[8] = rv * rw * r1;
+    F[9] = (rE + P) * rv * r1;
+    F[10] = rw;
+    F[11] = rw * ru * r1;
+    F[12] = rw * rv * r1;
+    F[13] = rw * rw * r1 + P;
+    F[14] = (rE + P) * rw * r1;
+}
+
+// BaseConvNumFluxType::compute_flux_laxfriedrichs<3>, base/functions.cpp:33-89.
+// N is the unnormalised normal of the left element (its length carries the
+// surface Jacobian).
+DG_HD void flux_lax_friedrichs(double gamma, const double* UL, const double* UR, const double* N,
+                               double* F)
+{
+    double n_mag = 0.0;
+    for (int d = 0; d < 3; ++d) n_mag += N[d] * N[d];
+    n_mag = sqrt(n_mag);
+    double n_hat[3];
+    for (int d = 0; d < 3; ++d) n_hat[d] = N[d] / n_mag;
+    double Fq[15], FqL[5] = {0, 0, 0, 0, 0}, FqR[5] = {0, 0, 0, 0, 0};
+    interior_flux(gamma, UL, Fq);
+    for (int s = 0; s < 5; ++s)
+        for (int d = 0; d < 3; ++d) FqL[s] += Fq[s + d * 5] * n_hat[d];
+    interior_flux(gamma, UR, Fq);
+    for (int s = 0; s < 5; ++s)
+        for (int d = 0; d < 3; ++d) FqR[s] += Fq[s + d * 5] * n_hat[d];
+    double a = max_wave_speed(gamma, UL);
+    const double aR = max_wave_speed(gamma, UR);
+    if (aR > a) a = aR;
+    for (int s = 0; s < 5; ++s) F[s] = n_mag * (0.5 * (FqL[s] + FqR[s]) - 0.5 * a * (UR[s] - UL[s]));
+}
+
+// EulerConvNumFluxType::compute_flux_hllc<3>, functions.cpp:298-399.
+// Returns false on the reference's assert branch (no valid wave ordering,
+// e.g. NaN input); F is zeroed then.
+DG_HD bool flux_hllc(double gam, const double* UL, const double* UR, const double* N, double* F)
+{
+    const double djac = sqrt(N[0] * N[0] + N[1] * N[1] + N[2] * N[2]);
+    const double djac1 = 1. / djac;
+    const double n[3] = {N[0] * djac1, N[1] * djac1, N[2] * djac1};
+    const double rhoL = UL[0], rhoL1 = 1. / rhoL;
+    const double unL = (UL[1] * n[0] + UL[2] * n[1] + UL[3] * n[2]) * rhoL1;
+    const double PL = pressure(gam, UL);
+    const double aL = sqrt(gam * PL * rhoL1);
+    const double rhoR = UR[0], rhoR1 = 1. / rhoR;
+    const double unR = (UR[1] * n[0] + UR[2] * n[1] + UR[3] * n[2]) * rhoR1;
+    const double PR = pressure(gam, UR);
+    const double aR = sqrt(gam * PR * rhoR1);
+    const double rAvg = 0.5 * (rhoL + rhoR);
+    const double aAvg = 0.5 * (aL + aR);
+    const double pStar = fmax(0., 0.5 * (PL + PR - (unR - unL) * rAvg * aAvg));
+    double qL = 1.0, qR = 1.0;
+    if (pStar / PL > 1.) qL = sqrt(1. + (gam + 1.) / (2. * gam) * (pStar / PL - 1.));
+    if (pStar / PR > 1.) qR = sqrt(1. + (gam + 1.) / (2. * gam) * (pStar / PR - 1.));
+    const double sL = unL - aL * qL;
+    const double sR = unR + aR * qR;
+    const double sStar = (PR - PL + rhoL * unL * (sL - unL) - rhoR * unR * (sR - unR)) /
+                         (rhoL * (sL - unL) - rhoR * (sR - unR));
+    if (sL >= 0.) {
+        F[0] = djac * rhoL * unL;
+        for (int i = 0; i < 3; ++i) F[1 + i] = djac * (UL[1 + i] * unL + PL * n[i]);
+        F[4] = djac * ((UL[4] + PL) * unL);
+    } else if (sR <= 0.) {
+        F[0] = djac * rhoR * unR;
+        for (int i = 0; i < 3; ++i) F[1 + i] = djac * (UR[1 + i] * unR + PR * n[i]);
+        F[4] = djac * (UR[4] + PR) * unR;
+    } else if ((sL < 0.) && (sStar >= 0.)) {
+        const double c = (sL - unL) / (sL - sStar);
+        const double f1 = sStar - unL;
+        const double f2 = sStar + PL / (rhoL * (sL - unL));
+        F[0] = djac * (rhoL * unL + rhoL * sL * (c - 1.));
+        for (int i = 0; i < 3; ++i)
+            F[1 + i] = djac * (UL[1 + i] * unL + PL * n[i] + sL * (UL[1 + i] * (c - 1.) + rhoL * c * f1 * n[i]));
+        F[4] = djac * ((UL[4] + PL) * unL + sL * (UL[4] * (c - 1.) + rhoL * c * f1 * f2));
+    } else if ((sStar < 0.) && (sR > 0.)) {
+        const double c = (sR - unR) / (sR - sStar);
+        const double f1 = sStar - unR;
+        const double f2 = sStar + PR / (rhoR * (sR - unR));
+        F[0] = djac * (rhoR * unR + rhoR * sR * (c - 1.));
+        for (int i = 0; i < 3; ++i)
+            F[1 + i] = djac * (UR[1 + i] * unR + PR * n[i] + sR * (UR[1 + i] * (c - 1.) + rhoR * c * f1 * n[i]));
+        F[4] = djac * ((UR[4] + PR) * unR + sR * (UR[4] * (c - 1.) + rhoR * c * f1 * f2));
+    } else {
+        for (int s = 0; s < 5; ++s) F[s] = 0.0;
+        return false;
+    }
+    return true;
+}
+
+// Initial conditions / exact solutions, Physics<3>::call_IC and
+// call_exact_solution (src/physics/base/base.cpp:90-137) plus the advected
+// xy vortex and Taylor-Green families.  Type codes match DG_IC_* in dg_b200.h.
+DG_HD void initial_state(int type, const double* data, double gamma, double R, const double* x,
+                         double t, double* U)
+{
+    if (type == 0) {  // Uniform, base.cpp:150-158
+        for (int s = 0; s < 5; ++s) U[s] = data[s];
+    } else if (type == 1) {  // reference 3D isentropic vortex, functions.cpp:147-191
+        const double rho0 = 1., sos0 = 1., L = 1., Mach = 1.0, radius = L / 10., sigma = 1;
+        const double beta = Mach * 5. * sqrt(2.) / (4. * kPi) * exp(0.5);
+        const double u0 = Mach * sos0;
+        const double x1 = x[0] - 0.5, y1 = x[2] - 0.5;
+        const double f = -0.5 / (sigma * sigma) * (x1 * x1 + y1 * y1) / (radius * radius);
+        const double Omega = beta * exp(f);
+        const double du = -y1 / radius * Omega, dv = x1 / radius * Omega;
+        const double dT = -(gamma - 1.) / 2. * Omega * Omega;
+        const double p = 1. / gamma * pow(1 + dT, gamma / (gamma - 1.));
+        U[0] = pow(rho0 + dT, 1. / (gamma - 1.));
+        U[1] = U[0] * (u0 + du);
+        U[2] = 0.;
+        U[3] = U[0] * dv;
+        const double rKE = (U[1] * U[1] + U[2] * U[2] + U[3] * U[3]) / U[0];
+        U[4] = p / (gamma - 1.0) + 0.5 * rKE;
+    } else if (type == 2) {  // smooth sphere, base.cpp:177-194
+        const double magR = sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+        for (int s = 0; s < 5; ++s) U[s] = 0.5 * (1. - 0.) * (tanh(kPi * (0.5 - magR) / 0.5) + 1.0) + 0.;
+    } else if (type == 3) {  // 2D vortex of functions.cpp:94-145, extruded in z, advected, periodic
+        const double rhob = data[0], ub = data[1], vb = data[2], pb = data[3], vs = data[4];
+        const double xc = data[5], yc = data[6], Lx = data[7], Ly = data[8];
+        const double Tb = pb / (rhob * R);
+        const double s = pb / pow(rhob, gamma);
+        double xr = x[0] - xc - ub * t;
+        double yr = x[1] - yc - vb * t;
+        xr -= Lx * floor(xr / Lx + 0.5);
+        yr -= Ly * floor(yr / Ly + 0.5);
+        const double r = sqrt(xr * xr + yr * yr);
+        const double r2 = r * r;
+        const double dUm = vs / (2.0 * kPi) * exp(0.5 * (1.0 - r2));
+        const double du = dUm * -1.0 * yr, dv = dUm * xr;
+        const double dT = -1.0 * (gamma - 1.0) * (vs * vs) / (8.0 * gamma * (kPi * kPi)) * exp(1.0 - r2);
+        const double u = ub + du, v = vb + dv, T = Tb + dT;
+        const double rho = pow(T / s, 1.0 / (gamma - 1.0));
+        const double rhou = rho * u, rhov = rho * v;
+        U[0] = rho;
+        U[1] = rhou;
+        U[2] = rhov;
+        U[3] = 0.0;
+        U[4] = rho * R / (gamma - 1.0) * T + 0.5 * (rhou * rhou + rhov * rhov) / rho;
+    } else if (type == 4) {  // Taylor-Green vortex, data = {Mach}
+        const double M = data[0];
+        const double u = sin(x[0]) * cos(x[1]) * cos(x[2]);
+        const double v = -cos(x[0]) * sin(x[1]) * cos(x[2]);
+        const double p = 1.0 / (gamma * M * M) + (cos(2.0 * x[0]) + cos(2.0 * x[1])) * (cos(2.0 * x[2]) + 2.0) / 16.0;
+        U[0] = 1.0;
+        U[1] = u;
+        U[2] = v;
+        U[3] = 0.0;
+        U[4] = p / (gamma - 1.0) + 0.5 * (u * u + v * v);
+    } else {
+        for (int s = 0; s < 5; ++s) U[s] = 0.0;
+    }
+}
+
+}  // namespace dgp

@@ -1,0 +1,292 @@
+"""Python binding of libdg_b200.so (the C ABI declared in include/dg_b200.h).
+
+The library is the product: CUDA kernels for sm_100a behind a C ABI plus the
+C++ host side (mesh, tables, initial conditions).  This module only marshals
+numpy arrays through ctypes; it computes nothing itself and has no fallback:
+if the shared library is missing or no GPU is present, the calls fail loudly.
+
+Names follow the reference's vocabulary (IhmeGroup/DG-MPI): a *case* is one
+mesh + order + physics setup, ``Uc`` is the solution-coefficient array
+[ne][nb][5] (src/solver/base.h), ``res`` the residual of
+Solver<3>::get_residual, ``interior_faces`` the [nface][8] connectivity of
+src/mesh/mesh.h:280-284.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_build", "libdg_b200.so")
+
+DG_OK = 0
+ERROR_NAMES = {1: "DG_ERR_ARG", 2: "DG_ERR_CUDA", 3: "DG_ERR_NONPHYSICAL", 4: "DG_ERR_TIMEOUT",
+               5: "DG_ERR_UNSUPPORTED", 6: "DG_ERR_NOMEM"}
+
+FLUX = {"LaxFriedrichs": 0, "HLLC": 1}
+PRECISION = {"fp64": 0, "mixed_fp32": 1}
+# [InitialCondition] name -> DG_IC_* (include/dg_b200.h)
+IC = {"Uniform": 0, "IsentropicVortex": 1, "Sphere": 2, "IsentropicVortexXY": 3, "TaylorGreen": 4}
+
+
+class DGError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{ERROR_NAMES.get(code, code)}: {message}")
+        self.code = code
+
+
+class _MeshDesc(ctypes.Structure):
+    _fields_ = [("nnode", ctypes.c_int), ("node_coords", ctypes.POINTER(ctypes.c_double)),
+                ("nelem", ctypes.c_int), ("elem_to_node_ids", ctypes.POINTER(ctypes.c_uint)),
+                ("nface", ctypes.c_int), ("interior_faces", ctypes.POINTER(ctypes.c_uint)),
+                ("rank", ctypes.c_int)]
+
+
+class _CaseDesc(ctypes.Structure):
+    _fields_ = [("order", ctypes.c_int), ("flux", ctypes.c_int), ("gamma", ctypes.c_double),
+                ("gas_constant", ctypes.c_double), ("precision", ctypes.c_int), ("device", ctypes.c_int)]
+
+
+_lib = None
+
+
+def library(path: str | None = None) -> ctypes.CDLL:
+    """Load libdg_b200.so once (raises OSError if it has not been built)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    lib = ctypes.CDLL(path or LIB_PATH)
+    dp = ctypes.POINTER(ctypes.c_double)
+    up = ctypes.POINTER(ctypes.c_uint)
+    ip = ctypes.POINTER(ctypes.c_int)
+    vp = ctypes.c_void_p
+    sig = {
+        "dg_create": (ctypes.c_int, [ctypes.POINTER(_CaseDesc), ctypes.POINTER(_MeshDesc), ctypes.POINTER(vp)]),
+        "dg_destroy": (None, [vp]),
+        "dg_last_error": (ctypes.c_char_p, [vp]),
+        "dg_num_basis": (ctypes.c_int, [vp]),
+        "dg_num_elements": (ctypes.c_int, [vp]),
+        "dg_set_state": (ctypes.c_int, [vp, dp]),
+        "dg_get_state": (ctypes.c_int, [vp, dp]),
+        "dg_residual": (ctypes.c_int, [vp, dp]),
+        "dg_mass_inverse_residual": (ctypes.c_int, [vp, ctypes.c_double, dp]),
+        "dg_rk4_steps": (ctypes.c_int, [vp, ctypes.c_double, ctypes.c_int]),
+        "dg_fe_steps": (ctypes.c_int, [vp, ctypes.c_double, ctypes.c_int]),
+        "dg_project_ic": (ctypes.c_int, [vp, ctypes.c_int, dp, ctypes.c_int, ctypes.c_double, dp]),
+        "dg_l2_error": (ctypes.c_int, [vp, ctypes.c_int, dp, ctypes.c_int, ctypes.c_double, dp]),
+        "dg_kinetic_energy": (ctypes.c_int, [vp, dp]),
+        "dg_total_volume": (ctypes.c_int, [vp, dp]),
+        "dg_status": (ctypes.c_int, [vp, up]),
+        "dg_sync": (ctypes.c_int, [vp]),
+        "dg_device_state": (vp, [vp]),
+        "dg_mesh_periodic_box": (ctypes.c_int, [ip, dp, dp, ctypes.c_uint, ip, dp, ip, up, ip, up]),
+        "dg_cfl_time_step": (ctypes.c_int, [vp, dp, ctypes.c_double, dp]),
+        "dg_gauss_legendre": (ctypes.c_int, [ctypes.c_int, dp, dp]),
+        "dg_face_orientation_order": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ip]),
+        "dg_basis_tables": (ctypes.c_int, [ctypes.c_int, dp, dp, dp]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _uptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_uint))
+
+
+@dataclass
+class Mesh:
+    """Hex mesh in the reference's in-memory form (src/mesh/mesh.h)."""
+    node_coords: np.ndarray      # [nnode][3] float64
+    elem_to_node_ids: np.ndarray  # [nelem][8] uint32
+    interior_faces: np.ndarray    # [nface][8] uint32
+
+    @property
+    def nelem(self) -> int:
+        return int(self.elem_to_node_ids.shape[0])
+
+    def iface_data(self) -> np.ndarray:
+        """The [nface][6] IFaceData of the mesh file (mesh/mesh.cpp:144-160)."""
+        f = self.interior_faces
+        return np.ascontiguousarray(f[:, [1, 2, 3, 5, 6, 7]].astype(np.int32))
+
+
+def periodic_box(n, x0=(0.0, 0.0, 0.0), length=(1.0, 1.0, 1.0), rotate_seed: int = 0) -> Mesh:
+    """Uniform periodic hex box from the library's host-side generator."""
+    lib = library()
+    n_arr = (ctypes.c_int * 3)(*[int(v) for v in n])
+    x_arr = (ctypes.c_double * 3)(*[float(v) for v in x0])
+    l_arr = (ctypes.c_double * 3)(*[float(v) for v in length])
+    nn, ne, nf = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    rc = lib.dg_mesh_periodic_box(n_arr, x_arr, l_arr, ctypes.c_uint(rotate_seed), ctypes.byref(nn), None,
+                                  ctypes.byref(ne), None, ctypes.byref(nf), None)
+    if rc:
+        raise DGError(rc, "dg_mesh_periodic_box: bad box")
+    coords = np.zeros((nn.value, 3), np.float64)
+    e2n = np.zeros((ne.value, 8), np.uint32)
+    faces = np.zeros((nf.value, 8), np.uint32)
+    rc = lib.dg_mesh_periodic_box(n_arr, x_arr, l_arr, ctypes.c_uint(rotate_seed), ctypes.byref(nn), _dptr(coords),
+                                  ctypes.byref(ne), _uptr(e2n), ctypes.byref(nf), _uptr(faces))
+    if rc:
+        raise DGError(rc, "dg_mesh_periodic_box failed")
+    return Mesh(coords, e2n, faces)
+
+
+class Case:
+    """One DG case on one GPU (a dg_ctx)."""
+
+    def __init__(self, mesh: Mesh, order: int, flux: str = "LaxFriedrichs", gamma: float = 1.4,
+                 gas_constant: float = 287.05, precision: str = "fp64", device: int = 0):
+        self._lib = library()
+        self.mesh = mesh
+        self.order = order
+        self.nb = (order + 1) ** 3
+        self.ne = mesh.nelem
+        self.gamma = gamma
+        self._coords = np.ascontiguousarray(mesh.node_coords, np.float64)
+        self._e2n = np.ascontiguousarray(mesh.elem_to_node_ids, np.uint32)
+        self._faces = np.ascontiguousarray(mesh.interior_faces, np.uint32)
+        md = _MeshDesc(self._coords.shape[0], _dptr(self._coords), self._e2n.shape[0], _uptr(self._e2n),
+                       self._faces.shape[0], _uptr(self._faces), 0)
+        cd = _CaseDesc(order, FLUX[flux], gamma, gas_constant, PRECISION[precision], device)
+        ctx = ctypes.c_void_p()
+        rc = self._lib.dg_create(ctypes.byref(cd), ctypes.byref(md), ctypes.byref(ctx))
+        if rc:
+            raise DGError(rc, self._lib.dg_last_error(None).decode())
+        self._ctx = ctx
+
+    # -- plumbing ---------------------------------------------------------
+    def _check(self, rc: int):
+        if rc:
+            raise DGError(rc, self._lib.dg_last_error(self._ctx).decode())
+
+    def close(self):
+        if getattr(self, "_ctx", None):
+            self._lib.dg_destroy(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _state_array(self) -> np.ndarray:
+        return np.empty((self.ne, self.nb, 5), np.float64)
+
+    # -- the path ------------------------------------------------------------
+    def set_state(self, Uc: np.ndarray):
+        Uc = np.ascontiguousarray(Uc, np.float64)
+        assert Uc.shape == (self.ne, self.nb, 5)
+        self._check(self._lib.dg_set_state(self._ctx, _dptr(Uc)))
+
+    def set_state_ptr(self, host_ptr: int):
+        """Upload from a host buffer given by address (e.g. a pinned tensor)."""
+        self._check(self._lib.dg_set_state(self._ctx, ctypes.cast(host_ptr, ctypes.POINTER(ctypes.c_double))))
+
+    def get_state(self, out: np.ndarray | None = None) -> np.ndarray:
+        out = self._state_array() if out is None else out
+        self._check(self._lib.dg_get_state(self._ctx, _dptr(out)))
+        return out
+
+    def get_state_ptr(self, host_ptr: int):
+        self._check(self._lib.dg_get_state(self._ctx, ctypes.cast(host_ptr, ctypes.POINTER(ctypes.c_double))))
+
+    def residual(self) -> np.ndarray:
+        out = self._state_array()
+        self._check(self._lib.dg_residual(self._ctx, _dptr(out)))
+        return out
+
+    def mass_inverse_residual(self, dt: float) -> np.ndarray:
+        out = self._state_array()
+        self._check(self._lib.dg_mass_inverse_residual(self._ctx, dt, _dptr(out)))
+        return out
+
+    def rk4(self, dt: float, nsteps: int):
+        self._check(self._lib.dg_rk4_steps(self._ctx, dt, int(nsteps)))
+
+    def fe(self, dt: float, nsteps: int):
+        self._check(self._lib.dg_fe_steps(self._ctx, dt, int(nsteps)))
+
+    def project_ic(self, name: str, data=(), t: float = 0.0) -> np.ndarray:
+        d = np.ascontiguousarray(np.asarray(data, np.float64).reshape(-1))
+        out = self._state_array()
+        self._check(self._lib.dg_project_ic(self._ctx, IC[name], _dptr(d) if d.size else None, d.size, t, _dptr(out)))
+        return out
+
+    def l2_error(self, name: str, data=(), t: float = 0.0) -> np.ndarray:
+        d = np.ascontiguousarray(np.asarray(data, np.float64).reshape(-1))
+        out = np.zeros(5, np.float64)
+        self._check(self._lib.dg_l2_error(self._ctx, IC[name], _dptr(d) if d.size else None, d.size, t, _dptr(out)))
+        return out
+
+    def kinetic_energy(self) -> float:
+        v = ctypes.c_double()
+        self._check(self._lib.dg_kinetic_energy(self._ctx, ctypes.byref(v)))
+        return v.value
+
+    def total_volume(self) -> float:
+        v = ctypes.c_double()
+        self._check(self._lib.dg_total_volume(self._ctx, ctypes.byref(v)))
+        return v.value
+
+    def status(self) -> int:
+        v = ctypes.c_uint()
+        self._check(self._lib.dg_status(self._ctx, ctypes.byref(v)))
+        return v.value
+
+    def sync(self):
+        self._check(self._lib.dg_sync(self._ctx))
+
+    def cfl_time_step(self, Uc: np.ndarray, cfl: float) -> float:
+        Uc = np.ascontiguousarray(Uc, np.float64)
+        v = ctypes.c_double()
+        self._check(self._lib.dg_cfl_time_step(self._ctx, _dptr(Uc), cfl, ctypes.byref(v)))
+        return v.value
+
+    def device_state_ptr(self) -> int:
+        return int(self._lib.dg_device_state(self._ctx) or 0)
+
+
+def gauss_legendre(n: int):
+    """n-point Gauss-Legendre rule of the host side."""
+    x, w = np.zeros(n), np.zeros(n)
+    rc = library().dg_gauss_legendre(n, _dptr(x), _dptr(w))
+    if rc:
+        raise DGError(rc, "dg_gauss_legendre")
+    return x, w
+
+
+def face_orientation_order(orient: int, npts: int) -> np.ndarray:
+    out = np.zeros(npts, np.int32)
+    rc = library().dg_face_orientation_order(orient, npts, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+    if rc:
+        raise DGError(rc, "dg_face_orientation_order")
+    return out
+
+
+def basis_tables(p: int):
+    """(B[m][n], D[m][n], Minv[n][n]) 1D tables of order p."""
+    n, m = p + 1, p + 2
+    B, D, Mi = np.zeros((m, n)), np.zeros((m, n)), np.zeros((n, n))
+    rc = library().dg_basis_tables(p, _dptr(B), _dptr(D), _dptr(Mi))
+    if rc:
+        raise DGError(rc, "dg_basis_tables")
+    return B, D, Mi

@@ -1,0 +1,208 @@
+/*
+ * dg_b200.h -- C ABI of the B200-native residual + RK-stage path for
+ * IhmeGroup/DG-MPI's 3D Euler solver on periodic hexahedral meshes.
+ *
+ * One library, libdg_b200.so, exports everything below.  Plain C types only
+ * (no CUDA or torch types), so a C++ stepper inside the reference, ctypes, or
+ * any FFI can bind it.  Paths in the comments are relative to the reference
+ * project root.
+ *
+ * Ownership: the caller owns every host buffer; buffers are read or written
+ * during the call and never retained.  A context owns all device memory,
+ * streams and graphs it creates.  Tables and connectivity are immutable after
+ * dg_create.
+ *
+ * Errors: every int-returning call returns DG_OK (0) or a DG_ERR_* code and
+ * never throws; dg_last_error() gives the message for the last failure on that
+ * context (the reference reports errors through C++ exceptions,
+ * src/common/my_exceptions.h:14-115, device printf and assert; none of those
+ * cross this boundary).
+ *
+ * Threading: a context is used by one host thread at a time; different
+ * contexts may run concurrently (each has its own stream).  All calls are
+ * synchronous with respect to the host buffers they take.
+ *
+ * Layout contract: host-side solution arrays are row-major Uc[ne][nb][5]
+ * (Kokkos LayoutRight, the CPU build's layout; src/io/writer.cpp:72), with
+ * nb = (p+1)^3 equidistant-Lagrange coefficients indexed k(p+1)^2+j(p+1)+i
+ * (src/numerics/basis/tools.cpp:215-247).  The device layout is private.
+ */
+#ifndef DG_B200_H
+#define DG_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DG_B200_ABI_VERSION 1
+
+/* ---- status codes ---- */
+#define DG_OK 0
+#define DG_ERR_ARG 1          /* bad argument or inconsistent mesh/tables */
+#define DG_ERR_CUDA 2         /* a CUDA runtime call failed */
+#define DG_ERR_NONPHYSICAL 3  /* device status word: rho<=0, p<=0 or NaN seen */
+#define DG_ERR_TIMEOUT 4      /* a bounded device wait gave up */
+#define DG_ERR_UNSUPPORTED 5  /* valid input this build does not handle */
+#define DG_ERR_NOMEM 6        /* device or host allocation failed */
+
+/* numerical flux, [Physics] convective_flux_fcn (src/common/enums.h:80-91) */
+#define DG_FLUX_LAX_FRIEDRICHS 0
+#define DG_FLUX_HLLC 1
+
+/* arithmetic of the residual (the stored solution, RK accumulation, inverse
+ * mass and geometric factors are FP64 in every mode) */
+#define DG_PREC_FP64 0
+#define DG_PREC_MIXED_FP32 1
+
+/* initial-condition / exact-solution families ([InitialCondition] name) */
+#define DG_IC_UNIFORM 0        /* "Uniform": data = conserved state[5] */
+#define DG_IC_VORTEX_REF 1     /* "IsentropicVortex": the reference's 3D vortex */
+#define DG_IC_SPHERE 2         /* "Sphere" */
+#define DG_IC_VORTEX_XY 3      /* "IsentropicVortexXY": data = rho,u,v,p,beta,xc,yc,Lx,Ly */
+#define DG_IC_TAYLOR_GREEN 4   /* "TaylorGreen": data = Mach */
+
+typedef struct dg_ctx dg_ctx;
+
+/* A hexahedral mesh in the reference's in-memory form (src/mesh/mesh.h:
+ * node_coords, elem_to_node_IDs, interior_faces).  interior_faces rows are
+ * (rankL, elemL, faceL, orientL, rankR, elemR, faceR, orientR)
+ * (src/mesh/mesh.h:280-284); on one GPU every rank entry must equal `rank`.
+ * Elements must be affine (parallelepipeds); every face must be interior
+ * (periodic meshes). */
+typedef struct dg_mesh_desc {
+    int nnode;
+    const double* node_coords;         /* [nnode][3] */
+    int nelem;
+    const unsigned* elem_to_node_ids;  /* [nelem][8], gbasis node order, x fastest */
+    int nface;
+    const unsigned* interior_faces;    /* [nface][8] */
+    int rank;
+} dg_mesh_desc;
+
+typedef struct dg_case_desc {
+    int order;       /* [Numerics] order, p = 0..5 */
+    int flux;        /* DG_FLUX_* */
+    double gamma;    /* [Physics] gamma (src/physics/base/base.cpp:28) */
+    double gas_constant; /* [Physics] GasConstant (base.cpp:29) */
+    int precision;   /* DG_PREC_* */
+    int device;      /* CUDA device ordinal */
+} dg_case_desc;
+
+/* Replaces Solver<3>::Solver + precompute_matrix_helpers +
+ * allocate_face_residual_views (src/solver/base.cpp:20-111, 563-598) and the
+ * stepper's allocate_helpers (src/numerics/timestepping/stepper.cpp:57-69):
+ * builds the 1D basis/quadrature tables, geometry classes, the periodic face
+ * gather table (from interior_faces and the face-point permutations of
+ * src/solver/helpers.cpp:326-378) and allocates device state. */
+int dg_create(const dg_case_desc* cd, const dg_mesh_desc* md, dg_ctx** out);
+
+/* Releases the context (Mesh::finalize / MemoryNetwork::finalize). */
+void dg_destroy(dg_ctx* ctx);
+
+/* Message of the last failing call on ctx (or of the last failing dg_create
+ * when ctx is NULL). Never NULL. */
+const char* dg_last_error(const dg_ctx* ctx);
+
+int dg_num_basis(const dg_ctx* ctx);     /* nb = (p+1)^3 */
+int dg_num_elements(const dg_ctx* ctx);
+
+/* Host -> device copy of Uc[ne][nb][5]; replaces Kokkos::deep_copy(Uc, h_Uc)
+ * after init_state_from_fcn / read_in_coefficients (base.cpp:113-279). */
+int dg_set_state(dg_ctx* ctx, const double* Uc);
+
+/* Device -> host copy of the current state; replaces
+ * Solver::copy_from_device_to_host (base.cpp:226-230). */
+int dg_get_state(dg_ctx* ctx, double* Uc);
+
+/* R(U) of the current state into res[ne][nb][5] (host); replaces
+ * Solver<3>::get_residual (base.cpp:401-561): volume integral, face traces,
+ * on-device periodic face gather (in place of construct_face_states +
+ * MemoryNetwork::communicate_face_solution, memory_network.cpp:55-175),
+ * numerical flux, L=-F/R=+F scatter and face lift. */
+int dg_residual(dg_ctx* ctx, double* res);
+
+/* dt * M^-1 R(U) into dU[ne][nb][5] (host); replaces get_residual followed
+ * by SolverTools::mult_inv_mass_matrix (src/solver/tools.cpp:124-139). */
+int dg_mass_inverse_residual(dg_ctx* ctx, double dt, double* dU);
+
+/* Advances the device state by nsteps classic RK4 steps of size dt; replaces
+ * nsteps calls of RK4<3>::take_time_step (stepper.cpp:71-142), one fused
+ * kernel per stage, the four stages of a step replayed from a CUDA graph. */
+int dg_rk4_steps(dg_ctx* ctx, double dt, int nsteps);
+
+/* Forward Euler, replaces FE<3>::take_time_step (stepper.cpp:23-55). */
+int dg_fe_steps(dg_ctx* ctx, double dt, int nsteps);
+
+/* L2 projection of an initial condition onto the basis, on the host side of
+ * the library (C++/OpenMP); replaces Solver::init_state_from_fcn
+ * (base.cpp:113-223) + SolverTools::L2_projection (tools.cpp:66-122).
+ * Writes the device state and, if Uc != NULL, a host copy. */
+int dg_project_ic(dg_ctx* ctx, int ic_type, const double* data, int ndata, double t, double* Uc);
+
+/* Volume-normalised L2 error of the device state against an exact solution
+ * (FP64 device reduction); replaces get_error(solver, 2, true)
+ * (src/post/main.cpp:30-201).  err[5], one per conserved variable. */
+int dg_l2_error(dg_ctx* ctx, int ic_type, const double* data, int ndata, double t, double* err);
+
+/* Volume-averaged kinetic energy (1/V) * integral of |rho u|^2 / (2 rho). */
+int dg_kinetic_energy(dg_ctx* ctx, double* ke);
+
+/* Total mesh volume (sum of element volumes, MeshTools::get_total_volume). */
+int dg_total_volume(const dg_ctx* ctx, double* vol);
+
+/* Device status word accumulated since the last call (bit 0: non-positive
+ * density, bit 1: non-positive pressure, bit 2: NaN, bit 3: HLLC found no
+ * valid wave ordering -- the reference's assert branch,
+ * src/physics/euler/functions.cpp:389-398); cleared by the call. */
+int dg_status(dg_ctx* ctx, unsigned* flags);
+
+/* Waits for all work of ctx. */
+int dg_sync(dg_ctx* ctx);
+
+/* Raw device pointers for callers that keep data resident (benchmarks,
+ * multi-GPU exchange).  Layout of the device state: [ne][5][nb]. */
+void* dg_device_state(dg_ctx* ctx);
+
+/* ---- host-side mesh helper (replaces reading an HDF5 mesh file,
+ * src/mesh/mesh.cpp:79-204, for periodic boxes) ---- */
+
+/* Uniform periodic box [x0,x0+L0]x[x1,x1+L1]x[x2,x2+L2] with n0*n1*n2 hex
+ * elements, element id i + n0*(j + n1*k).  Nodes are not shared across the
+ * periodic boundary (every element is a proper parallelepiped); periodicity
+ * lives in interior_faces.  If rotate_seed != 0, every element's local node
+ * numbering is replaced by one of the 24 proper rotations of the cube
+ * (seeded), which exercises non-trivial face orientations.  Sizes first:
+ * call with NULL arrays to get nnode/nelem/nface. */
+int dg_mesh_periodic_box(const int n[3], const double x0[3], const double len[3],
+                         unsigned rotate_seed,
+                         int* nnode, double* node_coords,
+                         int* nelem, unsigned* elem_to_node_ids,
+                         int* nface, unsigned* interior_faces);
+
+/* Host-side time step from a CFL number on a given state (the reference has
+ * none; [Stepper] timestep is used as is): dt = cfl * h_min /
+ * ((2p+1) * max over element nodes of (|u| + c)). */
+int dg_cfl_time_step(dg_ctx* ctx, const double* Uc, double cfl, double* dt);
+
+/* ---- host-side tables (no GPU needed) ---- */
+
+/* n-point Gauss-Legendre rule, ascending nodes; replaces the tables of
+ * Nodes::get_gauss_legendre_segment_nodes (src/numerics/nodes.cpp:97-) and
+ * SegmentQuadrature::get_segment_weights_gl (quadrature/segment.cpp:7-). */
+int dg_gauss_legendre(int n, double* x, double* w);
+
+/* Face-point order of orientation `orient` (0..7) on an npts = n1*n1 face
+ * grid; replaces get_face_pts_order_wrt_orient0_hexahedron
+ * (src/numerics/basis/shape.cpp:326-428). */
+int dg_face_orientation_order(int orient, int npts, int* order);
+
+/* 1D tables of order p: B[m][n] and D[m][n] (values / derivatives of the
+ * equidistant Lagrange basis at the m = p+2 Gauss-Legendre points) and the
+ * inverse 1D mass matrix Minv[n][n] (n = p+1); the 3D operators of
+ * src/solver/helpers.cpp:5-100 are their tensor products. */
+int dg_basis_tables(int p, double* B, double* D, double* Minv);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,159 @@
+"""Host side of the drop-in (CPU only): the C ABI library loads and exports
+every declared symbol, the product's own tables agree with the oracle's
+restatement of the reference, the periodic mesh generator produces the
+reference's mesh semantics, and mesh validation rejects what the device path
+cannot handle -- all without touching a GPU."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import dg_b200
+import pyoracle
+from conftest import ROOT, gpu_available
+
+
+def declared_symbols():
+    with open(os.path.join(ROOT, "include", "dg_b200.h")) as f:
+        text = f.read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(dg_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = ctypes.CDLL(dg_b200.LIB_PATH)
+    names = declared_symbols()
+    assert len(names) >= 20
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_binding_covers_every_declared_symbol():
+    lib = dg_b200.library()
+    for n in declared_symbols():
+        assert getattr(lib, n).argtypes is not None, n
+
+
+@pytest.mark.parametrize("n", range(1, 13))
+def test_gauss_legendre_matches_oracle(n):
+    x, w = dg_b200.gauss_legendre(n)
+    xo, wo = pyoracle.gauss_legendre(2 * n - 1)
+    np.testing.assert_array_equal(x, xo)
+    np.testing.assert_array_equal(w, wo)
+
+
+@pytest.mark.parametrize("n1", range(1, 9))
+def test_face_orientation_orders_match_reference_walks(n1):
+    # product: closed-form dihedral maps; oracle: shape.cpp:326-428 walks
+    for o in range(8):
+        np.testing.assert_array_equal(dg_b200.face_orientation_order(o, n1 * n1),
+                                      pyoracle.face_pts_order(o, n1 * n1))
+
+
+@pytest.mark.parametrize("p", range(0, 6))
+def test_1d_tables_reproduce_reference_3d_tables(p):
+    """The kernels' 1D tables, tensorised, equal the reference's dense 3D
+    basis / gradient tables at the volume points (helpers.cpp:143-183)."""
+    B, D, Mi = dg_b200.basis_tables(p)
+    lib = pyoracle.library()
+    m = p + 2
+    x, _ = pyoracle.gauss_legendre(lib.orc_hex_quadrature_order(p))
+    assert x.size == m
+    pts = np.array([[x[i], x[j], x[k]] for k in range(m) for j in range(m) for i in range(m)])
+    nb = (p + 1) ** 3
+    val = np.zeros((m ** 3, nb))
+    grad = np.zeros((m ** 3, nb, 3))
+    lib.orc_lagrange_hex_val(p, m ** 3, pyoracle._d(np.ascontiguousarray(pts)), pyoracle._d(val))
+    lib.orc_lagrange_hex_grad(p, m ** 3, pyoracle._d(np.ascontiguousarray(pts)), pyoracle._d(grad))
+    B3 = np.einsum("kc,jb,ia->kjicba", B, B, B).reshape(m ** 3, nb)
+    np.testing.assert_allclose(B3, val, atol=1e-14)
+    if p > 0:
+        Gx = np.einsum("kc,jb,ia->kjicba", B, B, D).reshape(m ** 3, nb)
+        Gz = np.einsum("kc,jb,ia->kjicba", D, B, B).reshape(m ** 3, nb)
+        np.testing.assert_allclose(Gx, grad[:, :, 0], atol=1e-13)
+        np.testing.assert_allclose(Gz, grad[:, :, 2], atol=1e-13)
+    # Minv is the inverse of the exactly integrated 1D mass matrix
+    n = p + 1
+    xm, wm = np.polynomial.legendre.leggauss(2 * p + 2)
+    xn = np.linspace(-1, 1, n) if n > 1 else np.zeros(1)
+    phi = np.ones((xm.size, n))
+    for i in range(n):
+        for j in range(n):
+            if i != j:
+                phi[:, i] *= (xm - xn[j]) / (xn[i] - xn[j])
+    M = (phi * wm[:, None]).T @ phi
+    np.testing.assert_allclose(Mi @ M, np.eye(n), atol=1e-11)
+
+
+@pytest.mark.parametrize("seed", [0, 1, 99])
+@pytest.mark.parametrize("p", [1, 3])
+def test_mesh_generator_matches_reference_face_semantics(seed, p):
+    """For every interior face, the left face point quad_idx_L[q] and the
+    right face point quad_idx_R[q] coincide physically (modulo the period),
+    and the normal (computed the reference's way, from the left element)
+    points out of the left element with |N| = face area / 4."""
+    L = np.array([1.0, 2.0, 0.5])
+    mesh = dg_b200.periodic_box((3, 2, 4), (0.1, -0.2, 0.0), L, rotate_seed=seed)
+    oc = pyoracle.OracleCase.from_mesh(mesh, p, gas_constant=1.0)
+    iL, iR = oc.quad_idx()
+    N = oc.face_normals()
+    ifd = mesh.iface_data()
+    h = L / np.array([3, 2, 4])
+    centers = mesh.node_coords[mesh.elem_to_node_ids].mean(axis=1)
+    for f in range(ifd.shape[0]):
+        eL, fL, _, eR, fR, _ = ifd[f]
+        XL = oc.face_points(eL, fL)[iL[f]]
+        XR = oc.face_points(eR, fR)[iR[f]]
+        d = XL - XR
+        d -= L * np.round(d / L)
+        assert np.abs(d).max() < 1e-12
+        n = N[f, 0]
+        out = XL[0] - centers[eL]
+        assert np.dot(n, out) > 0
+        axis = int(np.argmax(np.abs(n)))
+        area = np.prod(np.delete(h, axis))
+        assert abs(np.linalg.norm(n) - area / 4) < 1e-12
+        assert np.allclose(N[f], N[f, 0], atol=1e-14)
+
+
+def test_mesh_validation_rejects_boundary_faces_before_touching_the_gpu():
+    mesh = dg_b200.periodic_box((2, 2, 2))
+    broken = dg_b200.Mesh(mesh.node_coords, mesh.elem_to_node_ids, mesh.interior_faces[:-1].copy())
+    with pytest.raises(dg_b200.DGError) as ei:
+        dg_b200.Case(broken, 1)
+    assert ei.value.code == 5 and "boundary face" in str(ei.value)
+
+
+def test_mesh_validation_rejects_non_affine_elements():
+    mesh = dg_b200.periodic_box((2, 2, 2))
+    coords = mesh.node_coords.copy()
+    coords[13] += [0.05, 0.0, 0.0]  # the centre node: every element around it bends
+    with pytest.raises(dg_b200.DGError) as ei:
+        dg_b200.Case(dg_b200.Mesh(coords, mesh.elem_to_node_ids, mesh.interior_faces), 2)
+    assert ei.value.code == 5 and "not affine" in str(ei.value)
+
+
+def test_mesh_validation_rejects_out_of_range_entries():
+    mesh = dg_b200.periodic_box((2, 2, 2))
+    faces = mesh.interior_faces.copy()
+    faces[0, 3] = 9  # orientation must be 0..7
+    with pytest.raises(dg_b200.DGError) as ei:
+        dg_b200.Case(dg_b200.Mesh(mesh.node_coords, mesh.elem_to_node_ids, faces), 1)
+    assert ei.value.code == 1
+
+
+def test_unsupported_order_and_precision():
+    mesh = dg_b200.periodic_box((2, 2, 2))
+    with pytest.raises(dg_b200.DGError) as ei:
+        dg_b200.Case(mesh, 6)
+    assert ei.value.code == 5
+
+
+@pytest.mark.skipif(gpu_available(), reason="checks the no-GPU error path")
+def test_create_without_gpu_fails_cleanly():
+    mesh = dg_b200.periodic_box((2, 2, 2))
+    with pytest.raises(dg_b200.DGError) as ei:
+        dg_b200.Case(mesh, 1)
+    assert ei.value.code == 2
