@@ -1,0 +1,292 @@
+#!/usr/bin/env python
+"""Benchmark of the DG-MPI 3D Euler residual + RK4 hot path on B200.
+
+Workload: the plain-FP64 at-scale configuration -- isentropic vortex
+(x-y vortex extruded in z, beta 5, centre (5,5), freestream (1,1,0)) on a
+periodic [0,10]^3 box of 64^3 hexahedra, Lagrange p = 3 (83.9 M DOF),
+Lax-Friedrichs flux, classic RK4 at CFL 0.1.  One benchmark *step* is one
+RK4 step over the whole mesh (four fused stage launches replayed from a CUDA
+graph).  Metric: DOF-stage updates/s = DOF x 4 x steps / time.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+value    : device time (CUDA events on the kernels' stream), state resident in HBM
+e2e      : the same steps through the C ABI from pinned host buffers:
+           dg_set_state (H2D), K x dg_rk4_steps(dt, 1), dg_get_state (D2H)
+roofline : the stage kernel (the only kernel of the timed region)
+cpu_baseline / --impl reference : the CPU oracle (restatement of the
+           reference's dense Kokkos algorithm, OpenMP over elements) on a
+           16^3 sample of the same workload (same order, same per-element work)
+N > 1    : one independent replica of the workload per GPU (weak scaling)
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "dg-mpi_b200"))
+
+METRIC = "DOF-stage updates/s: FP64 vs mixed-precision (rel L2 diff <=1e-6 vs FP64)"
+UNIT = "DOF-stage updates/s"
+VORTEX = [1.0, 1.0, 1.0, 1.0, 5.0, 5.0, 5.0, 10.0, 10.0]
+NEL = 64
+ORDER = 3
+CFL = 0.1
+SAMPLE_NEL = 16
+BYTES_PER_DOF_STAGE = 40  # FP64: read U_s, U_0, acc; write acc, U_next
+FP64_NOMINAL_TFLOPS = 148 * 64 * 2 * 1.965e9 / 1e12  # 148 SMs x 64 FP64 FMA/clk x 1.965 GHz
+
+
+def algorithmic_flops_per_dof(p: int) -> float:
+    """Sum-factorised algorithmic flop count per DOF and stage (n = p+1, m = p+2)."""
+    n, m = p + 1, p + 2
+    E = 2 * (m * n ** 3 + m ** 2 * n ** 2 + m ** 3 * n)
+    trace = 6 * 5 * 2 * (n ** 3 + m * n ** 2 + m ** 2 * n)
+    total = 5 * E + 15 * E + 2 * trace + 5 * 3 * 2 * n ** 4 + 130 * m ** 3 + 600 * m ** 2 + 20 * n ** 3
+    return total / (5 * n ** 3)
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except OSError:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def profile_traffic(name="stage_kernel_p3_64cubed.md"):
+    """DRAM bytes per stage launch recorded from an ncu capture (profiles/)."""
+    try:
+        with open(os.path.join(ROOT, "profiles", name)) as f:
+            for line in f:
+                if line.strip().startswith("dram_bytes_per_launch:"):
+                    return float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"dg_clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            self.out = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.QUERY,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.out, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.out.close()
+
+    def summary(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        loaded = [s for s in sm if smax and s > 0.5 * max(smax)] or sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": reasons, "samples": len(rows)}
+
+
+def build_case(device: int):
+    import dg_b200
+    mesh = dg_b200.periodic_box((NEL, NEL, NEL), (0.0, 0.0, 0.0), (10.0, 10.0, 10.0))
+    case = dg_b200.Case(mesh, ORDER, flux="LaxFriedrichs", gas_constant=1.0, device=device)
+    U0 = case.project_ic("IsentropicVortexXY", VORTEX)
+    dt = case.cfl_time_step(U0, CFL)
+    return case, U0, dt
+
+
+def cpu_oracle_rate(warmup: int, steps: int | None, budget_s: float = 12.0):
+    """DOF-stage/s of the CPU oracle on the 16^3 sample; returns (rate, steps, seconds, threads)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import dg_b200
+    import pyoracle
+    mesh = dg_b200.periodic_box((SAMPLE_NEL,) * 3, (0.0, 0.0, 0.0), (10.0, 10.0, 10.0))
+    orc = pyoracle.OracleCase.from_mesh(mesh, ORDER, flux="LaxFriedrichs", gas_constant=1.0)
+    U = orc.project_ic("IsentropicVortexXY", VORTEX)
+    dt = 1e-3
+    if warmup:
+        U = orc.rk4(U, dt, warmup)
+    dof = orc.ne * orc.nb * 5
+    if steps is None:  # adaptive: one step to size a budget-bounded sample
+        t0 = time.perf_counter()
+        U = orc.rk4(U, dt, 1)
+        one = time.perf_counter() - t0
+        steps = max(1, min(50, int(budget_s / max(one, 1e-6))))
+    t0 = time.perf_counter()
+    orc.rk4(U, dt, steps)
+    sec = time.perf_counter() - t0
+    threads = pyoracle.library().orc_get_threads()
+    return dof * 4 * steps / sec, steps, sec, threads
+
+
+def run_reference(args, rank: int):
+    if rank != 0:
+        return
+    rate, steps, sec, threads = cpu_oracle_rate(args.warmup, args.steps)
+    sample = (f"{SAMPLE_NEL}^3 periodic hex sample of the {NEL}^3 workload, p={ORDER}, {steps} RK4 steps "
+              f"({sec:.2f} s) after {args.warmup} warm-up steps")
+    line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": steps, "warmup": args.warmup, "ms_per_step": 1e3 * sec / steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (analytic isentropic vortex IC, in-memory periodic mesh)",
+            "config": {"workload": f"vortex_xy_{NEL}cubed_p{ORDER}_fp64", "sample": f"{SAMPLE_NEL}^3",
+                       "order": ORDER, "flux": "LaxFriedrichs", "stepper": "RK4"},
+            "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(local)
+
+    case, U0, dt = build_case(local)
+    dof = case.ne * case.nb * 5
+    K, W = args.steps, args.warmup
+
+    # ---- device-timed region: state resident in HBM ----
+    case.set_state(U0)
+    case.rk4(dt, W)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        device_ms = case.rk4_timed(dt, K)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+        t = torch.tensor([device_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        device_ms = float(t.item())
+    value = world * dof * 4 * K / (device_ms / 1e3)
+
+    # ---- end to end through the C ABI with pinned host buffers ----
+    host_in = torch.from_numpy(U0).pin_memory()
+    host_out = torch.empty_like(host_in).pin_memory()
+    for _ in range(2):  # warm the copy path
+        case.set_state_ptr(host_in.data_ptr())
+        case.rk4(dt, 1)
+        case.get_state_ptr(host_out.data_ptr())
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    case.set_state_ptr(host_in.data_ptr())
+    for _ in range(K):
+        case.rk4(dt, 1)
+    case.get_state_ptr(host_out.data_ptr())
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        dist.barrier()
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = world * dof * 4 * K / e2e_s
+    state_bytes = dof * 8
+    if not torch.isfinite(host_out).all():
+        raise RuntimeError("non-finite state after the e2e run")
+
+    if rank == 0:
+        peaks, peak_kind = measured_peaks()
+        launch_s = device_ms / 1e3 / (4 * K)
+        achieved = BYTES_PER_DOF_STAGE * dof / launch_s / 1e9
+        flops = algorithmic_flops_per_dof(ORDER) * dof / launch_s / 1e12
+        traffic = profile_traffic()
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+            "ms_per_step": device_ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (analytic isentropic vortex IC, in-memory periodic mesh)",
+            "config": {"workload": f"vortex_xy_{NEL}cubed_p{ORDER}_fp64", "mesh": f"{NEL}^3 periodic hex on [0,10]^3",
+                       "order": ORDER, "dof": dof, "flux": "LaxFriedrichs", "stepper": "RK4, 4 fused stage launches/step",
+                       "cfl": CFL, "dt": dt, "l2": "inputs larger than L2 (each state buffer %.0f MB > 126 MB)" % (state_bytes / 1e6),
+                       "parallelism": "replicas" if world > 1 else "single-gpu"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                         "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
+                         "peak_source": peak_kind,
+                         "kernel": f"dgk::stage_kernel<{ORDER}>", "bytes_per_launch": BYTES_PER_DOF_STAGE * dof,
+                         "binding_roof": "fp64",
+                         "fp64": {"achieved_tflops": flops, "peak_tflops": FP64_NOMINAL_TFLOPS,
+                                  "peak_source": "nominal (148 SMs x 64 FP64 FMA/clk x 1.965 GHz)",
+                                  "frac": flops / FP64_NOMINAL_TFLOPS,
+                                  "flops_per_dof_stage": algorithmic_flops_per_dof(ORDER)}},
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": state_bytes / K,
+                    "d2h_bytes_per_step": state_bytes / K + 4,
+                    "timing": "host clock around synchronous C-ABI calls, device synchronised on both sides"},
+            "gpu_launches": 4 * K,
+            "clocks": clocks.summary(),
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            rate, steps, sec, threads = cpu_oracle_rate(1, None)
+            line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+                                    "sample": f"{SAMPLE_NEL}^3 periodic hex, p={ORDER}, {steps} RK4 steps ({sec:.1f} s), "
+                                              "dense per-element algorithm, OpenMP over elements"}
+        print(json.dumps(line), flush=True)
+    case.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

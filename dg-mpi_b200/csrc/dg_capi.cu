@@ -538,33 +538,65 @@ int dg_mass_inverse_residual(dg_ctx* c, double dt, double* dU)
     return check_status(c);
 }
 
+namespace {
+
+int prepare_rk4_graph(dg_ctx* c, double dt)
+{
+    if (c->graph_exec && c->graph_dt == dt) return DG_OK;
+    if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }
+    if (c->graph) { cudaGraphDestroy(c->graph); c->graph = nullptr; }
+    // a first launch outside capture sets the kernel attributes and the grid
+    if (c->stage_grid == 0) {
+        int rc = launch_stage(c, dgk::kModeMassInv, c->d_U0, c->d_U0, c->d_out, 0.0);
+        if (rc) return rc;
+        DG_CUDA(c, cudaStreamSynchronize(c->stream));
+    }
+    DG_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = launch_stage(c, dgk::kModeRK1, c->d_U0, c->d_U0, c->d_Ua, dt);
+    if (!rc) rc = launch_stage(c, dgk::kModeRK2, c->d_Ua, c->d_U0, c->d_Ub, dt);
+    if (!rc) rc = launch_stage(c, dgk::kModeRK3, c->d_Ub, c->d_U0, c->d_Ua, dt);
+    if (!rc) rc = launch_stage(c, dgk::kModeRK4, c->d_Ua, c->d_U0, c->d_U0, dt);
+    cudaGraph_t g = nullptr;
+    cudaError_t ce = cudaStreamEndCapture(c->stream, &g);
+    if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+    if (ce != cudaSuccess) return fail(c, DG_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+    c->graph = g;
+    DG_CUDA(c, cudaGraphInstantiate(&c->graph_exec, c->graph, 0));
+    c->graph_dt = dt;
+    return DG_OK;
+}
+
+}  // namespace
+
+int dg_rk4_steps_timed(dg_ctx* c, double dt, int nsteps, double* device_ms)
+{
+    if (!c || nsteps < 0 || !device_ms) return fail(c, DG_ERR_ARG, "dg_rk4_steps_timed: bad argument");
+    DG_CUDA(c, cudaSetDevice(c->device));
+    int rc = prepare_rk4_graph(c, dt);
+    if (rc) return rc;
+    cudaEvent_t ev[2];
+    DG_CUDA(c, cudaEventCreate(&ev[0]));
+    if (cudaEventCreate(&ev[1]) != cudaSuccess) { cudaEventDestroy(ev[0]); return fail(c, DG_ERR_CUDA, "cudaEventCreate"); }
+    cudaError_t ce = cudaEventRecord(ev[0], c->stream);
+    for (int s = 0; s < nsteps && ce == cudaSuccess; ++s) ce = cudaGraphLaunch(c->graph_exec, c->stream);
+    if (ce == cudaSuccess) ce = cudaEventRecord(ev[1], c->stream);
+    if (ce == cudaSuccess) ce = cudaEventSynchronize(ev[1]);
+    float ms = 0.0f;
+    if (ce == cudaSuccess) ce = cudaEventElapsedTime(&ms, ev[0], ev[1]);
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+    if (ce != cudaSuccess) return fail(c, DG_ERR_CUDA, std::string("timed RK4: ") + cudaGetErrorString(ce));
+    *device_ms = ms;
+    return check_status(c);
+}
+
 int dg_rk4_steps(dg_ctx* c, double dt, int nsteps)
 {
     if (!c || nsteps < 0) return fail(c, DG_ERR_ARG, "dg_rk4_steps: bad argument");
     if (nsteps == 0) return DG_OK;
     DG_CUDA(c, cudaSetDevice(c->device));
-    if (!c->graph_exec || c->graph_dt != dt) {
-        if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }
-        if (c->graph) { cudaGraphDestroy(c->graph); c->graph = nullptr; }
-        // first launches outside capture set the kernel attributes and grid
-        if (c->stage_grid == 0) {
-            int rc = launch_stage(c, dgk::kModeMassInv, c->d_U0, c->d_U0, c->d_out, 0.0);
-            if (rc) return rc;
-            DG_CUDA(c, cudaStreamSynchronize(c->stream));
-        }
-        DG_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-        int rc = launch_stage(c, dgk::kModeRK1, c->d_U0, c->d_U0, c->d_Ua, dt);
-        if (!rc) rc = launch_stage(c, dgk::kModeRK2, c->d_Ua, c->d_U0, c->d_Ub, dt);
-        if (!rc) rc = launch_stage(c, dgk::kModeRK3, c->d_Ub, c->d_U0, c->d_Ua, dt);
-        if (!rc) rc = launch_stage(c, dgk::kModeRK4, c->d_Ua, c->d_U0, c->d_U0, dt);
-        cudaGraph_t g = nullptr;
-        cudaError_t ce = cudaStreamEndCapture(c->stream, &g);
-        if (rc) { if (g) cudaGraphDestroy(g); return rc; }
-        if (ce != cudaSuccess) return fail(c, DG_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
-        c->graph = g;
-        DG_CUDA(c, cudaGraphInstantiate(&c->graph_exec, c->graph, 0));
-        c->graph_dt = dt;
-    }
+    int rc = prepare_rk4_graph(c, dt);
+    if (rc) return rc;
     for (int s = 0; s < nsteps; ++s) DG_CUDA(c, cudaGraphLaunch(c->graph_exec, c->stream));
     DG_CUDA(c, cudaStreamSynchronize(c->stream));
     return check_status(c);

@@ -74,6 +74,7 @@ def library(path: str | None = None) -> ctypes.CDLL:
         "dg_residual": (ctypes.c_int, [vp, dp]),
         "dg_mass_inverse_residual": (ctypes.c_int, [vp, ctypes.c_double, dp]),
         "dg_rk4_steps": (ctypes.c_int, [vp, ctypes.c_double, ctypes.c_int]),
+        "dg_rk4_steps_timed": (ctypes.c_int, [vp, ctypes.c_double, ctypes.c_int, dp]),
         "dg_fe_steps": (ctypes.c_int, [vp, ctypes.c_double, ctypes.c_int]),
         "dg_project_ic": (ctypes.c_int, [vp, ctypes.c_int, dp, ctypes.c_int, ctypes.c_double, dp]),
         "dg_l2_error": (ctypes.c_int, [vp, ctypes.c_int, dp, ctypes.c_int, ctypes.c_double, dp]),
@@ -221,6 +222,12 @@ class Case:
 
     def rk4(self, dt: float, nsteps: int):
         self._check(self._lib.dg_rk4_steps(self._ctx, dt, int(nsteps)))
+
+    def rk4_timed(self, dt: float, nsteps: int) -> float:
+        """RK4 steps; returns their device time in ms (CUDA events on the kernels' stream)."""
+        ms = ctypes.c_double()
+        self._check(self._lib.dg_rk4_steps_timed(self._ctx, dt, int(nsteps), ctypes.byref(ms)))
+        return ms.value
 
     def fe(self, dt: float, nsteps: int):
         self._check(self._lib.dg_fe_steps(self._ctx, dt, int(nsteps)))

@@ -130,6 +130,12 @@ int dg_mass_inverse_residual(dg_ctx* ctx, double dt, double* dU);
  * kernel per stage, the four stages of a step replayed from a CUDA graph. */
 int dg_rk4_steps(dg_ctx* ctx, double dt, int nsteps);
 
+/* dg_rk4_steps with CUDA events recorded on the context's stream around the
+ * graph launches; *device_ms receives the device time of the nsteps steps
+ * (the reference's Utils::Timer "Time to Solution", base.cpp:386-395, on the
+ * device clock). */
+int dg_rk4_steps_timed(dg_ctx* ctx, double dt, int nsteps, double* device_ms);
+
 /* Forward Euler, replaces FE<3>::take_time_step (stepper.cpp:23-55). */
 int dg_fe_steps(dg_ctx* ctx, double dt, int nsteps);
 
