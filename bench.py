@@ -173,15 +173,19 @@ def run_reference(args, rank: int):
 
 
 def main():
+    global NEL
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
+    ap.add_argument("--nel", type=int, default=NEL, help="elements per direction (profiling on a smaller box)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
+    NEL = args.nel
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -221,31 +225,33 @@ def main():
     value = world * dof * 4 * K / (device_ms / 1e3)
 
     # ---- end to end through the C ABI with pinned host buffers ----
-    host_in = torch.from_numpy(U0).pin_memory()
-    host_out = torch.empty_like(host_in).pin_memory()
-    for _ in range(2):  # warm the copy path
-        case.set_state_ptr(host_in.data_ptr())
-        case.rk4(dt, 1)
-        case.get_state_ptr(host_out.data_ptr())
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    case.set_state_ptr(host_in.data_ptr())
-    for _ in range(K):
-        case.rk4(dt, 1)
-    case.get_state_ptr(host_out.data_ptr())
-    torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
-    if dist:
-        dist.barrier()
-        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e = world * dof * 4 * K / e2e_s
     state_bytes = dof * 8
-    if not torch.isfinite(host_out).all():
-        raise RuntimeError("non-finite state after the e2e run")
+    e2e = None
+    if not args.no_e2e:
+        host_in = torch.from_numpy(U0).pin_memory()
+        host_out = torch.empty_like(host_in).pin_memory()
+        for _ in range(2):  # warm the copy path
+            case.set_state_ptr(host_in.data_ptr())
+            case.rk4(dt, 1)
+            case.get_state_ptr(host_out.data_ptr())
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        case.set_state_ptr(host_in.data_ptr())
+        for _ in range(K):
+            case.rk4(dt, 1)
+        case.get_state_ptr(host_out.data_ptr())
+        torch.cuda.synchronize()
+        e2e_s = time.perf_counter() - t0
+        if dist:
+            dist.barrier()
+            t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        e2e = world * dof * 4 * K / e2e_s
+        if not torch.isfinite(host_out).all():
+            raise RuntimeError("non-finite state after the e2e run")
 
     if rank == 0:
         peaks, peak_kind = measured_peaks()
@@ -270,9 +276,10 @@ def main():
                                   "peak_source": "nominal (148 SMs x 64 FP64 FMA/clk x 1.965 GHz)",
                                   "frac": flops / FP64_NOMINAL_TFLOPS,
                                   "flops_per_dof_stage": algorithmic_flops_per_dof(ORDER)}},
-            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": state_bytes / K,
-                    "d2h_bytes_per_step": state_bytes / K + 4,
-                    "timing": "host clock around synchronous C-ABI calls, device synchronised on both sides"},
+            "e2e": None if e2e is None else {
+                "value": e2e, "unit": UNIT, "h2d_bytes_per_step": state_bytes / K,
+                "d2h_bytes_per_step": state_bytes / K + 4,
+                "timing": "host clock around synchronous C-ABI calls, device synchronised on both sides"},
             "gpu_launches": 4 * K,
             "clocks": clocks.summary(),
         }
