@@ -88,6 +88,7 @@ int load_constant_tables(dg_ctx* c)
 {
     std::lock_guard<std::mutex> lk(g_table_mutex);
     if (c->device >= 0 && c->device < 64 && g_tables_loaded[c->device]) return DG_OK;
+    // the current device must be c->device: constant symbols are per device
     double B[dgk::kMaxP + 1][dgk::kTabB] = {}, Dm[dgk::kMaxP + 1][dgk::kTabB] = {};
     double W[dgk::kMaxP + 1][dgk::kMaxP + 2] = {}, Mi[dgk::kMaxP + 1][(dgk::kMaxP + 1) * (dgk::kMaxP + 1)] = {};
     double Be[dgk::kMaxP + 1][kMaxMe * (dgk::kMaxP + 1)] = {}, We[dgk::kMaxP + 1][kMaxMe] = {};
@@ -304,6 +305,97 @@ int run_reduce(dg_ctx* c, int kind, int ic_type, const double* data, int ndata, 
     for (int b = 0; b < c->red_grid; ++b)
         for (int v = 0; v < 5; ++v) out5[v] += part[static_cast<size_t>(b) * 5 + v];
     return DG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// allocation-free kinetic energy: the same per-element quadrature as
+// reduce_kernel (kind 1), with the per-block partial sums in a static device
+// array instead of context memory, and a one-block finalisation on the device
+
+constexpr int kNoAllocElemsPerBlock = 64;
+constexpr int kNoAllocMaxBlocks = 16384;  // two doubles each: 32768 doubles, 256 KB
+constexpr long long kNoAllocMaxElems = 1LL * kNoAllocElemsPerBlock * kNoAllocMaxBlocks;
+
+static __device__ __align__(256) double g_noalloc_scratch[2 * kNoAllocMaxBlocks];
+
+std::mutex g_noalloc_mutex;
+double* g_noalloc_ptr[64] = {};
+
+template <int P>
+__global__ void __launch_bounds__(256) ke_partials_noalloc(const double* __restrict__ U, const double* __restrict__ djac,
+                                                           int ne, double* __restrict__ scratch)
+{
+    constexpr int N = P + 1, NB = N * N * N, M = P + 2;
+    __shared__ double sU[5 * NB];
+    __shared__ double red[2][256];
+    const double* Bq = dgk::cB[P];
+    const double* Wq = dgk::cW[P];
+    double ke = 0.0, vol = 0.0;
+    const int e_begin = blockIdx.x * kNoAllocElemsPerBlock;
+    const int e_end = min(ne, e_begin + kNoAllocElemsPerBlock);
+    for (int e = e_begin; e < e_end; ++e) {
+        __syncthreads();
+        for (int i = threadIdx.x; i < 5 * NB; i += blockDim.x) sU[i] = U[(size_t)e * 5 * NB + i];
+        __syncthreads();
+        const double dj = djac[e];
+        for (int q = threadIdx.x; q < M * M * M; q += blockDim.x) {
+            const int i = q % M, j = (q / M) % M, k = q / (M * M);
+            double Uq[4];
+            for (int v = 0; v < 4; ++v) {
+                double sz = 0.0;
+                for (int bz = 0; bz < N; ++bz) {
+                    double sy = 0.0;
+                    for (int by = 0; by < N; ++by) {
+                        double sx = 0.0;
+                        for (int bx = 0; bx < N; ++bx) sx += Bq[i * N + bx] * sU[v * NB + (bz * N + by) * N + bx];
+                        sy += Bq[j * N + by] * sx;
+                    }
+                    sz += Bq[k * N + bz] * sy;
+                }
+                Uq[v] = sz;
+            }
+            const double w = (Wq[i] * Wq[j]) * Wq[k] * dj;
+            ke += 0.5 * (Uq[1] * Uq[1] + Uq[2] * Uq[2] + Uq[3] * Uq[3]) / Uq[0] * w;
+            vol += w;
+        }
+    }
+    red[0][threadIdx.x] = ke;
+    red[1][threadIdx.x] = vol;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) {
+            red[0][threadIdx.x] += red[0][threadIdx.x + s];
+            red[1][threadIdx.x] += red[1][threadIdx.x + s];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        scratch[2 * blockIdx.x] = red[0][0];
+        scratch[2 * blockIdx.x + 1] = red[1][0];
+    }
+}
+
+// sums the nblocks partials in a fixed order (deterministic) and writes KE / V
+__global__ void __launch_bounds__(256) ke_finalize_noalloc(const double* __restrict__ scratch, int nblocks,
+                                                           double* __restrict__ out)
+{
+    __shared__ double red[2][256];
+    double ke = 0.0, vol = 0.0;
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
+        ke += scratch[2 * b];
+        vol += scratch[2 * b + 1];
+    }
+    red[0][threadIdx.x] = ke;
+    red[1][threadIdx.x] = vol;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) {
+            red[0][threadIdx.x] += red[0][threadIdx.x + s];
+            red[1][threadIdx.x] += red[1][threadIdx.x + s];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[0] = red[0][0] / red[1][0];
 }
 
 int check_status(dg_ctx* c)
@@ -657,6 +749,56 @@ int dg_kinetic_energy(dg_ctx* c, double* ke)
     int rc = run_reduce(c, 1, 0, nullptr, 0, 0.0, sums);
     if (rc) return rc;
     *ke = sums[0] / c->pm.volume;
+    return DG_OK;
+}
+
+int dg_kinetic_energy_noalloc(int order, int nelem, const double* d_state, const double* d_djac, double* d_ke,
+                              void* stream)
+{
+    g_create_error.clear();
+    if (order < 0 || order > dgk::kMaxP) return fail(nullptr, DG_ERR_ARG, "dg_kinetic_energy_noalloc: order must be 0..5");
+    if (nelem <= 0 || !d_state || !d_djac || !d_ke)
+        return fail(nullptr, DG_ERR_ARG, "dg_kinetic_energy_noalloc: null pointer or empty mesh");
+    if (nelem > kNoAllocMaxElems)
+        return fail(nullptr, DG_ERR_ARG,
+                    "dg_kinetic_energy_noalloc: " + std::to_string(nelem) + " elements exceed the allocation-free limit of " +
+                        std::to_string(kNoAllocMaxElems) + " (16384 blocks of 64 elements in a 256 KB static scratch array)");
+    int dev = 0;
+    cudaError_t ce = cudaGetDevice(&dev);
+    if (ce != cudaSuccess) return fail(nullptr, DG_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(ce));
+    if (dev < 0 || dev >= 64) return fail(nullptr, DG_ERR_UNSUPPORTED, "device ordinal above 63");
+    double* scratch = nullptr;
+    {
+        // one-time set-up per device, with that device current: basis tables
+        // and the device address of the static scratch array
+        std::lock_guard<std::mutex> lk(g_noalloc_mutex);
+        if (!g_noalloc_ptr[dev]) {
+            dg_ctx tmp;
+            tmp.device = dev;
+            if (load_constant_tables(&tmp) != DG_OK) return fail(nullptr, DG_ERR_CUDA, tmp.err);
+            void* p = nullptr;
+            ce = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+            if (ce != cudaSuccess || !p)
+                return fail(nullptr, DG_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(ce));
+            g_noalloc_ptr[dev] = static_cast<double*>(p);
+        }
+        scratch = g_noalloc_ptr[dev];
+    }
+    const int nblocks = (nelem + kNoAllocElemsPerBlock - 1) / kNoAllocElemsPerBlock;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    switch (order) {
+        case 0: ke_partials_noalloc<0><<<nblocks, 256, 0, s>>>(d_state, d_djac, nelem, scratch); break;
+        case 1: ke_partials_noalloc<1><<<nblocks, 256, 0, s>>>(d_state, d_djac, nelem, scratch); break;
+        case 2: ke_partials_noalloc<2><<<nblocks, 256, 0, s>>>(d_state, d_djac, nelem, scratch); break;
+        case 3: ke_partials_noalloc<3><<<nblocks, 256, 0, s>>>(d_state, d_djac, nelem, scratch); break;
+        case 4: ke_partials_noalloc<4><<<nblocks, 256, 0, s>>>(d_state, d_djac, nelem, scratch); break;
+        default: ke_partials_noalloc<5><<<nblocks, 256, 0, s>>>(d_state, d_djac, nelem, scratch); break;
+    }
+    ce = cudaGetLastError();
+    if (ce != cudaSuccess) return fail(nullptr, DG_ERR_CUDA, std::string("kinetic-energy partials: ") + cudaGetErrorString(ce));
+    ke_finalize_noalloc<<<1, 256, 0, s>>>(scratch, nblocks, d_ke);
+    ce = cudaGetLastError();
+    if (ce != cudaSuccess) return fail(nullptr, DG_ERR_CUDA, std::string("kinetic-energy finalise: ") + cudaGetErrorString(ce));
     return DG_OK;
 }
 

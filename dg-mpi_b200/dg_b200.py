@@ -79,6 +79,7 @@ def library(path: str | None = None) -> ctypes.CDLL:
         "dg_project_ic": (ctypes.c_int, [vp, ctypes.c_int, dp, ctypes.c_int, ctypes.c_double, dp]),
         "dg_l2_error": (ctypes.c_int, [vp, ctypes.c_int, dp, ctypes.c_int, ctypes.c_double, dp]),
         "dg_kinetic_energy": (ctypes.c_int, [vp, dp]),
+        "dg_kinetic_energy_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, vp, vp, vp, vp]),
         "dg_total_volume": (ctypes.c_int, [vp, dp]),
         "dg_status": (ctypes.c_int, [vp, up]),
         "dg_sync": (ctypes.c_int, [vp]),
@@ -297,3 +298,16 @@ def basis_tables(p: int):
     if rc:
         raise DGError(rc, "dg_basis_tables")
     return B, D, Mi
+
+
+def kinetic_energy_noalloc(order: int, nelem: int, d_state: int, d_djac: int, d_ke: int, stream: int = 0):
+    """Allocation-free kinetic energy on device pointers (dg_kinetic_energy_noalloc).
+
+    For callers whose device memory is owned by their own allocator: the
+    library allocates nothing; the result lands in the device double d_ke and
+    the work is queued on `stream` without waiting for it."""
+    lib = library()
+    rc = lib.dg_kinetic_energy_noalloc(order, nelem, ctypes.c_void_p(d_state), ctypes.c_void_p(d_djac),
+                                       ctypes.c_void_p(d_ke), ctypes.c_void_p(stream))
+    if rc:
+        raise DGError(rc, lib.dg_last_error(None).decode())

@@ -153,6 +153,32 @@ int dg_l2_error(dg_ctx* ctx, int ic_type, const double* data, int ndata, double 
 /* Volume-averaged kinetic energy (1/V) * integral of |rho u|^2 / (2 rho). */
 int dg_kinetic_energy(dg_ctx* ctx, double* ke);
 
+/* Allocation-free kinetic energy.  No counterpart in the reference.
+ *
+ * For callers that cannot call cudaMalloc -- applications whose device memory
+ * is owned by a framework allocator or a fixed arena that forbids allocations
+ * behind its back: the call allocates nothing.  The caller passes device
+ * pointers to a state d_state [nelem][5][nb] (the device layout of
+ * dg_device_state) and to per-element Jacobian determinants d_djac [nelem];
+ * the result, (1/V) * integral of |rho u|^2 / (2 rho) over the mesh with
+ * V = sum of 8 * djac, is written to the device double d_ke.  Work is queued
+ * on `stream` (a cudaStream_t, NULL for the default stream) and the call does
+ * not wait for it.
+ *
+ * Scratch lives in a static device array of 32768 doubles (256 KB) that every
+ * GPU loading this library holds until the process exits; it holds two
+ * partial sums for each of at most 16384 blocks of 64 elements, which bounds
+ * nelem to 1,048,576 (a 96^3 mesh fits), and larger meshes are rejected with
+ * DG_ERR_ARG.  All calls on a device share that array: two calls whose
+ * work overlaps on the GPU (for example on two streams) race and corrupt each
+ * other's result, so serialise them.  Each call overwrites every scratch entry
+ * it reads, so nothing is carried over from an earlier call.  The first call on a device
+ * does a one-time set-up (loads the basis tables and looks up the array's
+ * device address with that device current); make that first call before any
+ * stream capture. */
+int dg_kinetic_energy_noalloc(int order, int nelem, const double* d_state, const double* d_djac,
+                              double* d_ke, void* stream);
+
 /* Total mesh volume (sum of element volumes, MeshTools::get_total_volume). */
 int dg_total_volume(const dg_ctx* ctx, double* vol);
 
