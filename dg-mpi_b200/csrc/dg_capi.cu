@@ -20,21 +20,28 @@
 using dgk::GeoDev;
 using dgk::StageArgs;
 
+int dgk::stage_variants(int p, const StageVariant** out)
+{
+    switch (p) {
+        case 0: return stage_variants_p0(out);
+        case 1: return stage_variants_p1(out);
+        case 2: return stage_variants_p2(out);
+        case 3: return stage_variants_p3(out);
+        case 4: return stage_variants_p4(out);
+        case 5: return stage_variants_p5(out);
+        default: *out = nullptr; return 0;
+    }
+}
+
 namespace {
 
-// ---------------------------------------------------------------------------
-// per-order launch configuration of the stage kernel: elements per CTA and
-// threads per CTA (shared memory = E * per-element working set)
-template <int P> struct Cfg;
-template <> struct Cfg<0> { static constexpr int E = 32, NT = 128; };
-template <> struct Cfg<1> { static constexpr int E = 8, NT = 128; };
-template <> struct Cfg<2> { static constexpr int E = 6, NT = 96; };
-template <> struct Cfg<3> { static constexpr int E = 4, NT = 128; };
-template <> struct Cfg<4> { static constexpr int E = 3, NT = 128; };
-template <> struct Cfg<5> { static constexpr int E = 3, NT = 160; };
+constexpr int kMaxVariants = 8;
 
-// tables of the IC / error rule (2*max(p,1)+2 points) and of the volume rule
+// tables of the IC / error rule (2*max(p,1)+2 points) and of the volume rule,
+// used by the reductions
 constexpr int kMaxMe = 12;
+__constant__ double cVB[dgk::kMaxP + 1][dgk::kTabB];
+__constant__ double cVW[dgk::kMaxP + 1][dgk::kMaxP + 2];
 __constant__ double cBe[dgk::kMaxP + 1][kMaxMe * (dgk::kMaxP + 1)];
 __constant__ double cWe[dgk::kMaxP + 1][kMaxMe];
 __constant__ double cXe[dgk::kMaxP + 1][kMaxMe];
@@ -58,7 +65,10 @@ struct dg_ctx {
     double* d_X0 = nullptr;
     double* d_partials = nullptr;
     unsigned* d_status = nullptr;
-    int stage_grid = 0, red_grid = 0;
+    int red_grid = 0;
+    int variant = 0;                          // index into dgk::stage_variants(p)
+    int variant_grid[kMaxVariants] = {};      // persistent grid per variant, 0 = not prepared
+    dgk::StageTables stage_tab{};
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
     double graph_dt = 0.0;
@@ -104,10 +114,10 @@ int load_constant_tables(dg_ctx* c)
         std::copy(t.we.begin(), t.we.end(), We[p]);
         std::copy(t.xe.begin(), t.xe.end(), Xe[p]);
     }
-    DG_CUDA(c, cudaMemcpyToSymbol(dgk::cB, B, sizeof(B)));
-    DG_CUDA(c, cudaMemcpyToSymbol(dgk::cD, Dm, sizeof(Dm)));
-    DG_CUDA(c, cudaMemcpyToSymbol(dgk::cW, W, sizeof(W)));
-    DG_CUDA(c, cudaMemcpyToSymbol(dgk::cMinv, Mi, sizeof(Mi)));
+    (void)Dm;
+    (void)Mi;
+    DG_CUDA(c, cudaMemcpyToSymbol(cVB, B, sizeof(B)));
+    DG_CUDA(c, cudaMemcpyToSymbol(cVW, W, sizeof(W)));
     DG_CUDA(c, cudaMemcpyToSymbol(cBe, Be, sizeof(Be)));
     DG_CUDA(c, cudaMemcpyToSymbol(cWe, We, sizeof(We)));
     DG_CUDA(c, cudaMemcpyToSymbol(cXe, Xe, sizeof(Xe)));
@@ -119,24 +129,22 @@ int load_constant_tables(dg_ctx* c)
 // ---------------------------------------------------------------------------
 // stage launches
 
-template <int P>
-int launch_stage_p(dg_ctx* c, const StageArgs& a)
+// Sets the variant's shared-memory attribute and its persistent grid size
+// (SM count x resident CTAs per SM, capped by the number of batches).
+int prepare_variant(dg_ctx* c, int v)
 {
-    constexpr int E = Cfg<P>::E, NT = Cfg<P>::NT;
-    constexpr size_t smem = dgk::stage_smem_bytes<P, E>();
-    static_assert(smem <= 227 * 1024, "stage kernel shared memory exceeds 227 KB");
-    auto kern = dgk::stage_kernel<P, E, NT>;
-    if (c->stage_grid == 0) {
-        DG_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        int dev_sms = 0, per_sm = 0;
-        DG_CUDA(c, cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, c->device));
-        DG_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem));
-        if (per_sm < 1) return fail(c, DG_ERR_UNSUPPORTED, "stage kernel does not fit on an SM");
-        const int batches = (c->ne + E - 1) / E;
-        c->stage_grid = std::max(1, std::min(batches, dev_sms * per_sm));
-    }
-    kern<<<c->stage_grid, NT, smem, c->stream>>>(a);
-    DG_CUDA(c, cudaGetLastError());
+    const dgk::StageVariant* vs = nullptr;
+    const int nv = dgk::stage_variants(c->p, &vs);
+    if (v < 0 || v >= nv) return fail(c, DG_ERR_ARG, "stage variant index out of range");
+    if (c->variant_grid[v] > 0) return DG_OK;
+    const dgk::StageVariant& sv = vs[v];
+    DG_CUDA(c, cudaFuncSetAttribute(sv.func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sv.smem));
+    int dev_sms = 0, per_sm = 0;
+    DG_CUDA(c, cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, c->device));
+    DG_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sv.func, sv.NT, sv.smem));
+    if (per_sm < 1) return fail(c, DG_ERR_UNSUPPORTED, "stage kernel variant does not fit on an SM");
+    const int batches = (c->ne + sv.E - 1) / sv.E;
+    c->variant_grid[v] = std::max(1, std::min(batches, dev_sms * per_sm));
     return DG_OK;
 }
 
@@ -157,15 +165,13 @@ int launch_stage(dg_ctx* c, int mode, const double* Us, const double* U0, double
     a.mode = mode;
     a.gamma = c->gamma;
     a.dt = dt;
-    switch (c->p) {
-        case 0: return launch_stage_p<0>(c, a);
-        case 1: return launch_stage_p<1>(c, a);
-        case 2: return launch_stage_p<2>(c, a);
-        case 3: return launch_stage_p<3>(c, a);
-        case 4: return launch_stage_p<4>(c, a);
-        case 5: return launch_stage_p<5>(c, a);
-        default: return fail(c, DG_ERR_UNSUPPORTED, "order out of range");
-    }
+    a.tab = c->stage_tab;
+    int rc = prepare_variant(c, c->variant);
+    if (rc) return rc;
+    const dgk::StageVariant* vs = nullptr;
+    dgk::stage_variants(c->p, &vs);
+    DG_CUDA(c, vs[c->variant].launch(a, c->variant_grid[c->variant], c->stream));
+    return DG_OK;
 }
 
 // ---------------------------------------------------------------------------
@@ -213,8 +219,8 @@ __global__ void __launch_bounds__(256) reduce_kernel(ReduceArgs a)
     __shared__ double sU[5 * NB];
     __shared__ double red[5][256];
     const int me = a.kind == 0 ? (P > 1 ? 2 * P + 2 : 4) : P + 2;
-    const double* Bq = a.kind == 0 ? cBe[P] : dgk::cB[P];
-    const double* Wq = a.kind == 0 ? cWe[P] : dgk::cW[P];
+    const double* Bq = a.kind == 0 ? cBe[P] : cVB[P];
+    const double* Wq = a.kind == 0 ? cWe[P] : cVW[P];
     const double* Xq = a.kind == 0 ? cXe[P] : cXq[P];
     double acc[5] = {0, 0, 0, 0, 0};
     for (int e = blockIdx.x; e < a.ne; e += gridDim.x) {
@@ -328,8 +334,8 @@ __global__ void __launch_bounds__(256) ke_partials_noalloc(const double* __restr
     constexpr int N = P + 1, NB = N * N * N, M = P + 2;
     __shared__ double sU[5 * NB];
     __shared__ double red[2][256];
-    const double* Bq = dgk::cB[P];
-    const double* Wq = dgk::cW[P];
+    const double* Bq = cVB[P];
+    const double* Wq = cVW[P];
     double ke = 0.0, vol = 0.0;
     const int e_begin = blockIdx.x * kNoAllocElemsPerBlock;
     const int e_end = min(ne, e_begin + kNoAllocElemsPerBlock);
@@ -494,6 +500,10 @@ int dg_create(const dg_case_desc* cd, const dg_mesh_desc* md, dg_ctx** out)
         return fail(nullptr, unsup ? DG_ERR_UNSUPPORTED : DG_ERR_ARG, perr);
     }
     c->ne = c->pm.ne;
+    std::copy(c->tab.B.begin(), c->tab.B.end(), c->stage_tab.B);
+    std::copy(c->tab.D.begin(), c->tab.D.end(), c->stage_tab.D);
+    std::copy(c->tab.wq.begin(), c->tab.wq.end(), c->stage_tab.W);
+    std::copy(c->tab.Minv.begin(), c->tab.Minv.end(), c->stage_tab.Minv);
 
     // the mesh is valid; now the device
     int ndev = 0;
@@ -637,14 +647,11 @@ int prepare_rk4_graph(dg_ctx* c, double dt)
     if (c->graph_exec && c->graph_dt == dt) return DG_OK;
     if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }
     if (c->graph) { cudaGraphDestroy(c->graph); c->graph = nullptr; }
-    // a first launch outside capture sets the kernel attributes and the grid
-    if (c->stage_grid == 0) {
-        int rc = launch_stage(c, dgk::kModeMassInv, c->d_U0, c->d_U0, c->d_out, 0.0);
-        if (rc) return rc;
-        DG_CUDA(c, cudaStreamSynchronize(c->stream));
-    }
+    // kernel attributes and the grid are set outside the capture
+    int rc = prepare_variant(c, c->variant);
+    if (rc) return rc;
     DG_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    int rc = launch_stage(c, dgk::kModeRK1, c->d_U0, c->d_U0, c->d_Ua, dt);
+    rc = launch_stage(c, dgk::kModeRK1, c->d_U0, c->d_U0, c->d_Ua, dt);
     if (!rc) rc = launch_stage(c, dgk::kModeRK2, c->d_Ua, c->d_U0, c->d_Ub, dt);
     if (!rc) rc = launch_stage(c, dgk::kModeRK3, c->d_Ub, c->d_U0, c->d_Ua, dt);
     if (!rc) rc = launch_stage(c, dgk::kModeRK4, c->d_Ua, c->d_U0, c->d_U0, dt);
@@ -680,6 +687,75 @@ int dg_rk4_steps_timed(dg_ctx* c, double dt, int nsteps, double* device_ms)
     if (ce != cudaSuccess) return fail(c, DG_ERR_CUDA, std::string("timed RK4: ") + cudaGetErrorString(ce));
     *device_ms = ms;
     return check_status(c);
+}
+
+int dg_num_stage_variants(int order)
+{
+    const dgk::StageVariant* vs = nullptr;
+    return dgk::stage_variants(order, &vs);
+}
+
+int dg_stage_variant_info(int order, int v, int* elems_per_cta, int* threads_per_cta, int* groups)
+{
+    const dgk::StageVariant* vs = nullptr;
+    const int nv = dgk::stage_variants(order, &vs);
+    if (v < 0 || v >= nv) return DG_ERR_ARG;
+    if (elems_per_cta) *elems_per_cta = vs[v].E;
+    if (threads_per_cta) *threads_per_cta = vs[v].NT;
+    if (groups) *groups = vs[v].G;
+    return DG_OK;
+}
+
+int dg_set_stage_variant(dg_ctx* c, int v)
+{
+    if (!c) return DG_ERR_ARG;
+    if (v < 0 || v >= dg_num_stage_variants(c->p)) return fail(c, DG_ERR_ARG, "stage variant index out of range");
+    if (v != c->variant) {
+        c->variant = v;
+        if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }
+        if (c->graph) { cudaGraphDestroy(c->graph); c->graph = nullptr; }
+    }
+    return DG_OK;
+}
+
+int dg_get_stage_variant(const dg_ctx* c) { return c ? c->variant : -1; }
+
+int dg_tune_stage(dg_ctx* c, int reps, int* best, double* ms_per_variant)
+{
+    if (!c || reps < 1) return fail(c, DG_ERR_ARG, "dg_tune_stage: bad argument");
+    DG_CUDA(c, cudaSetDevice(c->device));
+    const int nv = dg_num_stage_variants(c->p);
+    const int keep = c->variant;
+    int winner = keep;
+    double best_ms = 1e300;
+    cudaEvent_t ev[2];
+    DG_CUDA(c, cudaEventCreate(&ev[0]));
+    if (cudaEventCreate(&ev[1]) != cudaSuccess) { cudaEventDestroy(ev[0]); return fail(c, DG_ERR_CUDA, "cudaEventCreate"); }
+    int rc = DG_OK;
+    for (int v = 0; v < nv && rc == DG_OK; ++v) {
+        c->variant = v;
+        // one untimed launch, then `reps` timed ones; the mass-inverse mode
+        // writes scratch output only, so the state is unchanged
+        rc = launch_stage(c, dgk::kModeMassInv, c->d_U0, c->d_U0, c->d_out, 1e-3);
+        if (rc) break;
+        cudaEventRecord(ev[0], c->stream);
+        for (int r = 0; r < reps && rc == DG_OK; ++r) rc = launch_stage(c, dgk::kModeMassInv, c->d_U0, c->d_U0, c->d_out, 1e-3);
+        cudaEventRecord(ev[1], c->stream);
+        if (cudaEventSynchronize(ev[1]) != cudaSuccess) { rc = fail(c, DG_ERR_CUDA, "tuning launch failed"); break; }
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, ev[0], ev[1]);
+        const double per = ms / reps;
+        if (ms_per_variant) ms_per_variant[v] = per;
+        if (per < best_ms) { best_ms = per; winner = v; }
+    }
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+    c->variant = keep;
+    if (rc) return rc;
+    rc = dg_set_stage_variant(c, winner);
+    if (rc) return rc;
+    if (best) *best = winner;
+    return DG_OK;
 }
 
 int dg_rk4_steps(dg_ctx* c, double dt, int nsteps)

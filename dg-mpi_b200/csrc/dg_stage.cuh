@@ -1,7 +1,6 @@
 // dg_stage.cuh -- the fused DG stage kernel (sm_100a, FP64).
 //
-// One launch evaluates, for a batch of E elements per CTA (grid-stride over
-// element batches):
+// One launch evaluates, for batches of E elements per CTA (grid-stride):
 //   face traces of the element and of its six neighbours (2D sum-factorised
 //   interpolation of boundary coefficient slices; the neighbour read is the
 //   on-device periodic face gather that replaces construct_face_states +
@@ -16,9 +15,14 @@
 //   the inverse mass (Kronecker product of 1D inverses / det J for affine
 //   elements, replacing the dense per-element iMM of tools.cpp:124-139),
 //   and the RK4 / forward-Euler stage update (stepper.cpp:23-142).
-// Every 3D contraction is sum-factorised into 1D pencil passes through
-// shared memory; the last interpolation pass, the pointwise flux and the
-// first divergence pass are fused per (x,y) pencil in registers.
+//
+// Every 3D contraction is sum-factorised into 1D passes over shared memory;
+// the last interpolation pass, the pointwise flux and the first divergence
+// pass are fused per (x,y) pencil in registers; traces and lifts are 2D
+// interpolations done per (element, face, variable) in registers.  Shared
+// strides are odd so that FP64 accesses of consecutive tasks avoid bank
+// conflicts.  The coefficients of the next batch are prefetched with
+// cp.async while the current batch computes.
 #pragma once
 #include <cstdint>
 
@@ -29,11 +33,15 @@ namespace dgk {
 constexpr int kMaxP = 5;
 constexpr int kTabB = (kMaxP + 2) * (kMaxP + 1);
 
-// 1D tables per order (filled once per process; see dg_capi.cu)
-__constant__ double cB[kMaxP + 1][kTabB];      // B[q*N + b]
-__constant__ double cD[kMaxP + 1][kTabB];      // D[q*N + b]
-__constant__ double cW[kMaxP + 1][kMaxP + 2];  // GL weights
-__constant__ double cMinv[kMaxP + 1][(kMaxP + 1) * (kMaxP + 1)];
+// 1D tables of the case's order, passed in the kernel's parameter block (it
+// lives in the constant bank, so the unrolled loops read them as constant
+// operands); see dgh::make_tables
+struct StageTables {
+    double B[kTabB];                           // B[q*N + b]: basis at the GL points
+    double D[kTabB];                           // D[q*N + b]: its derivative
+    double W[kMaxP + 2];                       // GL weights
+    double Minv[(kMaxP + 1) * (kMaxP + 1)];    // inverse 1D mass matrix
+};
 
 struct GeoDev {
     double JD[9];
@@ -73,154 +81,170 @@ struct StageArgs {
     int mode;
     double gamma;
     double dt;
+    StageTables tab;
 };
 
-template <int P>
-struct Dim {
-    static constexpr int N = P + 1;
-    static constexpr int M = P + 2;
-    static constexpr int NB = N * N * N;
-    static constexpr int NF = M * M;
-    static constexpr int N2 = N * N;
+__host__ __device__ constexpr int odd(int x) { return x | 1; }
+__host__ __device__ constexpr int cmax(int a, int b) { return a > b ? a : b; }
+
+// G = number of variable groups of the fused pointwise phase (register budget)
+template <int P, int G>
+struct Lay {
+    static constexpr int N = P + 1, M = P + 2, NB = N * N * N, NF = M * M, N2 = N * N;
+    static constexpr int GV = G == 1 ? 5 : (G == 2 ? 3 : 2);  // variables per group (max)
+    static constexpr int VS = odd(NB);           // per-variable stride of U / residual
+    static constexpr int ES = 5 * VS;            // per-element stride of U / residual
+    static constexpr int FS = odd(NF);           // per-(face, variable) stride of traces
+    static constexpr int X1S = odd(N2 * M);      // [bz][by][qx] block
+    static constexpr int X2S = odd(N * NF);      // [bz][qy][qx] block
+    // per-element work area: face phase {Tr[6][5], Tn[6][5]} x FS;
+    // volume phase X2[5] | (X1[5] or A[GV][3] + C[GV][2])
+    static constexpr int face = 60 * FS;
+    static constexpr int vol = 5 * X2S + cmax(5 * X1S, GV * (3 * X2S + 2 * X1S));
+    static constexpr int W = odd(cmax(face, vol));
+    // U (double-buffered prefetch), residual, U0 and accumulator prefetch, work area
+    static constexpr int per_elem = 2 * ES + ES + 2 * ES + W;
 };
 
-// variable groups of the fused pointwise phase: all five variables at once up
-// to p = 3, two groups above (register budget)
-template <int P>
-struct Groups {
-    static constexpr int count = P <= 3 ? 1 : 2;
-    static constexpr int first(int g) { return count == 1 ? 0 : (g == 0 ? 0 : 3); }
-    static constexpr int size(int g) { return count == 1 ? 5 : (g == 0 ? 3 : 2); }
-    static constexpr int max_size = count == 1 ? 5 : 3;
-};
-
-template <int P>
-struct Work {
-    using D = Dim<P>;
-    // face phase: own traces [6][5][NF], neighbour traces [6][5][NF], pass buffer [6][5][N*M]
-    static constexpr int face = 60 * D::NF + 30 * D::N * D::M;
-    // volume phase: X2 [5][N][M][M] first; X1 [5][N][N][M] after it, later
-    // overlaid by the divergence buffers A [nv][3][N][M][M] and C [nv][2][N][N][M]
-    static constexpr int x2 = 5 * D::N * D::NF;
-    static constexpr int x1 = 5 * D::N2 * D::M;
-    static constexpr int div = Groups<P>::max_size * (3 * D::N * D::NF + 2 * D::N2 * D::M);
-    static constexpr int vol = x2 + (x1 > div ? x1 : div);
-    static constexpr int per_elem = face > vol ? face : vol;
-};
+template <int P, int G>
+__host__ __device__ constexpr int group_first(int g)
+{
+    return G == 1 ? 0 : (G == 2 ? (g == 0 ? 0 : 3) : (g == 0 ? 0 : (g == 1 ? 2 : 4)));
+}
+template <int P, int G>
+__host__ __device__ constexpr int group_size(int g)
+{
+    return G == 1 ? 5 : (G == 2 ? (g == 0 ? 3 : 2) : (g == 2 ? 1 : 2));
+}
 
 __device__ __forceinline__ int face_axis(int f) { return f == 2 || f == 4 ? 0 : (f == 1 || f == 3 ? 1 : 2); }
 __device__ __forceinline__ int face_side(int f) { return f == 2 || f == 3 || f == 5 ? 1 : 0; }
 
-// coefficient index of boundary-slice entry (b0, b1) of face f
-template <int P>
+// coefficient index (unpadded, x fastest) of boundary-slice entry (b0, b1) of face f
+template <int N>
 __device__ __forceinline__ int slice_index(int f, int b0, int b1)
 {
-    constexpr int N = P + 1;
     const int ax = face_axis(f), sidx = face_side(f) ? N - 1 : 0;
     if (ax == 0) return b1 * N * N + b0 * N + sidx;
     if (ax == 1) return b1 * N * N + sidx * N + b0;
     return sidx * N * N + b1 * N + b0;
 }
 
-template <int P, int E, int NT>
+__device__ __forceinline__ void cp_async8(double* smem_dst, const double* gmem_src)
+{
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+// all but the most recent group complete
+__device__ __forceinline__ void cp_async_wait_older() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+// queue the coefficients of batch e0 of a global state into the padded buffer dst
+template <int P, int G, int E, int NT>
+__device__ __forceinline__ void prefetch_batch(const double* __restrict__ Us, int ne, int e0, double* dst)
+{
+    using L = Lay<P, G>;
+    for (int i = threadIdx.x; i < E * 5 * L::NB; i += NT) {
+        const int e = i / (5 * L::NB), r = i - e * (5 * L::NB), v = r / L::NB, b = r - v * L::NB;
+        const int ge = min(e0 + e, ne - 1);
+        cp_async8(dst + e * L::ES + v * L::VS + b, Us + (size_t)ge * 5 * L::NB + r);
+    }
+}
+
+// 2D interpolation of an N x N slice s[b1][b0] to the M x M face grid,
+// written to out[t1*M + t0]
+template <int N, int M>
+__device__ __forceinline__ void interp2d(const double* __restrict__ Bt, const double (&s)[N][N], double* out)
+{
+    double tmp[N][M];
+#pragma unroll
+    for (int b1 = 0; b1 < N; ++b1)
+#pragma unroll
+        for (int t0 = 0; t0 < M; ++t0) {
+            double a = 0.0;
+#pragma unroll
+            for (int b0 = 0; b0 < N; ++b0) a += Bt[t0 * N + b0] * s[b1][b0];
+            tmp[b1][t0] = a;
+        }
+#pragma unroll
+    for (int t1 = 0; t1 < M; ++t1)
+#pragma unroll
+        for (int t0 = 0; t0 < M; ++t0) {
+            double a = 0.0;
+#pragma unroll
+            for (int b1 = 0; b1 < N; ++b1) a += Bt[t1 * N + b1] * tmp[b1][t0];
+            out[t1 * M + t0] = a;
+        }
+}
+
+template <int P, int E, int NT, int G>
 __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
 {
-    using D = Dim<P>;
-    constexpr int N = D::N, M = D::M, NB = D::NB, NF = D::NF, N2 = D::N2;
-    constexpr int W = Work<P>::per_elem;
+    using L = Lay<P, G>;
+    constexpr int N = L::N, M = L::M, NB = L::NB, NF = L::NF, N2 = L::N2;
+    constexpr int VS = L::VS, ES = L::ES, FS = L::FS, X1S = L::X1S, X2S = L::X2S, W = L::W, GV = L::GV;
     extern __shared__ double smem[];
-    double* sU = smem;                  // [E][5][NB]
-    double* sRes = sU + E * 5 * NB;     // [E][5][NB]
-    double* sW = sRes + E * 5 * NB;     // [E][W]
-    const double* __restrict__ Bt = cB[P];
-    const double* __restrict__ Dt = cD[P];
-    const double* __restrict__ Wt = cW[P];
-    const double* __restrict__ Mi = cMinv[P];
+    double* sUbuf = smem;                  // [2][E][ES]
+    double* sRes = sUbuf + 2 * E * ES;     // [E][ES]
+    double* sU0 = sRes + E * ES;           // [E][ES] step-start state of the batch
+    double* sAcc = sU0 + E * ES;           // [E][ES] RK accumulator of the batch
+    double* sW = sAcc + E * ES;            // [E][W]
+    const bool need_u0_acc = a.mode == kModeRK2 || a.mode == kModeRK3 || a.mode == kModeRK4;
+    const double* __restrict__ Bt = a.tab.B;
+    const double* __restrict__ Dt = a.tab.D;
+    const double* __restrict__ Wt = a.tab.W;
+    const double* __restrict__ Mi = a.tab.Minv;
     const int tid = threadIdx.x;
     const double gamma = a.gamma;
     unsigned status = 0;
+    const int stride = gridDim.x * E;
 
-    for (int e0 = blockIdx.x * E; e0 < a.ne; e0 += gridDim.x * E) {
-        // ---- load the batch's coefficients (tail elements repeat the last) ----
-        for (int i = tid; i < E * 5 * NB; i += NT) {
-            const int e = i / (5 * NB), r = i - e * (5 * NB);
-            const int ge = min(e0 + e, a.ne - 1);
-            sU[i] = a.Us[(size_t)ge * 5 * NB + r];
-        }
-        __syncthreads();
+    int buf = 0;
+    if (blockIdx.x * E < a.ne) prefetch_batch<P, G, E, NT>(a.Us, a.ne, blockIdx.x * E, sUbuf);
+    cp_async_commit();
 
-        // ---- own face traces: slice rows -> [b1][t0] -> [t1][t0] ----
-        for (int i = tid; i < E * 30 * N; i += NT) {
-            const int b1 = i % N, v = (i / N) % 5, f = (i / (5 * N)) % 6, e = i / (30 * N);
-            double row[N];
-#pragma unroll
-            for (int b0 = 0; b0 < N; ++b0) row[b0] = sU[(e * 5 + v) * NB + slice_index<P>(f, b0, b1)];
-            double* T1 = sW + e * W + 60 * NF + ((f * 5 + v) * N + b1) * M;
-#pragma unroll
-            for (int t = 0; t < M; ++t) {
-                double s = 0.0;
-#pragma unroll
-                for (int b0 = 0; b0 < N; ++b0) s += Bt[t * N + b0] * row[b0];
-                T1[t] = s;
-            }
-        }
+    for (int e0 = blockIdx.x * E; e0 < a.ne; e0 += stride, buf ^= 1) {
+        double* sU = sUbuf + buf * E * ES;
+        cp_async_wait_all();
         __syncthreads();
-        for (int i = tid; i < E * 30 * M; i += NT) {
-            const int t0 = i % M, v = (i / M) % 5, f = (i / (5 * M)) % 6, e = i / (30 * M);
-            const double* T1 = sW + e * W + 60 * NF + (f * 5 + v) * N * M;
-            double col[N];
-#pragma unroll
-            for (int b1 = 0; b1 < N; ++b1) col[b1] = T1[b1 * M + t0];
-            double* Tr = sW + e * W + (f * 5 + v) * NF;
-#pragma unroll
-            for (int t1 = 0; t1 < M; ++t1) {
-                double s = 0.0;
-#pragma unroll
-                for (int b1 = 0; b1 < N; ++b1) s += Bt[t1 * N + b1] * col[b1];
-                Tr[t1 * M + t0] = s;
-            }
+        // the RK operands of this batch (needed only at the end) and the next
+        // batch's coefficients stream in while this batch computes
+        if (need_u0_acc) {
+            prefetch_batch<P, G, E, NT>(a.U0, a.ne, e0, sU0);
+            prefetch_batch<P, G, E, NT>(a.acc, a.ne, e0, sAcc);
         }
-        __syncthreads();
+        cp_async_commit();
+        if (e0 + stride < a.ne) prefetch_batch<P, G, E, NT>(a.Us, a.ne, e0 + stride, sUbuf + (buf ^ 1) * E * ES);
+        cp_async_commit();
 
-        // ---- neighbour traces (periodic face gather) on the neighbour's face ----
-        for (int i = tid; i < E * 30 * N; i += NT) {
-            const int b1 = i % N, v = (i / N) % 5, f = (i / (5 * N)) % 6, e = i / (30 * N);
+        // ---- own and neighbour traces: one task per (element, face, variable) ----
+        for (int t = tid; t < E * 30; t += NT) {
+            const int v = t % 5, f = (t / 5) % 6, e = t / 30;
             const int ge = min(e0 + e, a.ne - 1);
             const int2 c = a.conn[ge * 6 + f];
             const int fn = c.y & 7;
-            double row[N];
+            double sn[N][N], so[N][N];
             if (c.x >= e0 && c.x < e0 + E) {
+                const double* src = sU + (c.x - e0) * ES + v * VS;
 #pragma unroll
-                for (int b0 = 0; b0 < N; ++b0) row[b0] = sU[((c.x - e0) * 5 + v) * NB + slice_index<P>(fn, b0, b1)];
+                for (int b1 = 0; b1 < N; ++b1)
+#pragma unroll
+                    for (int b0 = 0; b0 < N; ++b0) sn[b1][b0] = src[slice_index<N>(fn, b0, b1)];
             } else {
                 const double* src = a.Us + ((size_t)c.x * 5 + v) * NB;
 #pragma unroll
-                for (int b0 = 0; b0 < N; ++b0) row[b0] = __ldg(src + slice_index<P>(fn, b0, b1));
+                for (int b1 = 0; b1 < N; ++b1)
+#pragma unroll
+                    for (int b0 = 0; b0 < N; ++b0) sn[b1][b0] = __ldg(src + slice_index<N>(fn, b0, b1));
             }
-            double* T1 = sW + e * W + 60 * NF + ((f * 5 + v) * N + b1) * M;
+            const double* own = sU + e * ES + v * VS;
 #pragma unroll
-            for (int t = 0; t < M; ++t) {
-                double s = 0.0;
+            for (int b1 = 0; b1 < N; ++b1)
 #pragma unroll
-                for (int b0 = 0; b0 < N; ++b0) s += Bt[t * N + b0] * row[b0];
-                T1[t] = s;
-            }
-        }
-        __syncthreads();
-        for (int i = tid; i < E * 30 * M; i += NT) {
-            const int t0 = i % M, v = (i / M) % 5, f = (i / (5 * M)) % 6, e = i / (30 * M);
-            const double* T1 = sW + e * W + 60 * NF + (f * 5 + v) * N * M;
-            double col[N];
-#pragma unroll
-            for (int b1 = 0; b1 < N; ++b1) col[b1] = T1[b1 * M + t0];
-            double* Tn = sW + e * W + 30 * NF + (f * 5 + v) * NF;
-#pragma unroll
-            for (int t1 = 0; t1 < M; ++t1) {
-                double s = 0.0;
-#pragma unroll
-                for (int b1 = 0; b1 < N; ++b1) s += Bt[t1 * N + b1] * col[b1];
-                Tn[t1 * M + t0] = s;
-            }
+                for (int b0 = 0; b0 < N; ++b0) so[b1][b0] = own[slice_index<N>(f, b0, b1)];
+            interp2d<N, M>(Bt, so, sW + e * W + (f * 5 + v) * FS);
+            interp2d<N, M>(Bt, sn, sW + e * W + 30 * FS + (f * 5 + v) * FS);
         }
         __syncthreads();
 
@@ -231,19 +255,23 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
             const int2 c = a.conn[ge * 6 + f];
             const int fn = c.y & 7, isL = (c.y >> 3) & 1, code = c.y >> 4;
             const int cn = a.cmap[code * NF + cidx];
-            double* Tr = sW + e * W + f * 5 * NF;
-            const double* Tn = sW + e * W + 30 * NF + f * 5 * NF;
+            double* Tr = sW + e * W + f * 5 * FS;
+            const double* Tn = sW + e * W + 30 * FS + f * 5 * FS;
             double Uo[5], Un[5], F[5];
 #pragma unroll
             for (int v = 0; v < 5; ++v) {
-                Uo[v] = Tr[v * NF + cidx];
-                Un[v] = Tn[v * NF + cn];
+                Uo[v] = Tr[v * FS + cidx];
+                Un[v] = Tn[v * FS + cn];
             }
             const GeoDev* g = a.geo + (isL ? a.geo_class[ge] : a.geo_class[c.x]);
             const int fl = isL ? f : fn;
             const double Nv[3] = {g->N[fl][0], g->N[fl][1], g->N[fl][2]};
-            const double* UL = isL ? Uo : Un;
-            const double* UR = isL ? Un : Uo;
+            double UL[5], UR[5];  // selected element-wise so that both stay in registers
+#pragma unroll
+            for (int v = 0; v < 5; ++v) {
+                UL[v] = isL ? Uo[v] : Un[v];
+                UR[v] = isL ? Un[v] : Uo[v];
+            }
             if (a.flux == 1) {
                 if (!dgp::flux_hllc(gamma, UL, UR, Nv, F)) status |= kStatusHLLC;
             } else {
@@ -252,48 +280,41 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
             const double w = Wt[cidx % M] * Wt[cidx / M];
             const double sgn = isL ? -1.0 : 1.0;
 #pragma unroll
-            for (int v = 0; v < 5; ++v) Tr[v * NF + cidx] = sgn * (F[v] * w);
+            for (int v = 0; v < 5; ++v) Tr[v * FS + cidx] = sgn * (F[v] * w);
         }
         __syncthreads();
 
-        // ---- face lift: [t1][t0] -> [t1][b0] -> [b1][b0] ----
-        for (int i = tid; i < E * 30 * M; i += NT) {
-            const int t1 = i % M, v = (i / M) % 5, f = (i / (5 * M)) % 6, e = i / (30 * M);
-            const double* Fq = sW + e * W + (f * 5 + v) * NF + t1 * M;
-            double row[M];
+        // ---- face lift per (element, face, variable) into Tn's space ----
+        for (int t = tid; t < E * 30; t += NT) {
+            const int v = t % 5, f = (t / 5) % 6, e = t / 30;
+            const double* Fq = sW + e * W + (f * 5 + v) * FS;
+            double tmp[M][N];
 #pragma unroll
-            for (int t0 = 0; t0 < M; ++t0) row[t0] = Fq[t0];
-            double* T1 = sW + e * W + 60 * NF + ((f * 5 + v) * M + t1) * N;
+            for (int t1 = 0; t1 < M; ++t1)
 #pragma unroll
-            for (int b0 = 0; b0 < N; ++b0) {
-                double s = 0.0;
+                for (int b0 = 0; b0 < N; ++b0) {
+                    double s = 0.0;
 #pragma unroll
-                for (int t0 = 0; t0 < M; ++t0) s += Bt[t0 * N + b0] * row[t0];
-                T1[b0] = s;
-            }
-        }
-        __syncthreads();
-        for (int i = tid; i < E * 30 * N; i += NT) {
-            const int b0 = i % N, v = (i / N) % 5, f = (i / (5 * N)) % 6, e = i / (30 * N);
-            const double* T1 = sW + e * W + 60 * NF + (f * 5 + v) * M * N;
-            double col[M];
+                    for (int t0 = 0; t0 < M; ++t0) s += Bt[t0 * N + b0] * Fq[t1 * M + t0];
+                    tmp[t1][b0] = s;
+                }
+            double* Lf = sW + e * W + 30 * FS + (f * 5 + v) * FS;
 #pragma unroll
-            for (int t1 = 0; t1 < M; ++t1) col[t1] = T1[t1 * N + b0];
-            double* L = sW + e * W + 30 * NF + (f * 5 + v) * N2;
+            for (int b1 = 0; b1 < N; ++b1)
 #pragma unroll
-            for (int b1 = 0; b1 < N; ++b1) {
-                double s = 0.0;
+                for (int b0 = 0; b0 < N; ++b0) {
+                    double s = 0.0;
 #pragma unroll
-                for (int t1 = 0; t1 < M; ++t1) s += Bt[t1 * N + b1] * col[t1];
-                L[b1 * N + b0] = s;
-            }
+                    for (int t1 = 0; t1 < M; ++t1) s += Bt[t1 * N + b1] * tmp[t1][b0];
+                    Lf[b1 * N + b0] = s;
+                }
         }
         __syncthreads();
         // gather the six face contributions into the residual
         for (int i = tid; i < E * 5 * NB; i += NT) {
             const int b = i % NB, v = (i / NB) % 5, e = i / (5 * NB);
             const int bc[3] = {b % N, (b / N) % N, b / N2};
-            const double* L = sW + e * W + 30 * NF + v * N2;
+            const double* Lf = sW + e * W + 30 * FS + v * FS;
             double s = 0.0;
 #pragma unroll
             for (int f = 0; f < 6; ++f) {
@@ -301,23 +322,23 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
                 if (bc[ax] == sidx) {
                     const int b0 = ax == 0 ? bc[1] : bc[0];
                     const int b1 = ax == 2 ? bc[1] : bc[2];
-                    s += L[f * 5 * N2 + b1 * N + b0];
+                    s += Lf[f * 5 * FS + b1 * N + b0];
                 }
             }
-            sRes[i] = s;
+            sRes[e * ES + v * VS + b] = s;
         }
         __syncthreads();
 
         // ---- volume: interpolation passes x, y ----
-        double* X2 = sW;                     // per element: [5][N][M][M]
-        double* X1 = sW + Work<P>::x2;       // per element: [5][N][N][M]
+        double* X2 = sW;               // per element: [5][X2S] with [bz][qy][qx]
+        double* X1 = sW + 5 * X2S;     // per element: [5][X1S] with [bz][by][qx]
         for (int i = tid; i < E * 5 * N2; i += NT) {
-            const int byz = i % N2, v = (i / N2) % 5, e = i / (5 * N2);
-            const double* u = sU + (e * 5 + v) * NB + byz * N;
+            const int v = i % 5, byz = (i / 5) % N2, e = i / (5 * N2);
+            const double* u = sU + e * ES + v * VS + byz * N;
             double row[N];
 #pragma unroll
             for (int bx = 0; bx < N; ++bx) row[bx] = u[bx];
-            double* o = X1 + e * W + (v * N2 + byz) * M;
+            double* o = X1 + e * W + v * X1S + byz * M;
 #pragma unroll
             for (int qx = 0; qx < M; ++qx) {
                 double s = 0.0;
@@ -328,108 +349,100 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
         }
         __syncthreads();
         for (int i = tid; i < E * 5 * N * M; i += NT) {
-            const int qx = i % M, bz = (i / M) % N, v = (i / (M * N)) % 5, e = i / (5 * N * M);
-            const double* x1 = X1 + e * W + (v * N + bz) * N * M;
+            const int v = i % 5, r = i / 5;
+            const int qx = r % M, bz = (r / M) % N, e = r / (M * N);
+            const double* x1 = X1 + e * W + v * X1S + bz * N * M + qx;
             double col[N];
 #pragma unroll
-            for (int by = 0; by < N; ++by) col[by] = x1[by * M + qx];
-            double* o = X2 + e * W + (v * N + bz) * NF;
+            for (int by = 0; by < N; ++by) col[by] = x1[by * M];
+            double* o = X2 + e * W + v * X2S + bz * NF + qx;
 #pragma unroll
             for (int qy = 0; qy < M; ++qy) {
                 double s = 0.0;
 #pragma unroll
                 for (int by = 0; by < N; ++by) s += Bt[qy * N + by] * col[by];
-                o[qy * M + qx] = s;
+                o[qy * M] = s;
             }
         }
         __syncthreads();
 
-        // ---- fused: z interpolation, Euler flux, contravariant transform,
+        // ---- fused: z interpolation, Euler flux, contravariant transform and
         //      first (z) divergence contraction; then y and x contractions ----
 #pragma unroll
-        for (int g = 0; g < Groups<P>::count; ++g) {
-            constexpr int GMAX = Groups<P>::max_size;
-            const int gv0 = Groups<P>::first(g), gnv = Groups<P>::size(g);
-            // A: [nv][3][N][M][M] over X1 ; C: [nv][2][N][N][M] after it
-            double* Abuf = sW + Work<P>::x2;
-            double* Cbuf = Abuf + GMAX * 3 * N * NF;
-            for (int i0 = 0; i0 < E * NF; i0 += NT) {
-                const int i = i0 + tid;
-                const bool active = i < E * NF;
-                const int e = active ? i / NF : 0, qxy = active ? i % NF : 0;
+        for (int g = 0; g < G; ++g) {
+            const int gv0 = group_first<P, G>(g), gnv = group_size<P, G>(g);
+            double* Abuf = sW + 5 * X2S;            // [GV][3][X2S] over X1
+            double* Cbuf = Abuf + GV * 3 * X2S;     // [GV][2][X1S]
+            for (int i = tid; i < E * NF; i += NT) {
+                const int e = i / NF, qxy = i % NF;
                 const int qx = qxy % M, qy = qxy / M;
                 double xz[5][N];
-                if (active) {
 #pragma unroll
-                    for (int v = 0; v < 5; ++v)
+                for (int v = 0; v < 5; ++v)
 #pragma unroll
-                        for (int bz = 0; bz < N; ++bz) xz[v][bz] = X2[e * W + (v * N + bz) * NF + qxy];
-                }
-                if (active) {
-                    const int ge = min(e0 + e, a.ne - 1);
-                    const GeoDev* geo = a.geo + a.geo_class[ge];
-                    double JD[9];
+                    for (int bz = 0; bz < N; ++bz) xz[v][bz] = X2[e * W + v * X2S + bz * NF + qxy];
+                const int ge = min(e0 + e, a.ne - 1);
+                const GeoDev* geo = a.geo + a.geo_class[ge];
+                double JD[9];
 #pragma unroll
-                    for (int k = 0; k < 9; ++k) JD[k] = geo->JD[k];
-                    double acc[GMAX][3][N];
+                for (int k = 0; k < 9; ++k) JD[k] = geo->JD[k];
+                double acc[GV][3][N];
 #pragma unroll
-                    for (int v = 0; v < GMAX; ++v)
+                for (int v = 0; v < GV; ++v)
 #pragma unroll
-                        for (int d = 0; d < 3; ++d)
+                    for (int d = 0; d < 3; ++d)
 #pragma unroll
-                            for (int bz = 0; bz < N; ++bz) acc[v][d][bz] = 0.0;
-                    const double wxy = Wt[qx] * Wt[qy];
+                        for (int bz = 0; bz < N; ++bz) acc[v][d][bz] = 0.0;
+                const double wxy = Wt[qx] * Wt[qy];
 #pragma unroll
-                    for (int qz = 0; qz < M; ++qz) {
-                        double U[5];
+                for (int qz = 0; qz < M; ++qz) {
+                    double U[5];
 #pragma unroll
-                        for (int v = 0; v < 5; ++v) {
-                            double s = 0.0;
+                    for (int v = 0; v < 5; ++v) {
+                        double s = 0.0;
 #pragma unroll
-                            for (int bz = 0; bz < N; ++bz) s += Bt[qz * N + bz] * xz[v][bz];
-                            U[v] = s;
-                        }
-                        if (g == 0) {
-                            const double p = dgp::pressure(gamma, U);
-                            if (!(U[0] > 0.0)) status |= kStatusRho;
-                            if (!(p > 0.0)) status |= kStatusPressure;
-                            if (U[0] != U[0] || p != p) status |= kStatusNaN;
-                        }
-                        double F[15];
-                        dgp::interior_flux(gamma, U, F);
-                        const double wq = wxy * Wt[qz];
+                        for (int bz = 0; bz < N; ++bz) s += Bt[qz * N + bz] * xz[v][bz];
+                        U[v] = s;
+                    }
+                    if (g == 0) {
+                        const double p = dgp::pressure(gamma, U);
+                        if (!(U[0] > 0.0)) status |= kStatusRho;
+                        if (!(p > 0.0)) status |= kStatusPressure;
+                        if (U[0] != U[0] || p != p) status |= kStatusNaN;
+                    }
+                    double F[15];
+                    dgp::interior_flux(gamma, U, F);
+                    const double wq = wxy * Wt[qz];
 #pragma unroll
-                        for (int vv = 0; vv < GMAX; ++vv) {
-                            if (vv < gnv) {
-                                const int v = gv0 + vv;
+                    for (int vv = 0; vv < GV; ++vv) {
+                        if (vv < gnv) {
+                            const int v = gv0 + vv;
 #pragma unroll
-                                for (int d = 0; d < 3; ++d) {
-                                    const double G = (F[v] * JD[d * 3 + 0] + F[5 + v] * JD[d * 3 + 1] +
-                                                      F[10 + v] * JD[d * 3 + 2]) * wq;
+                            for (int d = 0; d < 3; ++d) {
+                                const double Gd =
+                                    (F[v] * JD[d * 3 + 0] + F[5 + v] * JD[d * 3 + 1] + F[10 + v] * JD[d * 3 + 2]) * wq;
 #pragma unroll
-                                    for (int bz = 0; bz < N; ++bz)
-                                        acc[vv][d][bz] += (d == 2 ? Dt[qz * N + bz] : Bt[qz * N + bz]) * G;
-                                }
+                                for (int bz = 0; bz < N; ++bz)
+                                    acc[vv][d][bz] += (d == 2 ? Dt[qz * N + bz] : Bt[qz * N + bz]) * Gd;
                             }
                         }
                     }
-#pragma unroll
-                    for (int vv = 0; vv < GMAX; ++vv)
-                        if (vv < gnv)
-#pragma unroll
-                            for (int d = 0; d < 3; ++d)
-#pragma unroll
-                                for (int bz = 0; bz < N; ++bz)
-                                    Abuf[e * W + ((vv * 3 + d) * N + bz) * NF + qxy] = acc[vv][d][bz];
                 }
+#pragma unroll
+                for (int vv = 0; vv < GV; ++vv)
+                    if (vv < gnv)
+#pragma unroll
+                        for (int d = 0; d < 3; ++d)
+#pragma unroll
+                            for (int bz = 0; bz < N; ++bz) Abuf[e * W + (vv * 3 + d) * X2S + bz * NF + qxy] = acc[vv][d][bz];
             }
             __syncthreads();
             // y contraction: C0 = By^T A0 ; C12 = Dy^T A1 + By^T A2
             for (int i = tid; i < E * gnv * N * M; i += NT) {
                 const int qx = i % M, bz = (i / M) % N, vv = (i / (M * N)) % gnv, e = i / (gnv * N * M);
-                const double* A0 = Abuf + e * W + ((vv * 3 + 0) * N + bz) * NF + qx;
-                const double* A1 = Abuf + e * W + ((vv * 3 + 1) * N + bz) * NF + qx;
-                const double* A2 = Abuf + e * W + ((vv * 3 + 2) * N + bz) * NF + qx;
+                const double* A0 = Abuf + e * W + (vv * 3 + 0) * X2S + bz * NF + qx;
+                const double* A1 = A0 + X2S;
+                const double* A2 = A1 + X2S;
                 double c0[N], c12[N];
 #pragma unroll
                 for (int by = 0; by < N; ++by) { c0[by] = 0.0; c12[by] = 0.0; }
@@ -442,20 +455,19 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
                         c12[by] += Dt[qy * N + by] * a1 + Bt[qy * N + by] * a2;
                     }
                 }
-                double* C = Cbuf + e * W + ((vv * 2) * N + bz) * N * M + qx;
+                double* C0 = Cbuf + e * W + (vv * 2) * X1S + bz * N * M + qx;
 #pragma unroll
                 for (int by = 0; by < N; ++by) {
-                    C[by * M] = c0[by];
-                    C[N * N * M + by * M] = c12[by];
+                    C0[by * M] = c0[by];
+                    C0[X1S + by * M] = c12[by];
                 }
             }
             __syncthreads();
             // x contraction into the residual: res += Dx^T C0 + Bx^T C12
             for (int i = tid; i < E * gnv * N2; i += NT) {
-                const int byz = i % N2, vv = (i / N2) % gnv, e = i / (gnv * N2);
-                const int bz = byz / N, by = byz % N;
-                const double* C0 = Cbuf + e * W + ((vv * 2) * N + bz) * N * M + by * M;
-                const double* C12 = C0 + N * N * M;
+                const int vv = i % gnv, byz = (i / gnv) % N2, e = i / (gnv * N2);
+                const double* C0 = Cbuf + e * W + (vv * 2) * X1S + byz * M;
+                const double* C12 = C0 + X1S;
                 double r[N];
 #pragma unroll
                 for (int bx = 0; bx < N; ++bx) r[bx] = 0.0;
@@ -465,7 +477,7 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
 #pragma unroll
                     for (int bx = 0; bx < N; ++bx) r[bx] += Dt[qx * N + bx] * c0 + Bt[qx * N + bx] * c12;
                 }
-                double* res = sRes + (e * 5 + gv0 + vv) * NB + byz * N;
+                double* res = sRes + e * ES + (gv0 + vv) * VS + byz * N;
 #pragma unroll
                 for (int bx = 0; bx < N; ++bx) res[bx] += r[bx];
             }
@@ -474,16 +486,16 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
 
         if (a.mode == kModeResidual) {
             for (int i = tid; i < E * 5 * NB; i += NT) {
-                const int e = i / (5 * NB);
-                if (e0 + e < a.ne) a.out[(size_t)e0 * 5 * NB + i] = sRes[i];
+                const int e = i / (5 * NB), r = i - e * (5 * NB), v = r / NB, b = r - v * NB;
+                if (e0 + e < a.ne) a.out[(size_t)e0 * 5 * NB + i] = sRes[e * ES + v * VS + b];
             }
-            __syncthreads();
             continue;
         }
 
         // ---- inverse mass: x and y passes in place, z pass fused with the update ----
         for (int i = tid; i < E * 5 * N2; i += NT) {
-            double* r = sRes + i * N;  // pencil along x
+            const int v = i % 5, byz = (i / 5) % N2, e = i / (5 * N2);
+            double* r = sRes + e * ES + v * VS + byz * N;  // pencil along x
             double t[N];
 #pragma unroll
             for (int k = 0; k < N; ++k) t[k] = r[k];
@@ -498,7 +510,7 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
         __syncthreads();
         for (int i = tid; i < E * 5 * N2; i += NT) {
             const int bx = i % N, bz = (i / N) % N, ev = i / N2;
-            double* r = sRes + ev * NB + bz * N2 + bx;  // pencil along y
+            double* r = sRes + (ev / 5) * ES + (ev % 5) * VS + bz * N2 + bx;  // pencil along y
             double t[N];
 #pragma unroll
             for (int k = 0; k < N; ++k) t[k] = r[k * N];
@@ -510,13 +522,19 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
                 r[j * N] = s;
             }
         }
+        cp_async_wait_older();  // this batch's U0 / accumulator have landed
         __syncthreads();
         for (int i = tid; i < E * 5 * N2; i += NT) {
             const int bxy = i % N2, ev = i / N2, e = ev / 5;
             if (e0 + e >= a.ne) continue;
             const int ge = e0 + e;
             const double scale = a.dt * a.geo[a.geo_class[ge]].inv_djac;
-            const double* r = sRes + ev * NB + bxy;  // pencil along z
+            const int soff = e * ES + (ev % 5) * VS + bxy;
+            const double* r = sRes + soff;  // pencil along z
+            // step-start state: the prefetched U0, or the stage state itself in
+            // RK1 / FE where the two coincide
+            const double* u0 = (need_u0_acc ? sU0 : sU) + soff;
+            const double* ac = sAcc + soff;
             double t[N];
 #pragma unroll
             for (int k = 0; k < N; ++k) t[k] = r[k * N2];
@@ -530,23 +548,56 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
                 const size_t gi = gbase + (size_t)j * N2;
                 switch (a.mode) {
                     case kModeMassInv: a.out[gi] = kk; break;
-                    case kModeRK1: a.acc[gi] = kk; a.out[gi] = 0.5 * kk + a.U0[gi]; break;
-                    case kModeRK2: a.acc[gi] = a.acc[gi] + 2.0 * kk; a.out[gi] = 0.5 * kk + a.U0[gi]; break;
-                    case kModeRK3: a.acc[gi] = a.acc[gi] + 2.0 * kk; a.out[gi] = 1.0 * kk + a.U0[gi]; break;
-                    case kModeRK4: a.out[gi] = a.U0[gi] + (1.0 / 6.0) * (a.acc[gi] + kk); break;
-                    default: a.out[gi] = a.U0[gi] + 1.0 * kk; break;
+                    case kModeRK1: a.acc[gi] = kk; a.out[gi] = 0.5 * kk + u0[j * N2]; break;
+                    case kModeRK2: a.acc[gi] = ac[j * N2] + 2.0 * kk; a.out[gi] = 0.5 * kk + u0[j * N2]; break;
+                    case kModeRK3: a.acc[gi] = ac[j * N2] + 2.0 * kk; a.out[gi] = 1.0 * kk + u0[j * N2]; break;
+                    case kModeRK4: a.out[gi] = u0[j * N2] + (1.0 / 6.0) * (ac[j * N2] + kk); break;
+                    default: a.out[gi] = u0[j * N2] + 1.0 * kk; break;
                 }
             }
         }
-        __syncthreads();
     }
+    cp_async_wait_all();
     if (status) atomicOr(a.status, status);
 }
 
-template <int P, int E>
+template <int P, int E, int G>
 constexpr size_t stage_smem_bytes()
 {
-    return sizeof(double) * (size_t)E * (10 * Dim<P>::NB + Work<P>::per_elem);
+    return sizeof(double) * (size_t)E * Lay<P, G>::per_elem;
 }
+
+// ---- compiled launch variants (one translation unit per order) ----
+
+struct StageVariant {
+    int E, NT, G;        // elements per CTA, threads per CTA, variable groups
+    size_t smem;         // dynamic shared memory per CTA
+    const void* func;    // the kernel, for attributes / occupancy queries
+    cudaError_t (*launch)(const StageArgs&, int grid, cudaStream_t);
+};
+
+template <int P, int E, int NT, int G>
+cudaError_t launch_stage_variant(const StageArgs& a, int grid, cudaStream_t s)
+{
+    stage_kernel<P, E, NT, G><<<grid, NT, stage_smem_bytes<P, E, G>(), s>>>(a);
+    return cudaGetLastError();
+}
+
+template <int P, int E, int NT, int G>
+constexpr StageVariant make_variant()
+{
+    static_assert(stage_smem_bytes<P, E, G>() <= 227 * 1024, "stage kernel shared memory exceeds 227 KB");
+    return StageVariant{E, NT, G, stage_smem_bytes<P, E, G>(), (const void*)stage_kernel<P, E, NT, G>,
+                        launch_stage_variant<P, E, NT, G>};
+}
+
+// the variants compiled for order p (defined in dg_stage_p<p>.cu)
+int stage_variants(int p, const StageVariant** out);
+int stage_variants_p0(const StageVariant** out);
+int stage_variants_p1(const StageVariant** out);
+int stage_variants_p2(const StageVariant** out);
+int stage_variants_p3(const StageVariant** out);
+int stage_variants_p4(const StageVariant** out);
+int stage_variants_p5(const StageVariant** out);
 
 }  // namespace dgk

@@ -1,0 +1,21 @@
+// dg_stage_p1.cu -- compiled launch variants of the stage kernel for order p = 1
+// (elements per CTA, threads per CTA, variable groups); the first entry is
+// the default, the tuner (dg_tune_stage) may pick another.
+#include "dg_stage.cuh"
+
+namespace dgk {
+
+static const StageVariant kVariants1[] = {
+    make_variant<1, 8, 128, 1>(),
+    make_variant<1, 1, 32, 1>(),
+    make_variant<1, 2, 64, 1>(),
+    make_variant<1, 4, 64, 1>(),
+};
+
+int stage_variants_p1(const StageVariant** out)
+{
+    *out = kVariants1;
+    return static_cast<int>(sizeof(kVariants1) / sizeof(kVariants1[0]));
+}
+
+}  // namespace dgk

@@ -1,0 +1,21 @@
+// dg_stage_p2.cu -- compiled launch variants of the stage kernel for order p = 2
+// (elements per CTA, threads per CTA, variable groups); the first entry is
+// the default, the tuner (dg_tune_stage) may pick another.
+#include "dg_stage.cuh"
+
+namespace dgk {
+
+static const StageVariant kVariants2[] = {
+    make_variant<2, 6, 96, 1>(),
+    make_variant<2, 1, 32, 1>(),
+    make_variant<2, 2, 64, 1>(),
+    make_variant<2, 1, 32, 2>(),
+};
+
+int stage_variants_p2(const StageVariant** out)
+{
+    *out = kVariants2;
+    return static_cast<int>(sizeof(kVariants2) / sizeof(kVariants2[0]));
+}
+
+}  // namespace dgk

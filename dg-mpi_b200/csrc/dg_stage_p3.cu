@@ -1,0 +1,22 @@
+// dg_stage_p3.cu -- compiled launch variants of the stage kernel for order p = 3
+// (elements per CTA, threads per CTA, variable groups); the first entry is
+// the default, the tuner (dg_tune_stage) may pick another.
+#include "dg_stage.cuh"
+
+namespace dgk {
+
+static const StageVariant kVariants3[] = {
+    make_variant<3, 1, 32, 2>(),
+    make_variant<3, 3, 96, 2>(),
+    make_variant<3, 1, 32, 1>(),
+    make_variant<3, 2, 64, 2>(),
+    make_variant<3, 1, 64, 2>(),
+};
+
+int stage_variants_p3(const StageVariant** out)
+{
+    *out = kVariants3;
+    return static_cast<int>(sizeof(kVariants3) / sizeof(kVariants3[0]));
+}
+
+}  // namespace dgk

@@ -1,0 +1,21 @@
+// dg_stage_p4.cu -- compiled launch variants of the stage kernel for order p = 4
+// (elements per CTA, threads per CTA, variable groups); the first entry is
+// the default, the tuner (dg_tune_stage) may pick another.
+#include "dg_stage.cuh"
+
+namespace dgk {
+
+static const StageVariant kVariants4[] = {
+    make_variant<4, 1, 32, 2>(),
+    make_variant<4, 2, 96, 2>(),
+    make_variant<4, 1, 64, 2>(),
+    make_variant<4, 1, 32, 3>(),
+};
+
+int stage_variants_p4(const StageVariant** out)
+{
+    *out = kVariants4;
+    return static_cast<int>(sizeof(kVariants4) / sizeof(kVariants4[0]));
+}
+
+}  // namespace dgk

@@ -89,6 +89,11 @@ def library(path: str | None = None) -> ctypes.CDLL:
         "dg_gauss_legendre": (ctypes.c_int, [ctypes.c_int, dp, dp]),
         "dg_face_orientation_order": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ip]),
         "dg_basis_tables": (ctypes.c_int, [ctypes.c_int, dp, dp, dp]),
+        "dg_num_stage_variants": (ctypes.c_int, [ctypes.c_int]),
+        "dg_stage_variant_info": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ip, ip, ip]),
+        "dg_set_stage_variant": (ctypes.c_int, [vp, ctypes.c_int]),
+        "dg_get_stage_variant": (ctypes.c_int, [vp]),
+        "dg_tune_stage": (ctypes.c_int, [vp, ctypes.c_int, ip, dp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -271,6 +276,33 @@ class Case:
 
     def device_state_ptr(self) -> int:
         return int(self._lib.dg_device_state(self._ctx) or 0)
+
+    # -- launch variants ---------------------------------------------------
+    def stage_variants(self):
+        """[(elements per CTA, threads per CTA, variable groups)] compiled for this order."""
+        out = []
+        for v in range(self._lib.dg_num_stage_variants(self.order)):
+            E, NT, G = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+            self._lib.dg_stage_variant_info(self.order, v, ctypes.byref(E), ctypes.byref(NT), ctypes.byref(G))
+            out.append((E.value, NT.value, G.value))
+        return out
+
+    @property
+    def stage_variant(self) -> int:
+        return self._lib.dg_get_stage_variant(self._ctx)
+
+    @stage_variant.setter
+    def stage_variant(self, v: int):
+        self._check(self._lib.dg_set_stage_variant(self._ctx, int(v)))
+
+    def tune_stage(self, reps: int = 3):
+        """Times every variant on this case (state unchanged), selects the fastest.
+        Returns (best index, [ms per stage launch for each variant])."""
+        n = self._lib.dg_num_stage_variants(self.order)
+        ms = np.zeros(n, np.float64)
+        best = ctypes.c_int()
+        self._check(self._lib.dg_tune_stage(self._ctx, int(reps), ctypes.byref(best), _dptr(ms)))
+        return best.value, ms.tolist()
 
 
 def gauss_legendre(n: int):

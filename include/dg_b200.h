@@ -136,6 +136,18 @@ int dg_rk4_steps(dg_ctx* ctx, double dt, int nsteps);
  * device clock). */
 int dg_rk4_steps_timed(dg_ctx* ctx, double dt, int nsteps, double* device_ms);
 
+/* ---- stage-kernel launch variants and their tuner ----
+ * Each order has a few compiled variants of the fused stage kernel (elements
+ * per CTA, threads per CTA, variable groups of the pointwise phase).  The
+ * tuner times one stage of every variant on the context's mesh and current
+ * state (the state is not modified) and selects the fastest; callers cache
+ * the result per (order, GPU) and restore it with dg_set_stage_variant. */
+int dg_num_stage_variants(int order);
+int dg_stage_variant_info(int order, int variant, int* elems_per_cta, int* threads_per_cta, int* groups);
+int dg_set_stage_variant(dg_ctx* ctx, int variant);
+int dg_get_stage_variant(const dg_ctx* ctx);
+int dg_tune_stage(dg_ctx* ctx, int reps, int* best_variant, double* ms_per_variant);
+
 /* Forward Euler, replaces FE<3>::take_time_step (stepper.cpp:23-55). */
 int dg_fe_steps(dg_ctx* ctx, double dt, int nsteps);
 
