@@ -35,7 +35,7 @@ int dgk::stage_variants(int p, const StageVariant** out)
 
 namespace {
 
-constexpr int kMaxVariants = 8;
+constexpr int kMaxVariants = 16;  // launch variants per order (checked in prepare_variant)
 
 // tables of the IC / error rule (2*max(p,1)+2 points) and of the volume rule,
 // used by the reductions
@@ -129,13 +129,20 @@ int load_constant_tables(dg_ctx* c)
 // ---------------------------------------------------------------------------
 // stage launches
 
+bool variant_matches(const dg_ctx* c, int v)
+{
+    const dgk::StageVariant* vs = nullptr;
+    const int nv = dgk::stage_variants(c->p, &vs);
+    return v >= 0 && v < nv && (vs[v].fp32 != 0) == (c->precision == DG_PREC_MIXED_FP32);
+}
+
 // Sets the variant's shared-memory attribute and its persistent grid size
 // (SM count x resident CTAs per SM, capped by the number of batches).
 int prepare_variant(dg_ctx* c, int v)
 {
     const dgk::StageVariant* vs = nullptr;
     const int nv = dgk::stage_variants(c->p, &vs);
-    if (v < 0 || v >= nv) return fail(c, DG_ERR_ARG, "stage variant index out of range");
+    if (v < 0 || v >= nv || v >= kMaxVariants) return fail(c, DG_ERR_ARG, "stage variant index out of range");
     if (c->variant_grid[v] > 0) return DG_OK;
     const dgk::StageVariant& sv = vs[v];
     DG_CUDA(c, cudaFuncSetAttribute(sv.func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sv.smem));
@@ -466,8 +473,8 @@ int dg_create(const dg_case_desc* cd, const dg_mesh_desc* md, dg_ctx** out)
     if (cd->order < 0 || cd->order > dgk::kMaxP) return fail(nullptr, DG_ERR_UNSUPPORTED, "order must be 0..5");
     if (cd->flux != DG_FLUX_LAX_FRIEDRICHS && cd->flux != DG_FLUX_HLLC) return fail(nullptr, DG_ERR_ARG, "unknown flux");
     if (!(cd->gamma > 1.0)) return fail(nullptr, DG_ERR_ARG, "gamma must exceed 1");
-    if (cd->precision != DG_PREC_FP64)
-        return fail(nullptr, DG_ERR_UNSUPPORTED, "only the FP64 residual is built into this library");
+    if (cd->precision != DG_PREC_FP64 && cd->precision != DG_PREC_MIXED_FP32)
+        return fail(nullptr, DG_ERR_ARG, "unknown precision mode");
 
     dg_ctx* c = new (std::nothrow) dg_ctx();
     if (!c) return fail(nullptr, DG_ERR_NOMEM, "host allocation failed");
@@ -504,6 +511,20 @@ int dg_create(const dg_case_desc* cd, const dg_mesh_desc* md, dg_ctx** out)
     std::copy(c->tab.D.begin(), c->tab.D.end(), c->stage_tab.D);
     std::copy(c->tab.wq.begin(), c->tab.wq.end(), c->stage_tab.W);
     std::copy(c->tab.Minv.begin(), c->tab.Minv.end(), c->stage_tab.Minv);
+    for (size_t i = 0; i < c->tab.B.size(); ++i) c->stage_tab.Bf[i] = static_cast<float>(c->tab.B[i]);
+    for (size_t i = 0; i < c->tab.D.size(); ++i) c->stage_tab.Df[i] = static_cast<float>(c->tab.D[i]);
+    for (size_t i = 0; i < c->tab.wq.size(); ++i) c->stage_tab.Wf[i] = static_cast<float>(c->tab.wq[i]);
+    {   // default launch variant: the first one compiled for the requested precision
+        const dgk::StageVariant* vs = nullptr;
+        const int nv = dgk::stage_variants(c->p, &vs);
+        c->variant = -1;
+        for (int v = 0; v < nv && c->variant < 0; ++v)
+            if ((vs[v].fp32 != 0) == (c->precision == DG_PREC_MIXED_FP32)) c->variant = v;
+        if (c->variant < 0) {
+            delete c;
+            return fail(nullptr, DG_ERR_UNSUPPORTED, "no stage kernel compiled for this order and precision");
+        }
+    }
 
     // the mesh is valid; now the device
     int ndev = 0;
@@ -695,7 +716,7 @@ int dg_num_stage_variants(int order)
     return dgk::stage_variants(order, &vs);
 }
 
-int dg_stage_variant_info(int order, int v, int* elems_per_cta, int* threads_per_cta, int* groups)
+int dg_stage_variant_info(int order, int v, int* elems_per_cta, int* threads_per_cta, int* groups, int* precision)
 {
     const dgk::StageVariant* vs = nullptr;
     const int nv = dgk::stage_variants(order, &vs);
@@ -703,6 +724,7 @@ int dg_stage_variant_info(int order, int v, int* elems_per_cta, int* threads_per
     if (elems_per_cta) *elems_per_cta = vs[v].E;
     if (threads_per_cta) *threads_per_cta = vs[v].NT;
     if (groups) *groups = vs[v].G;
+    if (precision) *precision = vs[v].fp32 ? DG_PREC_MIXED_FP32 : DG_PREC_FP64;
     return DG_OK;
 }
 
@@ -710,6 +732,7 @@ int dg_set_stage_variant(dg_ctx* c, int v)
 {
     if (!c) return DG_ERR_ARG;
     if (v < 0 || v >= dg_num_stage_variants(c->p)) return fail(c, DG_ERR_ARG, "stage variant index out of range");
+    if (!variant_matches(c, v)) return fail(c, DG_ERR_ARG, "stage variant has the other residual precision");
     if (v != c->variant) {
         c->variant = v;
         if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }
@@ -733,6 +756,10 @@ int dg_tune_stage(dg_ctx* c, int reps, int* best, double* ms_per_variant)
     if (cudaEventCreate(&ev[1]) != cudaSuccess) { cudaEventDestroy(ev[0]); return fail(c, DG_ERR_CUDA, "cudaEventCreate"); }
     int rc = DG_OK;
     for (int v = 0; v < nv && rc == DG_OK; ++v) {
+        if (!variant_matches(c, v)) {
+            if (ms_per_variant) ms_per_variant[v] = -1.0;
+            continue;
+        }
         c->variant = v;
         // one untimed launch, then `reps` timed ones; the mass-inverse mode
         // writes scratch output only, so the state is unchanged

@@ -4,6 +4,7 @@
 // order follows the reference's functions so that a face flux computed here
 // rounds like the reference's; citations are relative to the reference root.
 #pragma once
+#include <cmath>
 #include <math.h>
 
 #ifdef __CUDACC__
@@ -16,27 +17,35 @@ namespace dgp {
 
 constexpr double kPi = 3.14159265358979323846;
 
+// The flux functions are templates on the arithmetic type T: double on the
+// FP64 path (operation order identical to the reference's), float on the
+// mixed-precision path.  Literals are written as T(...) so that the float
+// instantiation stays in FP32.
+
 // EulerFcnType::get_pressure<3>, src/physics/euler/functions.cpp:10-23
-DG_HD double pressure(double gamma, const double* U)
+template <typename T>
+DG_HD T pressure(T gamma, const T* U)
 {
-    const double rKE = (U[1] * U[1] + U[2] * U[2] + U[3] * U[3]) / U[0];
-    return (gamma - 1.0) * (U[4] - 0.5 * rKE);
+    const T rKE = (U[1] * U[1] + U[2] * U[2] + U[3] * U[3]) / U[0];
+    return (gamma - T(1.0)) * (U[4] - T(0.5) * rKE);
 }
 
 // EulerFcnType::get_maxwavespeed<3>, functions.cpp:25-40
-DG_HD double max_wave_speed(double gamma, const double* U)
+template <typename T>
+DG_HD T max_wave_speed(T gamma, const T* U)
 {
-    const double rho1 = 1. / U[0];
-    const double sqrtrKE = sqrt(U[1] * U[1] + U[2] * U[2] + U[3] * U[3]) * rho1;
+    const T rho1 = T(1.) / U[0];
+    const T sqrtrKE = sqrt(U[1] * U[1] + U[2] * U[2] + U[3] * U[3]) * rho1;
     return sqrtrKE + sqrt(gamma * pressure(gamma, U) * rho1);
 }
 
 // EulerFcnType::conv_flux_interior<3>, functions.cpp:64-91; F[j*5+s]
-DG_HD void interior_flux(double gamma, const double* U, double* F)
+template <typename T>
+DG_HD void interior_flux(T gamma, const T* U, T* F)
 {
-    const double r1 = 1. / U[0];
-    const double ru = U[1], rv = U[2], rw = U[3], rE = U[4];
-    const double P = pressure(gamma, U);
+    const T r1 = T(1.) / U[0];
+    const T ru = U[1], rv = U[2], rw = U[3], rE = U[4];
+    const T P = pressure(gamma, U);
     F[0] = ru;
     F[1] = ru * ru * r1 + P;
     F[2] = ru * rv * r1;
@@ -57,79 +66,80 @@ DG_HD void interior_flux(double gamma, const double* U, double* F)
 // BaseConvNumFluxType::compute_flux_laxfriedrichs<3>, base/functions.cpp:33-89.
 // N is the unnormalised normal of the left element (its length carries the
 // surface Jacobian).
-DG_HD void flux_lax_friedrichs(double gamma, const double* UL, const double* UR, const double* N,
-                               double* F)
+template <typename T>
+DG_HD void flux_lax_friedrichs(T gamma, const T* UL, const T* UR, const T* N, T* F)
 {
-    double n_mag = 0.0;
+    T n_mag = T(0.0);
     for (int d = 0; d < 3; ++d) n_mag += N[d] * N[d];
     n_mag = sqrt(n_mag);
-    double n_hat[3];
+    T n_hat[3];
     for (int d = 0; d < 3; ++d) n_hat[d] = N[d] / n_mag;
-    double Fq[15], FqL[5] = {0, 0, 0, 0, 0}, FqR[5] = {0, 0, 0, 0, 0};
+    T Fq[15], FqL[5] = {T(0), T(0), T(0), T(0), T(0)}, FqR[5] = {T(0), T(0), T(0), T(0), T(0)};
     interior_flux(gamma, UL, Fq);
     for (int s = 0; s < 5; ++s)
         for (int d = 0; d < 3; ++d) FqL[s] += Fq[s + d * 5] * n_hat[d];
     interior_flux(gamma, UR, Fq);
     for (int s = 0; s < 5; ++s)
         for (int d = 0; d < 3; ++d) FqR[s] += Fq[s + d * 5] * n_hat[d];
-    double a = max_wave_speed(gamma, UL);
-    const double aR = max_wave_speed(gamma, UR);
+    T a = max_wave_speed(gamma, UL);
+    const T aR = max_wave_speed(gamma, UR);
     if (aR > a) a = aR;
-    for (int s = 0; s < 5; ++s) F[s] = n_mag * (0.5 * (FqL[s] + FqR[s]) - 0.5 * a * (UR[s] - UL[s]));
+    for (int s = 0; s < 5; ++s) F[s] = n_mag * (T(0.5) * (FqL[s] + FqR[s]) - T(0.5) * a * (UR[s] - UL[s]));
 }
 
 // EulerConvNumFluxType::compute_flux_hllc<3>, functions.cpp:298-399.
 // Returns false on the reference's assert branch (no valid wave ordering,
 // e.g. NaN input); F is zeroed then.
-DG_HD bool flux_hllc(double gam, const double* UL, const double* UR, const double* N, double* F)
+template <typename T>
+DG_HD bool flux_hllc(T gam, const T* UL, const T* UR, const T* N, T* F)
 {
-    const double djac = sqrt(N[0] * N[0] + N[1] * N[1] + N[2] * N[2]);
-    const double djac1 = 1. / djac;
-    const double n[3] = {N[0] * djac1, N[1] * djac1, N[2] * djac1};
-    const double rhoL = UL[0], rhoL1 = 1. / rhoL;
-    const double unL = (UL[1] * n[0] + UL[2] * n[1] + UL[3] * n[2]) * rhoL1;
-    const double PL = pressure(gam, UL);
-    const double aL = sqrt(gam * PL * rhoL1);
-    const double rhoR = UR[0], rhoR1 = 1. / rhoR;
-    const double unR = (UR[1] * n[0] + UR[2] * n[1] + UR[3] * n[2]) * rhoR1;
-    const double PR = pressure(gam, UR);
-    const double aR = sqrt(gam * PR * rhoR1);
-    const double rAvg = 0.5 * (rhoL + rhoR);
-    const double aAvg = 0.5 * (aL + aR);
-    const double pStar = fmax(0., 0.5 * (PL + PR - (unR - unL) * rAvg * aAvg));
-    double qL = 1.0, qR = 1.0;
-    if (pStar / PL > 1.) qL = sqrt(1. + (gam + 1.) / (2. * gam) * (pStar / PL - 1.));
-    if (pStar / PR > 1.) qR = sqrt(1. + (gam + 1.) / (2. * gam) * (pStar / PR - 1.));
-    const double sL = unL - aL * qL;
-    const double sR = unR + aR * qR;
-    const double sStar = (PR - PL + rhoL * unL * (sL - unL) - rhoR * unR * (sR - unR)) /
-                         (rhoL * (sL - unL) - rhoR * (sR - unR));
-    if (sL >= 0.) {
+    const T djac = sqrt(N[0] * N[0] + N[1] * N[1] + N[2] * N[2]);
+    const T djac1 = T(1.) / djac;
+    const T n[3] = {N[0] * djac1, N[1] * djac1, N[2] * djac1};
+    const T rhoL = UL[0], rhoL1 = T(1.) / rhoL;
+    const T unL = (UL[1] * n[0] + UL[2] * n[1] + UL[3] * n[2]) * rhoL1;
+    const T PL = pressure(gam, UL);
+    const T aL = sqrt(gam * PL * rhoL1);
+    const T rhoR = UR[0], rhoR1 = T(1.) / rhoR;
+    const T unR = (UR[1] * n[0] + UR[2] * n[1] + UR[3] * n[2]) * rhoR1;
+    const T PR = pressure(gam, UR);
+    const T aR = sqrt(gam * PR * rhoR1);
+    const T rAvg = T(0.5) * (rhoL + rhoR);
+    const T aAvg = T(0.5) * (aL + aR);
+    const T pStar = fmax(T(0.), T(0.5) * (PL + PR - (unR - unL) * rAvg * aAvg));
+    T qL = T(1.0), qR = T(1.0);
+    if (pStar / PL > T(1.)) qL = sqrt(T(1.) + (gam + T(1.)) / (T(2.) * gam) * (pStar / PL - T(1.)));
+    if (pStar / PR > T(1.)) qR = sqrt(T(1.) + (gam + T(1.)) / (T(2.) * gam) * (pStar / PR - T(1.)));
+    const T sL = unL - aL * qL;
+    const T sR = unR + aR * qR;
+    const T sStar = (PR - PL + rhoL * unL * (sL - unL) - rhoR * unR * (sR - unR)) /
+                    (rhoL * (sL - unL) - rhoR * (sR - unR));
+    if (sL >= T(0.)) {
         F[0] = djac * rhoL * unL;
         for (int i = 0; i < 3; ++i) F[1 + i] = djac * (UL[1 + i] * unL + PL * n[i]);
         F[4] = djac * ((UL[4] + PL) * unL);
-    } else if (sR <= 0.) {
+    } else if (sR <= T(0.)) {
         F[0] = djac * rhoR * unR;
         for (int i = 0; i < 3; ++i) F[1 + i] = djac * (UR[1 + i] * unR + PR * n[i]);
         F[4] = djac * (UR[4] + PR) * unR;
-    } else if ((sL < 0.) && (sStar >= 0.)) {
-        const double c = (sL - unL) / (sL - sStar);
-        const double f1 = sStar - unL;
-        const double f2 = sStar + PL / (rhoL * (sL - unL));
-        F[0] = djac * (rhoL * unL + rhoL * sL * (c - 1.));
+    } else if ((sL < T(0.)) && (sStar >= T(0.))) {
+        const T c = (sL - unL) / (sL - sStar);
+        const T f1 = sStar - unL;
+        const T f2 = sStar + PL / (rhoL * (sL - unL));
+        F[0] = djac * (rhoL * unL + rhoL * sL * (c - T(1.)));
         for (int i = 0; i < 3; ++i)
-            F[1 + i] = djac * (UL[1 + i] * unL + PL * n[i] + sL * (UL[1 + i] * (c - 1.) + rhoL * c * f1 * n[i]));
-        F[4] = djac * ((UL[4] + PL) * unL + sL * (UL[4] * (c - 1.) + rhoL * c * f1 * f2));
-    } else if ((sStar < 0.) && (sR > 0.)) {
-        const double c = (sR - unR) / (sR - sStar);
-        const double f1 = sStar - unR;
-        const double f2 = sStar + PR / (rhoR * (sR - unR));
-        F[0] = djac * (rhoR * unR + rhoR * sR * (c - 1.));
+            F[1 + i] = djac * (UL[1 + i] * unL + PL * n[i] + sL * (UL[1 + i] * (c - T(1.)) + rhoL * c * f1 * n[i]));
+        F[4] = djac * ((UL[4] + PL) * unL + sL * (UL[4] * (c - T(1.)) + rhoL * c * f1 * f2));
+    } else if ((sStar < T(0.)) && (sR > T(0.))) {
+        const T c = (sR - unR) / (sR - sStar);
+        const T f1 = sStar - unR;
+        const T f2 = sStar + PR / (rhoR * (sR - unR));
+        F[0] = djac * (rhoR * unR + rhoR * sR * (c - T(1.)));
         for (int i = 0; i < 3; ++i)
-            F[1 + i] = djac * (UR[1 + i] * unR + PR * n[i] + sR * (UR[1 + i] * (c - 1.) + rhoR * c * f1 * n[i]));
-        F[4] = djac * ((UR[4] + PR) * unR + sR * (UR[4] * (c - 1.) + rhoR * c * f1 * f2));
+            F[1 + i] = djac * (UR[1 + i] * unR + PR * n[i] + sR * (UR[1 + i] * (c - T(1.)) + rhoR * c * f1 * n[i]));
+        F[4] = djac * ((UR[4] + PR) * unR + sR * (UR[4] * (c - T(1.)) + rhoR * c * f1 * f2));
     } else {
-        for (int s = 0; s < 5; ++s) F[s] = 0.0;
+        for (int s = 0; s < 5; ++s) F[s] = T(0.0);
         return false;
     }
     return true;

@@ -1,4 +1,4 @@
-// dg_stage.cuh -- the fused DG stage kernel (sm_100a, FP64).
+// dg_stage.cuh -- the fused DG stage kernel (sm_100a; FP64, or FP32 residual with FP64 state).
 //
 // One launch evaluates, for batches of E elements per CTA (grid-stride):
 //   face traces of the element and of its six neighbours (2D sum-factorised
@@ -40,7 +40,22 @@ struct StageTables {
     double B[kTabB];                           // B[q*N + b]: basis at the GL points
     double D[kTabB];                           // D[q*N + b]: its derivative
     double W[kMaxP + 2];                       // GL weights
-    double Minv[(kMaxP + 1) * (kMaxP + 1)];    // inverse 1D mass matrix
+    double Minv[(kMaxP + 1) * (kMaxP + 1)];    // inverse 1D mass matrix (always FP64)
+    float Bf[kTabB];                           // FP32 copies for the mixed-precision residual
+    float Df[kTabB];
+    float Wf[kMaxP + 2];
+};
+
+template <typename T> struct TabSel;
+template <> struct TabSel<double> {
+    static __device__ __forceinline__ const double* B(const StageTables& t) { return t.B; }
+    static __device__ __forceinline__ const double* D(const StageTables& t) { return t.D; }
+    static __device__ __forceinline__ const double* W(const StageTables& t) { return t.W; }
+};
+template <> struct TabSel<float> {
+    static __device__ __forceinline__ const float* B(const StageTables& t) { return t.Bf; }
+    static __device__ __forceinline__ const float* D(const StageTables& t) { return t.Df; }
+    static __device__ __forceinline__ const float* W(const StageTables& t) { return t.Wf; }
 };
 
 struct GeoDev {
@@ -87,8 +102,10 @@ struct StageArgs {
 __host__ __device__ constexpr int odd(int x) { return x | 1; }
 __host__ __device__ constexpr int cmax(int a, int b) { return a > b ? a : b; }
 
-// G = number of variable groups of the fused pointwise phase (register budget)
-template <int P, int G>
+// G = number of variable groups of the fused pointwise phase (register budget);
+// T = arithmetic of the residual (the work area W holds T values, everything
+// else FP64)
+template <int P, int G, typename T = double>
 struct Lay {
     static constexpr int N = P + 1, M = P + 2, NB = N * N * N, NF = M * M, N2 = N * N;
     static constexpr int GV = G == 1 ? 5 : (G == 2 ? 3 : 2);  // variables per group (max)
@@ -102,8 +119,10 @@ struct Lay {
     static constexpr int face = 60 * FS;
     static constexpr int vol = 5 * X2S + cmax(5 * X1S, GV * (3 * X2S + 2 * X1S));
     static constexpr int W = odd(cmax(face, vol));
-    // U (double-buffered prefetch), residual, U0 and accumulator prefetch, work area
-    static constexpr int per_elem = 2 * ES + ES + 2 * ES + W;
+    // FP64: U (double-buffered prefetch), residual, U0 and accumulator prefetch
+    static constexpr int per_elem_f64 = 2 * ES + ES + 2 * ES;
+    // bytes per element, work area in T
+    static constexpr size_t bytes_per_elem = sizeof(double) * per_elem_f64 + sizeof(T) * W;
 };
 
 template <int P, int G>
@@ -154,15 +173,15 @@ __device__ __forceinline__ void prefetch_batch(const double* __restrict__ Us, in
 
 // 2D interpolation of an N x N slice s[b1][b0] to the M x M face grid,
 // written to out[t1*M + t0]
-template <int N, int M>
-__device__ __forceinline__ void interp2d(const double* __restrict__ Bt, const double (&s)[N][N], double* out)
+template <int N, int M, typename T>
+__device__ __forceinline__ void interp2d(const T* __restrict__ Bt, const T (&s)[N][N], T* out)
 {
-    double tmp[N][M];
+    T tmp[N][M];
 #pragma unroll
     for (int b1 = 0; b1 < N; ++b1)
 #pragma unroll
         for (int t0 = 0; t0 < M; ++t0) {
-            double a = 0.0;
+            T a = T(0);
 #pragma unroll
             for (int b0 = 0; b0 < N; ++b0) a += Bt[t0 * N + b0] * s[b1][b0];
             tmp[b1][t0] = a;
@@ -171,17 +190,17 @@ __device__ __forceinline__ void interp2d(const double* __restrict__ Bt, const do
     for (int t1 = 0; t1 < M; ++t1)
 #pragma unroll
         for (int t0 = 0; t0 < M; ++t0) {
-            double a = 0.0;
+            T a = T(0);
 #pragma unroll
             for (int b1 = 0; b1 < N; ++b1) a += Bt[t1 * N + b1] * tmp[b1][t0];
             out[t1 * M + t0] = a;
         }
 }
 
-template <int P, int E, int NT, int G>
+template <int P, int E, int NT, int G, typename T>
 __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
 {
-    using L = Lay<P, G>;
+    using L = Lay<P, G, T>;
     constexpr int N = L::N, M = L::M, NB = L::NB, NF = L::NF, N2 = L::N2;
     constexpr int VS = L::VS, ES = L::ES, FS = L::FS, X1S = L::X1S, X2S = L::X2S, W = L::W, GV = L::GV;
     extern __shared__ double smem[];
@@ -189,14 +208,14 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
     double* sRes = sUbuf + 2 * E * ES;     // [E][ES]
     double* sU0 = sRes + E * ES;           // [E][ES] step-start state of the batch
     double* sAcc = sU0 + E * ES;           // [E][ES] RK accumulator of the batch
-    double* sW = sAcc + E * ES;            // [E][W]
+    T* sW = reinterpret_cast<T*>(sAcc + E * ES);  // [E][W] in the residual's arithmetic
     const bool need_u0_acc = a.mode == kModeRK2 || a.mode == kModeRK3 || a.mode == kModeRK4;
-    const double* __restrict__ Bt = a.tab.B;
-    const double* __restrict__ Dt = a.tab.D;
-    const double* __restrict__ Wt = a.tab.W;
+    const T* __restrict__ Bt = TabSel<T>::B(a.tab);
+    const T* __restrict__ Dt = TabSel<T>::D(a.tab);
+    const T* __restrict__ Wt = TabSel<T>::W(a.tab);
     const double* __restrict__ Mi = a.tab.Minv;
     const int tid = threadIdx.x;
-    const double gamma = a.gamma;
+    const T gamma = T(a.gamma);
     unsigned status = 0;
     const int stride = gridDim.x * E;
 
@@ -224,27 +243,27 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
             const int ge = min(e0 + e, a.ne - 1);
             const int2 c = a.conn[ge * 6 + f];
             const int fn = c.y & 7;
-            double sn[N][N], so[N][N];
+            T sn[N][N], so[N][N];
             if (c.x >= e0 && c.x < e0 + E) {
                 const double* src = sU + (c.x - e0) * ES + v * VS;
 #pragma unroll
                 for (int b1 = 0; b1 < N; ++b1)
 #pragma unroll
-                    for (int b0 = 0; b0 < N; ++b0) sn[b1][b0] = src[slice_index<N>(fn, b0, b1)];
+                    for (int b0 = 0; b0 < N; ++b0) sn[b1][b0] = T(src[slice_index<N>(fn, b0, b1)]);
             } else {
                 const double* src = a.Us + ((size_t)c.x * 5 + v) * NB;
 #pragma unroll
                 for (int b1 = 0; b1 < N; ++b1)
 #pragma unroll
-                    for (int b0 = 0; b0 < N; ++b0) sn[b1][b0] = __ldg(src + slice_index<N>(fn, b0, b1));
+                    for (int b0 = 0; b0 < N; ++b0) sn[b1][b0] = T(__ldg(src + slice_index<N>(fn, b0, b1)));
             }
             const double* own = sU + e * ES + v * VS;
 #pragma unroll
             for (int b1 = 0; b1 < N; ++b1)
 #pragma unroll
-                for (int b0 = 0; b0 < N; ++b0) so[b1][b0] = own[slice_index<N>(f, b0, b1)];
-            interp2d<N, M>(Bt, so, sW + e * W + (f * 5 + v) * FS);
-            interp2d<N, M>(Bt, sn, sW + e * W + 30 * FS + (f * 5 + v) * FS);
+                for (int b0 = 0; b0 < N; ++b0) so[b1][b0] = T(own[slice_index<N>(f, b0, b1)]);
+            interp2d<N, M, T>(Bt, so, sW + e * W + (f * 5 + v) * FS);
+            interp2d<N, M, T>(Bt, sn, sW + e * W + 30 * FS + (f * 5 + v) * FS);
         }
         __syncthreads();
 
@@ -255,9 +274,9 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
             const int2 c = a.conn[ge * 6 + f];
             const int fn = c.y & 7, isL = (c.y >> 3) & 1, code = c.y >> 4;
             const int cn = a.cmap[code * NF + cidx];
-            double* Tr = sW + e * W + f * 5 * FS;
-            const double* Tn = sW + e * W + 30 * FS + f * 5 * FS;
-            double Uo[5], Un[5], F[5];
+            T* Tr = sW + e * W + f * 5 * FS;
+            const T* Tn = sW + e * W + 30 * FS + f * 5 * FS;
+            T Uo[5], Un[5], F[5];
 #pragma unroll
             for (int v = 0; v < 5; ++v) {
                 Uo[v] = Tr[v * FS + cidx];
@@ -265,8 +284,8 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
             }
             const GeoDev* g = a.geo + (isL ? a.geo_class[ge] : a.geo_class[c.x]);
             const int fl = isL ? f : fn;
-            const double Nv[3] = {g->N[fl][0], g->N[fl][1], g->N[fl][2]};
-            double UL[5], UR[5];  // selected element-wise so that both stay in registers
+            const T Nv[3] = {T(g->N[fl][0]), T(g->N[fl][1]), T(g->N[fl][2])};
+            T UL[5], UR[5];  // selected element-wise so that both stay in registers
 #pragma unroll
             for (int v = 0; v < 5; ++v) {
                 UL[v] = isL ? Uo[v] : Un[v];
@@ -277,8 +296,8 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
             } else {
                 dgp::flux_lax_friedrichs(gamma, UL, UR, Nv, F);
             }
-            const double w = Wt[cidx % M] * Wt[cidx / M];
-            const double sgn = isL ? -1.0 : 1.0;
+            const T w = Wt[cidx % M] * Wt[cidx / M];
+            const T sgn = isL ? T(-1.0) : T(1.0);
 #pragma unroll
             for (int v = 0; v < 5; ++v) Tr[v * FS + cidx] = sgn * (F[v] * w);
         }
@@ -287,34 +306,34 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
         // ---- face lift per (element, face, variable) into Tn's space ----
         for (int t = tid; t < E * 30; t += NT) {
             const int v = t % 5, f = (t / 5) % 6, e = t / 30;
-            const double* Fq = sW + e * W + (f * 5 + v) * FS;
-            double tmp[M][N];
+            const T* Fq = sW + e * W + (f * 5 + v) * FS;
+            T tmp[M][N];
 #pragma unroll
             for (int t1 = 0; t1 < M; ++t1)
 #pragma unroll
                 for (int b0 = 0; b0 < N; ++b0) {
-                    double s = 0.0;
+                    T s = T(0);
 #pragma unroll
                     for (int t0 = 0; t0 < M; ++t0) s += Bt[t0 * N + b0] * Fq[t1 * M + t0];
                     tmp[t1][b0] = s;
                 }
-            double* Lf = sW + e * W + 30 * FS + (f * 5 + v) * FS;
+            T* Lf = sW + e * W + 30 * FS + (f * 5 + v) * FS;
 #pragma unroll
             for (int b1 = 0; b1 < N; ++b1)
 #pragma unroll
                 for (int b0 = 0; b0 < N; ++b0) {
-                    double s = 0.0;
+                    T s = T(0);
 #pragma unroll
                     for (int t1 = 0; t1 < M; ++t1) s += Bt[t1 * N + b1] * tmp[t1][b0];
                     Lf[b1 * N + b0] = s;
                 }
         }
         __syncthreads();
-        // gather the six face contributions into the residual
+        // gather the six face contributions into the (FP64) residual
         for (int i = tid; i < E * 5 * NB; i += NT) {
             const int b = i % NB, v = (i / NB) % 5, e = i / (5 * NB);
             const int bc[3] = {b % N, (b / N) % N, b / N2};
-            const double* Lf = sW + e * W + 30 * FS + v * FS;
+            const T* Lf = sW + e * W + 30 * FS + v * FS;
             double s = 0.0;
 #pragma unroll
             for (int f = 0; f < 6; ++f) {
@@ -322,7 +341,7 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
                 if (bc[ax] == sidx) {
                     const int b0 = ax == 0 ? bc[1] : bc[0];
                     const int b1 = ax == 2 ? bc[1] : bc[2];
-                    s += Lf[f * 5 * FS + b1 * N + b0];
+                    s += double(Lf[f * 5 * FS + b1 * N + b0]);
                 }
             }
             sRes[e * ES + v * VS + b] = s;
@@ -330,18 +349,18 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
         __syncthreads();
 
         // ---- volume: interpolation passes x, y ----
-        double* X2 = sW;               // per element: [5][X2S] with [bz][qy][qx]
-        double* X1 = sW + 5 * X2S;     // per element: [5][X1S] with [bz][by][qx]
+        T* X2 = sW;               // per element: [5][X2S] with [bz][qy][qx]
+        T* X1 = sW + 5 * X2S;     // per element: [5][X1S] with [bz][by][qx]
         for (int i = tid; i < E * 5 * N2; i += NT) {
             const int v = i % 5, byz = (i / 5) % N2, e = i / (5 * N2);
             const double* u = sU + e * ES + v * VS + byz * N;
-            double row[N];
+            T row[N];
 #pragma unroll
-            for (int bx = 0; bx < N; ++bx) row[bx] = u[bx];
-            double* o = X1 + e * W + v * X1S + byz * M;
+            for (int bx = 0; bx < N; ++bx) row[bx] = T(u[bx]);
+            T* o = X1 + e * W + v * X1S + byz * M;
 #pragma unroll
             for (int qx = 0; qx < M; ++qx) {
-                double s = 0.0;
+                T s = T(0);
 #pragma unroll
                 for (int bx = 0; bx < N; ++bx) s += Bt[qx * N + bx] * row[bx];
                 o[qx] = s;
@@ -351,14 +370,14 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
         for (int i = tid; i < E * 5 * N * M; i += NT) {
             const int v = i % 5, r = i / 5;
             const int qx = r % M, bz = (r / M) % N, e = r / (M * N);
-            const double* x1 = X1 + e * W + v * X1S + bz * N * M + qx;
-            double col[N];
+            const T* x1 = X1 + e * W + v * X1S + bz * N * M + qx;
+            T col[N];
 #pragma unroll
             for (int by = 0; by < N; ++by) col[by] = x1[by * M];
-            double* o = X2 + e * W + v * X2S + bz * NF + qx;
+            T* o = X2 + e * W + v * X2S + bz * NF + qx;
 #pragma unroll
             for (int qy = 0; qy < M; ++qy) {
-                double s = 0.0;
+                T s = T(0);
 #pragma unroll
                 for (int by = 0; by < N; ++by) s += Bt[qy * N + by] * col[by];
                 o[qy * M] = s;
@@ -371,55 +390,55 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
 #pragma unroll
         for (int g = 0; g < G; ++g) {
             const int gv0 = group_first<P, G>(g), gnv = group_size<P, G>(g);
-            double* Abuf = sW + 5 * X2S;            // [GV][3][X2S] over X1
-            double* Cbuf = Abuf + GV * 3 * X2S;     // [GV][2][X1S]
+            T* Abuf = sW + 5 * X2S;            // [GV][3][X2S] over X1
+            T* Cbuf = Abuf + GV * 3 * X2S;     // [GV][2][X1S]
             for (int i = tid; i < E * NF; i += NT) {
                 const int e = i / NF, qxy = i % NF;
                 const int qx = qxy % M, qy = qxy / M;
-                double xz[5][N];
+                T xz[5][N];
 #pragma unroll
                 for (int v = 0; v < 5; ++v)
 #pragma unroll
                     for (int bz = 0; bz < N; ++bz) xz[v][bz] = X2[e * W + v * X2S + bz * NF + qxy];
                 const int ge = min(e0 + e, a.ne - 1);
                 const GeoDev* geo = a.geo + a.geo_class[ge];
-                double JD[9];
+                T JD[9];
 #pragma unroll
-                for (int k = 0; k < 9; ++k) JD[k] = geo->JD[k];
-                double acc[GV][3][N];
+                for (int k = 0; k < 9; ++k) JD[k] = T(geo->JD[k]);
+                T acc[GV][3][N];
 #pragma unroll
                 for (int v = 0; v < GV; ++v)
 #pragma unroll
                     for (int d = 0; d < 3; ++d)
 #pragma unroll
-                        for (int bz = 0; bz < N; ++bz) acc[v][d][bz] = 0.0;
-                const double wxy = Wt[qx] * Wt[qy];
+                        for (int bz = 0; bz < N; ++bz) acc[v][d][bz] = T(0);
+                const T wxy = Wt[qx] * Wt[qy];
 #pragma unroll
                 for (int qz = 0; qz < M; ++qz) {
-                    double U[5];
+                    T U[5];
 #pragma unroll
                     for (int v = 0; v < 5; ++v) {
-                        double s = 0.0;
+                        T s = T(0);
 #pragma unroll
                         for (int bz = 0; bz < N; ++bz) s += Bt[qz * N + bz] * xz[v][bz];
                         U[v] = s;
                     }
                     if (g == 0) {
-                        const double p = dgp::pressure(gamma, U);
-                        if (!(U[0] > 0.0)) status |= kStatusRho;
-                        if (!(p > 0.0)) status |= kStatusPressure;
+                        const T p = dgp::pressure(gamma, U);
+                        if (!(U[0] > T(0))) status |= kStatusRho;
+                        if (!(p > T(0))) status |= kStatusPressure;
                         if (U[0] != U[0] || p != p) status |= kStatusNaN;
                     }
-                    double F[15];
+                    T F[15];
                     dgp::interior_flux(gamma, U, F);
-                    const double wq = wxy * Wt[qz];
+                    const T wq = wxy * Wt[qz];
 #pragma unroll
                     for (int vv = 0; vv < GV; ++vv) {
                         if (vv < gnv) {
                             const int v = gv0 + vv;
 #pragma unroll
                             for (int d = 0; d < 3; ++d) {
-                                const double Gd =
+                                const T Gd =
                                     (F[v] * JD[d * 3 + 0] + F[5 + v] * JD[d * 3 + 1] + F[10 + v] * JD[d * 3 + 2]) * wq;
 #pragma unroll
                                 for (int bz = 0; bz < N; ++bz)
@@ -440,22 +459,22 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
             // y contraction: C0 = By^T A0 ; C12 = Dy^T A1 + By^T A2
             for (int i = tid; i < E * gnv * N * M; i += NT) {
                 const int qx = i % M, bz = (i / M) % N, vv = (i / (M * N)) % gnv, e = i / (gnv * N * M);
-                const double* A0 = Abuf + e * W + (vv * 3 + 0) * X2S + bz * NF + qx;
-                const double* A1 = A0 + X2S;
-                const double* A2 = A1 + X2S;
-                double c0[N], c12[N];
+                const T* A0 = Abuf + e * W + (vv * 3 + 0) * X2S + bz * NF + qx;
+                const T* A1 = A0 + X2S;
+                const T* A2 = A1 + X2S;
+                T c0[N], c12[N];
 #pragma unroll
-                for (int by = 0; by < N; ++by) { c0[by] = 0.0; c12[by] = 0.0; }
+                for (int by = 0; by < N; ++by) { c0[by] = T(0); c12[by] = T(0); }
 #pragma unroll
                 for (int qy = 0; qy < M; ++qy) {
-                    const double a0 = A0[qy * M], a1 = A1[qy * M], a2 = A2[qy * M];
+                    const T a0 = A0[qy * M], a1 = A1[qy * M], a2 = A2[qy * M];
 #pragma unroll
                     for (int by = 0; by < N; ++by) {
                         c0[by] += Bt[qy * N + by] * a0;
                         c12[by] += Dt[qy * N + by] * a1 + Bt[qy * N + by] * a2;
                     }
                 }
-                double* C0 = Cbuf + e * W + (vv * 2) * X1S + bz * N * M + qx;
+                T* C0 = Cbuf + e * W + (vv * 2) * X1S + bz * N * M + qx;
 #pragma unroll
                 for (int by = 0; by < N; ++by) {
                     C0[by * M] = c0[by];
@@ -463,23 +482,23 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
                 }
             }
             __syncthreads();
-            // x contraction into the residual: res += Dx^T C0 + Bx^T C12
+            // x contraction into the (FP64) residual: res += Dx^T C0 + Bx^T C12
             for (int i = tid; i < E * gnv * N2; i += NT) {
                 const int vv = i % gnv, byz = (i / gnv) % N2, e = i / (gnv * N2);
-                const double* C0 = Cbuf + e * W + (vv * 2) * X1S + byz * M;
-                const double* C12 = C0 + X1S;
-                double r[N];
+                const T* C0 = Cbuf + e * W + (vv * 2) * X1S + byz * M;
+                const T* C12 = C0 + X1S;
+                T r[N];
 #pragma unroll
-                for (int bx = 0; bx < N; ++bx) r[bx] = 0.0;
+                for (int bx = 0; bx < N; ++bx) r[bx] = T(0);
 #pragma unroll
                 for (int qx = 0; qx < M; ++qx) {
-                    const double c0 = C0[qx], c12 = C12[qx];
+                    const T c0 = C0[qx], c12 = C12[qx];
 #pragma unroll
                     for (int bx = 0; bx < N; ++bx) r[bx] += Dt[qx * N + bx] * c0 + Bt[qx * N + bx] * c12;
                 }
                 double* res = sRes + e * ES + (gv0 + vv) * VS + byz * N;
 #pragma unroll
-                for (int bx = 0; bx < N; ++bx) res[bx] += r[bx];
+                for (int bx = 0; bx < N; ++bx) res[bx] += double(r[bx]);
             }
             __syncthreads();
         }
@@ -492,7 +511,7 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
             continue;
         }
 
-        // ---- inverse mass: x and y passes in place, z pass fused with the update ----
+        // ---- inverse mass (FP64): x and y passes in place, z pass fused with the update ----
         for (int i = tid; i < E * 5 * N2; i += NT) {
             const int v = i % 5, byz = (i / 5) % N2, e = i / (5 * N2);
             double* r = sRes + e * ES + v * VS + byz * N;  // pencil along x
@@ -561,34 +580,35 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
     if (status) atomicOr(a.status, status);
 }
 
-template <int P, int E, int G>
+template <int P, int E, int G, typename T>
 constexpr size_t stage_smem_bytes()
 {
-    return sizeof(double) * (size_t)E * Lay<P, G>::per_elem;
+    return (size_t)E * Lay<P, G, T>::bytes_per_elem;
 }
 
 // ---- compiled launch variants (one translation unit per order) ----
 
 struct StageVariant {
     int E, NT, G;        // elements per CTA, threads per CTA, variable groups
+    int fp32;            // 1: residual arithmetic in FP32 (mixed precision), 0: FP64
     size_t smem;         // dynamic shared memory per CTA
     const void* func;    // the kernel, for attributes / occupancy queries
     cudaError_t (*launch)(const StageArgs&, int grid, cudaStream_t);
 };
 
-template <int P, int E, int NT, int G>
+template <int P, int E, int NT, int G, typename T>
 cudaError_t launch_stage_variant(const StageArgs& a, int grid, cudaStream_t s)
 {
-    stage_kernel<P, E, NT, G><<<grid, NT, stage_smem_bytes<P, E, G>(), s>>>(a);
+    stage_kernel<P, E, NT, G, T><<<grid, NT, stage_smem_bytes<P, E, G, T>(), s>>>(a);
     return cudaGetLastError();
 }
 
-template <int P, int E, int NT, int G>
+template <int P, int E, int NT, int G, typename T = double>
 constexpr StageVariant make_variant()
 {
-    static_assert(stage_smem_bytes<P, E, G>() <= 227 * 1024, "stage kernel shared memory exceeds 227 KB");
-    return StageVariant{E, NT, G, stage_smem_bytes<P, E, G>(), (const void*)stage_kernel<P, E, NT, G>,
-                        launch_stage_variant<P, E, NT, G>};
+    static_assert(stage_smem_bytes<P, E, G, T>() <= 227 * 1024, "stage kernel shared memory exceeds 227 KB");
+    return StageVariant{E, NT, G, sizeof(T) == 4 ? 1 : 0, stage_smem_bytes<P, E, G, T>(),
+                        (const void*)stage_kernel<P, E, NT, G, T>, launch_stage_variant<P, E, NT, G, T>};
 }
 
 // the variants compiled for order p (defined in dg_stage_p<p>.cu)

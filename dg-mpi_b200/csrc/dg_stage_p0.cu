@@ -1,14 +1,17 @@
 // dg_stage_p0.cu -- compiled launch variants of the stage kernel for order p = 0
-// (elements per CTA, threads per CTA, variable groups); the first entry is
-// the default, the tuner (dg_tune_stage) may pick another.
+// (elements per CTA, threads per CTA, variable groups; FP64 residual first,
+// then the mixed-precision FP32 residual).  The first variant of each
+// precision is the default; the tuner (dg_tune_stage) may pick another.
 #include "dg_stage.cuh"
 
 namespace dgk {
 
 static const StageVariant kVariants0[] = {
-    make_variant<0, 32, 128, 1>(),
-    make_variant<0, 8, 32, 1>(),
-    make_variant<0, 16, 64, 1>(),
+    make_variant<0, 32, 128, 1, double>(),
+    make_variant<0, 8, 32, 1, double>(),
+    make_variant<0, 16, 64, 1, double>(),
+    make_variant<0, 32, 128, 1, float>(),
+    make_variant<0, 16, 64, 1, float>(),
 };
 
 int stage_variants_p0(const StageVariant** out)

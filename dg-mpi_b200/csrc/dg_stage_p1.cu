@@ -1,15 +1,19 @@
 // dg_stage_p1.cu -- compiled launch variants of the stage kernel for order p = 1
-// (elements per CTA, threads per CTA, variable groups); the first entry is
-// the default, the tuner (dg_tune_stage) may pick another.
+// (elements per CTA, threads per CTA, variable groups; FP64 residual first,
+// then the mixed-precision FP32 residual).  The first variant of each
+// precision is the default; the tuner (dg_tune_stage) may pick another.
 #include "dg_stage.cuh"
 
 namespace dgk {
 
 static const StageVariant kVariants1[] = {
-    make_variant<1, 8, 128, 1>(),
-    make_variant<1, 1, 32, 1>(),
-    make_variant<1, 2, 64, 1>(),
-    make_variant<1, 4, 64, 1>(),
+    make_variant<1, 8, 128, 1, double>(),
+    make_variant<1, 1, 32, 1, double>(),
+    make_variant<1, 2, 64, 1, double>(),
+    make_variant<1, 4, 64, 1, double>(),
+    make_variant<1, 8, 128, 1, float>(),
+    make_variant<1, 2, 64, 1, float>(),
+    make_variant<1, 4, 64, 1, float>(),
 };
 
 int stage_variants_p1(const StageVariant** out)

@@ -1,15 +1,20 @@
 // dg_stage_p5.cu -- compiled launch variants of the stage kernel for order p = 5
-// (elements per CTA, threads per CTA, variable groups); the first entry is
-// the default, the tuner (dg_tune_stage) may pick another.
+// (elements per CTA, threads per CTA, variable groups; FP64 residual first,
+// then the mixed-precision FP32 residual).  The first variant of each
+// precision is the default; the tuner (dg_tune_stage) may pick another.
 #include "dg_stage.cuh"
 
 namespace dgk {
 
 static const StageVariant kVariants5[] = {
-    make_variant<5, 1, 32, 3>(),
-    make_variant<5, 2, 128, 3>(),
-    make_variant<5, 1, 64, 3>(),
-    make_variant<5, 2, 64, 3>(),
+    make_variant<5, 1, 32, 3, double>(),
+    make_variant<5, 2, 128, 3, double>(),
+    make_variant<5, 1, 64, 3, double>(),
+    make_variant<5, 2, 64, 3, double>(),
+    make_variant<5, 1, 32, 2, float>(),
+    make_variant<5, 2, 64, 2, float>(),
+    make_variant<5, 1, 32, 1, float>(),
+    make_variant<5, 1, 64, 2, float>(),
 };
 
 int stage_variants_p5(const StageVariant** out)

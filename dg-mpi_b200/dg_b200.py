@@ -90,7 +90,7 @@ def library(path: str | None = None) -> ctypes.CDLL:
         "dg_face_orientation_order": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ip]),
         "dg_basis_tables": (ctypes.c_int, [ctypes.c_int, dp, dp, dp]),
         "dg_num_stage_variants": (ctypes.c_int, [ctypes.c_int]),
-        "dg_stage_variant_info": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ip, ip, ip]),
+        "dg_stage_variant_info": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ip, ip, ip, ip]),
         "dg_set_stage_variant": (ctypes.c_int, [vp, ctypes.c_int]),
         "dg_get_stage_variant": (ctypes.c_int, [vp]),
         "dg_tune_stage": (ctypes.c_int, [vp, ctypes.c_int, ip, dp]),
@@ -279,12 +279,13 @@ class Case:
 
     # -- launch variants ---------------------------------------------------
     def stage_variants(self):
-        """[(elements per CTA, threads per CTA, variable groups)] compiled for this order."""
+        """[(elements per CTA, threads per CTA, variable groups, precision)] compiled for this order."""
         out = []
         for v in range(self._lib.dg_num_stage_variants(self.order)):
-            E, NT, G = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
-            self._lib.dg_stage_variant_info(self.order, v, ctypes.byref(E), ctypes.byref(NT), ctypes.byref(G))
-            out.append((E.value, NT.value, G.value))
+            E, NT, G, pr = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+            self._lib.dg_stage_variant_info(self.order, v, ctypes.byref(E), ctypes.byref(NT), ctypes.byref(G),
+                                            ctypes.byref(pr))
+            out.append((E.value, NT.value, G.value, "mixed_fp32" if pr.value == 1 else "fp64"))
         return out
 
     @property

@@ -1,1 +1,221 @@
-int main(){return 0;}
+// main.cpp -- dg_solve: the reference's driver (src/exec/main.cpp +
+// src/post/main.cpp) on the B200 path.  It keeps the reference's TOML deck,
+// its Solver / StepperBase / take_time_step structure and its post-processing
+// L2 error, and calls libdg_b200.so through the C ABI for the hot path.
+//
+//   dg_solve [-input input.toml] [-check]     (default deck: input.toml)
+//
+// Deck keys (as in the reference, src/exec/main.cpp:52-119,
+// src/solver/base.cpp:20-67, src/physics/base/base.cpp:25-32):
+//   [Mesh]     file = "...cube_<N>.h5"  -> periodic N^3 box on [0,1]^3 (the
+//              reference's cube meshes; no HDF5 reader in this build), or
+//              periodic_box = [nx, ny, nz], origin = [..], length = [..]
+//   [Numerics] order, basis = "LagrangeHex"
+//   [Stepper]  type = "FE" | "RK4" (default "FE"), timestep, end;
+//              extensions: cfl (derive timestep from the IC), steps (count)
+//   [Physics]  name = "Euler", dim = 3, gamma = 1.4, GasConstant = 287.05,
+//              convective_flux_fcn = "LaxFriedrichs" | "HLLC"
+//   [InitialCondition] name, data
+//   [Output]   (extension) print_every = N, state_file = "path"
+#include <cfloat>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <memory>
+#include <regex>
+#include <string>
+#include <vector>
+
+#include "../../include/dg_b200.h"
+#include "toml_lite.h"
+
+namespace {
+
+struct Solver;
+
+// StepperBase / FE / RK4 of src/numerics/timestepping/stepper.h:14-90; the
+// step itself is the device path behind the C ABI.
+struct StepperBase {
+    virtual ~StepperBase() = default;
+    void set_time_step(double dt_) { dt = dt_; }
+    void set_final_time(double t) { tfinal = t; }
+    double get_time_step() const { return dt; }
+    double get_tfinal() const { return tfinal; }
+    virtual int take_time_step(Solver& solver) = 0;
+    double dt = 0.0, tfinal = 0.0;
+};
+
+struct Solver {
+    dg_ctx* ctx = nullptr;
+    double time = 0.0;
+    long num_iterations = 0;
+    int print_every = 0;
+    std::unique_ptr<StepperBase> stepper;
+
+    // Solver::solve, src/solver/base.cpp:377-399
+    int solve()
+    {
+        const auto t0 = std::chrono::steady_clock::now();
+        for (long it = 0; it < num_iterations; ++it) {
+            int rc = stepper->take_time_step(*this);
+            if (rc) return rc;
+            if (print_every > 0 && (it + 1) % print_every == 0) std::printf("Time = %.10g\n", time);
+        }
+        const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        std::printf("Time to Solution: %.6f s (%ld steps)\n", sec, num_iterations);
+        return DG_OK;
+    }
+};
+
+struct RK4Gpu : StepperBase {
+    int take_time_step(Solver& s) override
+    {
+        const int rc = dg_rk4_steps(s.ctx, dt, 1);
+        s.time += dt;  // stage times t, t+dt/2, t+dt/2, t+dt (stepper.cpp:98,125)
+        return rc;
+    }
+};
+
+struct FEGpu : StepperBase {
+    int take_time_step(Solver& s) override
+    {
+        const int rc = dg_fe_steps(s.ctx, dt, 1);
+        s.time += dt;
+        return rc;
+    }
+};
+
+int ic_code(const std::string& name)
+{
+    if (name == "Uniform") return DG_IC_UNIFORM;
+    if (name == "IsentropicVortex") return DG_IC_VORTEX_REF;
+    if (name == "Sphere") return DG_IC_SPHERE;
+    if (name == "IsentropicVortexXY") return DG_IC_VORTEX_XY;
+    if (name == "TaylorGreen") return DG_IC_TAYLOR_GREEN;
+    throw std::runtime_error("unknown [InitialCondition] name " + name);
+}
+
+int run(const dgh::Toml& deck, bool check_only)
+{
+    // ---- mesh ----
+    int n[3] = {0, 0, 0};
+    double x0[3] = {0, 0, 0}, len[3] = {1, 1, 1};
+    if (deck.has("Mesh", "periodic_box")) {
+        const auto b = deck.nums("Mesh", "periodic_box");
+        if (b.size() != 3) throw std::runtime_error("[Mesh] periodic_box needs 3 entries");
+        for (int i = 0; i < 3; ++i) n[i] = static_cast<int>(b[i]);
+        if (deck.has("Mesh", "origin")) { auto o = deck.nums("Mesh", "origin"); for (int i = 0; i < 3; ++i) x0[i] = o.at(i); }
+        if (deck.has("Mesh", "length")) { auto l = deck.nums("Mesh", "length"); for (int i = 0; i < 3; ++i) len[i] = l.at(i); }
+    } else {
+        const std::string file = deck.str("Mesh", "file");
+        std::smatch m;
+        if (!std::regex_search(file, m, std::regex("cube_([0-9]+)\\.h5$")))
+            throw std::runtime_error("[Mesh] file " + file + ": only the reference's periodic cube_<N>.h5 meshes are "
+                                     "generated in memory (no HDF5 reader); use periodic_box");
+        n[0] = n[1] = n[2] = std::stoi(m[1]);
+    }
+    // ---- numerics / physics ----
+    const int order = static_cast<int>(deck.num("Numerics", "order"));
+    const std::string basis = deck.str_or("Numerics", "basis", "LagrangeHex");
+    if (basis != "LagrangeHex") throw std::runtime_error("[Numerics] basis " + basis + " is not on the device path");
+    if (deck.str_or("Physics", "name", "Euler") != "Euler") throw std::runtime_error("[Physics] name must be Euler");
+    if (static_cast<int>(deck.num_or("Physics", "dim", 3)) != 3) throw std::runtime_error("[Physics] dim must be 3");
+    const double gamma = deck.num_or("Physics", "gamma", 1.4);
+    const double R = deck.num_or("Physics", "GasConstant", 287.05);
+    const std::string flux_name = deck.str_or("Physics", "convective_flux_fcn", "LaxFriedrichs");
+    int flux = DG_FLUX_LAX_FRIEDRICHS;
+    if (flux_name == "HLLC") flux = DG_FLUX_HLLC;
+    else if (flux_name != "LaxFriedrichs") throw std::runtime_error("unknown convective_flux_fcn " + flux_name);
+    const std::string ic_name = deck.str("InitialCondition", "name");
+    const int ic = ic_code(ic_name);
+    std::vector<double> ic_data = deck.has("InitialCondition", "data") ? deck.nums("InitialCondition", "data")
+                                                                          : std::vector<double>();
+    if (ic_data.size() > 10) throw std::runtime_error("[InitialCondition] data holds at most 10 values");
+    const std::string stype = deck.str_or("Stepper", "type", "FE");
+    if (stype != "FE" && stype != "RK4") throw std::runtime_error("[Stepper] type must be FE or RK4");
+
+    std::printf("case: %dx%dx%d periodic hex, p=%d, %s flux, %s, IC %s\n", n[0], n[1], n[2], order, flux_name.c_str(),
+                stype.c_str(), ic_name.c_str());
+    if (check_only) return 0;
+
+    int nn = 0, ne = 0, nf = 0;
+    if (dg_mesh_periodic_box(n, x0, len, 0, &nn, nullptr, &ne, nullptr, &nf, nullptr)) throw std::runtime_error("bad box");
+    std::vector<double> coords(static_cast<size_t>(nn) * 3);
+    std::vector<unsigned> e2n(static_cast<size_t>(ne) * 8), faces(static_cast<size_t>(nf) * 8);
+    dg_mesh_periodic_box(n, x0, len, 0, &nn, coords.data(), &ne, e2n.data(), &nf, faces.data());
+    dg_mesh_desc md{nn, coords.data(), ne, e2n.data(), nf, faces.data(), 0};
+    dg_case_desc cd{order, flux, gamma, R, DG_PREC_FP64, 0};
+
+    Solver solver;
+    if (dg_create(&cd, &md, &solver.ctx)) throw std::runtime_error(std::string("dg_create: ") + dg_last_error(nullptr));
+    const int nb = dg_num_basis(solver.ctx);
+    std::vector<double> Uc(static_cast<size_t>(ne) * nb * 5);
+    // Solver::init_state_from_fcn (L2 projection), base.cpp:113-223
+    if (dg_project_ic(solver.ctx, ic, ic_data.data(), static_cast<int>(ic_data.size()), 0.0, Uc.data()))
+        throw std::runtime_error(std::string("dg_project_ic: ") + dg_last_error(solver.ctx));
+
+    double dt = deck.num_or("Stepper", "timestep", 0.0);
+    if (deck.has("Stepper", "cfl")) {
+        if (dg_cfl_time_step(solver.ctx, Uc.data(), deck.num("Stepper", "cfl"), &dt))
+            throw std::runtime_error(std::string("cfl: ") + dg_last_error(solver.ctx));
+    }
+    if (!(dt > 0.0)) throw std::runtime_error("[Stepper] needs timestep > 0 (or cfl)");
+    if (deck.has("Stepper", "steps")) {
+        solver.num_iterations = static_cast<long>(deck.num("Stepper", "steps"));
+    } else {
+        // num_iterations = (int)(tfinal / dt), base.cpp:383
+        solver.num_iterations = static_cast<int>(deck.num("Stepper", "end") / dt);
+    }
+    if (stype == "RK4") solver.stepper = std::make_unique<RK4Gpu>();
+    else solver.stepper = std::make_unique<FEGpu>();
+    solver.stepper->set_time_step(dt);
+    solver.stepper->set_final_time(dt * solver.num_iterations);
+    solver.print_every = static_cast<int>(deck.num_or("Output", "print_every", 0));
+    std::printf("timestep = %.17g, number of iterations = %ld, DOF = %lld\n", dt, solver.num_iterations,
+                static_cast<long long>(ne) * nb * 5);
+
+    int rc = solver.solve();
+    if (rc) throw std::runtime_error(std::string("solve: ") + dg_last_error(solver.ctx));
+
+    // post: volume-normalised L2 error against the exact solution
+    // (get_error, src/post/main.cpp:30-201); TaylorGreen has none: kinetic energy instead
+    if (ic == DG_IC_TAYLOR_GREEN) {
+        double ke = 0.0;
+        dg_kinetic_energy(solver.ctx, &ke);
+        std::printf("kinetic_energy=%.*e\n", DECIMAL_DIG, ke);
+    } else {
+        double err[5];
+        if (dg_l2_error(solver.ctx, ic, ic_data.data(), static_cast<int>(ic_data.size()), solver.time, err))
+            throw std::runtime_error(std::string("l2 error: ") + dg_last_error(solver.ctx));
+        for (int s = 0; s < 5; ++s) std::printf("norm_total_error(%d)=%.*e\n", s, DECIMAL_DIG, err[s]);
+    }
+    if (deck.has("Output", "state_file")) {
+        dg_get_state(solver.ctx, Uc.data());
+        std::ofstream f(deck.str("Output", "state_file"), std::ios::binary);
+        const long long hdr[3] = {ne, nb, 5};
+        f.write(reinterpret_cast<const char*>(hdr), sizeof(hdr));
+        f.write(reinterpret_cast<const char*>(&solver.time), sizeof(double));
+        f.write(reinterpret_cast<const char*>(Uc.data()), static_cast<std::streamsize>(Uc.size() * sizeof(double)));
+    }
+    dg_destroy(solver.ctx);
+    return 0;
+}
+
+}  // namespace
+
+int main(int argc, char* argv[])
+{
+    std::string deck_path = "input.toml";
+    bool check_only = false;
+    for (int i = 1; i < argc; ++i) {
+        if (!std::strcmp(argv[i], "-input") && i + 1 < argc) deck_path = argv[++i];
+        else if (!std::strcmp(argv[i], "-check")) check_only = true;
+    }
+    try {
+        return run(dgh::Toml::parse_file(deck_path), check_only);
+    } catch (const std::exception& ex) {
+        std::fprintf(stderr, "dg_solve: %s\n", ex.what());
+        return 2;
+    }
+}

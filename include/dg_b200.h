@@ -49,8 +49,10 @@ extern "C" {
 #define DG_FLUX_LAX_FRIEDRICHS 0
 #define DG_FLUX_HLLC 1
 
-/* arithmetic of the residual (the stored solution, RK accumulation, inverse
- * mass and geometric factors are FP64 in every mode) */
+/* arithmetic of the residual: FP64 throughout, or the mixed-precision form
+ * whose traces, fluxes and volume / lift contractions run in FP32 while the
+ * stored solution, the residual accumulation, the inverse mass, the geometric
+ * factors and the RK stage update stay FP64 */
 #define DG_PREC_FP64 0
 #define DG_PREC_MIXED_FP32 1
 
@@ -139,11 +141,13 @@ int dg_rk4_steps_timed(dg_ctx* ctx, double dt, int nsteps, double* device_ms);
 /* ---- stage-kernel launch variants and their tuner ----
  * Each order has a few compiled variants of the fused stage kernel (elements
  * per CTA, threads per CTA, variable groups of the pointwise phase).  The
- * tuner times one stage of every variant on the context's mesh and current
- * state (the state is not modified) and selects the fastest; callers cache
- * the result per (order, GPU) and restore it with dg_set_stage_variant. */
+ * tuner times one stage of every variant of the context's precision on its
+ * mesh and current state (the state is not modified) and selects the
+ * fastest (entries of other precision report -1 ms); callers cache the result
+ * per (order, precision, GPU) and restore it with dg_set_stage_variant. */
 int dg_num_stage_variants(int order);
-int dg_stage_variant_info(int order, int variant, int* elems_per_cta, int* threads_per_cta, int* groups);
+int dg_stage_variant_info(int order, int variant, int* elems_per_cta, int* threads_per_cta, int* groups,
+                          int* precision);
 int dg_set_stage_variant(dg_ctx* ctx, int variant);
 int dg_get_stage_variant(const dg_ctx* ctx);
 int dg_tune_stage(dg_ctx* ctx, int reps, int* best_variant, double* ms_per_variant);

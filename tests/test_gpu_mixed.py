@@ -1,0 +1,71 @@
+"""Mixed-precision residual (FP32 traces, fluxes and contractions; FP64 state,
+residual accumulation, inverse mass and RK update) against the FP64 path.
+
+Bar: relative L2 difference per conserved variable <= 1e-6 after time
+stepping (a variable that is identically zero in exact arithmetic is
+normalised by the largest variable's norm), and the same L2 error against
+the exact advected vortex to within that difference.
+"""
+import numpy as np
+import pytest
+
+import dg_b200
+
+pytestmark = pytest.mark.gpu
+
+VORTEX_XY = [1.0, 1.0, 1.0, 1.0, 5.0, 5.0, 5.0, 10.0, 10.0]
+TOL = 1e-6
+
+
+def rel_l2(a, b):
+    a = a.reshape(-1, 5)
+    b = b.reshape(-1, 5)
+    nb = np.linalg.norm(b, axis=0)
+    # a variable below 1e-3 of the largest norm is zero in exact arithmetic:
+    # measure it against the largest variable's norm
+    den = np.where(nb > 1e-3 * nb.max(), nb, nb.max())
+    return np.linalg.norm(a - b, axis=0) / den
+
+
+@pytest.mark.parametrize("p,n,steps", [(1, 12, 60), (3, 8, 60), (5, 8, 100)])
+def test_mixed_matches_fp64_on_vortex(p, n, steps):
+    mesh = dg_b200.periodic_box((n, n, n), (0, 0, 0), (10.0, 10.0, 10.0))
+    f64 = dg_b200.Case(mesh, p, gas_constant=1.0, precision="fp64")
+    mix = dg_b200.Case(mesh, p, gas_constant=1.0, precision="mixed_fp32")
+    U0 = f64.project_ic("IsentropicVortexXY", VORTEX_XY)
+    dt = f64.cfl_time_step(U0, 0.1)
+    mix.set_state(U0)
+    f64.rk4(dt, steps)
+    mix.rk4(dt, steps)
+    d = rel_l2(mix.get_state(), f64.get_state())
+    assert d.max() < TOL, d
+    t = steps * dt
+    e64 = f64.l2_error("IsentropicVortexXY", VORTEX_XY, t)
+    emx = mix.l2_error("IsentropicVortexXY", VORTEX_XY, t)
+    np.testing.assert_allclose(emx[[0, 1, 2, 4]], e64[[0, 1, 2, 4]], rtol=1e-3)
+    assert mix.status() == 0
+
+
+@pytest.mark.parametrize("flux", ["LaxFriedrichs", "HLLC"])
+def test_mixed_residual_is_fp32_accurate(flux):
+    mesh = dg_b200.periodic_box((3, 2, 2), (0, 0, 0), (10.0, 10.0, 10.0), rotate_seed=21)
+    f64 = dg_b200.Case(mesh, 3, flux=flux, gas_constant=1.0)
+    mix = dg_b200.Case(mesh, 3, flux=flux, gas_constant=1.0, precision="mixed_fp32")
+    U = f64.project_ic("IsentropicVortexXY", VORTEX_XY)
+    mix.set_state(U)
+    R64, Rmx = f64.residual(), mix.residual()
+    # FP32 arithmetic on O(1) fluxes: errors of a few ulp of float relative to the flux scale
+    scale = np.abs(R64).max()
+    assert np.abs(Rmx - R64).max() < 1e-5 * scale
+
+
+def test_mixed_free_stream_and_tuner():
+    mesh = dg_b200.periodic_box((4, 3, 2), (0, 0, 0), (1.0, 1.0, 1.0), rotate_seed=3)
+    mix = dg_b200.Case(mesh, 2, flux="HLLC", precision="mixed_fp32")
+    U = mix.project_ic("Uniform", [1.1, 0.2, 0.1, -0.3, 2.6])
+    best, ms = mix.tune_stage(reps=1)
+    variants = mix.stage_variants()
+    assert variants[best][3] == "mixed_fp32"
+    assert all((t < 0) == (v[3] != "mixed_fp32") for v, t in zip(variants, ms))
+    mix.rk4(1e-3, 5)
+    assert np.abs(mix.get_state() - U).max() < 1e-6
