@@ -588,6 +588,9 @@ int dg_create(const dg_case_desc* cd, const dg_mesh_desc* md, dg_ctx** out)
         std::memcpy(g.JD, src.JD, sizeof(g.JD));
         g.inv_djac = src.inv_djac;
         std::memcpy(g.N, src.N, sizeof(g.N));
+        std::memcpy(g.nmag, src.nmag, sizeof(g.nmag));
+        std::memcpy(g.nhat, src.nhat, sizeof(g.nhat));
+        std::memcpy(g.nunit, src.nunit, sizeof(g.nunit));
         std::memcpy(geo_blob.data() + k * sizeof(GeoDev), &g, sizeof(GeoDev));
         std::memcpy(geo_blob.data() + ncls * sizeof(GeoDev) + k * 9 * sizeof(double), src.J, 9 * sizeof(double));
     }

@@ -87,15 +87,45 @@ DG_HD void flux_lax_friedrichs(T gamma, const T* UL, const T* UR, const T* N, T*
     for (int s = 0; s < 5; ++s) F[s] = n_mag * (T(0.5) * (FqL[s] + FqR[s]) - T(0.5) * a * (UR[s] - UL[s]));
 }
 
+// Lax-Friedrichs with the face's normal data precomputed (it is constant on a
+// face of an affine element): n_mag = |N| and n_hat = N / n_mag, evaluated
+// once on the host by the formulas of flux_lax_friedrichs.
+template <typename T>
+DG_HD void flux_lax_friedrichs_n(T gamma, const T* UL, const T* UR, const T* n_hat, T n_mag, T* F)
+{
+    T Fq[15], FqL[5] = {T(0), T(0), T(0), T(0), T(0)}, FqR[5] = {T(0), T(0), T(0), T(0), T(0)};
+    interior_flux(gamma, UL, Fq);
+    for (int s = 0; s < 5; ++s)
+        for (int d = 0; d < 3; ++d) FqL[s] += Fq[s + d * 5] * n_hat[d];
+    interior_flux(gamma, UR, Fq);
+    for (int s = 0; s < 5; ++s)
+        for (int d = 0; d < 3; ++d) FqR[s] += Fq[s + d * 5] * n_hat[d];
+    T a = max_wave_speed(gamma, UL);
+    const T aR = max_wave_speed(gamma, UR);
+    if (aR > a) a = aR;
+    for (int s = 0; s < 5; ++s) F[s] = n_mag * (T(0.5) * (FqL[s] + FqR[s]) - T(0.5) * a * (UR[s] - UL[s]));
+}
+
 // EulerConvNumFluxType::compute_flux_hllc<3>, functions.cpp:298-399.
 // Returns false on the reference's assert branch (no valid wave ordering,
 // e.g. NaN input); F is zeroed then.
+template <typename T>
+DG_HD bool flux_hllc_n(T gam, const T* UL, const T* UR, const T* n, T djac, T* F);
+
 template <typename T>
 DG_HD bool flux_hllc(T gam, const T* UL, const T* UR, const T* N, T* F)
 {
     const T djac = sqrt(N[0] * N[0] + N[1] * N[1] + N[2] * N[2]);
     const T djac1 = T(1.) / djac;
     const T n[3] = {N[0] * djac1, N[1] * djac1, N[2] * djac1};
+    return flux_hllc_n(gam, UL, UR, n, djac, F);
+}
+
+// HLLC with the face's unit normal n = N * (1/|N|) and djac = |N| precomputed
+// by the same operations as in flux_hllc.
+template <typename T>
+DG_HD bool flux_hllc_n(T gam, const T* UL, const T* UR, const T* n, T djac, T* F)
+{
     const T rhoL = UL[0], rhoL1 = T(1.) / rhoL;
     const T unL = (UL[1] * n[0] + UL[2] * n[1] + UL[3] * n[2]) * rhoL1;
     const T PL = pressure(gam, UL);

@@ -62,6 +62,9 @@ struct GeoDev {
     double JD[9];
     double inv_djac;
     double N[6][3];
+    double nmag[6];       // |N| per face
+    double nhat[6][3];    // N / |N| (Lax-Friedrichs)
+    double nunit[6][3];   // N * (1/|N|) (HLLC)
 };
 
 enum StageMode : int {
@@ -119,8 +122,12 @@ struct Lay {
     static constexpr int face = 60 * FS;
     static constexpr int vol = 5 * X2S + cmax(5 * X1S, GV * (3 * X2S + 2 * X1S));
     static constexpr int W = odd(cmax(face, vol));
-    // FP64: U (double-buffered prefetch), residual, U0 and accumulator prefetch
-    static constexpr int per_elem_f64 = 2 * ES + ES + 2 * ES;
+    // FP64 operand region: first the neighbours' boundary slices [30][N2]
+    // (streamed in during the volume phase), then the batch's U0 and RK
+    // accumulator [2][ES] (streamed in during the face phase)
+    static constexpr int OPS = cmax(2 * ES, 30 * N2);
+    // FP64: U (double-buffered prefetch), residual, operand region
+    static constexpr int per_elem_f64 = 2 * ES + ES + OPS;
     // bytes per element, work area in T
     static constexpr size_t bytes_per_elem = sizeof(double) * per_elem_f64 + sizeof(T) * W;
 };
@@ -159,15 +166,17 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // all but the most recent group complete
 __device__ __forceinline__ void cp_async_wait_older() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
-// queue the coefficients of batch e0 of a global state into the padded buffer dst
+// queue the coefficients of batch e0 of a global state into the padded
+// buffer dst (element stride estride)
 template <int P, int G, int E, int NT>
-__device__ __forceinline__ void prefetch_batch(const double* __restrict__ Us, int ne, int e0, double* dst)
+__device__ __forceinline__ void prefetch_batch(const double* __restrict__ Us, int ne, int e0, double* dst,
+                                               int estride)
 {
     using L = Lay<P, G>;
     for (int i = threadIdx.x; i < E * 5 * L::NB; i += NT) {
         const int e = i / (5 * L::NB), r = i - e * (5 * L::NB), v = r / L::NB, b = r - v * L::NB;
         const int ge = min(e0 + e, ne - 1);
-        cp_async8(dst + e * L::ES + v * L::VS + b, Us + (size_t)ge * 5 * L::NB + r);
+        cp_async8(dst + e * estride + v * L::VS + b, Us + (size_t)ge * 5 * L::NB + r);
     }
 }
 
@@ -203,12 +212,12 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
     using L = Lay<P, G, T>;
     constexpr int N = L::N, M = L::M, NB = L::NB, NF = L::NF, N2 = L::N2;
     constexpr int VS = L::VS, ES = L::ES, FS = L::FS, X1S = L::X1S, X2S = L::X2S, W = L::W, GV = L::GV;
+    constexpr int OPS = L::OPS;
     extern __shared__ double smem[];
     double* sUbuf = smem;                  // [2][E][ES]
     double* sRes = sUbuf + 2 * E * ES;     // [E][ES]
-    double* sU0 = sRes + E * ES;           // [E][ES] step-start state of the batch
-    double* sAcc = sU0 + E * ES;           // [E][ES] RK accumulator of the batch
-    T* sW = reinterpret_cast<T*>(sAcc + E * ES);  // [E][W] in the residual's arithmetic
+    double* sOps = sRes + E * ES;          // [E][OPS] neighbour slices, then U0 | acc
+    T* sW = reinterpret_cast<T*>(sOps + E * OPS);  // [E][W] in the residual's arithmetic
     const bool need_u0_acc = a.mode == kModeRK2 || a.mode == kModeRK3 || a.mode == kModeRK4;
     const T* __restrict__ Bt = TabSel<T>::B(a.tab);
     const T* __restrict__ Dt = TabSel<T>::D(a.tab);
@@ -220,133 +229,29 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
     const int stride = gridDim.x * E;
 
     int buf = 0;
-    if (blockIdx.x * E < a.ne) prefetch_batch<P, G, E, NT>(a.Us, a.ne, blockIdx.x * E, sUbuf);
+    if (blockIdx.x * E < a.ne) prefetch_batch<P, G, E, NT>(a.Us, a.ne, blockIdx.x * E, sUbuf, ES);
     cp_async_commit();
 
     for (int e0 = blockIdx.x * E; e0 < a.ne; e0 += stride, buf ^= 1) {
         double* sU = sUbuf + buf * E * ES;
         cp_async_wait_all();
         __syncthreads();
-        // the RK operands of this batch (needed only at the end) and the next
-        // batch's coefficients stream in while this batch computes
-        if (need_u0_acc) {
-            prefetch_batch<P, G, E, NT>(a.U0, a.ne, e0, sU0);
-            prefetch_batch<P, G, E, NT>(a.acc, a.ne, e0, sAcc);
-        }
-        cp_async_commit();
-        if (e0 + stride < a.ne) prefetch_batch<P, G, E, NT>(a.Us, a.ne, e0 + stride, sUbuf + (buf ^ 1) * E * ES);
-        cp_async_commit();
-
-        // ---- own and neighbour traces: one task per (element, face, variable) ----
+        // stream in the neighbours' boundary slices (the periodic face gather)
+        // for the face phase, then the next batch's coefficients
         for (int t = tid; t < E * 30; t += NT) {
-            const int v = t % 5, f = (t / 5) % 6, e = t / 30;
+            const int fv = t % 30, e = t / 30, v = fv % 5, f = fv / 5;
             const int ge = min(e0 + e, a.ne - 1);
             const int2 c = a.conn[ge * 6 + f];
-            const int fn = c.y & 7;
-            T sn[N][N], so[N][N];
-            if (c.x >= e0 && c.x < e0 + E) {
-                const double* src = sU + (c.x - e0) * ES + v * VS;
-#pragma unroll
-                for (int b1 = 0; b1 < N; ++b1)
-#pragma unroll
-                    for (int b0 = 0; b0 < N; ++b0) sn[b1][b0] = T(src[slice_index<N>(fn, b0, b1)]);
-            } else {
-                const double* src = a.Us + ((size_t)c.x * 5 + v) * NB;
-#pragma unroll
-                for (int b1 = 0; b1 < N; ++b1)
-#pragma unroll
-                    for (int b0 = 0; b0 < N; ++b0) sn[b1][b0] = T(__ldg(src + slice_index<N>(fn, b0, b1)));
-            }
-            const double* own = sU + e * ES + v * VS;
+            const double* src = a.Us + ((size_t)c.x * 5 + v) * NB;
+            double* dst = sOps + e * OPS + fv * N2;
 #pragma unroll
             for (int b1 = 0; b1 < N; ++b1)
 #pragma unroll
-                for (int b0 = 0; b0 < N; ++b0) so[b1][b0] = T(own[slice_index<N>(f, b0, b1)]);
-            interp2d<N, M, T>(Bt, so, sW + e * W + (f * 5 + v) * FS);
-            interp2d<N, M, T>(Bt, sn, sW + e * W + 30 * FS + (f * 5 + v) * FS);
+                for (int b0 = 0; b0 < N; ++b0) cp_async8(dst + b1 * N + b0, src + slice_index<N>(c.y & 7, b0, b1));
         }
-        __syncthreads();
-
-        // ---- numerical flux at every face point, written over the own trace ----
-        for (int i = tid; i < E * 6 * NF; i += NT) {
-            const int cidx = i % NF, f = (i / NF) % 6, e = i / (6 * NF);
-            const int ge = min(e0 + e, a.ne - 1);
-            const int2 c = a.conn[ge * 6 + f];
-            const int fn = c.y & 7, isL = (c.y >> 3) & 1, code = c.y >> 4;
-            const int cn = a.cmap[code * NF + cidx];
-            T* Tr = sW + e * W + f * 5 * FS;
-            const T* Tn = sW + e * W + 30 * FS + f * 5 * FS;
-            T Uo[5], Un[5], F[5];
-#pragma unroll
-            for (int v = 0; v < 5; ++v) {
-                Uo[v] = Tr[v * FS + cidx];
-                Un[v] = Tn[v * FS + cn];
-            }
-            const GeoDev* g = a.geo + (isL ? a.geo_class[ge] : a.geo_class[c.x]);
-            const int fl = isL ? f : fn;
-            const T Nv[3] = {T(g->N[fl][0]), T(g->N[fl][1]), T(g->N[fl][2])};
-            T UL[5], UR[5];  // selected element-wise so that both stay in registers
-#pragma unroll
-            for (int v = 0; v < 5; ++v) {
-                UL[v] = isL ? Uo[v] : Un[v];
-                UR[v] = isL ? Un[v] : Uo[v];
-            }
-            if (a.flux == 1) {
-                if (!dgp::flux_hllc(gamma, UL, UR, Nv, F)) status |= kStatusHLLC;
-            } else {
-                dgp::flux_lax_friedrichs(gamma, UL, UR, Nv, F);
-            }
-            const T w = Wt[cidx % M] * Wt[cidx / M];
-            const T sgn = isL ? T(-1.0) : T(1.0);
-#pragma unroll
-            for (int v = 0; v < 5; ++v) Tr[v * FS + cidx] = sgn * (F[v] * w);
-        }
-        __syncthreads();
-
-        // ---- face lift per (element, face, variable) into Tn's space ----
-        for (int t = tid; t < E * 30; t += NT) {
-            const int v = t % 5, f = (t / 5) % 6, e = t / 30;
-            const T* Fq = sW + e * W + (f * 5 + v) * FS;
-            T tmp[M][N];
-#pragma unroll
-            for (int t1 = 0; t1 < M; ++t1)
-#pragma unroll
-                for (int b0 = 0; b0 < N; ++b0) {
-                    T s = T(0);
-#pragma unroll
-                    for (int t0 = 0; t0 < M; ++t0) s += Bt[t0 * N + b0] * Fq[t1 * M + t0];
-                    tmp[t1][b0] = s;
-                }
-            T* Lf = sW + e * W + 30 * FS + (f * 5 + v) * FS;
-#pragma unroll
-            for (int b1 = 0; b1 < N; ++b1)
-#pragma unroll
-                for (int b0 = 0; b0 < N; ++b0) {
-                    T s = T(0);
-#pragma unroll
-                    for (int t1 = 0; t1 < M; ++t1) s += Bt[t1 * N + b1] * tmp[t1][b0];
-                    Lf[b1 * N + b0] = s;
-                }
-        }
-        __syncthreads();
-        // gather the six face contributions into the (FP64) residual
-        for (int i = tid; i < E * 5 * NB; i += NT) {
-            const int b = i % NB, v = (i / NB) % 5, e = i / (5 * NB);
-            const int bc[3] = {b % N, (b / N) % N, b / N2};
-            const T* Lf = sW + e * W + 30 * FS + v * FS;
-            double s = 0.0;
-#pragma unroll
-            for (int f = 0; f < 6; ++f) {
-                const int ax = face_axis(f), sidx = face_side(f) ? N - 1 : 0;
-                if (bc[ax] == sidx) {
-                    const int b0 = ax == 0 ? bc[1] : bc[0];
-                    const int b1 = ax == 2 ? bc[1] : bc[2];
-                    s += double(Lf[f * 5 * FS + b1 * N + b0]);
-                }
-            }
-            sRes[e * ES + v * VS + b] = s;
-        }
-        __syncthreads();
+        cp_async_commit();
+        if (e0 + stride < a.ne) prefetch_batch<P, G, E, NT>(a.Us, a.ne, e0 + stride, sUbuf + (buf ^ 1) * E * ES, ES);
+        cp_async_commit();
 
         // ---- volume: interpolation passes x, y ----
         T* X2 = sW;               // per element: [5][X2S] with [bz][qy][qx]
@@ -482,7 +387,7 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
                 }
             }
             __syncthreads();
-            // x contraction into the (FP64) residual: res += Dx^T C0 + Bx^T C12
+            // x contraction into the (FP64) residual: res = Dx^T C0 + Bx^T C12
             for (int i = tid; i < E * gnv * N2; i += NT) {
                 const int vv = i % gnv, byz = (i / gnv) % N2, e = i / (gnv * N2);
                 const T* C0 = Cbuf + e * W + (vv * 2) * X1S + byz * M;
@@ -498,10 +403,135 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
                 }
                 double* res = sRes + e * ES + (gv0 + vv) * VS + byz * N;
 #pragma unroll
-                for (int bx = 0; bx < N; ++bx) res[bx] += double(r[bx]);
+                for (int bx = 0; bx < N; ++bx) res[bx] = double(r[bx]);
             }
             __syncthreads();
         }
+
+        // ---- faces: the neighbours' slices have landed (the next batch's
+        //      coefficients may still be in flight) ----
+        cp_async_wait_older();
+        __syncthreads();
+        // own and neighbour traces: one task per (element, face, variable)
+        for (int t = tid; t < E * 30; t += NT) {
+            const int v = t % 5, f = (t / 5) % 6, e = t / 30;
+            T sn[N][N], so[N][N];
+            const double* nb = sOps + e * OPS + (f * 5 + v) * N2;
+            const double* own = sU + e * ES + v * VS;
+#pragma unroll
+            for (int b1 = 0; b1 < N; ++b1)
+#pragma unroll
+                for (int b0 = 0; b0 < N; ++b0) {
+                    sn[b1][b0] = T(nb[b1 * N + b0]);
+                    so[b1][b0] = T(own[slice_index<N>(f, b0, b1)]);
+                }
+            interp2d<N, M, T>(Bt, so, sW + e * W + (f * 5 + v) * FS);
+            interp2d<N, M, T>(Bt, sn, sW + e * W + 30 * FS + (f * 5 + v) * FS);
+        }
+        __syncthreads();
+        // the staging area is free: stream in this batch's RK operands
+        if (need_u0_acc) {
+            prefetch_batch<P, G, E, NT>(a.U0, a.ne, e0, sOps, OPS);
+            prefetch_batch<P, G, E, NT>(a.acc, a.ne, e0, sOps + ES, OPS);
+        }
+        cp_async_commit();
+
+        // numerical flux at every face point, written over the own trace; two
+        // points per thread and iteration for instruction-level parallelism
+        {
+            constexpr int total = E * 6 * NF;
+            auto point = [&](int i, T (&Fo)[5], int& off) {
+                const int cidx = i % NF, f = (i / NF) % 6, e = i / (6 * NF);
+                const int ge = min(e0 + e, a.ne - 1);
+                const int2 c = a.conn[ge * 6 + f];
+                const int fn = c.y & 7, isL = (c.y >> 3) & 1, code = c.y >> 4;
+                const int cn = a.cmap[code * NF + cidx];
+                const T* Tr = sW + e * W + f * 5 * FS;
+                const T* Tn = sW + e * W + 30 * FS + f * 5 * FS;
+                T UL[5], UR[5];
+#pragma unroll
+                for (int v = 0; v < 5; ++v) {
+                    const T uo = Tr[v * FS + cidx], un = Tn[v * FS + cn];
+                    UL[v] = isL ? uo : un;  // element-wise selects keep both in registers
+                    UR[v] = isL ? un : uo;
+                }
+                // the normal is the left element's (helpers.cpp:440-446)
+                const GeoDev* g = a.geo + (isL ? a.geo_class[ge] : a.geo_class[c.x]);
+                const int fl = isL ? f : fn;
+                const T nmag = T(g->nmag[fl]);
+                if (a.flux == 1) {
+                    const T nu[3] = {T(g->nunit[fl][0]), T(g->nunit[fl][1]), T(g->nunit[fl][2])};
+                    if (!dgp::flux_hllc_n(gamma, UL, UR, nu, nmag, Fo)) status |= kStatusHLLC;
+                } else {
+                    const T nh[3] = {T(g->nhat[fl][0]), T(g->nhat[fl][1]), T(g->nhat[fl][2])};
+                    dgp::flux_lax_friedrichs_n(gamma, UL, UR, nh, nmag, Fo);
+                }
+                const T w = Wt[cidx % M] * Wt[cidx / M];
+                const T sgn = isL ? T(-1.0) : T(1.0);
+#pragma unroll
+                for (int v = 0; v < 5; ++v) Fo[v] = sgn * (Fo[v] * w);
+                off = e * W + f * 5 * FS + cidx;
+            };
+            for (int i0 = tid; i0 < total; i0 += 2 * NT) {
+                const int i1 = i0 + NT;
+                T F0[5], F1[5];
+                int o0, o1;
+                point(i0, F0, o0);
+                point(i1 < total ? i1 : i0, F1, o1);
+#pragma unroll
+                for (int v = 0; v < 5; ++v) sW[o0 + v * FS] = F0[v];
+                if (i1 < total) {
+#pragma unroll
+                    for (int v = 0; v < 5; ++v) sW[o1 + v * FS] = F1[v];
+                }
+            }
+        }
+        __syncthreads();
+
+        // face lift per (element, face, variable) into Tn's space
+        for (int t = tid; t < E * 30; t += NT) {
+            const int v = t % 5, f = (t / 5) % 6, e = t / 30;
+            const T* Fq = sW + e * W + (f * 5 + v) * FS;
+            T tmp[M][N];
+#pragma unroll
+            for (int t1 = 0; t1 < M; ++t1)
+#pragma unroll
+                for (int b0 = 0; b0 < N; ++b0) {
+                    T s = T(0);
+#pragma unroll
+                    for (int t0 = 0; t0 < M; ++t0) s += Bt[t0 * N + b0] * Fq[t1 * M + t0];
+                    tmp[t1][b0] = s;
+                }
+            T* Lf = sW + e * W + 30 * FS + (f * 5 + v) * FS;
+#pragma unroll
+            for (int b1 = 0; b1 < N; ++b1)
+#pragma unroll
+                for (int b0 = 0; b0 < N; ++b0) {
+                    T s = T(0);
+#pragma unroll
+                    for (int t1 = 0; t1 < M; ++t1) s += Bt[t1 * N + b1] * tmp[t1][b0];
+                    Lf[b1 * N + b0] = s;
+                }
+        }
+        __syncthreads();
+        // add the six face contributions to the (FP64) residual
+        for (int i = tid; i < E * 5 * NB; i += NT) {
+            const int b = i % NB, v = (i / NB) % 5, e = i / (5 * NB);
+            const int bc[3] = {b % N, (b / N) % N, b / N2};
+            const T* Lf = sW + e * W + 30 * FS + v * FS;
+            double s = 0.0;
+#pragma unroll
+            for (int f = 0; f < 6; ++f) {
+                const int ax = face_axis(f), sidx = face_side(f) ? N - 1 : 0;
+                if (bc[ax] == sidx) {
+                    const int b0 = ax == 0 ? bc[1] : bc[0];
+                    const int b1 = ax == 2 ? bc[1] : bc[2];
+                    s += double(Lf[f * 5 * FS + b1 * N + b0]);
+                }
+            }
+            sRes[e * ES + v * VS + b] += s;
+        }
+        __syncthreads();
 
         if (a.mode == kModeResidual) {
             for (int i = tid; i < E * 5 * NB; i += NT) {
@@ -541,19 +571,19 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
                 r[j * N] = s;
             }
         }
-        cp_async_wait_older();  // this batch's U0 / accumulator have landed
+        cp_async_wait_all();  // this batch's U0 / accumulator have landed
         __syncthreads();
         for (int i = tid; i < E * 5 * N2; i += NT) {
             const int bxy = i % N2, ev = i / N2, e = ev / 5;
             if (e0 + e >= a.ne) continue;
             const int ge = e0 + e;
             const double scale = a.dt * a.geo[a.geo_class[ge]].inv_djac;
-            const int soff = e * ES + (ev % 5) * VS + bxy;
-            const double* r = sRes + soff;  // pencil along z
+            const int v = ev % 5;
+            const double* r = sRes + e * ES + v * VS + bxy;  // pencil along z
             // step-start state: the prefetched U0, or the stage state itself in
             // RK1 / FE where the two coincide
-            const double* u0 = (need_u0_acc ? sU0 : sU) + soff;
-            const double* ac = sAcc + soff;
+            const double* u0 = (need_u0_acc ? sOps + e * OPS : sU + e * ES) + v * VS + bxy;
+            const double* ac = sOps + e * OPS + ES + v * VS + bxy;
             double t[N];
 #pragma unroll
             for (int k = 0; k < N; ++k) t[k] = r[k * N2];

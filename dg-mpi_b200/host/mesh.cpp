@@ -265,6 +265,15 @@ std::string prepare_mesh(const MeshView& mv, int m, PreparedMesh& out)
             g.N[f][0] = t1[1] * t2[2] - t1[2] * t2[1];
             g.N[f][1] = t1[2] * t2[0] - t1[0] * t2[2];
             g.N[f][2] = t1[0] * t2[1] - t1[1] * t2[0];
+            double nm = 0.0;
+            for (int d = 0; d < 3; ++d) nm += g.N[f][d] * g.N[f][d];
+            nm = std::sqrt(nm);
+            const double inv = 1. / nm;
+            g.nmag[f] = nm;
+            for (int d = 0; d < 3; ++d) {
+                g.nhat[f][d] = g.N[f][d] / nm;
+                g.nunit[f][d] = g.N[f][d] * inv;
+            }
         }
         const int cid = static_cast<int>(out.classes.size());
         out.classes.push_back(g);

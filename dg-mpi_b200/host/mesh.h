@@ -35,6 +35,11 @@ struct GeoClass {
     double djac;      // det J
     double inv_djac;  // 1 / det J
     double N[6][3];   // unnormalised outward normal of each reference face
+    // the numerical fluxes' per-face normal data (base/functions.cpp:40-49,
+    // euler/functions.cpp:309-311): |N|, N / |N| and N * (1 / |N|)
+    double nmag[6];
+    double nhat[6][3];
+    double nunit[6][3];
 };
 
 // Everything the kernels need besides the state.
