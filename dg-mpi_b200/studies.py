@@ -1,0 +1,104 @@
+#!/usr/bin/env python
+"""Accuracy / precision studies of the configurations beyond the bench workload.
+
+  python dg-mpi_b200/studies.py precision   # 64^3, p=5, x-y vortex, 500 RK4 steps
+  python dg-mpi_b200/studies.py taylor_green # 96^3, p=4, Taylor-Green, 200 RK4 steps
+  python dg-mpi_b200/studies.py <name> --scale 0.25  # smaller mesh, same order
+
+Each study runs the FP64 path and the mixed-precision path (FP32 residual,
+FP64 state) from the same projected initial condition and prints one JSON line:
+per-variable relative L2 difference mixed vs FP64, L2 error of both against the
+exact advected vortex (precision) or the kinetic-energy histories of both
+(Taylor-Green), and the device-timed DOF-stage update rate of both paths.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import sys
+import time
+
+import numpy as np
+
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+import dg_b200  # noqa: E402
+
+VORTEX = [1.0, 1.0, 1.0, 1.0, 5.0, 5.0, 5.0, 10.0, 10.0]
+
+
+def rel_l2(a, b):
+    a = a.reshape(-1, 5)
+    b = b.reshape(-1, 5)
+    nb = np.linalg.norm(b, axis=0)
+    den = np.where(nb > 1e-3 * nb.max(), nb, nb.max())  # zero-in-exact-arithmetic fields
+    return (np.linalg.norm(a - b, axis=0) / den).tolist()
+
+
+def run_pair(mesh, order, ic, data, steps, cfl, ke_every=0):
+    cases = {p: dg_b200.Case(mesh, order, flux="LaxFriedrichs", gas_constant=1.0, precision=p)
+             for p in ("fp64", "mixed_fp32")}
+    t0 = time.perf_counter()
+    U0 = cases["fp64"].project_ic(ic, data)
+    setup_s = time.perf_counter() - t0
+    dt = cases["fp64"].cfl_time_step(U0, cfl)
+    out = {"dt": dt, "steps": steps, "ic_projection_s": setup_s}
+    for name, case in cases.items():
+        case.set_state(U0)
+        best, _ = case.tune_stage(reps=1)
+        case.set_state(U0)
+        hist, ms_total, done = [], 0.0, 0
+        chunk = ke_every if ke_every else steps
+        if ke_every:
+            hist.append(case.kinetic_energy())
+        while done < steps:
+            n = min(chunk, steps - done)
+            ms_total += case.rk4_timed(dt, n)
+            done += n
+            if ke_every:
+                hist.append(case.kinetic_energy())
+        dof = case.ne * case.nb * 5
+        out[name] = {"dof_stage_per_s": dof * 4 * steps / (ms_total / 1e3), "ms_per_step": ms_total / steps,
+                     "stage_variant": case.stage_variants()[best], "status": case.status()}
+        if ke_every:
+            out[name]["kinetic_energy"] = hist
+    out["rel_l2_mixed_vs_fp64"] = rel_l2(cases["mixed_fp32"].get_state(), cases["fp64"].get_state())
+    return cases, out
+
+
+def precision(scale: float):
+    n = max(4, int(round(64 * scale)))
+    mesh = dg_b200.periodic_box((n, n, n), (0, 0, 0), (10.0, 10.0, 10.0))
+    cases, out = run_pair(mesh, 5, "IsentropicVortexXY", VORTEX, 500, 0.1)
+    t = out["steps"] * out["dt"]
+    for name, case in cases.items():
+        out[name]["l2_error_vs_exact"] = case.l2_error("IsentropicVortexXY", VORTEX, t).tolist()
+    out.update({"config": f"x-y isentropic vortex, [0,10]^3, {n}^3 hex, p=5, LF flux, RK4 CFL 0.1", "time": t})
+    return out
+
+
+def taylor_green(scale: float):
+    n = max(4, int(round(96 * scale)))
+    L = 2 * math.pi
+    mesh = dg_b200.periodic_box((n, n, n), (0, 0, 0), (L, L, L))
+    cases, out = run_pair(mesh, 4, "TaylorGreen", [0.1], 200, 0.1, ke_every=20)
+    k64 = np.array(out["fp64"]["kinetic_energy"])
+    kmx = np.array(out["mixed_fp32"]["kinetic_energy"])
+    out["ke_max_rel_diff"] = float(np.max(np.abs(kmx - k64) / np.abs(k64)))
+    out.update({"config": f"Taylor-Green, [0,2pi]^3, {n}^3 hex, p=4, Mach 0.1, LF flux, RK4 CFL 0.1"})
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("study", choices=["precision", "taylor_green"])
+    ap.add_argument("--scale", type=float, default=1.0)
+    args = ap.parse_args()
+    res = precision(args.scale) if args.study == "precision" else taylor_green(args.scale)
+    res["study"] = args.study
+    print(json.dumps(res), flush=True)
+
+
+if __name__ == "__main__":
+    main()
