@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -11,11 +12,8 @@
 #include <string>
 #include <vector>
 
-#include "../../include/dg_b200.h"
 #include "../host/case.h"
-#include "../host/mesh.h"
-#include "../host/numerics.h"
-#include "dg_stage.cuh"
+#include "dg_ctx.cuh"
 
 using dgk::GeoDev;
 using dgk::StageArgs;
@@ -35,8 +33,6 @@ int dgk::stage_variants(int p, const StageVariant** out)
 
 namespace {
 
-constexpr int kMaxVariants = 16;  // launch variants per order (checked in prepare_variant)
-
 // tables of the IC / error rule (2*max(p,1)+2 points) and of the volume rule,
 // used by the reductions
 constexpr int kMaxMe = 12;
@@ -53,32 +49,7 @@ thread_local std::string g_create_error;
 
 }  // namespace
 
-struct dg_ctx {
-    int device = 0, p = 0, nb = 0, ne = 0, flux = 0, precision = 0;
-    double gamma = 1.4, R = 287.05;
-    cudaStream_t stream = nullptr;
-    double *d_U0 = nullptr, *d_Ua = nullptr, *d_Ub = nullptr, *d_acc = nullptr, *d_out = nullptr;
-    int2* d_conn = nullptr;
-    int* d_geo_class = nullptr;
-    GeoDev* d_geo = nullptr;
-    uint8_t* d_cmap = nullptr;
-    double* d_X0 = nullptr;
-    double* d_partials = nullptr;
-    unsigned* d_status = nullptr;
-    int red_grid = 0;
-    int variant = 0;                          // index into dgk::stage_variants(p)
-    int variant_grid[kMaxVariants] = {};      // persistent grid per variant, 0 = not prepared
-    dgk::StageTables stage_tab{};
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t graph_exec = nullptr;
-    double graph_dt = 0.0;
-    dgh::PreparedMesh pm;
-    dgh::Tables1D tab;
-    unsigned status_accum = 0;
-    std::string err;
-};
-
-namespace {
+namespace dgi {
 
 int fail(dg_ctx* c, int code, const std::string& msg)
 {
@@ -86,13 +57,6 @@ int fail(dg_ctx* c, int code, const std::string& msg)
     else g_create_error = msg;
     return code;
 }
-
-#define DG_CUDA(c, call)                                                                         \
-    do {                                                                                         \
-        cudaError_t e_ = (call);                                                                 \
-        if (e_ != cudaSuccess)                                                                   \
-            return fail((c), DG_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));   \
-    } while (0)
 
 int load_constant_tables(dg_ctx* c)
 {
@@ -284,19 +248,20 @@ __global__ void __launch_bounds__(256) reduce_kernel(ReduceArgs a)
         for (int v = 0; v < 5; ++v) a.partials[blockIdx.x * 5 + v] = red[v][0];
 }
 
-int run_reduce(dg_ctx* c, int kind, int ic_type, const double* data, int ndata, double t, double* out5)
+int run_reduce(dg_ctx* c, int kind, int ic_type, const double* data, int ndata, double t, double* out5, int e0, int ne,
+               double gamma, double R)
 {
     ReduceArgs a{};
-    a.U = c->d_U0;
-    a.geo_class = c->d_geo_class;
+    a.U = c->d_U0 + static_cast<size_t>(e0) * 5 * c->nb;
+    a.geo_class = c->d_geo_class + e0;
     a.geo = c->d_geo;
-    a.X0 = c->d_X0;
+    a.X0 = c->d_X0 + static_cast<size_t>(e0) * 3;
     a.partials = c->d_partials;
-    a.ne = c->ne;
+    a.ne = ne;
     a.ic_type = ic_type;
     a.kind = kind;
-    a.gamma = c->gamma;
-    a.R = c->R;
+    a.gamma = gamma;
+    a.R = R;
     a.t = t;
     for (int i = 0; i < ndata && i < 16; ++i) a.data[i] = data[i];
     // per-class Jacobians, kept on the device after the classes
@@ -427,24 +392,52 @@ int check_status(dg_ctx* c)
     return DG_OK;
 }
 
-int upload_state_host_layout(dg_ctx* c, const double* Uc, double* dst)
+int upload_range(dg_ctx* c, const double* Uc, double* dst, int e0, int ne)
 {
-    const size_t n = static_cast<size_t>(c->ne) * c->nb * 5;
-    DG_CUDA(c, cudaMemcpyAsync(c->d_out, Uc, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-    to_device_layout<<<1024, 256, 0, c->stream>>>(c->d_out, dst, (long long)n, c->nb);
+    const size_t n = static_cast<size_t>(ne) * c->nb * 5, off = static_cast<size_t>(e0) * c->nb * 5;
+    if (n == 0) return DG_OK;
+    DG_CUDA(c, cudaMemcpyAsync(c->d_out + off, Uc, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    to_device_layout<<<1024, 256, 0, c->stream>>>(c->d_out + off, dst + off, (long long)n, c->nb);
     DG_CUDA(c, cudaGetLastError());
     DG_CUDA(c, cudaStreamSynchronize(c->stream));
     return DG_OK;
 }
 
-int download_host_layout(dg_ctx* c, const double* src, double* Uc)
+int download_range(dg_ctx* c, const double* src, double* Uc, int e0, int ne)
 {
-    const size_t n = static_cast<size_t>(c->ne) * c->nb * 5;
-    to_host_layout<<<1024, 256, 0, c->stream>>>(src, c->d_acc == src ? c->d_out : c->d_Ub, (long long)n, c->nb);
+    const size_t n = static_cast<size_t>(ne) * c->nb * 5, off = static_cast<size_t>(e0) * c->nb * 5;
+    if (n == 0) return DG_OK;
+    double* stage = (c->d_acc == src ? c->d_out : c->d_Ub) + off;
+    to_host_layout<<<1024, 256, 0, c->stream>>>(src + off, stage, (long long)n, c->nb);
     DG_CUDA(c, cudaGetLastError());
-    DG_CUDA(c, cudaMemcpyAsync(Uc, c->d_acc == src ? c->d_out : c->d_Ub, n * sizeof(double), cudaMemcpyDeviceToHost,
-                               c->stream));
+    DG_CUDA(c, cudaMemcpyAsync(Uc, stage, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     DG_CUDA(c, cudaStreamSynchronize(c->stream));
+    return DG_OK;
+}
+
+int upload_state_host_layout(dg_ctx* c, const double* Uc, double* dst) { return upload_range(c, Uc, dst, 0, c->ne); }
+int download_host_layout(dg_ctx* c, const double* src, double* Uc) { return download_range(c, src, Uc, 0, c->ne); }
+
+int upload_geometry(dg_ctx* c, const double* dtf, cudaStream_t s)
+{
+    // geometry classes, followed by their Jacobians (used by the reductions)
+    const size_t ncls = c->pm.classes.size();
+    std::vector<unsigned char> blob(ncls * (sizeof(GeoDev) + 9 * sizeof(double)));
+    for (size_t k = 0; k < ncls; ++k) {
+        GeoDev g{};
+        const auto& src = c->pm.classes[k];
+        std::memcpy(g.JD, src.JD, sizeof(g.JD));
+        g.inv_djac = src.inv_djac;
+        g.dtf = dtf ? dtf[k] : 1.0;
+        std::memcpy(g.N, src.N, sizeof(g.N));
+        std::memcpy(g.nmag, src.nmag, sizeof(g.nmag));
+        std::memcpy(g.nhat, src.nhat, sizeof(g.nhat));
+        std::memcpy(g.nunit, src.nunit, sizeof(g.nunit));
+        std::memcpy(blob.data() + k * sizeof(GeoDev), &g, sizeof(GeoDev));
+        std::memcpy(blob.data() + ncls * sizeof(GeoDev) + k * 9 * sizeof(double), src.J, 9 * sizeof(double));
+    }
+    DG_CUDA(c, cudaMemcpyAsync(c->d_geo, blob.data(), blob.size(), cudaMemcpyHostToDevice, s));
+    DG_CUDA(c, cudaStreamSynchronize(s));
     return DG_OK;
 }
 
@@ -460,12 +453,11 @@ void release(dg_ctx* c)
     if (c->stream) cudaStreamDestroy(c->stream);
 }
 
-}  // namespace
+}  // namespace dgi
 
-// ===========================================================================
-extern "C" {
+using namespace dgi;
 
-int dg_create(const dg_case_desc* cd, const dg_mesh_desc* md, dg_ctx** out)
+int dgi::create_ctx(const dg_case_desc* cd, const dg_mesh_desc* md, const int* elem_tag, dg_ctx** out)
 {
     g_create_error.clear();
     if (!cd || !md || !out) return fail(nullptr, DG_ERR_ARG, "dg_create: null argument");
@@ -494,6 +486,7 @@ int dg_create(const dg_case_desc* cd, const dg_mesh_desc* md, dg_ctx** out)
     mv.coords = md->node_coords;
     mv.e2n = md->elem_to_node_ids;
     mv.faces = md->interior_faces;
+    mv.tag = elem_tag;
     std::string perr;
     try {
         perr = dgh::prepare_mesh(mv, c->p + 2, c->pm);
@@ -580,24 +573,9 @@ int dg_create(const dg_case_desc* cd, const dg_mesh_desc* md, dg_ctx** out)
             return bail(DG_ERR_NOMEM);
         }
     }
-    // geometry classes, followed by their Jacobians (used by the reductions)
-    std::vector<unsigned char> geo_blob(ncls * (sizeof(GeoDev) + 9 * sizeof(double)));
-    for (size_t k = 0; k < ncls; ++k) {
-        GeoDev g{};
-        const auto& src = c->pm.classes[k];
-        std::memcpy(g.JD, src.JD, sizeof(g.JD));
-        g.inv_djac = src.inv_djac;
-        std::memcpy(g.N, src.N, sizeof(g.N));
-        std::memcpy(g.nmag, src.nmag, sizeof(g.nmag));
-        std::memcpy(g.nhat, src.nhat, sizeof(g.nhat));
-        std::memcpy(g.nunit, src.nunit, sizeof(g.nunit));
-        std::memcpy(geo_blob.data() + k * sizeof(GeoDev), &g, sizeof(GeoDev));
-        std::memcpy(geo_blob.data() + ncls * sizeof(GeoDev) + k * 9 * sizeof(double), src.J, 9 * sizeof(double));
-    }
     std::vector<int2> conn(static_cast<size_t>(c->ne) * 6);
     for (size_t i = 0; i < conn.size(); ++i) conn[i] = make_int2(c->pm.conn[i * 2], c->pm.conn[i * 2 + 1]);
-    bool ok = cudaMemcpy(c->d_geo, geo_blob.data(), geo_blob.size(), cudaMemcpyHostToDevice) == cudaSuccess &&
-              cudaMemcpy(c->d_conn, conn.data(), conn.size() * sizeof(int2), cudaMemcpyHostToDevice) == cudaSuccess &&
+    bool ok = cudaMemcpy(c->d_conn, conn.data(), conn.size() * sizeof(int2), cudaMemcpyHostToDevice) == cudaSuccess &&
               cudaMemcpy(c->d_geo_class, c->pm.geo_class.data(), c->ne * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess &&
               cudaMemcpy(c->d_X0, c->pm.X0.data(), c->pm.X0.size() * sizeof(double), cudaMemcpyHostToDevice) == cudaSuccess &&
               (c->pm.cmap.empty() || cudaMemcpy(c->d_cmap, c->pm.cmap.data(), c->pm.cmap.size(), cudaMemcpyHostToDevice) == cudaSuccess) &&
@@ -608,16 +586,27 @@ int dg_create(const dg_case_desc* cd, const dg_mesh_desc* md, dg_ctx** out)
         c->err = std::string("table upload failed: ") + cudaGetErrorString(cudaGetLastError());
         return bail(DG_ERR_CUDA);
     }
+    if ((rc = upload_geometry(c, nullptr, c->stream)) != DG_OK) return bail(rc);
     *out = c;
     return DG_OK;
 }
 
-void dg_destroy(dg_ctx* ctx)
+void dgi::destroy_ctx(dg_ctx* c)
 {
-    if (!ctx) return;
-    release(ctx);
-    delete ctx;
+    if (!c) return;
+    release(c);
+    delete c;
 }
+
+// ===========================================================================
+extern "C" {
+
+int dg_create(const dg_case_desc* cd, const dg_mesh_desc* md, dg_ctx** out)
+{
+    return create_ctx(cd, md, nullptr, out);
+}
+
+void dg_destroy(dg_ctx* ctx) { destroy_ctx(ctx); }
 
 const char* dg_last_error(const dg_ctx* ctx)
 {
@@ -841,7 +830,7 @@ int dg_l2_error(dg_ctx* c, int ic_type, const double* data, int ndata, double t,
     if (ic_type < DG_IC_UNIFORM || ic_type > DG_IC_TAYLOR_GREEN) return fail(c, DG_ERR_ARG, "unknown exact solution");
     DG_CUDA(c, cudaSetDevice(c->device));
     double sums[5];
-    int rc = run_reduce(c, 0, ic_type, data, ndata, t, sums);
+    int rc = run_reduce(c, 0, ic_type, data, ndata, t, sums, 0, c->ne, c->gamma, c->R);
     if (rc) return rc;
     for (int v = 0; v < 5; ++v) err[v] = std::sqrt(sums[v] / c->pm.volume);
     return DG_OK;
@@ -852,7 +841,7 @@ int dg_kinetic_energy(dg_ctx* c, double* ke)
     if (!c || !ke) return fail(c, DG_ERR_ARG, "dg_kinetic_energy: null argument");
     DG_CUDA(c, cudaSetDevice(c->device));
     double sums[5];
-    int rc = run_reduce(c, 1, 0, nullptr, 0, 0.0, sums);
+    int rc = run_reduce(c, 1, 0, nullptr, 0, 0.0, sums, 0, c->ne, c->gamma, c->R);
     if (rc) return rc;
     *ke = sums[0] / c->pm.volume;
     return DG_OK;

@@ -1,0 +1,80 @@
+// dg_ctx.cuh -- the context behind the C ABI's dg_ctx handle and the internal
+// helpers shared by the single-case entry points (dg_capi.cu) and the batched
+// ensembles (dg_batch.cu).  Not part of the public interface.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "../../include/dg_b200.h"
+#include "../host/mesh.h"
+#include "../host/numerics.h"
+#include "dg_stage.cuh"
+
+namespace dgi {
+constexpr int kMaxVariants = 16;  // launch variants per order (checked in prepare_variant)
+}
+
+struct dg_ctx {
+    int device = 0, p = 0, nb = 0, ne = 0, flux = 0, precision = 0;
+    double gamma = 1.4, R = 287.05;
+    cudaStream_t stream = nullptr;
+    double *d_U0 = nullptr, *d_Ua = nullptr, *d_Ub = nullptr, *d_acc = nullptr, *d_out = nullptr;
+    int2* d_conn = nullptr;
+    int* d_geo_class = nullptr;
+    dgk::GeoDev* d_geo = nullptr;
+    uint8_t* d_cmap = nullptr;
+    double* d_X0 = nullptr;
+    double* d_partials = nullptr;
+    unsigned* d_status = nullptr;
+    int red_grid = 0;
+    int variant = 0;                                // index into dgk::stage_variants(p)
+    int variant_grid[dgi::kMaxVariants] = {};       // persistent grid per variant, 0 = not prepared
+    dgk::StageTables stage_tab{};
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    double graph_dt = 0.0;
+    dgh::PreparedMesh pm;
+    dgh::Tables1D tab;
+    unsigned status_accum = 0;
+    std::string err;
+};
+
+namespace dgi {
+
+// records msg in the context (or, for c == nullptr, in the thread's creation
+// error) and returns code
+int fail(dg_ctx* c, int code, const std::string& msg);
+
+#define DG_CUDA(c, call)                                                                         \
+    do {                                                                                         \
+        cudaError_t e_ = (call);                                                                 \
+        if (e_ != cudaSuccess)                                                                   \
+            return ::dgi::fail((c), DG_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+// dg_create with an optional per-element tag: elements with different tags
+// never share a geometry class (each class then carries one case's time step)
+int create_ctx(const dg_case_desc* cd, const dg_mesh_desc* md, const int* elem_tag, dg_ctx** out);
+void destroy_ctx(dg_ctx* c);
+
+int prepare_variant(dg_ctx* c, int v);
+bool variant_matches(const dg_ctx* c, int v);
+int launch_stage(dg_ctx* c, int mode, const double* Us, const double* U0, double* out, double dt);
+int check_status(dg_ctx* c);
+
+// state of elements [e0, e0 + ne) between the host layout [ne][nb][5] and the
+// device layout [ne][5][nb] (staged through d_out / d_Ub); synchronous
+int upload_range(dg_ctx* c, const double* Uc, double* dst, int e0, int ne);
+int download_range(dg_ctx* c, const double* src, double* Uc, int e0, int ne);
+
+// kind 0: sum over [e0, e0+ne) of the squared error against an exact solution
+// per variable; kind 1: kinetic energy (out5[0]); deterministic order
+int run_reduce(dg_ctx* c, int kind, int ic_type, const double* data, int ndata, double t, double* out5, int e0, int ne,
+               double gamma, double R);
+
+// uploads the geometry classes with per-class time-step factors dtf[class]
+// (nullptr: all 1)
+int upload_geometry(dg_ctx* c, const double* dtf, cudaStream_t s);
+
+}  // namespace dgi

@@ -61,6 +61,7 @@ template <> struct TabSel<float> {
 struct GeoDev {
     double JD[9];
     double inv_djac;
+    double dtf;           // time-step factor: the stage update scales by dt * dtf (1, or a case's dt in a batch)
     double N[6][3];
     double nmag[6];       // |N| per face
     double nhat[6][3];    // N / |N| (Lax-Friedrichs)
@@ -577,7 +578,8 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
             const int bxy = i % N2, ev = i / N2, e = ev / 5;
             if (e0 + e >= a.ne) continue;
             const int ge = e0 + e;
-            const double scale = a.dt * a.geo[a.geo_class[ge]].inv_djac;
+            const GeoDev& gg = a.geo[a.geo_class[ge]];
+            const double scale = a.dt * gg.dtf * gg.inv_djac;
             const int v = ev % 5;
             const double* r = sRes + e * ES + v * VS + bxy;  // pencil along z
             // step-start state: the prefetched U0, or the stage state itself in

@@ -94,6 +94,23 @@ def library(path: str | None = None) -> ctypes.CDLL:
         "dg_set_stage_variant": (ctypes.c_int, [vp, ctypes.c_int]),
         "dg_get_stage_variant": (ctypes.c_int, [vp]),
         "dg_tune_stage": (ctypes.c_int, [vp, ctypes.c_int, ip, dp]),
+        "dg_batch_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_CaseDesc), ctypes.POINTER(_MeshDesc),
+                                           ctypes.POINTER(vp)]),
+        "dg_batch_destroy": (None, [vp]),
+        "dg_batch_last_error": (ctypes.c_char_p, [vp]),
+        "dg_batch_num_groups": (ctypes.c_int, [vp]),
+        "dg_batch_group_info": (ctypes.c_int, [vp, ctypes.c_int, ip, ip, ip, ip]),
+        "dg_batch_case_info": (ctypes.c_int, [vp, ctypes.c_int, ip, ip, ip, dp]),
+        "dg_batch_set_state": (ctypes.c_int, [vp, ctypes.c_int, dp]),
+        "dg_batch_get_state": (ctypes.c_int, [vp, ctypes.c_int, dp]),
+        "dg_batch_project_ic": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, dp, ctypes.c_int, ctypes.c_double, dp]),
+        "dg_batch_cfl_time_step": (ctypes.c_int, [vp, ctypes.c_int, dp, ctypes.c_double, dp]),
+        "dg_batch_set_time_step": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_double]),
+        "dg_batch_rk4_steps": (ctypes.c_int, [vp, ctypes.c_int]),
+        "dg_batch_rk4_steps_timed": (ctypes.c_int, [vp, ctypes.c_int, dp]),
+        "dg_batch_tune": (ctypes.c_int, [vp, ctypes.c_int]),
+        "dg_batch_l2_error": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, dp, ctypes.c_int, ctypes.c_double, dp]),
+        "dg_batch_status": (ctypes.c_int, [vp, up]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -304,6 +321,116 @@ class Case:
         best = ctypes.c_int()
         self._check(self._lib.dg_tune_stage(self._ctx, int(reps), ctypes.byref(best), _dptr(ms)))
         return best.value, ms.tolist()
+
+
+class Batch:
+    """An ensemble of independent cases advanced together (a dg_batch).
+
+    ``cases`` is a sequence of (mesh, order) pairs; flux, gamma, gas constant,
+    precision and device apply to all of them.  Cases of the same order share
+    one stage launch per RK stage; every case has its own time step."""
+
+    def __init__(self, cases, flux: str = "LaxFriedrichs", gamma: float = 1.4, gas_constant: float = 287.05,
+                 precision: str = "fp64", device: int = 0):
+        self._lib = library()
+        self.orders = [int(o) for _, o in cases]
+        self.nelem = [m.nelem for m, _ in cases]
+        self._keep = []
+        mds = (_MeshDesc * len(cases))()
+        cds = (_CaseDesc * len(cases))()
+        for i, (mesh, order) in enumerate(cases):
+            c = np.ascontiguousarray(mesh.node_coords, np.float64)
+            e = np.ascontiguousarray(mesh.elem_to_node_ids, np.uint32)
+            f = np.ascontiguousarray(mesh.interior_faces, np.uint32)
+            self._keep += [c, e, f]
+            mds[i] = _MeshDesc(c.shape[0], _dptr(c), e.shape[0], _uptr(e), f.shape[0], _uptr(f), 0)
+            cds[i] = _CaseDesc(int(order), FLUX[flux], gamma, gas_constant, PRECISION[precision], device)
+        h = ctypes.c_void_p()
+        rc = self._lib.dg_batch_create(len(cases), cds, mds, ctypes.byref(h))
+        self._keep = None  # the library copied what it needs
+        if rc:
+            raise DGError(rc, self._lib.dg_batch_last_error(None).decode())
+        self._b = h
+
+    def _check(self, rc: int):
+        if rc:
+            raise DGError(rc, self._lib.dg_batch_last_error(self._b).decode())
+
+    def close(self):
+        if getattr(self, "_b", None):
+            self._lib.dg_batch_destroy(self._b)
+            self._b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __len__(self) -> int:
+        return len(self.orders)
+
+    def _state_array(self, c: int) -> np.ndarray:
+        return np.empty((self.nelem[c], (self.orders[c] + 1) ** 3, 5), np.float64)
+
+    def groups(self):
+        """[(order, cases, elements, stage variant)] per group."""
+        out = []
+        for g in range(self._lib.dg_batch_num_groups(self._b)):
+            o, n, e, v = (ctypes.c_int() for _ in range(4))
+            self._check(self._lib.dg_batch_group_info(self._b, g, ctypes.byref(o), ctypes.byref(n), ctypes.byref(e),
+                                                      ctypes.byref(v)))
+            out.append((o.value, n.value, e.value, v.value))
+        return out
+
+    def set_state(self, c: int, Uc: np.ndarray):
+        Uc = np.ascontiguousarray(Uc, np.float64)
+        assert Uc.shape == self._state_array(c).shape
+        self._check(self._lib.dg_batch_set_state(self._b, c, _dptr(Uc)))
+
+    def get_state(self, c: int) -> np.ndarray:
+        out = self._state_array(c)
+        self._check(self._lib.dg_batch_get_state(self._b, c, _dptr(out)))
+        return out
+
+    def project_ic(self, c: int, name: str, data=(), t: float = 0.0) -> np.ndarray:
+        d = np.ascontiguousarray(np.asarray(data, np.float64).reshape(-1))
+        out = self._state_array(c)
+        self._check(self._lib.dg_batch_project_ic(self._b, c, IC[name], _dptr(d) if d.size else None, d.size, t,
+                                                  _dptr(out)))
+        return out
+
+    def cfl_time_step(self, c: int, Uc: np.ndarray, cfl: float) -> float:
+        Uc = np.ascontiguousarray(Uc, np.float64)
+        v = ctypes.c_double()
+        self._check(self._lib.dg_batch_cfl_time_step(self._b, c, _dptr(Uc), cfl, ctypes.byref(v)))
+        return v.value
+
+    def set_time_step(self, c: int, dt: float):
+        self._check(self._lib.dg_batch_set_time_step(self._b, c, float(dt)))
+
+    def rk4(self, nsteps: int):
+        self._check(self._lib.dg_batch_rk4_steps(self._b, int(nsteps)))
+
+    def rk4_timed(self, nsteps: int) -> float:
+        ms = ctypes.c_double()
+        self._check(self._lib.dg_batch_rk4_steps_timed(self._b, int(nsteps), ctypes.byref(ms)))
+        return ms.value
+
+    def tune(self, reps: int = 2):
+        self._check(self._lib.dg_batch_tune(self._b, int(reps)))
+
+    def l2_error(self, c: int, name: str, data=(), t: float = 0.0) -> np.ndarray:
+        d = np.ascontiguousarray(np.asarray(data, np.float64).reshape(-1))
+        out = np.zeros(5, np.float64)
+        self._check(self._lib.dg_batch_l2_error(self._b, c, IC[name], _dptr(d) if d.size else None, d.size, t,
+                                                _dptr(out)))
+        return out
+
+    def status(self) -> int:
+        v = ctypes.c_uint()
+        self._check(self._lib.dg_batch_status(self._b, ctypes.byref(v)))
+        return v.value
 
 
 def gauss_legendre(n: int):

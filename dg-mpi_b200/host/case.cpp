@@ -8,17 +8,17 @@
 namespace dgh {
 
 void project_initial_condition(const PreparedMesh& pm, const Tables1D& t, int ic_type, const double* data,
-                               double gamma, double R, double time, double* Uc)
+                               double gamma, double R, double time, double* Uc, int e_begin, int e_end)
 {
     const int n = t.n, me = t.me, nb = n * n * n;
-    const int ne = pm.ne;
+    const int ne = e_end < 0 ? pm.ne : e_end;
 #pragma omp parallel
     {
         std::vector<double> f(static_cast<size_t>(me) * me * me * kNS);
         std::vector<double> t1(static_cast<size_t>(kNS) * me * me * n), t2(static_cast<size_t>(kNS) * me * n * n),
             r(static_cast<size_t>(kNS) * nb), r2(static_cast<size_t>(kNS) * nb);
 #pragma omp for schedule(static)
-        for (int e = 0; e < ne; ++e) {
+        for (int e = e_begin; e < ne; ++e) {
             const GeoClass& g = pm.classes[pm.geo_class[e]];
             const double* X0 = &pm.X0[static_cast<size_t>(e) * 3];
             // f(q) * w_q * djac at the over-integration points
@@ -85,17 +85,42 @@ void project_initial_condition(const PreparedMesh& pm, const Tables1D& t, int ic
                         for (int bx = 0; bx < n; ++bx) {
                             double acc = 0.0;
                             for (int k = 0; k < n; ++k) acc += t.Minv[bz * n + k] * rs[(k * n + by) * n + bx];
-                            Uc[(static_cast<size_t>(e) * nb + (bz * n + by) * n + bx) * kNS + s] = acc * g.inv_djac;
+                            Uc[(static_cast<size_t>(e - e_begin) * nb + (bz * n + by) * n + bx) * kNS + s] =
+                                acc * g.inv_djac;
                         }
             }
         }
     }
 }
 
-double cfl_time_step(const PreparedMesh& pm, int p, double gamma, const double* Uc, double cfl)
+double range_volume(const PreparedMesh& pm, int e_begin, int e_end)
+{
+    double v = 0.0;
+    for (int e = e_begin; e < e_end; ++e) v += 8.0 * pm.classes[pm.geo_class[e]].djac;
+    return v;
+}
+
+double range_hmin(const PreparedMesh& pm, int e_begin, int e_end)
+{
+    std::vector<char> seen(pm.classes.size(), 0);
+    double h = 1e300;
+    for (int e = e_begin; e < e_end; ++e) {
+        const int k = pm.geo_class[e];
+        if (seen[k]) continue;
+        seen[k] = 1;
+        const GeoClass& g = pm.classes[k];
+        for (int a = 0; a < 3; ++a)
+            h = std::fmin(h, 2.0 * std::sqrt(g.J[0 * 3 + a] * g.J[0 * 3 + a] + g.J[1 * 3 + a] * g.J[1 * 3 + a] +
+                                             g.J[2 * 3 + a] * g.J[2 * 3 + a]));
+    }
+    return h;
+}
+
+double cfl_time_step(const PreparedMesh& pm, int p, double gamma, const double* Uc, double cfl, int e_begin, int e_end)
 {
     const int nb = (p + 1) * (p + 1) * (p + 1);
-    const size_t n = static_cast<size_t>(pm.ne) * nb;
+    if (e_end < 0) e_end = pm.ne;
+    const size_t n = static_cast<size_t>(e_end - e_begin) * nb;
     double smax = 0.0;
     bool bad = false;
 #pragma omp parallel for reduction(max : smax) reduction(|| : bad)
@@ -110,7 +135,8 @@ double cfl_time_step(const PreparedMesh& pm, int p, double gamma, const double* 
         smax = std::fmax(smax, s);
     }
     if (bad || !(smax > 0.0)) return -1.0;
-    return cfl * pm.hmin / ((2.0 * p + 1.0) * smax);
+    const double hmin = (e_begin == 0 && e_end == pm.ne) ? pm.hmin : range_hmin(pm, e_begin, e_end);
+    return cfl * hmin / ((2.0 * p + 1.0) * smax);
 }
 
 }  // namespace dgh

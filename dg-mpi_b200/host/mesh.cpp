@@ -216,13 +216,14 @@ std::string prepare_mesh(const MeshView& mv, int m, PreparedMesh& out)
             }
         for (int a = 0; a < 3; ++a) out.X0[static_cast<size_t>(e) * 3 + a] = X[a];
     }
-    std::map<std::array<long long, 9>, int> class_of;
+    std::map<std::array<long long, 10>, int> class_of;
     out.geo_class.resize(ne);
     out.hmin = 1e300;
     for (int e = 0; e < ne; ++e) {
         const double* J = &Jall[static_cast<size_t>(e) * 9];
-        std::array<long long, 9> key{};
+        std::array<long long, 10> key{};
         for (int i = 0; i < 9; ++i) key[i] = std::llround(J[i] / hs * 68719476736.0);  // 2^36
+        key[9] = mv.tag ? mv.tag[e] : 0;
         auto it = class_of.find(key);
         if (it != class_of.end()) {
             out.geo_class[e] = it->second;

@@ -16,6 +16,7 @@ struct MeshView {
     const double* coords = nullptr;
     const unsigned* e2n = nullptr;
     const unsigned* faces = nullptr;
+    const int* tag = nullptr;  // optional [ne]: elements with different tags get different geometry classes
 };
 
 struct BoxMesh {

@@ -3,13 +3,17 @@
 
   python dg-mpi_b200/studies.py precision   # 64^3, p=5, x-y vortex, 500 RK4 steps
   python dg-mpi_b200/studies.py taylor_green # 96^3, p=4, Taylor-Green, 200 RK4 steps
-  python dg-mpi_b200/studies.py <name> --scale 0.25  # smaller mesh, same order
+  python dg-mpi_b200/studies.py ensemble     # 256 seeded vortex cases, p=1..5, 8^3..32^3, 100 steps
+  python dg-mpi_b200/studies.py <name> --scale 0.25  # smaller mesh (fewer cases), same orders
 
 Each study runs the FP64 path and the mixed-precision path (FP32 residual,
 FP64 state) from the same projected initial condition and prints one JSON line:
 per-variable relative L2 difference mixed vs FP64, L2 error of both against the
 exact advected vortex (precision) or the kinetic-energy histories of both
 (Taylor-Green), and the device-timed DOF-stage update rate of both paths.
+The ensemble study advances all cases as one batch (dg_batch_*, one graph of
+per-order stage launches) in mixed precision and in FP64, and the same cases
+one context at a time, and reports the aggregate rates and errors.
 """
 from __future__ import annotations
 
@@ -90,12 +94,72 @@ def taylor_green(scale: float):
     return out
 
 
+def ensemble_cases(ncases: int, seed: int = 2024):
+    """Seeded ensemble: mesh N in {8,12,16,24,32}, order in 1..5, vortex
+    strength U[1,5], centre U[3,7]^2, free stream U[0.5,1.5]^2 on [0,10]^3."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(ncases):
+        n = int(rng.choice([8, 12, 16, 24, 32]))
+        p = int(rng.integers(1, 6))
+        beta = float(rng.uniform(1, 5))
+        xc, yc = (float(v) for v in rng.uniform(3, 7, 2))
+        u, v = (float(w) for w in rng.uniform(0.5, 1.5, 2))
+        out.append((n, p, [1.0, u, v, 1.0, beta, xc, yc, 10.0, 10.0]))
+    return out
+
+
+def ensemble(scale: float, steps: int = 100, cfl: float = 0.1):
+    spec = ensemble_cases(max(8, int(round(256 * scale))))
+    box = {n: dg_b200.periodic_box((n, n, n), (0, 0, 0), (10.0, 10.0, 10.0)) for n in {c[0] for c in spec}}
+    cases = [(box[n], p) for n, p, _ in spec]
+    dof = [box[n].nelem * (p + 1) ** 3 * 5 for n, p, _ in spec]
+    out = {"ncases": len(spec), "steps": steps, "total_dof": int(sum(dof)),
+           "orders": {str(p): sum(1 for c in spec if c[1] == p) for p in range(1, 6)}}
+    finals = {}
+    for prec in ("mixed_fp32", "fp64"):
+        t0 = time.perf_counter()
+        b = dg_b200.Batch(cases, gas_constant=1.0, precision=prec)
+        dts = []
+        for i, (_, _, data) in enumerate(spec):
+            U = b.project_ic(i, "IsentropicVortexXY", data)
+            dts.append(b.cfl_time_step(i, U, cfl))
+            b.set_time_step(i, dts[-1])
+        setup = time.perf_counter() - t0
+        b.tune(reps=1)
+        for i, (_, _, data) in enumerate(spec):   # the tuner left the state unchanged; restart anyway
+            b.project_ic(i, "IsentropicVortexXY", data)
+        ms = b.rk4_timed(steps)
+        errs = [b.l2_error(i, "IsentropicVortexXY", data, steps * dts[i]) for i, (_, _, data) in enumerate(spec)]
+        finals[prec] = [b.get_state(i) for i in range(0, len(spec), 4)]  # host memory: every 4th case
+        out[prec] = {"dof_stage_per_s": sum(dof) * 4 * steps / (ms / 1e3), "ms_total": ms, "setup_s": setup,
+                     "groups": b.groups(), "status": b.status(),
+                     "max_l2_error_vs_exact": np.max(np.array(errs), axis=0).tolist(),
+                     "median_l2_error_vs_exact": np.median(np.array(errs), axis=0).tolist()}
+        b.close()
+    diffs = np.array([rel_l2(a, c) for a, c in zip(finals["mixed_fp32"], finals["fp64"])])
+    out["max_rel_l2_mixed_vs_fp64_every_4th_case"] = diffs.max(axis=0).tolist()
+    del finals
+    # the same cases one context at a time (device time of each case's steps)
+    ms_seq = 0.0
+    for i, (mesh, p) in enumerate(cases):
+        c = dg_b200.Case(mesh, p, gas_constant=1.0, precision="mixed_fp32")
+        U = c.project_ic("IsentropicVortexXY", spec[i][2])
+        ms_seq += c.rk4_timed(c.cfl_time_step(U, cfl), steps)
+        c.close()
+    out["sequential_mixed"] = {"dof_stage_per_s": sum(dof) * 4 * steps / (ms_seq / 1e3), "ms_total": ms_seq}
+    out["config"] = (f"{len(spec)} x-y vortex cases on [0,10]^3, N in {{8,12,16,24,32}}, p in 1..5, seeded, "
+                     f"LF flux, RK4 CFL 0.1 per case, {steps} steps")
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("study", choices=["precision", "taylor_green"])
+    ap.add_argument("study", choices=["precision", "taylor_green", "ensemble"])
     ap.add_argument("--scale", type=float, default=1.0)
     args = ap.parse_args()
-    res = precision(args.scale) if args.study == "precision" else taylor_green(args.scale)
+    run = {"precision": precision, "taylor_green": taylor_green, "ensemble": ensemble}[args.study]
+    res = run(args.scale)
     res["study"] = args.study
     print(json.dumps(res), flush=True)
 

@@ -211,6 +211,52 @@ int dg_sync(dg_ctx* ctx);
  * multi-GPU exchange).  Layout of the device state: [ne][5][nb]. */
 void* dg_device_state(dg_ctx* ctx);
 
+/* ---- batched ensembles ----
+ *
+ * Many independent cases (each its own periodic mesh, order and time step)
+ * advanced together; the ensemble driver of the `dg_batch_*` entry points in
+ * the survey's C ABI (the reference runs one case per process, so there is no
+ * reference function it replaces; each case's arithmetic is exactly that of a
+ * dg_ctx on the same case).  Cases of the same (order, flux, gamma, gas
+ * constant) share one group: their meshes are concatenated and one stage
+ * launch per group and RK stage advances all of them, each element scaling its
+ * update by its own case's dt.  dg_batch_rk4_steps replays a CUDA graph in
+ * which the groups' launches are independent branches.  All cases must name
+ * the same device and precision.  Results per case are bit-identical to a
+ * dg_ctx of that case running the same stage variant. */
+typedef struct dg_batch dg_batch;
+
+int dg_batch_create(int ncases, const dg_case_desc* cases, const dg_mesh_desc* meshes, dg_batch** out);
+void dg_batch_destroy(dg_batch* b);
+/* Message of the last failed call on b (or of the last failed dg_batch_create
+ * of this thread when b is NULL). */
+const char* dg_batch_last_error(const dg_batch* b);
+int dg_batch_num_groups(const dg_batch* b);
+/* order, number of cases, elements and current stage variant of group g */
+int dg_batch_group_info(const dg_batch* b, int g, int* order, int* ncases, int* nelem, int* variant);
+/* order, elements, group and time step of case c */
+int dg_batch_case_info(const dg_batch* b, int c, int* order, int* nelem, int* group, double* dt);
+/* host state of case c, layout [nelem][nb][5] as for dg_set_state */
+int dg_batch_set_state(dg_batch* b, int c, const double* Uc);
+int dg_batch_get_state(dg_batch* b, int c, double* Uc);
+/* dg_project_ic for case c (Uc may be NULL) */
+int dg_batch_project_ic(dg_batch* b, int c, int ic_type, const double* data, int ndata, double t, double* Uc);
+/* dg_cfl_time_step for case c on a host state of that case */
+int dg_batch_cfl_time_step(dg_batch* b, int c, const double* Uc, double cfl, double* dt);
+/* time step of case c (default 0: the case does not move) */
+int dg_batch_set_time_step(dg_batch* b, int c, double dt);
+/* nsteps RK4 steps of every case, each with its own dt */
+int dg_batch_rk4_steps(dg_batch* b, int nsteps);
+/* the same, device time of the graph launches in milliseconds */
+int dg_batch_rk4_steps_timed(dg_batch* b, int nsteps, double* device_ms);
+/* picks the fastest stage variant of every group (dg_tune_stage per group,
+ * on the group's current state; the state is unchanged) */
+int dg_batch_tune(dg_batch* b, int reps);
+/* dg_l2_error for case c */
+int dg_batch_l2_error(dg_batch* b, int c, int ic_type, const double* data, int ndata, double t, double* err);
+/* status flags of all groups since the last call (bits as dg_status) */
+int dg_batch_status(dg_batch* b, unsigned* flags);
+
 /* ---- host-side mesh helper (replaces reading an HDF5 mesh file,
  * src/mesh/mesh.cpp:79-204, for periodic boxes) ---- */
 
