@@ -275,7 +275,7 @@ int dg_batch_create(int ncases, const dg_case_desc* cases, const dg_mesh_desc* m
         dg_mesh_desc gm{static_cast<int>(nnode), coords.data(), static_cast<int>(nelem), e2n.data(),
                         static_cast<int>(nface), faces.data(), 0};
         dg_case_desc gc = cases[g.cases[0]];
-        const int rc = dgi::create_ctx(&gc, &gm, tags.data(), &g.ctx);
+        const int rc = dgi::create_ctx(&gc, &gm, tags.data(), nullptr, &g.ctx);
         if (rc) return bail(rc, "group of order " + std::to_string(g.order) + ": " + dg_last_error(nullptr));
         const dgh::PreparedMesh& pm = g.ctx->pm;
         g.class_case.assign(pm.classes.size(), -1);

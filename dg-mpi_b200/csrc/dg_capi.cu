@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "../host/case.h"
+#include "../host/partition.h"
 #include "dg_ctx.cuh"
 
 using dgk::GeoDev;
@@ -119,8 +120,11 @@ int prepare_variant(dg_ctx* c, int v)
     return DG_OK;
 }
 
-int launch_stage(dg_ctx* c, int mode, const double* Us, const double* U0, double* out, double dt)
+int launch_stage(dg_ctx* c, int mode, const double* Us, const double* U0, double* out, double dt, int e_begin, int e_end)
 {
+    if (e_end < 0) e_end = c->ne;
+    if (e_begin < 0 || e_end > c->ne || e_begin > e_end) return fail(c, DG_ERR_ARG, "stage element range out of bounds");
+    if (e_begin == e_end) return DG_OK;
     StageArgs a{};
     a.Us = Us;
     a.U0 = U0;
@@ -131,7 +135,8 @@ int launch_stage(dg_ctx* c, int mode, const double* Us, const double* U0, double
     a.geo = c->d_geo;
     a.cmap = c->d_cmap;
     a.status = c->d_status;
-    a.ne = c->ne;
+    a.e_begin = e_begin;
+    a.ne = e_end;
     a.flux = c->flux;
     a.mode = mode;
     a.gamma = c->gamma;
@@ -141,7 +146,8 @@ int launch_stage(dg_ctx* c, int mode, const double* Us, const double* U0, double
     if (rc) return rc;
     const dgk::StageVariant* vs = nullptr;
     dgk::stage_variants(c->p, &vs);
-    DG_CUDA(c, vs[c->variant].launch(a, c->variant_grid[c->variant], c->stream));
+    const int batches = (e_end - e_begin + vs[c->variant].E - 1) / vs[c->variant].E;
+    DG_CUDA(c, vs[c->variant].launch(a, std::min(c->variant_grid[c->variant], batches), c->stream));
     return DG_OK;
 }
 
@@ -164,6 +170,42 @@ __global__ void to_host_layout(const double* __restrict__ src, double* __restric
         const long long e = i / (5LL * nb);
         const int r = (int)(i - e * 5LL * nb), b = r / 5, v = r - b * 5;
         dst[i] = src[(e * 5 + v) * nb + b];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// halo exchange: boundary slices [nslices][5][n*n] of the (element, face)
+// pairs of the plan, gathered from owned elements / scattered into ghosts
+
+__device__ __forceinline__ int slice_index_rt(int n, int f, int b0, int b1)
+{
+    const int ax = dgk::face_axis(f), sidx = dgk::face_side(f) ? n - 1 : 0;
+    if (ax == 0) return b1 * n * n + b0 * n + sidx;
+    if (ax == 1) return b1 * n * n + sidx * n + b0;
+    return sidx * n * n + b1 * n + b0;
+}
+
+__global__ void halo_pack_kernel(const double* __restrict__ U, const int2* __restrict__ list, int nslices, int n,
+                                 double* __restrict__ out)
+{
+    const int n2 = n * n, nb = n2 * n, per = 5 * n2;
+    const long long total = (long long)nslices * per;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+        const int s = (int)(i / per), r = (int)(i - (long long)s * per), v = r / n2, b = r - v * n2;
+        const int2 ef = list[s];
+        out[i] = U[((size_t)ef.x * 5 + v) * nb + slice_index_rt(n, ef.y, b % n, b / n)];
+    }
+}
+
+__global__ void halo_unpack_kernel(double* __restrict__ U, const int2* __restrict__ list, int nslices, int n,
+                                   const double* __restrict__ in)
+{
+    const int n2 = n * n, nb = n2 * n, per = 5 * n2;
+    const long long total = (long long)nslices * per;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+        const int s = (int)(i / per), r = (int)(i - (long long)s * per), v = r / n2, b = r - v * n2;
+        const int2 ef = list[s];
+        U[((size_t)ef.x * 5 + v) * nb + slice_index_rt(n, ef.y, b % n, b / n)] = in[i];
     }
 }
 
@@ -450,6 +492,7 @@ void release(dg_ctx* c)
     cudaFree(c->d_U0); cudaFree(c->d_Ua); cudaFree(c->d_Ub); cudaFree(c->d_acc); cudaFree(c->d_out);
     cudaFree(c->d_conn); cudaFree(c->d_geo_class); cudaFree(c->d_geo); cudaFree(c->d_cmap);
     cudaFree(c->d_X0); cudaFree(c->d_partials); cudaFree(c->d_status);
+    cudaFree(c->d_halo_send); cudaFree(c->d_halo_recv);
     if (c->stream) cudaStreamDestroy(c->stream);
 }
 
@@ -457,7 +500,8 @@ void release(dg_ctx* c)
 
 using namespace dgi;
 
-int dgi::create_ctx(const dg_case_desc* cd, const dg_mesh_desc* md, const int* elem_tag, dg_ctx** out)
+int dgi::create_ctx(const dg_case_desc* cd, const dg_mesh_desc* md, const int* elem_tag, const dg_part_desc* part,
+                    dg_ctx** out)
 {
     g_create_error.clear();
     if (!cd || !md || !out) return fail(nullptr, DG_ERR_ARG, "dg_create: null argument");
@@ -487,19 +531,49 @@ int dgi::create_ctx(const dg_case_desc* cd, const dg_mesh_desc* md, const int* e
     mv.e2n = md->elem_to_node_ids;
     mv.faces = md->interior_faces;
     mv.tag = elem_tag;
+    std::vector<int> elem_rank;
+    dgh::HaloPlan plan;
     std::string perr;
+    if (part) {
+        const int ng = md->nelem - part->nowned;
+        if (part->nowned < 1 || ng < 0 || part->ninterior < 0 || part->ninterior > part->nowned ||
+            (ng > 0 && (!part->ghost_rank || !part->ghost_elem)))
+            perr = "partition description out of range";
+        for (int g = 0; perr.empty() && g < ng; ++g)
+            if (part->ghost_rank[g] < 0 || part->ghost_elem[g] < 0) perr = "ghost " + std::to_string(g) + " has no owner";
+        if (perr.empty()) {
+            elem_rank.assign(md->nelem, md->rank);
+            for (int g = 0; g < ng; ++g) elem_rank[part->nowned + g] = part->ghost_rank[g];
+            mv.nowned = part->nowned;
+            mv.elem_rank = elem_rank.data();
+        }
+    }
     try {
-        perr = dgh::prepare_mesh(mv, c->p + 2, c->pm);
+        if (perr.empty()) perr = dgh::prepare_mesh(mv, c->p + 2, c->pm);
+        if (perr.empty() && part) perr = dgh::make_halo_plan(mv, part->ghost_elem, plan);
         c->tab = dgh::make_tables(c->p);
     } catch (const std::exception& ex) {
         perr = std::string("mesh preparation failed: ") + ex.what();
+    }
+    if (perr.empty() && part) {
+        // the interior elements must not read a ghost: they run while the exchange is in flight
+        for (int e = 0; e < part->ninterior && perr.empty(); ++e)
+            for (int f = 0; f < 6; ++f)
+                if (c->pm.conn[(static_cast<size_t>(e) * 6 + f) * 2] >= part->nowned)
+                    perr = "element " + std::to_string(e) + " is counted as interior but has a ghost neighbour";
     }
     if (!perr.empty()) {
         delete c;
         const bool unsup = perr.rfind("unsupported:", 0) == 0;
         return fail(nullptr, unsup ? DG_ERR_UNSUPPORTED : DG_ERR_ARG, perr);
     }
-    c->ne = c->pm.ne;
+    c->ne = c->pm.nowned;
+    c->ne_alloc = c->pm.ne;
+    c->ninterior = part ? part->ninterior : 0;
+    c->nslices = static_cast<int>(plan.send_elem.size());
+    c->peer_rank = plan.peer_rank;
+    c->peer_offset = plan.peer_offset;
+    c->peer_count = plan.peer_count;
     std::copy(c->tab.B.begin(), c->tab.B.end(), c->stage_tab.B);
     std::copy(c->tab.D.begin(), c->tab.D.end(), c->stage_tab.D);
     std::copy(c->tab.wq.begin(), c->tab.wq.end(), c->stage_tab.W);
@@ -547,7 +621,7 @@ int dgi::create_ctx(const dg_case_desc* cd, const dg_mesh_desc* md, const int* e
         c->err = "cudaStreamCreate failed";
         return bail(DG_ERR_CUDA);
     }
-    const size_t nstate = static_cast<size_t>(c->ne) * c->nb * 5;
+    const size_t nstate = static_cast<size_t>(c->ne_alloc) * c->nb * 5;
     const size_t ncls = c->pm.classes.size();
     int dev_sms = 0;
     cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, c->device);
@@ -558,11 +632,13 @@ int dgi::create_ctx(const dg_case_desc* cd, const dg_mesh_desc* md, const int* e
         {(void**)&c->d_Ub, nstate * sizeof(double)},
         {(void**)&c->d_acc, nstate * sizeof(double)},
         {(void**)&c->d_out, nstate * sizeof(double)},
-        {(void**)&c->d_conn, static_cast<size_t>(c->ne) * 6 * sizeof(int2)},
-        {(void**)&c->d_geo_class, static_cast<size_t>(c->ne) * sizeof(int)},
+        {(void**)&c->d_conn, static_cast<size_t>(c->ne_alloc) * 6 * sizeof(int2)},
+        {(void**)&c->d_geo_class, static_cast<size_t>(c->ne_alloc) * sizeof(int)},
         {(void**)&c->d_geo, ncls * (sizeof(GeoDev) + 9 * sizeof(double))},
         {(void**)&c->d_cmap, std::max<size_t>(1, c->pm.cmap.size())},
-        {(void**)&c->d_X0, static_cast<size_t>(c->ne) * 3 * sizeof(double)},
+        {(void**)&c->d_X0, static_cast<size_t>(c->ne_alloc) * 3 * sizeof(double)},
+        {(void**)&c->d_halo_send, std::max<size_t>(1, c->nslices) * sizeof(int2)},
+        {(void**)&c->d_halo_recv, std::max<size_t>(1, c->nslices) * sizeof(int2)},
         {(void**)&c->d_partials, static_cast<size_t>(c->red_grid) * 5 * sizeof(double)},
         {(void**)&c->d_status, sizeof(unsigned)},
     };
@@ -573,10 +649,17 @@ int dgi::create_ctx(const dg_case_desc* cd, const dg_mesh_desc* md, const int* e
             return bail(DG_ERR_NOMEM);
         }
     }
-    std::vector<int2> conn(static_cast<size_t>(c->ne) * 6);
+    std::vector<int2> conn(static_cast<size_t>(c->ne_alloc) * 6);
     for (size_t i = 0; i < conn.size(); ++i) conn[i] = make_int2(c->pm.conn[i * 2], c->pm.conn[i * 2 + 1]);
+    std::vector<int2> hs(std::max(1, c->nslices)), hr(std::max(1, c->nslices));
+    for (int i = 0; i < c->nslices; ++i) {
+        hs[i] = make_int2(plan.send_elem[i], plan.send_face[i]);
+        hr[i] = make_int2(plan.recv_elem[i], plan.recv_face[i]);
+    }
     bool ok = cudaMemcpy(c->d_conn, conn.data(), conn.size() * sizeof(int2), cudaMemcpyHostToDevice) == cudaSuccess &&
-              cudaMemcpy(c->d_geo_class, c->pm.geo_class.data(), c->ne * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess &&
+              cudaMemcpy(c->d_geo_class, c->pm.geo_class.data(), c->ne_alloc * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess &&
+              cudaMemcpy(c->d_halo_send, hs.data(), hs.size() * sizeof(int2), cudaMemcpyHostToDevice) == cudaSuccess &&
+              cudaMemcpy(c->d_halo_recv, hr.data(), hr.size() * sizeof(int2), cudaMemcpyHostToDevice) == cudaSuccess &&
               cudaMemcpy(c->d_X0, c->pm.X0.data(), c->pm.X0.size() * sizeof(double), cudaMemcpyHostToDevice) == cudaSuccess &&
               (c->pm.cmap.empty() || cudaMemcpy(c->d_cmap, c->pm.cmap.data(), c->pm.cmap.size(), cudaMemcpyHostToDevice) == cudaSuccess) &&
               cudaMemset(c->d_status, 0, sizeof(unsigned)) == cudaSuccess &&
@@ -603,8 +686,146 @@ extern "C" {
 
 int dg_create(const dg_case_desc* cd, const dg_mesh_desc* md, dg_ctx** out)
 {
-    return create_ctx(cd, md, nullptr, out);
+    return create_ctx(cd, md, nullptr, nullptr, out);
 }
+
+int dg_create_partitioned(const dg_case_desc* cd, const dg_mesh_desc* md, const dg_part_desc* part, dg_ctx** out)
+{
+    if (!part) return fail(nullptr, DG_ERR_ARG, "dg_create_partitioned: null partition");
+    return create_ctx(cd, md, nullptr, part, out);
+}
+
+int dg_partition_periodic_box(const int n[3], const double x0[3], const double len[3], unsigned rotate_seed, int nparts,
+                              int part, int axis, int* nnode, double* node_coords, int* nelem, unsigned* elem_to_node_ids,
+                              int* nface, unsigned* interior_faces, int* nowned, int* ninterior, int* ghost_rank,
+                              int* ghost_elem, int* global_elem)
+{
+    if (!n || !x0 || !len || !nnode || !nelem || !nface || !nowned || !ninterior) return DG_ERR_ARG;
+    if (n[0] < 1 || n[1] < 1 || n[2] < 1 || 1LL * n[0] * n[1] * n[2] > (1LL << 30)) return DG_ERR_ARG;
+    if (axis < 0 || axis > 2 || nparts < 1 || nparts > n[axis] || part < 0 || part >= nparts) return DG_ERR_ARG;
+    try {
+        const dgh::BoxMesh g = dgh::make_periodic_box(n, x0, len, rotate_seed);
+        const dgh::LocalMesh lm = dgh::partition_mesh(g, dgh::slab_partition(n, nparts, axis), part);
+        *nnode = lm.mesh.nnode;
+        *nelem = lm.mesh.nelem;
+        *nface = lm.mesh.nface;
+        *nowned = lm.nowned;
+        *ninterior = lm.ninterior;
+        const bool none = !node_coords && !elem_to_node_ids && !interior_faces && !ghost_rank && !ghost_elem && !global_elem;
+        if (none) return DG_OK;
+        if (!node_coords || !elem_to_node_ids || !interior_faces || !ghost_rank || !ghost_elem || !global_elem)
+            return DG_ERR_ARG;
+        std::memcpy(node_coords, lm.mesh.coords.data(), lm.mesh.coords.size() * sizeof(double));
+        std::memcpy(elem_to_node_ids, lm.mesh.e2n.data(), lm.mesh.e2n.size() * sizeof(unsigned));
+        std::memcpy(interior_faces, lm.mesh.faces.data(), lm.mesh.faces.size() * sizeof(unsigned));
+        std::copy(lm.ghost_rank.begin(), lm.ghost_rank.end(), ghost_rank);
+        std::copy(lm.ghost_elem.begin(), lm.ghost_elem.end(), ghost_elem);
+        std::copy(lm.global_elem.begin(), lm.global_elem.end(), global_elem);
+    } catch (const std::exception&) {
+        return DG_ERR_ARG;
+    }
+    return DG_OK;
+}
+
+int dg_halo_plan(const dg_mesh_desc* md, const dg_part_desc* part, int* npeers, int* peer_rank, int* peer_offset,
+                 int* peer_count, int* nslices, int* send_elem, int* send_face, int* recv_elem, int* recv_face)
+{
+    g_create_error.clear();
+    if (!md || !part || !npeers || !nslices) return fail(nullptr, DG_ERR_ARG, "dg_halo_plan: null argument");
+    const int ng = md->nelem - part->nowned;
+    if (part->nowned < 1 || ng < 0 || (ng > 0 && (!part->ghost_rank || !part->ghost_elem)) || !md->interior_faces)
+        return fail(nullptr, DG_ERR_ARG, "dg_halo_plan: partition description out of range");
+    std::vector<int> er(md->nelem, md->rank);
+    for (int g = 0; g < ng; ++g) er[part->nowned + g] = part->ghost_rank[g];
+    dgh::MeshView mv;
+    mv.nnode = md->nnode;
+    mv.nelem = md->nelem;
+    mv.nface = md->nface;
+    mv.rank = md->rank;
+    mv.coords = md->node_coords;
+    mv.e2n = md->elem_to_node_ids;
+    mv.faces = md->interior_faces;
+    mv.nowned = part->nowned;
+    mv.elem_rank = er.data();
+    dgh::HaloPlan plan;
+    const std::string err = dgh::make_halo_plan(mv, part->ghost_elem, plan);
+    if (!err.empty()) return fail(nullptr, DG_ERR_ARG, err);
+    *npeers = static_cast<int>(plan.peer_rank.size());
+    *nslices = static_cast<int>(plan.send_elem.size());
+    if (peer_rank) std::copy(plan.peer_rank.begin(), plan.peer_rank.end(), peer_rank);
+    if (peer_offset) std::copy(plan.peer_offset.begin(), plan.peer_offset.end(), peer_offset);
+    if (peer_count) std::copy(plan.peer_count.begin(), plan.peer_count.end(), peer_count);
+    if (send_elem) std::copy(plan.send_elem.begin(), plan.send_elem.end(), send_elem);
+    if (send_face) std::copy(plan.send_face.begin(), plan.send_face.end(), send_face);
+    if (recv_elem) std::copy(plan.recv_elem.begin(), plan.recv_elem.end(), recv_elem);
+    if (recv_face) std::copy(plan.recv_face.begin(), plan.recv_face.end(), recv_face);
+    return DG_OK;
+}
+
+int dg_halo_num_peers(const dg_ctx* c) { return c ? static_cast<int>(c->peer_rank.size()) : 0; }
+
+int dg_halo_peer(const dg_ctx* c, int i, int* rank, int* offset, int* count)
+{
+    if (!c || i < 0 || i >= static_cast<int>(c->peer_rank.size())) return DG_ERR_ARG;
+    if (rank) *rank = c->peer_rank[i];
+    if (offset) *offset = c->peer_offset[i];
+    if (count) *count = c->peer_count[i];
+    return DG_OK;
+}
+
+int dg_halo_slice_doubles(const dg_ctx* c) { return c ? 5 * (c->p + 1) * (c->p + 1) : 0; }
+
+namespace {
+
+double* rk_buffer(dg_ctx* c, int buf)
+{
+    return buf == DG_BUF_U0 ? c->d_U0 : buf == DG_BUF_STAGE_A ? c->d_Ua : buf == DG_BUF_STAGE_B ? c->d_Ub : nullptr;
+}
+
+int halo_launch(dg_ctx* c, int buf, double* d_data, void* stream, bool pack)
+{
+    double* U = rk_buffer(c, buf);
+    if (!U) return fail(c, DG_ERR_ARG, "unknown state buffer");
+    if (c->nslices == 0) return DG_OK;
+    if (!d_data) return fail(c, DG_ERR_ARG, "null halo buffer");
+    DG_CUDA(c, cudaSetDevice(c->device));
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+    const long long total = 5LL * (c->p + 1) * (c->p + 1) * c->nslices;
+    const int grid = static_cast<int>(std::min<long long>((total + 255) / 256, 4096));
+    if (pack) halo_pack_kernel<<<grid, 256, 0, s>>>(U, c->d_halo_send, c->nslices, c->p + 1, d_data);
+    else halo_unpack_kernel<<<grid, 256, 0, s>>>(U, c->d_halo_recv, c->nslices, c->p + 1, d_data);
+    DG_CUDA(c, cudaGetLastError());
+    return DG_OK;
+}
+
+}  // namespace
+
+int dg_halo_pack(dg_ctx* c, int buf, double* d_send, void* stream)
+{
+    if (!c) return DG_ERR_ARG;
+    return halo_launch(c, buf, d_send, stream, true);
+}
+
+int dg_halo_unpack(dg_ctx* c, int buf, const double* d_recv, void* stream)
+{
+    if (!c) return DG_ERR_ARG;
+    return halo_launch(c, buf, const_cast<double*>(d_recv), stream, false);
+}
+
+int dg_rk4_stage(dg_ctx* c, int stage, double dt, int range)
+{
+    if (!c || stage < 1 || stage > 4 || range < 0 || range > 2) return fail(c, DG_ERR_ARG, "dg_rk4_stage: bad argument");
+    DG_CUDA(c, cudaSetDevice(c->device));
+    const int e0 = range == 2 ? c->ninterior : 0, e1 = range == 1 ? c->ninterior : c->ne;
+    switch (stage) {
+        case 1: return launch_stage(c, dgk::kModeRK1, c->d_U0, c->d_U0, c->d_Ua, dt, e0, e1);
+        case 2: return launch_stage(c, dgk::kModeRK2, c->d_Ua, c->d_U0, c->d_Ub, dt, e0, e1);
+        case 3: return launch_stage(c, dgk::kModeRK3, c->d_Ub, c->d_U0, c->d_Ua, dt, e0, e1);
+        default: return launch_stage(c, dgk::kModeRK4, c->d_Ua, c->d_U0, c->d_U0, dt, e0, e1);
+    }
+}
+
+void* dg_stream(dg_ctx* c) { return c ? static_cast<void*>(c->stream) : nullptr; }
 
 void dg_destroy(dg_ctx* ctx) { destroy_ctx(ctx); }
 
@@ -818,7 +1039,7 @@ int dg_project_ic(dg_ctx* c, int ic_type, const double* data, int ndata, double 
     const int need[] = {5, 0, 0, 9, 1};
     if (ndata < need[ic_type]) return fail(c, DG_ERR_ARG, "initial condition needs more data values");
     std::vector<double> U(static_cast<size_t>(c->ne) * c->nb * 5);
-    dgh::project_initial_condition(c->pm, c->tab, ic_type, d, c->gamma, c->R, t, U.data());
+    dgh::project_initial_condition(c->pm, c->tab, ic_type, d, c->gamma, c->R, t, U.data(), 0, c->ne);
     if (Uc) std::memcpy(Uc, U.data(), U.size() * sizeof(double));
     DG_CUDA(c, cudaSetDevice(c->device));
     return upload_state_host_layout(c, U.data(), c->d_U0);
@@ -982,7 +1203,7 @@ int dg_basis_tables(int p, double* B, double* D, double* Minv)
 int dg_cfl_time_step(dg_ctx* c, const double* Uc, double cfl, double* dt)
 {
     if (!c || !Uc || !dt || !(cfl > 0.0)) return fail(c, DG_ERR_ARG, "dg_cfl_time_step: bad argument");
-    const double v = dgh::cfl_time_step(c->pm, c->p, c->gamma, Uc, cfl);
+    const double v = dgh::cfl_time_step(c->pm, c->p, c->gamma, Uc, cfl, 0, c->ne);
     if (!(v > 0.0)) return fail(c, DG_ERR_NONPHYSICAL, "state has non-positive density or pressure");
     *dt = v;
     return DG_OK;

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <string>
+#include <vector>
 
 #include "../../include/dg_b200.h"
 #include "../host/mesh.h"
@@ -17,6 +18,13 @@ constexpr int kMaxVariants = 16;  // launch variants per order (checked in prepa
 
 struct dg_ctx {
     int device = 0, p = 0, nb = 0, ne = 0, flux = 0, precision = 0;
+    // partitioned contexts: ne owned elements (the first ninterior share no
+    // face with a ghost), ne_alloc = ne + ghosts element slots in every state
+    // buffer, and the halo plan on the device as (element, face) pairs
+    int ne_alloc = 0, ninterior = 0, nslices = 0;
+    int2* d_halo_send = nullptr;
+    int2* d_halo_recv = nullptr;
+    std::vector<int> peer_rank, peer_offset, peer_count;
     double gamma = 1.4, R = 287.05;
     cudaStream_t stream = nullptr;
     double *d_U0 = nullptr, *d_Ua = nullptr, *d_Ub = nullptr, *d_acc = nullptr, *d_out = nullptr;
@@ -53,14 +61,18 @@ int fail(dg_ctx* c, int code, const std::string& msg);
             return ::dgi::fail((c), DG_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
     } while (0)
 
-// dg_create with an optional per-element tag: elements with different tags
-// never share a geometry class (each class then carries one case's time step)
-int create_ctx(const dg_case_desc* cd, const dg_mesh_desc* md, const int* elem_tag, dg_ctx** out);
+// dg_create with an optional per-element tag (elements with different tags
+// never share a geometry class, so each class can carry one case's time step)
+// and an optional partition (ghost elements after the owned ones)
+int create_ctx(const dg_case_desc* cd, const dg_mesh_desc* md, const int* elem_tag, const dg_part_desc* part,
+               dg_ctx** out);
 void destroy_ctx(dg_ctx* c);
 
 int prepare_variant(dg_ctx* c, int v);
 bool variant_matches(const dg_ctx* c, int v);
-int launch_stage(dg_ctx* c, int mode, const double* Us, const double* U0, double* out, double dt);
+// stage launch over the owned elements [e_begin, e_end) (e_end < 0: all)
+int launch_stage(dg_ctx* c, int mode, const double* Us, const double* U0, double* out, double dt, int e_begin = 0,
+                 int e_end = -1);
 int check_status(dg_ctx* c);
 
 // state of elements [e0, e0 + ne) between the host layout [ne][nb][5] and the

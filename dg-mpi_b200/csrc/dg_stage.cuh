@@ -95,7 +95,7 @@ struct StageArgs {
     const GeoDev* geo;      // [nclasses]
     const uint8_t* cmap;    // [ncodes][m*m]
     unsigned* status;
-    int ne;
+    int e_begin, ne;        // the launch computes elements [e_begin, ne)
     int flux;               // 0 = Lax-Friedrichs, 1 = HLLC
     int mode;
     double gamma;
@@ -228,12 +228,13 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
     const T gamma = T(a.gamma);
     unsigned status = 0;
     const int stride = gridDim.x * E;
+    const int e_first = a.e_begin + blockIdx.x * E;
 
     int buf = 0;
-    if (blockIdx.x * E < a.ne) prefetch_batch<P, G, E, NT>(a.Us, a.ne, blockIdx.x * E, sUbuf, ES);
+    if (e_first < a.ne) prefetch_batch<P, G, E, NT>(a.Us, a.ne, e_first, sUbuf, ES);
     cp_async_commit();
 
-    for (int e0 = blockIdx.x * E; e0 < a.ne; e0 += stride, buf ^= 1) {
+    for (int e0 = e_first; e0 < a.ne; e0 += stride, buf ^= 1) {
         double* sU = sUbuf + buf * E * ES;
         cp_async_wait_all();
         __syncthreads();

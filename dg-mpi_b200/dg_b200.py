@@ -50,6 +50,15 @@ class _CaseDesc(ctypes.Structure):
                 ("gas_constant", ctypes.c_double), ("precision", ctypes.c_int), ("device", ctypes.c_int)]
 
 
+class _PartDesc(ctypes.Structure):
+    _fields_ = [("nowned", ctypes.c_int), ("ninterior", ctypes.c_int), ("ghost_rank", ctypes.POINTER(ctypes.c_int)),
+                ("ghost_elem", ctypes.POINTER(ctypes.c_int))]
+
+
+# RK4 buffers (DG_BUF_*): the state, and the two stage buffers; stage s reads STAGE_INPUT[s]
+BUF_U0, BUF_STAGE_A, BUF_STAGE_B = 0, 1, 2
+STAGE_INPUT = {1: BUF_U0, 2: BUF_STAGE_A, 3: BUF_STAGE_B, 4: BUF_STAGE_A}
+
 _lib = None
 
 
@@ -94,6 +103,19 @@ def library(path: str | None = None) -> ctypes.CDLL:
         "dg_set_stage_variant": (ctypes.c_int, [vp, ctypes.c_int]),
         "dg_get_stage_variant": (ctypes.c_int, [vp]),
         "dg_tune_stage": (ctypes.c_int, [vp, ctypes.c_int, ip, dp]),
+        "dg_create_partitioned": (ctypes.c_int, [ctypes.POINTER(_CaseDesc), ctypes.POINTER(_MeshDesc),
+                                                 ctypes.POINTER(_PartDesc), ctypes.POINTER(vp)]),
+        "dg_partition_periodic_box": (ctypes.c_int, [ip, dp, dp, ctypes.c_uint, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                     ip, dp, ip, up, ip, up, ip, ip, ip, ip, ip]),
+        "dg_halo_plan": (ctypes.c_int, [ctypes.POINTER(_MeshDesc), ctypes.POINTER(_PartDesc), ip, ip, ip, ip, ip,
+                                        ip, ip, ip, ip]),
+        "dg_halo_num_peers": (ctypes.c_int, [vp]),
+        "dg_halo_peer": (ctypes.c_int, [vp, ctypes.c_int, ip, ip, ip]),
+        "dg_halo_slice_doubles": (ctypes.c_int, [vp]),
+        "dg_halo_pack": (ctypes.c_int, [vp, ctypes.c_int, vp, vp]),
+        "dg_halo_unpack": (ctypes.c_int, [vp, ctypes.c_int, vp, vp]),
+        "dg_rk4_stage": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int]),
+        "dg_stream": (vp, [vp]),
         "dg_batch_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_CaseDesc), ctypes.POINTER(_MeshDesc),
                                            ctypes.POINTER(vp)]),
         "dg_batch_destroy": (None, [vp]),
@@ -167,25 +189,107 @@ def periodic_box(n, x0=(0.0, 0.0, 0.0), length=(1.0, 1.0, 1.0), rotate_seed: int
     return Mesh(coords, e2n, faces)
 
 
+def _iptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+
+
+@dataclass
+class Partition:
+    """One rank's share of a partitioned mesh: owned elements [0, nowned) (the
+    first ninterior without ghost neighbours), then ghosts, each with its
+    owner rank and its local id there (dg_part_desc)."""
+    rank: int
+    nowned: int
+    ninterior: int
+    ghost_rank: np.ndarray   # int32 [nghost]
+    ghost_elem: np.ndarray   # int32 [nghost]
+    global_elem: np.ndarray  # int32 [nowned + nghost], ids in the unpartitioned mesh
+
+    def desc(self) -> _PartDesc:
+        self.ghost_rank = np.ascontiguousarray(self.ghost_rank, np.int32)
+        self.ghost_elem = np.ascontiguousarray(self.ghost_elem, np.int32)
+        return _PartDesc(self.nowned, self.ninterior, _iptr(self.ghost_rank), _iptr(self.ghost_elem))
+
+
+def partition_periodic_box(n, x0, length, nparts: int, part: int, axis: int = 2, rotate_seed: int = 0):
+    """Slab `part` of `nparts` along `axis` of periodic_box(n, x0, length): (Mesh, Partition)."""
+    lib = library()
+    n_arr = (ctypes.c_int * 3)(*[int(v) for v in n])
+    x_arr = (ctypes.c_double * 3)(*[float(v) for v in x0])
+    l_arr = (ctypes.c_double * 3)(*[float(v) for v in length])
+    nn, ne, nf, no, ni = (ctypes.c_int() for _ in range(5))
+    args = (n_arr, x_arr, l_arr, ctypes.c_uint(rotate_seed), nparts, part, axis)
+    rc = lib.dg_partition_periodic_box(*args, ctypes.byref(nn), None, ctypes.byref(ne), None, ctypes.byref(nf), None,
+                                       ctypes.byref(no), ctypes.byref(ni), None, None, None)
+    if rc:
+        raise DGError(rc, "dg_partition_periodic_box: bad arguments")
+    coords = np.zeros((nn.value, 3), np.float64)
+    e2n = np.zeros((ne.value, 8), np.uint32)
+    faces = np.zeros((nf.value, 8), np.uint32)
+    ng = ne.value - no.value
+    gr, ge, gl = np.zeros(ng, np.int32), np.zeros(ng, np.int32), np.zeros(ne.value, np.int32)
+    rc = lib.dg_partition_periodic_box(*args, ctypes.byref(nn), _dptr(coords), ctypes.byref(ne), _uptr(e2n),
+                                       ctypes.byref(nf), _uptr(faces), ctypes.byref(no), ctypes.byref(ni), _iptr(gr),
+                                       _iptr(ge), _iptr(gl))
+    if rc:
+        raise DGError(rc, "dg_partition_periodic_box failed")
+    return Mesh(coords, e2n, faces), Partition(part, no.value, ni.value, gr, ge, gl)
+
+
+def _mesh_desc(mesh: Mesh, rank: int, keep: list) -> _MeshDesc:
+    c = np.ascontiguousarray(mesh.node_coords, np.float64)
+    e = np.ascontiguousarray(mesh.elem_to_node_ids, np.uint32)
+    f = np.ascontiguousarray(mesh.interior_faces, np.uint32)
+    keep += [c, e, f]
+    return _MeshDesc(c.shape[0], _dptr(c), e.shape[0], _uptr(e), f.shape[0], _uptr(f), rank)
+
+
+def halo_plan(mesh: Mesh, part: Partition):
+    """Host-side halo plan (dg_halo_plan): ([(peer rank, offset, count)], send (elem, face) [nslices][2],
+    recv (ghost elem, face) [nslices][2])."""
+    lib = library()
+    keep = []
+    md = _mesh_desc(mesh, part.rank, keep)
+    pd = part.desc()
+    npeer, nsl = ctypes.c_int(), ctypes.c_int()
+    rc = lib.dg_halo_plan(ctypes.byref(md), ctypes.byref(pd), ctypes.byref(npeer), None, None, None, ctypes.byref(nsl),
+                          None, None, None, None)
+    if rc:
+        raise DGError(rc, lib.dg_last_error(None).decode())
+    pr, po, pc = (np.zeros(npeer.value, np.int32) for _ in range(3))
+    se, sf, re_, rf = (np.zeros(nsl.value, np.int32) for _ in range(4))
+    rc = lib.dg_halo_plan(ctypes.byref(md), ctypes.byref(pd), ctypes.byref(npeer), _iptr(pr), _iptr(po), _iptr(pc),
+                          ctypes.byref(nsl), _iptr(se), _iptr(sf), _iptr(re_), _iptr(rf))
+    if rc:
+        raise DGError(rc, lib.dg_last_error(None).decode())
+    peers = [(int(a), int(b), int(c)) for a, b, c in zip(pr, po, pc)]
+    return peers, np.stack([se, sf], 1), np.stack([re_, rf], 1)
+
+
 class Case:
-    """One DG case on one GPU (a dg_ctx)."""
+    """One DG case on one GPU (a dg_ctx); with `part`, one rank's share of a
+    partitioned mesh (dg_create_partitioned), whose ghost slices the caller
+    exchanges through halo_pack / halo_unpack between rk4_stage calls."""
 
     def __init__(self, mesh: Mesh, order: int, flux: str = "LaxFriedrichs", gamma: float = 1.4,
-                 gas_constant: float = 287.05, precision: str = "fp64", device: int = 0):
+                 gas_constant: float = 287.05, precision: str = "fp64", device: int = 0,
+                 part: Partition | None = None):
         self._lib = library()
         self.mesh = mesh
         self.order = order
         self.nb = (order + 1) ** 3
-        self.ne = mesh.nelem
+        self.ne = mesh.nelem if part is None else part.nowned
         self.gamma = gamma
-        self._coords = np.ascontiguousarray(mesh.node_coords, np.float64)
-        self._e2n = np.ascontiguousarray(mesh.elem_to_node_ids, np.uint32)
-        self._faces = np.ascontiguousarray(mesh.interior_faces, np.uint32)
-        md = _MeshDesc(self._coords.shape[0], _dptr(self._coords), self._e2n.shape[0], _uptr(self._e2n),
-                       self._faces.shape[0], _uptr(self._faces), 0)
+        self.part = part
+        keep = []
+        md = _mesh_desc(mesh, 0 if part is None else part.rank, keep)
         cd = _CaseDesc(order, FLUX[flux], gamma, gas_constant, PRECISION[precision], device)
         ctx = ctypes.c_void_p()
-        rc = self._lib.dg_create(ctypes.byref(cd), ctypes.byref(md), ctypes.byref(ctx))
+        if part is None:
+            rc = self._lib.dg_create(ctypes.byref(cd), ctypes.byref(md), ctypes.byref(ctx))
+        else:
+            pd = part.desc()
+            rc = self._lib.dg_create_partitioned(ctypes.byref(cd), ctypes.byref(md), ctypes.byref(pd), ctypes.byref(ctx))
         if rc:
             raise DGError(rc, self._lib.dg_last_error(None).decode())
         self._ctx = ctx
@@ -293,6 +397,32 @@ class Case:
 
     def device_state_ptr(self) -> int:
         return int(self._lib.dg_device_state(self._ctx) or 0)
+
+    # -- partitioned cases ---------------------------------------------------
+    def halo_peers(self):
+        """[(peer rank, slice offset, slice count)] of this rank's halo."""
+        out = []
+        for i in range(self._lib.dg_halo_num_peers(self._ctx)):
+            r, o, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+            self._check(self._lib.dg_halo_peer(self._ctx, i, ctypes.byref(r), ctypes.byref(o), ctypes.byref(c)))
+            out.append((r.value, o.value, c.value))
+        return out
+
+    def halo_slice_doubles(self) -> int:
+        return self._lib.dg_halo_slice_doubles(self._ctx)
+
+    def halo_pack(self, buf: int, d_send: int, stream: int = 0):
+        self._check(self._lib.dg_halo_pack(self._ctx, buf, ctypes.c_void_p(d_send), ctypes.c_void_p(stream or None)))
+
+    def halo_unpack(self, buf: int, d_recv: int, stream: int = 0):
+        self._check(self._lib.dg_halo_unpack(self._ctx, buf, ctypes.c_void_p(d_recv), ctypes.c_void_p(stream or None)))
+
+    def rk4_stage(self, stage: int, dt: float, rng: int = 0):
+        """Queue RK4 stage 1..4 on the context's stream over all owned (0), interior (1) or boundary (2) elements."""
+        self._check(self._lib.dg_rk4_stage(self._ctx, int(stage), float(dt), int(rng)))
+
+    def stream_ptr(self) -> int:
+        return int(self._lib.dg_stream(self._ctx) or 0)
 
     # -- launch variants ---------------------------------------------------
     def stage_variants(self):

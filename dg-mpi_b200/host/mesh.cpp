@@ -186,6 +186,7 @@ std::string prepare_mesh(const MeshView& mv, int m, PreparedMesh& out)
     out = PreparedMesh{};
     out.ne = ne;
     out.m = m;
+    out.nowned = mv.nowned < 0 ? ne : mv.nowned;
 
     // ---- geometry: affine check and classes ----
     std::vector<double> Jall(static_cast<size_t>(ne) * 9);
@@ -282,7 +283,7 @@ std::string prepare_mesh(const MeshView& mv, int m, PreparedMesh& out)
         out.geo_class[e] = cid;
     }
     out.volume = 0.0;
-    for (int e = 0; e < ne; ++e) {
+    for (int e = 0; e < (mv.nowned < 0 ? ne : std::min(mv.nowned, ne)); ++e) {  // owned elements
         const GeoClass& g = out.classes[out.geo_class[e]];
         out.volume += 8.0 * g.djac;
         for (int a = 0; a < 3; ++a) {
@@ -330,20 +331,30 @@ std::string prepare_mesh(const MeshView& mv, int m, PreparedMesh& out)
         slot[1] = fn | (isL << 3) | (code << 4);
         return "";
     };
+    const int nowned = mv.nowned < 0 ? ne : mv.nowned;
+    if (nowned > ne || nowned < 1) return "owned element count out of range";
+    for (int e = 0; mv.elem_rank && e < nowned; ++e)
+        if (mv.elem_rank[e] != mv.rank) return "owned element " + std::to_string(e) + " has another rank";
     for (int i = 0; i < mv.nface; ++i) {
         const unsigned* r = &mv.faces[static_cast<size_t>(i) * 8];
-        if (static_cast<int>(r[0]) != mv.rank || static_cast<int>(r[4]) != mv.rank)
-            return "unsupported: face " + std::to_string(i) + " crosses ranks (single-GPU build)";
         const int eL = r[1], fL = r[2], oL = r[3], eR = r[5], fR = r[6], oR = r[7];
         if (eL >= ne || eR >= ne || fL > 5 || fR > 5 || oL > 7 || oR > 7)
             return "face " + std::to_string(i) + " has an out-of-range entry";
+        if (!mv.elem_rank) {
+            if (static_cast<int>(r[0]) != mv.rank || static_cast<int>(r[4]) != mv.rank)
+                return "unsupported: face " + std::to_string(i) + " crosses ranks (single-GPU build)";
+        } else if (static_cast<int>(r[0]) != mv.elem_rank[eL] || static_cast<int>(r[4]) != mv.elem_rank[eR]) {
+            return "face " + std::to_string(i) + " names a rank that does not own its element";
+        }
+        if (eL >= nowned && eR >= nowned) return "face " + std::to_string(i) + " joins two ghost elements";
         if (eL == eR && fL == fR) return "face " + std::to_string(i) + " connects a face to itself";
-        std::string err = add_side(eL, fL, eR, fR, oL, oR, 1);
+        // only owned elements get connectivity: ghosts are read, never computed
+        std::string err = eL < nowned ? add_side(eL, fL, eR, fR, oL, oR, 1) : std::string();
         if (!err.empty()) return err;
-        err = add_side(eR, fR, eL, fL, oR, oL, 0);
+        err = eR < nowned ? add_side(eR, fR, eL, fL, oR, oL, 0) : std::string();
         if (!err.empty()) return err;
     }
-    for (int e = 0; e < ne; ++e)
+    for (int e = 0; e < nowned; ++e)
         for (int f = 0; f < 6; ++f)
             if (out.conn[(static_cast<size_t>(e) * 6 + f) * 2] < 0)
                 return "unsupported: face " + std::to_string(f) + " of element " + std::to_string(e) +

@@ -17,6 +17,11 @@ struct MeshView {
     const unsigned* e2n = nullptr;
     const unsigned* faces = nullptr;
     const int* tag = nullptr;  // optional [ne]: elements with different tags get different geometry classes
+    // partitioned meshes: elements [nowned, nelem) are ghosts (copies of other
+    // ranks' elements whose boundary slices arrive by halo exchange), and
+    // elem_rank[e] is the owner of local element e; nowned < 0: no ghosts
+    int nowned = -1;
+    const int* elem_rank = nullptr;
 };
 
 struct BoxMesh {
@@ -46,6 +51,7 @@ struct GeoClass {
 // Everything the kernels need besides the state.
 struct PreparedMesh {
     int ne = 0, m = 0;
+    int nowned = 0;                    // elements [nowned, ne) are ghosts
     std::vector<int> geo_class;        // [ne]
     std::vector<GeoClass> classes;
     std::vector<int> conn;             // [ne][6][2]: neighbour element, packed (fn | isL<<3 | code<<4)

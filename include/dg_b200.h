@@ -211,6 +211,82 @@ int dg_sync(dg_ctx* ctx);
  * multi-GPU exchange).  Layout of the device state: [ne][5][nb]. */
 void* dg_device_state(dg_ctx* ctx);
 
+/* ---- domain decomposition over several GPUs ----
+ *
+ * Replaces the partitioned mesh of src/mesh/mesh.cpp:399-470 and the ghost
+ * trace exchange MemoryNetwork::communicate_face_solution
+ * (src/memory/memory_network.cpp:55-175).  A rank's mesh lists its owned
+ * elements first -- the first `ninterior` of them share no face with another
+ * rank -- followed by ghost elements: copies of the neighbouring ranks'
+ * elements across the partition faces (node coordinates included, so the
+ * face normals are computed exactly as on the owner).  Face rows carry the
+ * owners' ranks in columns 0 and 4 like the reference's partitioned
+ * interior_faces; elements are local ids of this mesh.
+ *
+ * The exchange moves, per face between an owned element and a ghost, one
+ * boundary slice of 5 (p+1)^2 coefficients each way (the coefficients of the
+ * element on that face; the receiver interpolates them as the on-device
+ * gather does).  Slices are grouped per peer rank and ordered by the face's
+ * left side (rank, owner-local element id, face), so slot i of one rank's
+ * send range for a peer is slot i of the peer's receive range.  Transport is
+ * the caller's (NCCL, CUDA-aware MPI, a peer copy): per RK stage s the caller
+ * packs the stage's input buffer, exchanges, unpacks, and launches the stage
+ * (the interior part may run while the exchange is in flight). */
+typedef struct dg_part_desc {
+    int nowned;              /* owned elements: local ids [0, nowned) */
+    int ninterior;           /* owned elements [0, ninterior) have no ghost neighbour */
+    const int* ghost_rank;   /* [nelem - nowned] owner rank of each ghost */
+    const int* ghost_elem;   /* [nelem - nowned] the ghost's local id on its owner */
+} dg_part_desc;
+
+/* buffers of the RK4 stepper: stage s (1..4) reads DG_BUF_U0, DG_BUF_STAGE_A,
+ * DG_BUF_STAGE_B, DG_BUF_STAGE_A and writes STAGE_A, STAGE_B, STAGE_A, U0 */
+#define DG_BUF_U0 0
+#define DG_BUF_STAGE_A 1
+#define DG_BUF_STAGE_B 2
+
+/* dg_create for one rank of a partitioned mesh (md->rank is this rank). */
+int dg_create_partitioned(const dg_case_desc* c, const dg_mesh_desc* m, const dg_part_desc* part, dg_ctx** out);
+
+/* Slab decomposition of the periodic box of dg_mesh_periodic_box along `axis`
+ * (layer * nparts / n[axis]) into the mesh of rank `part` in the form above.
+ * Sizes first: call with NULL arrays to get nnode / nelem / nface / nowned /
+ * ninterior.  global_elem[nelem] receives each local element's id in the
+ * unpartitioned box. */
+int dg_partition_periodic_box(const int n[3], const double x0[3], const double len[3], unsigned rotate_seed,
+                              int nparts, int part, int axis,
+                              int* nnode, double* node_coords, int* nelem, unsigned* elem_to_node_ids,
+                              int* nface, unsigned* interior_faces,
+                              int* nowned, int* ninterior, int* ghost_rank, int* ghost_elem, int* global_elem);
+
+/* Host-side halo plan of a partitioned mesh (no GPU needed): per peer its
+ * rank and its [offset, offset + count) range of slices; per slice the owned
+ * (element, face) sent and the ghost (element, face) received.  Sizes first:
+ * with NULL arrays, *npeers and *nslices only. */
+int dg_halo_plan(const dg_mesh_desc* m, const dg_part_desc* part, int* npeers, int* peer_rank, int* peer_offset,
+                 int* peer_count, int* nslices, int* send_elem, int* send_face, int* recv_elem, int* recv_face);
+
+/* The context's halo: number of peers, a peer's rank and slice range, and
+ * the doubles per slice (5 (p+1)^2). */
+int dg_halo_num_peers(const dg_ctx* ctx);
+int dg_halo_peer(const dg_ctx* ctx, int i, int* rank, int* offset, int* count);
+int dg_halo_slice_doubles(const dg_ctx* ctx);
+
+/* Gathers the outgoing slices of buffer `buf` (DG_BUF_*) into the device
+ * array d_send [nslices][5][(p+1)^2] / scatters d_recv into the ghost
+ * elements of `buf`.  Queued on `stream` (NULL: the context's stream). */
+int dg_halo_pack(dg_ctx* ctx, int buf, double* d_send, void* stream);
+int dg_halo_unpack(dg_ctx* ctx, int buf, const double* d_recv, void* stream);
+
+/* RK4 stage s (1..4) with time step dt on the context's stream, over the
+ * owned elements (range 0), the interior ones (range 1) or the others
+ * (range 2); not synchronised.  Four stages on all owned elements make one
+ * dg_rk4_steps step. */
+int dg_rk4_stage(dg_ctx* ctx, int stage, double dt, int range);
+
+/* The context's CUDA stream (a cudaStream_t), for ordering a transport. */
+void* dg_stream(dg_ctx* ctx);
+
 /* ---- batched ensembles ----
  *
  * Many independent cases (each its own periodic mesh, order and time step)
