@@ -87,6 +87,65 @@ DG_HD void flux_lax_friedrichs(T gamma, const T* UL, const T* UR, const T* N, T*
     for (int s = 0; s < 5; ++s) F[s] = n_mag * (T(0.5) * (FqL[s] + FqR[s]) - T(0.5) * a * (UR[s] - UL[s]));
 }
 
+// The interior flux with one reciprocal of the density: P = (gamma-1)(rE -
+// |m|^2 r1 / 2) instead of the reference's division of |m|^2 by rho (the same
+// quantity, rounded differently); returns P for the positivity check.
+template <typename T>
+DG_HD T interior_flux_r1(T gamma, const T* U, T* F)
+{
+    const T r1 = T(1.) / U[0];
+    const T ru = U[1], rv = U[2], rw = U[3], rE = U[4];
+    const T P = (gamma - T(1.0)) * (rE - T(0.5) * ((ru * ru + rv * rv + rw * rw) * r1));
+    const T u = ru * r1, v = rv * r1, w = rw * r1, H = rE + P;
+    F[0] = ru;
+    F[1] = ru * u + P;
+    F[2] = rv * u;
+    F[3] = rw * u;
+    F[4] = H * u;
+    F[5] = rv;
+    F[6] = ru * v;
+    F[7] = rv * v + P;
+    F[8] = rw * v;
+    F[9] = H * v;
+    F[10] = rw;
+    F[11] = ru * w;
+    F[12] = rv * w;
+    F[13] = rw * w + P;
+    F[14] = H * w;
+    return P;
+}
+
+// One side of a face for the Lax-Friedrichs flux: the normal flux F(U).n_hat
+// = m (m.n_hat)/rho + P n_hat, (rE + P)(m.n_hat)/rho, and the wave speed
+// |m|/rho + sqrt(gamma P / rho) of get_maxwavespeed, with one reciprocal.
+template <typename T>
+DG_HD T lf_side(T gamma, const T* U, const T* n_hat, T* Fn)
+{
+    const T r1 = T(1.) / U[0];
+    const T m2 = U[1] * U[1] + U[2] * U[2] + U[3] * U[3];
+    const T P = (gamma - T(1.0)) * (U[4] - T(0.5) * (m2 * r1));
+    const T mn = U[1] * n_hat[0] + U[2] * n_hat[1] + U[3] * n_hat[2];
+    const T vn = mn * r1;
+    Fn[0] = mn;
+    Fn[1] = U[1] * vn + P * n_hat[0];
+    Fn[2] = U[2] * vn + P * n_hat[1];
+    Fn[3] = U[3] * vn + P * n_hat[2];
+    Fn[4] = (U[4] + P) * vn;
+    return sqrt(m2) * r1 + sqrt(gamma * P * r1);
+}
+
+// Lax-Friedrichs of the stage kernel: compute_flux_laxfriedrichs with the
+// face's |N| and N/|N| precomputed and lf_side for each state.
+template <typename T>
+DG_HD void flux_lax_friedrichs_fast(T gamma, const T* UL, const T* UR, const T* n_hat, T n_mag, T* F)
+{
+    T FnL[5], FnR[5];
+    const T aL = lf_side(gamma, UL, n_hat, FnL);
+    const T aR = lf_side(gamma, UR, n_hat, FnR);
+    const T a = aR > aL ? aR : aL;
+    for (int s = 0; s < 5; ++s) F[s] = n_mag * (T(0.5) * (FnL[s] + FnR[s]) - T(0.5) * a * (UR[s] - UL[s]));
+}
+
 // Lax-Friedrichs with the face's normal data precomputed (it is constant on a
 // face of an affine element): n_mag = |N| and n_hat = N / n_mag, evaluated
 // once on the host by the formulas of flux_lax_friedrichs.

@@ -116,6 +116,7 @@ struct Lay {
     static constexpr int VS = odd(NB);           // per-variable stride of U / residual
     static constexpr int ES = 5 * VS;            // per-element stride of U / residual
     static constexpr int FS = odd(NF);           // per-(face, variable) stride of traces
+    static constexpr int NS = odd(N2);           // per-(face, variable) stride of neighbour slices
     static constexpr int X1S = odd(N2 * M);      // [bz][by][qx] block
     static constexpr int X2S = odd(N * NF);      // [bz][qy][qx] block
     // per-element work area: face phase {Tr[6][5], Tn[6][5]} x FS;
@@ -123,10 +124,10 @@ struct Lay {
     static constexpr int face = 60 * FS;
     static constexpr int vol = 5 * X2S + cmax(5 * X1S, GV * (3 * X2S + 2 * X1S));
     static constexpr int W = odd(cmax(face, vol));
-    // FP64 operand region: first the neighbours' boundary slices [30][N2]
+    // FP64 operand region: first the neighbours' boundary slices [30][NS]
     // (streamed in during the volume phase), then the batch's U0 and RK
     // accumulator [2][ES] (streamed in during the face phase)
-    static constexpr int OPS = cmax(2 * ES, 30 * N2);
+    static constexpr int OPS = cmax(2 * ES, 30 * NS);
     // FP64: U (double-buffered prefetch), residual, operand region
     static constexpr int per_elem_f64 = 2 * ES + ES + OPS;
     // bytes per element, work area in T
@@ -212,7 +213,7 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
 {
     using L = Lay<P, G, T>;
     constexpr int N = L::N, M = L::M, NB = L::NB, NF = L::NF, N2 = L::N2;
-    constexpr int VS = L::VS, ES = L::ES, FS = L::FS, X1S = L::X1S, X2S = L::X2S, W = L::W, GV = L::GV;
+    constexpr int VS = L::VS, ES = L::ES, FS = L::FS, NS = L::NS, X1S = L::X1S, X2S = L::X2S, W = L::W, GV = L::GV;
     constexpr int OPS = L::OPS;
     extern __shared__ double smem[];
     double* sUbuf = smem;                  // [2][E][ES]
@@ -245,7 +246,7 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
             const int ge = min(e0 + e, a.ne - 1);
             const int2 c = a.conn[ge * 6 + f];
             const double* src = a.Us + ((size_t)c.x * 5 + v) * NB;
-            double* dst = sOps + e * OPS + fv * N2;
+            double* dst = sOps + e * OPS + fv * NS;
 #pragma unroll
             for (int b1 = 0; b1 < N; ++b1)
 #pragma unroll
@@ -330,14 +331,13 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
                         for (int bz = 0; bz < N; ++bz) s += Bt[qz * N + bz] * xz[v][bz];
                         U[v] = s;
                     }
+                    T F[15];
+                    const T p = dgp::interior_flux_r1(gamma, U, F);
                     if (g == 0) {
-                        const T p = dgp::pressure(gamma, U);
                         if (!(U[0] > T(0))) status |= kStatusRho;
                         if (!(p > T(0))) status |= kStatusPressure;
                         if (U[0] != U[0] || p != p) status |= kStatusNaN;
                     }
-                    T F[15];
-                    dgp::interior_flux(gamma, U, F);
                     const T wq = wxy * Wt[qz];
 #pragma unroll
                     for (int vv = 0; vv < GV; ++vv) {
@@ -418,7 +418,7 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
         for (int t = tid; t < E * 30; t += NT) {
             const int v = t % 5, f = (t / 5) % 6, e = t / 30;
             T sn[N][N], so[N][N];
-            const double* nb = sOps + e * OPS + (f * 5 + v) * N2;
+            const double* nb = sOps + e * OPS + (f * 5 + v) * NS;
             const double* own = sU + e * ES + v * VS;
 #pragma unroll
             for (int b1 = 0; b1 < N; ++b1)
@@ -466,7 +466,7 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
                     if (!dgp::flux_hllc_n(gamma, UL, UR, nu, nmag, Fo)) status |= kStatusHLLC;
                 } else {
                     const T nh[3] = {T(g->nhat[fl][0]), T(g->nhat[fl][1]), T(g->nhat[fl][2])};
-                    dgp::flux_lax_friedrichs_n(gamma, UL, UR, nh, nmag, Fo);
+                    dgp::flux_lax_friedrichs_fast(gamma, UL, UR, nh, nmag, Fo);
                 }
                 const T w = Wt[cidx % M] * Wt[cidx / M];
                 const T sgn = isL ? T(-1.0) : T(1.0);
@@ -560,7 +560,8 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
         }
         __syncthreads();
         for (int i = tid; i < E * 5 * N2; i += NT) {
-            const int bx = i % N, bz = (i / N) % N, ev = i / N2;
+            // (element, variable) fastest: consecutive threads are VS apart (odd)
+            const int ev = i % (5 * E), bxz = i / (5 * E), bx = bxz % N, bz = bxz / N;
             double* r = sRes + (ev / 5) * ES + (ev % 5) * VS + bz * N2 + bx;  // pencil along y
             double t[N];
 #pragma unroll
