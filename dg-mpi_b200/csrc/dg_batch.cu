@@ -38,7 +38,7 @@ struct BatchGroup {
 
 struct BatchCase {
     int group = 0, e0 = 0, ne = 0, order = 0;
-    double dt = 0.0, volume = 0.0;
+    double dt = 0.0, volume = 0.0, eref = 0.0;
 };
 
 }  // namespace
@@ -91,15 +91,17 @@ void release_batch(dg_batch* b)
 
 bool case_ok(const dg_batch* b, int c) { return b && c >= 0 && c < static_cast<int>(b->cases.size()); }
 
-// per-class time steps of every group to the device; the previous graph
-// launches have finished (every stepping call synchronises)
+// per-class time steps and energy references of every group to the device;
+// the previous graph launches have finished (every stepping call synchronises)
 int upload_time_steps(dg_batch* b)
 {
     if (!b->geo_dirty) return DG_OK;
     for (auto& g : b->groups) {
-        std::vector<double> dtf(g.class_case.size());
-        for (size_t k = 0; k < dtf.size(); ++k) dtf[k] = b->cases[g.class_case[k]].dt;
-        const int rc = dgi::upload_geometry(g.ctx, dtf.data(), g.ctx->stream);
+        for (size_t k = 0; k < g.class_case.size(); ++k) {
+            g.ctx->class_dtf[k] = b->cases[g.class_case[k]].dt;
+            g.ctx->class_eref[k] = b->cases[g.class_case[k]].eref;
+        }
+        const int rc = dgi::upload_geometry(g.ctx, g.ctx->stream);
         if (rc) return gfail(b, rc, g);
     }
     b->geo_dirty = false;
@@ -330,9 +332,14 @@ int dg_batch_case_info(const dg_batch* b, int c, int* order, int* nelem, int* gr
 int dg_batch_set_state(dg_batch* b, int c, const double* Uc)
 {
     if (!case_ok(b, c) || !Uc) return bfail(b, DG_ERR_ARG, "dg_batch_set_state: bad argument");
-    const BatchCase& k = b->cases[c];
+    BatchCase& k = b->cases[c];
     BatchGroup& g = b->groups[k.group];
     if (cudaSetDevice(b->device) != cudaSuccess) return bfail(b, DG_ERR_CUDA, "cudaSetDevice failed");
+    const double e = dgi::energy_reference(g.ctx, Uc, k.ne);
+    if (e != k.eref) {
+        k.eref = e;
+        b->geo_dirty = true;
+    }
     const int rc = dgi::upload_range(g.ctx, Uc, g.ctx->d_U0, k.e0, k.ne);
     return rc ? gfail(b, rc, g) : DG_OK;
 }
@@ -355,12 +362,17 @@ int dg_batch_project_ic(dg_batch* b, int c, int ic_type, const double* data, int
     if (ndata < need[ic_type] || (ndata > 0 && !data)) return bfail(b, DG_ERR_ARG, "initial condition needs more data values");
     double d[16] = {0};
     for (int i = 0; i < ndata && i < 16; ++i) d[i] = data[i];
-    const BatchCase& k = b->cases[c];
+    BatchCase& k = b->cases[c];
     BatchGroup& g = b->groups[k.group];
     std::vector<double> U(static_cast<size_t>(k.ne) * g.ctx->nb * 5);
     dgh::project_initial_condition(g.ctx->pm, g.ctx->tab, ic_type, d, g.gamma, g.R, t, U.data(), k.e0, k.e0 + k.ne);
     if (Uc) std::memcpy(Uc, U.data(), U.size() * sizeof(double));
     if (cudaSetDevice(b->device) != cudaSuccess) return bfail(b, DG_ERR_CUDA, "cudaSetDevice failed");
+    const double e = dgi::energy_reference(g.ctx, U.data(), k.ne);
+    if (e != k.eref) {
+        k.eref = e;
+        b->geo_dirty = true;
+    }
     const int rc = dgi::upload_range(g.ctx, U.data(), g.ctx->d_U0, k.e0, k.ne);
     return rc ? gfail(b, rc, g) : DG_OK;
 }

@@ -460,7 +460,18 @@ int download_range(dg_ctx* c, const double* src, double* Uc, int e0, int ne)
 int upload_state_host_layout(dg_ctx* c, const double* Uc, double* dst) { return upload_range(c, Uc, dst, 0, c->ne); }
 int download_host_layout(dg_ctx* c, const double* src, double* Uc) { return download_range(c, src, Uc, 0, c->ne); }
 
-int upload_geometry(dg_ctx* c, const double* dtf, cudaStream_t s)
+double energy_reference(const dg_ctx* c, const double* Uc, int ne)
+{
+    if (c->precision != DG_PREC_MIXED_FP32 || ne <= 0) return 0.0;
+    const long long n = 1LL * ne * c->nb;
+    double sum = 0.0;
+#pragma omp parallel for reduction(+ : sum)
+    for (long long i = 0; i < n; ++i) sum += Uc[i * 5 + 4];
+    const double m = sum / static_cast<double>(n);
+    return std::isfinite(m) ? m : 0.0;
+}
+
+int upload_geometry(dg_ctx* c, cudaStream_t s)
 {
     // geometry classes, followed by their Jacobians (used by the reductions)
     const size_t ncls = c->pm.classes.size();
@@ -470,7 +481,8 @@ int upload_geometry(dg_ctx* c, const double* dtf, cudaStream_t s)
         const auto& src = c->pm.classes[k];
         std::memcpy(g.JD, src.JD, sizeof(g.JD));
         g.inv_djac = src.inv_djac;
-        g.dtf = dtf ? dtf[k] : 1.0;
+        g.dtf = c->class_dtf[k];
+        g.eref = c->class_eref[k];
         std::memcpy(g.N, src.N, sizeof(g.N));
         std::memcpy(g.nmag, src.nmag, sizeof(g.nmag));
         std::memcpy(g.nhat, src.nhat, sizeof(g.nhat));
@@ -669,7 +681,9 @@ int dgi::create_ctx(const dg_case_desc* cd, const dg_mesh_desc* md, const int* e
         c->err = std::string("table upload failed: ") + cudaGetErrorString(cudaGetLastError());
         return bail(DG_ERR_CUDA);
     }
-    if ((rc = upload_geometry(c, nullptr, c->stream)) != DG_OK) return bail(rc);
+    c->class_dtf.assign(ncls, 1.0);
+    c->class_eref.assign(ncls, 0.0);
+    if ((rc = upload_geometry(c, c->stream)) != DG_OK) return bail(rc);
     *out = c;
     return DG_OK;
 }
@@ -838,10 +852,26 @@ const char* dg_last_error(const dg_ctx* ctx)
 int dg_num_basis(const dg_ctx* ctx) { return ctx ? ctx->nb : 0; }
 int dg_num_elements(const dg_ctx* ctx) { return ctx ? ctx->ne : 0; }
 
+namespace {
+
+// the FP32 residual's energy reference follows the uploaded state
+int set_energy_reference(dg_ctx* c, const double* Uc)
+{
+    if (c->precision != DG_PREC_MIXED_FP32) return DG_OK;
+    const double e = energy_reference(c, Uc, c->ne);
+    if (c->class_eref.empty() || c->class_eref[0] == e) return DG_OK;
+    std::fill(c->class_eref.begin(), c->class_eref.end(), e);
+    return upload_geometry(c, c->stream);
+}
+
+}  // namespace
+
 int dg_set_state(dg_ctx* c, const double* Uc)
 {
     if (!c || !Uc) return fail(c, DG_ERR_ARG, "dg_set_state: null argument");
     DG_CUDA(c, cudaSetDevice(c->device));
+    const int rc = set_energy_reference(c, Uc);
+    if (rc) return rc;
     return upload_state_host_layout(c, Uc, c->d_U0);
 }
 
@@ -1042,6 +1072,8 @@ int dg_project_ic(dg_ctx* c, int ic_type, const double* data, int ndata, double 
     dgh::project_initial_condition(c->pm, c->tab, ic_type, d, c->gamma, c->R, t, U.data(), 0, c->ne);
     if (Uc) std::memcpy(Uc, U.data(), U.size() * sizeof(double));
     DG_CUDA(c, cudaSetDevice(c->device));
+    const int rc = set_energy_reference(c, U.data());
+    if (rc) return rc;
     return upload_state_host_layout(c, U.data(), c->d_U0);
 }
 

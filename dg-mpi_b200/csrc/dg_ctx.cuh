@@ -43,6 +43,9 @@ struct dg_ctx {
     cudaGraphExec_t graph_exec = nullptr;
     double graph_dt = 0.0;
     dgh::PreparedMesh pm;
+    // per geometry class: time-step factor (a case's dt in a batch, else 1)
+    // and the FP32 residual's energy reference (0 on the FP64 path)
+    std::vector<double> class_dtf, class_eref;
     dgh::Tables1D tab;
     unsigned status_accum = 0;
     std::string err;
@@ -85,8 +88,11 @@ int download_range(dg_ctx* c, const double* src, double* Uc, int e0, int ne);
 int run_reduce(dg_ctx* c, int kind, int ic_type, const double* data, int ndata, double t, double* out5, int e0, int ne,
                double gamma, double R);
 
-// uploads the geometry classes with per-class time-step factors dtf[class]
-// (nullptr: all 1)
-int upload_geometry(dg_ctx* c, const double* dtf, cudaStream_t s);
+// uploads the geometry classes with class_dtf / class_eref
+int upload_geometry(dg_ctx* c, cudaStream_t s);
+
+// mean of rE over a host state [ne][nb][5] (the FP32 residual's energy
+// reference), 0 for an FP64 context
+double energy_reference(const dg_ctx* c, const double* Uc, int ne);
 
 }  // namespace dgi

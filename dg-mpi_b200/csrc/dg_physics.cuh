@@ -90,13 +90,21 @@ DG_HD void flux_lax_friedrichs(T gamma, const T* UL, const T* UR, const T* N, T*
 // The interior flux with one reciprocal of the density: P = (gamma-1)(rE -
 // |m|^2 r1 / 2) instead of the reference's division of |m|^2 by rho (the same
 // quantity, rounded differently); returns P for the positivity check.
-template <typename T>
-DG_HD T interior_flux_r1(T gamma, const T* U, T* F)
+//
+// SHIFT: the state's energy is stored relative to a constant E_ref
+// (U[4] = rE - E_ref, so that FP32 keeps its digits for the fluctuation when
+// rE is large, as at low Mach).  P is then P - (gamma-1) E_ref: the constant
+// part of the pressure is left out of the momentum fluxes -- a constant flux
+// has zero weak divergence (the volume and face quadratures integrate it
+// exactly, so the two terms cancel) -- and the energy flux adds it back,
+// (rE + P) u = (U[4] + P + hr) u with hr = gamma E_ref.
+template <typename T, bool SHIFT = false>
+DG_HD T interior_flux_r1(T gamma, const T* U, T* F, T hr = T(0))
 {
     const T r1 = T(1.) / U[0];
     const T ru = U[1], rv = U[2], rw = U[3], rE = U[4];
     const T P = (gamma - T(1.0)) * (rE - T(0.5) * ((ru * ru + rv * rv + rw * rw) * r1));
-    const T u = ru * r1, v = rv * r1, w = rw * r1, H = rE + P;
+    const T u = ru * r1, v = rv * r1, w = rw * r1, H = SHIFT ? rE + P + hr : rE + P;
     F[0] = ru;
     F[1] = ru * u + P;
     F[2] = rv * u;
@@ -118,8 +126,10 @@ DG_HD T interior_flux_r1(T gamma, const T* U, T* F)
 // One side of a face for the Lax-Friedrichs flux: the normal flux F(U).n_hat
 // = m (m.n_hat)/rho + P n_hat, (rE + P)(m.n_hat)/rho, and the wave speed
 // |m|/rho + sqrt(gamma P / rho) of get_maxwavespeed, with one reciprocal.
-template <typename T>
-DG_HD T lf_side(T gamma, const T* U, const T* n_hat, T* Fn)
+// SHIFT as for interior_flux_r1, with pref = (gamma-1) E_ref restoring the
+// full pressure in the wave speed.
+template <typename T, bool SHIFT = false>
+DG_HD T lf_side(T gamma, const T* U, const T* n_hat, T* Fn, T hr = T(0), T pref = T(0))
 {
     const T r1 = T(1.) / U[0];
     const T m2 = U[1] * U[1] + U[2] * U[2] + U[3] * U[3];
@@ -130,18 +140,19 @@ DG_HD T lf_side(T gamma, const T* U, const T* n_hat, T* Fn)
     Fn[1] = U[1] * vn + P * n_hat[0];
     Fn[2] = U[2] * vn + P * n_hat[1];
     Fn[3] = U[3] * vn + P * n_hat[2];
-    Fn[4] = (U[4] + P) * vn;
-    return sqrt(m2) * r1 + sqrt(gamma * P * r1);
+    Fn[4] = (SHIFT ? U[4] + P + hr : U[4] + P) * vn;
+    return sqrt(m2) * r1 + sqrt(gamma * (SHIFT ? P + pref : P) * r1);
 }
 
 // Lax-Friedrichs of the stage kernel: compute_flux_laxfriedrichs with the
 // face's |N| and N/|N| precomputed and lf_side for each state.
-template <typename T>
-DG_HD void flux_lax_friedrichs_fast(T gamma, const T* UL, const T* UR, const T* n_hat, T n_mag, T* F)
+template <typename T, bool SHIFT = false>
+DG_HD void flux_lax_friedrichs_fast(T gamma, const T* UL, const T* UR, const T* n_hat, T n_mag, T* F, T hr = T(0),
+                                    T pref = T(0))
 {
     T FnL[5], FnR[5];
-    const T aL = lf_side(gamma, UL, n_hat, FnL);
-    const T aR = lf_side(gamma, UR, n_hat, FnR);
+    const T aL = lf_side<T, SHIFT>(gamma, UL, n_hat, FnL, hr, pref);
+    const T aR = lf_side<T, SHIFT>(gamma, UR, n_hat, FnR, hr, pref);
     const T a = aR > aL ? aR : aL;
     for (int s = 0; s < 5; ++s) F[s] = n_mag * (T(0.5) * (FnL[s] + FnR[s]) - T(0.5) * a * (UR[s] - UL[s]));
 }

@@ -62,6 +62,7 @@ struct GeoDev {
     double JD[9];
     double inv_djac;
     double dtf;           // time-step factor: the stage update scales by dt * dtf (1, or a case's dt in a batch)
+    double eref;          // FP32 residual: energy reference E_ref (state energy enters as rE - E_ref); 0 for FP64
     double N[6][3];
     double nmag[6];       // |N| per face
     double nhat[6][3];    // N / |N| (Lax-Friedrichs)
@@ -227,6 +228,8 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
     const double* __restrict__ Mi = a.tab.Minv;
     const int tid = threadIdx.x;
     const T gamma = T(a.gamma);
+    // the FP32 residual works on rE - E_ref (see dgp::interior_flux_r1)
+    constexpr bool kShift = sizeof(T) == 4;
     unsigned status = 0;
     const int stride = gridDim.x * E;
     const int e_first = a.e_begin + blockIdx.x * E;
@@ -262,9 +265,10 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
         for (int i = tid; i < E * 5 * N2; i += NT) {
             const int v = i % 5, byz = (i / 5) % N2, e = i / (5 * N2);
             const double* u = sU + e * ES + v * VS + byz * N;
+            const double sh = kShift && v == 4 ? a.geo[a.geo_class[min(e0 + e, a.ne - 1)]].eref : 0.0;
             T row[N];
 #pragma unroll
-            for (int bx = 0; bx < N; ++bx) row[bx] = T(u[bx]);
+            for (int bx = 0; bx < N; ++bx) row[bx] = kShift ? T(u[bx] - sh) : T(u[bx]);
             T* o = X1 + e * W + v * X1S + byz * M;
 #pragma unroll
             for (int qx = 0; qx < M; ++qx) {
@@ -310,6 +314,8 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
                     for (int bz = 0; bz < N; ++bz) xz[v][bz] = X2[e * W + v * X2S + bz * NF + qxy];
                 const int ge = min(e0 + e, a.ne - 1);
                 const GeoDev* geo = a.geo + a.geo_class[ge];
+                const T hr = kShift ? T(a.gamma * geo->eref) : T(0);
+                const T pref = kShift ? T((a.gamma - 1.0) * geo->eref) : T(0);
                 T JD[9];
 #pragma unroll
                 for (int k = 0; k < 9; ++k) JD[k] = T(geo->JD[k]);
@@ -332,10 +338,10 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
                         U[v] = s;
                     }
                     T F[15];
-                    const T p = dgp::interior_flux_r1(gamma, U, F);
+                    const T p = dgp::interior_flux_r1<T, kShift>(gamma, U, F, hr);
                     if (g == 0) {
                         if (!(U[0] > T(0))) status |= kStatusRho;
-                        if (!(p > T(0))) status |= kStatusPressure;
+                        if (!(p + pref > T(0))) status |= kStatusPressure;
                         if (U[0] != U[0] || p != p) status |= kStatusNaN;
                     }
                     const T wq = wxy * Wt[qz];
@@ -420,12 +426,14 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
             T sn[N][N], so[N][N];
             const double* nb = sOps + e * OPS + (f * 5 + v) * NS;
             const double* own = sU + e * ES + v * VS;
+            // both sides in the own element's energy frame
+            const double sh = kShift && v == 4 ? a.geo[a.geo_class[min(e0 + e, a.ne - 1)]].eref : 0.0;
 #pragma unroll
             for (int b1 = 0; b1 < N; ++b1)
 #pragma unroll
                 for (int b0 = 0; b0 < N; ++b0) {
-                    sn[b1][b0] = T(nb[b1 * N + b0]);
-                    so[b1][b0] = T(own[slice_index<N>(f, b0, b1)]);
+                    sn[b1][b0] = kShift ? T(nb[b1 * N + b0] - sh) : T(nb[b1 * N + b0]);
+                    so[b1][b0] = kShift ? T(own[slice_index<N>(f, b0, b1)] - sh) : T(own[slice_index<N>(f, b0, b1)]);
                 }
             interp2d<N, M, T>(Bt, so, sW + e * W + (f * 5 + v) * FS);
             interp2d<N, M, T>(Bt, sn, sW + e * W + 30 * FS + (f * 5 + v) * FS);
@@ -461,12 +469,23 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
                 const GeoDev* g = a.geo + (isL ? a.geo_class[ge] : a.geo_class[c.x]);
                 const int fl = isL ? f : fn;
                 const T nmag = T(g->nmag[fl]);
+                const double eref = kShift ? a.geo[a.geo_class[ge]].eref : 0.0;
                 if (a.flux == 1) {
                     const T nu[3] = {T(g->nunit[fl][0]), T(g->nunit[fl][1]), T(g->nunit[fl][2])};
+                    if (kShift) {  // HLLC takes the full energy
+                        UL[4] += T(eref);
+                        UR[4] += T(eref);
+                    }
                     if (!dgp::flux_hllc_n(gamma, UL, UR, nu, nmag, Fo)) status |= kStatusHLLC;
+                    if (kShift) {  // every HLLC branch carries P_side |N| n in the momenta: drop the constant part
+                        const T pn = nmag * T((a.gamma - 1.0) * eref);
+#pragma unroll
+                        for (int d = 0; d < 3; ++d) Fo[1 + d] -= pn * nu[d];
+                    }
                 } else {
                     const T nh[3] = {T(g->nhat[fl][0]), T(g->nhat[fl][1]), T(g->nhat[fl][2])};
-                    dgp::flux_lax_friedrichs_fast(gamma, UL, UR, nh, nmag, Fo);
+                    dgp::flux_lax_friedrichs_fast<T, kShift>(gamma, UL, UR, nh, nmag, Fo, T(a.gamma * eref),
+                                                             T((a.gamma - 1.0) * eref));
                 }
                 const T w = Wt[cidx % M] * Wt[cidx / M];
                 const T sgn = isL ? T(-1.0) : T(1.0);
