@@ -133,6 +133,11 @@ struct Lay {
     static constexpr int per_elem_f64 = 2 * ES + ES + OPS;
     // bytes per element, work area in T
     static constexpr size_t bytes_per_elem = sizeof(double) * per_elem_f64 + sizeof(T) * W;
+    // face metadata of a batch, staged once per batch for the flux phase:
+    // per element its energy reference, per face the left element's normal
+    // data {n (LF: N/|N|, HLLC: N*(1/|N|)), |N|}, the role bit and the row of
+    // the face-point permutation
+    static constexpr size_t meta_bytes_per_elem = sizeof(double) + sizeof(T) * 24 + sizeof(int) * 6 + 6 * NF;
 };
 
 template <int P, int G>
@@ -221,6 +226,12 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
     double* sRes = sUbuf + 2 * E * ES;     // [E][ES]
     double* sOps = sRes + E * ES;          // [E][OPS] neighbour slices, then U0 | acc
     T* sW = reinterpret_cast<T*>(sOps + E * OPS);  // [E][W] in the residual's arithmetic
+    // face metadata (see Lay::meta_bytes_per_elem), 16-byte aligned after sW
+    unsigned char* meta = reinterpret_cast<unsigned char*>(smem) + ((E * L::bytes_per_elem + 15) / 16) * 16;
+    double* sEref = reinterpret_cast<double*>(meta);                  // [E]
+    T* sFn = reinterpret_cast<T*>(sEref + E);                          // [E*6][4]
+    int* sFi = reinterpret_cast<int*>(sFn + E * 24);                   // [E*6] left-role bit
+    unsigned char* sCm = reinterpret_cast<unsigned char*>(sFi + E * 6); // [E*6][NF]
     const bool need_u0_acc = a.mode == kModeRK2 || a.mode == kModeRK3 || a.mode == kModeRK4;
     const T* __restrict__ Bt = TabSel<T>::B(a.tab);
     const T* __restrict__ Dt = TabSel<T>::D(a.tab);
@@ -254,6 +265,21 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
             for (int b1 = 0; b1 < N; ++b1)
 #pragma unroll
                 for (int b0 = 0; b0 < N; ++b0) cp_async8(dst + b1 * N + b0, src + slice_index<N>(c.y & 7, b0, b1));
+            // this face's metadata for the flux phase, shared out over the five variable tasks
+            const int fm = e * 6 + f, isL = (c.y >> 3) & 1, code = c.y >> 4;
+            for (int q = v; q < NF; q += 5) sCm[fm * NF + q] = a.cmap[code * NF + q];
+            if (v == 0) {
+                // the normal is the left element's (helpers.cpp:440-446)
+                const GeoDev* g = a.geo + (isL ? a.geo_class[ge] : a.geo_class[c.x]);
+                const int fl = isL ? f : (c.y & 7);
+                const double* n = a.flux == 1 ? g->nunit[fl] : g->nhat[fl];
+                sFn[fm * 4 + 0] = T(n[0]);
+                sFn[fm * 4 + 1] = T(n[1]);
+                sFn[fm * 4 + 2] = T(n[2]);
+                sFn[fm * 4 + 3] = T(g->nmag[fl]);
+                sFi[fm] = isL;
+                if (f == 0) sEref[e] = kShift ? a.geo[a.geo_class[ge]].eref : 0.0;
+            }
         }
         cp_async_commit();
         if (e0 + stride < a.ne) prefetch_batch<P, G, E, NT>(a.Us, a.ne, e0 + stride, sUbuf + (buf ^ 1) * E * ES, ES);
@@ -452,10 +478,8 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
             constexpr int total = E * 6 * NF;
             auto point = [&](int i, T (&Fo)[5], int& off) {
                 const int cidx = i % NF, f = (i / NF) % 6, e = i / (6 * NF);
-                const int ge = min(e0 + e, a.ne - 1);
-                const int2 c = a.conn[ge * 6 + f];
-                const int fn = c.y & 7, isL = (c.y >> 3) & 1, code = c.y >> 4;
-                const int cn = a.cmap[code * NF + cidx];
+                const int fm = e * 6 + f, isL = sFi[fm];
+                const int cn = sCm[fm * NF + cidx];
                 const T* Tr = sW + e * W + f * 5 * FS;
                 const T* Tn = sW + e * W + 30 * FS + f * 5 * FS;
                 T UL[5], UR[5];
@@ -465,13 +489,11 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
                     UL[v] = isL ? uo : un;  // element-wise selects keep both in registers
                     UR[v] = isL ? un : uo;
                 }
-                // the normal is the left element's (helpers.cpp:440-446)
-                const GeoDev* g = a.geo + (isL ? a.geo_class[ge] : a.geo_class[c.x]);
-                const int fl = isL ? f : fn;
-                const T nmag = T(g->nmag[fl]);
-                const double eref = kShift ? a.geo[a.geo_class[ge]].eref : 0.0;
+                // the left element's normal data, staged with the neighbour slices
+                const T nmag = sFn[fm * 4 + 3];
+                const double eref = kShift ? sEref[e] : 0.0;
                 if (a.flux == 1) {
-                    const T nu[3] = {T(g->nunit[fl][0]), T(g->nunit[fl][1]), T(g->nunit[fl][2])};
+                    const T nu[3] = {sFn[fm * 4 + 0], sFn[fm * 4 + 1], sFn[fm * 4 + 2]};
                     if (kShift) {  // HLLC takes the full energy
                         UL[4] += T(eref);
                         UR[4] += T(eref);
@@ -483,7 +505,7 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
                         for (int d = 0; d < 3; ++d) Fo[1 + d] -= pn * nu[d];
                     }
                 } else {
-                    const T nh[3] = {T(g->nhat[fl][0]), T(g->nhat[fl][1]), T(g->nhat[fl][2])};
+                    const T nh[3] = {sFn[fm * 4 + 0], sFn[fm * 4 + 1], sFn[fm * 4 + 2]};
                     dgp::flux_lax_friedrichs_fast<T, kShift>(gamma, UL, UR, nh, nmag, Fo, T(a.gamma * eref),
                                                              T((a.gamma - 1.0) * eref));
                 }
@@ -636,7 +658,7 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
 template <int P, int E, int G, typename T>
 constexpr size_t stage_smem_bytes()
 {
-    return (size_t)E * Lay<P, G, T>::bytes_per_elem;
+    return ((E * Lay<P, G, T>::bytes_per_elem + 15) / 16) * 16 + E * Lay<P, G, T>::meta_bytes_per_elem;
 }
 
 // ---- compiled launch variants (one translation unit per order) ----
