@@ -364,17 +364,28 @@ int dg_batch_project_ic(dg_batch* b, int c, int ic_type, const double* data, int
     for (int i = 0; i < ndata && i < 16; ++i) d[i] = data[i];
     BatchCase& k = b->cases[c];
     BatchGroup& g = b->groups[k.group];
-    std::vector<double> U(static_cast<size_t>(k.ne) * g.ctx->nb * 5);
-    dgh::project_initial_condition(g.ctx->pm, g.ctx->tab, ic_type, d, g.gamma, g.R, t, U.data(), k.e0, k.e0 + k.ne);
-    if (Uc) std::memcpy(Uc, U.data(), U.size() * sizeof(double));
     if (cudaSetDevice(b->device) != cudaSuccess) return bfail(b, DG_ERR_CUDA, "cudaSetDevice failed");
-    const double e = dgi::energy_reference(g.ctx, U.data(), k.ne);
+    int rc = dgi::project_ic_device(g.ctx, ic_type, d, 16, t, g.gamma, g.R, k.e0, k.ne);
+    if (rc) return gfail(b, rc, g);
+    const bool mixed = g.ctx->precision == DG_PREC_MIXED_FP32;
+    if (!Uc && !mixed) {
+        if (cudaStreamSynchronize(g.ctx->stream) != cudaSuccess) return bfail(b, DG_ERR_CUDA, "projection failed");
+        return DG_OK;
+    }
+    std::vector<double> tmp;
+    double* host = Uc;
+    if (!host) {
+        tmp.resize(static_cast<size_t>(k.ne) * g.ctx->nb * 5);
+        host = tmp.data();
+    }
+    rc = dgi::download_range(g.ctx, g.ctx->d_U0, host, k.e0, k.ne);
+    if (rc) return gfail(b, rc, g);
+    const double e = dgi::energy_reference(g.ctx, host, k.ne);
     if (e != k.eref) {
         k.eref = e;
         b->geo_dirty = true;
     }
-    const int rc = dgi::upload_range(g.ctx, U.data(), g.ctx->d_U0, k.e0, k.ne);
-    return rc ? gfail(b, rc, g) : DG_OK;
+    return DG_OK;
 }
 
 int dg_batch_cfl_time_step(dg_batch* b, int c, const double* Uc, double cfl, double* dt)

@@ -43,6 +43,7 @@ __constant__ double cBe[dgk::kMaxP + 1][kMaxMe * (dgk::kMaxP + 1)];
 __constant__ double cWe[dgk::kMaxP + 1][kMaxMe];
 __constant__ double cXe[dgk::kMaxP + 1][kMaxMe];
 __constant__ double cXq[dgk::kMaxP + 1][dgk::kMaxP + 2];
+__constant__ double cMi[dgk::kMaxP + 1][(dgk::kMaxP + 1) * (dgk::kMaxP + 1)];
 
 std::mutex g_table_mutex;
 bool g_tables_loaded[64] = {};
@@ -80,7 +81,7 @@ int load_constant_tables(dg_ctx* c)
         std::copy(t.xe.begin(), t.xe.end(), Xe[p]);
     }
     (void)Dm;
-    (void)Mi;
+    DG_CUDA(c, cudaMemcpyToSymbol(cMi, Mi, sizeof(Mi)));
     DG_CUDA(c, cudaMemcpyToSymbol(cVB, B, sizeof(B)));
     DG_CUDA(c, cudaMemcpyToSymbol(cVW, W, sizeof(W)));
     DG_CUDA(c, cudaMemcpyToSymbol(cBe, Be, sizeof(Be)));
@@ -325,6 +326,151 @@ int run_reduce(dg_ctx* c, int kind, int ic_type, const double* data, int ndata, 
     for (int b = 0; b < c->red_grid; ++b)
         for (int v = 0; v < 5; ++v) out5[v] += part[static_cast<size_t>(b) * 5 + v];
     return DG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// L2 projection of an initial condition on the device: the steps of
+// dgh::project_initial_condition (Solver::init_state_from_fcn +
+// SolverTools::L2_projection, src/solver/base.cpp:113-223,
+// src/solver/tools.cpp:66-122) for affine elements, one CTA per element:
+// f = U_ic(x_q) w_q det J at the 2*max(p,1)+2 point rule, rhs = (Be x Be x Be)^T f
+// contracted x, y, z, then U = (Minv x Minv x Minv) rhs / det J.
+
+struct ProjectArgs {
+    double* U;              // device state [ne][5][nb]
+    const int* geo_class;
+    const GeoDev* geo;
+    const double* X0;       // [ne][3]
+    const double* J;        // [nclasses][9]
+    int e_begin, e_end, ic_type;
+    double gamma, R, t;
+    double data[16];
+};
+
+template <int P>
+constexpr int project_points() { return P > 1 ? 2 * P + 2 : 4; }
+
+template <int P>
+constexpr size_t project_smem_bytes()
+{
+    constexpr int N = P + 1, ME = project_points<P>();
+    return sizeof(double) * 5 * (ME * ME * ME + ME * ME * N + ME * N * N + N * N * N);
+}
+
+template <int P>
+__global__ void __launch_bounds__(256) project_kernel(ProjectArgs a)
+{
+    constexpr int N = P + 1, NB = N * N * N, ME = project_points<P>(), Q = ME * ME * ME;
+    extern __shared__ double psm[];
+    double* f = psm;                     // [5][k][j][i]
+    double* t1 = f + 5 * Q;              // [5][k][j][bx]
+    double* t2 = t1 + 5 * ME * ME * N;   // [5][k][by][bx]
+    double* r = t2 + 5 * ME * N * N;     // [5][bz][by][bx]
+    const double* Be = cBe[P];
+    const double* We = cWe[P];
+    const double* Xe = cXe[P];
+    const double* Mi = cMi[P];
+    for (int e = a.e_begin + blockIdx.x; e < a.e_end; e += gridDim.x) {
+        const int cls = a.geo_class[e];
+        const double* J = a.J + cls * 9;
+        const double inv_djac = a.geo[cls].inv_djac, djac = 1.0 / inv_djac;
+        __syncthreads();
+        for (int q = threadIdx.x; q < Q; q += blockDim.x) {
+            const int i = q % ME, j = (q / ME) % ME, k = q / (ME * ME);
+            const double xi[3] = {Xe[i] + 1.0, Xe[j] + 1.0, Xe[k] + 1.0};
+            double x[3], U[5];
+            for (int d = 0; d < 3; ++d)
+                x[d] = a.X0[(size_t)e * 3 + d] + J[d * 3 + 0] * xi[0] + J[d * 3 + 1] * xi[1] + J[d * 3 + 2] * xi[2];
+            dgp::initial_state(a.ic_type, a.data, a.gamma, a.R, x, a.t, U);
+            const double cw = (We[i] * We[j]) * We[k] * djac;
+#pragma unroll
+            for (int v = 0; v < 5; ++v) f[v * Q + q] = U[v] * cw;
+        }
+        __syncthreads();
+        for (int o = threadIdx.x; o < 5 * ME * ME * N; o += blockDim.x) {  // x
+            const int bx = o % N, kj = o / N;  // kj = (v*ME + k)*ME + j
+            double acc = 0.0;
+            for (int i = 0; i < ME; ++i) acc += Be[i * N + bx] * f[kj * ME + i];
+            t1[o] = acc;
+        }
+        __syncthreads();
+        for (int o = threadIdx.x; o < 5 * ME * N * N; o += blockDim.x) {  // y
+            const int bx = o % N, by = (o / N) % N, vk = o / (N * N);
+            double acc = 0.0;
+            for (int j = 0; j < ME; ++j) acc += Be[j * N + by] * t1[(vk * ME + j) * N + bx];
+            t2[o] = acc;
+        }
+        __syncthreads();
+        for (int o = threadIdx.x; o < 5 * NB; o += blockDim.x) {  // z
+            const int byx = o % (N * N), bz = (o / (N * N)) % N, v = o / NB;
+            double acc = 0.0;
+            for (int k = 0; k < ME; ++k) acc += Be[k * N + bz] * t2[((v * ME + k) * N * N) + byx];
+            r[o] = acc;
+        }
+        __syncthreads();
+        for (int o = threadIdx.x; o < 5 * NB; o += blockDim.x) {  // Minv along x, into t2
+            const int bx = o % N, row = o / N;
+            double acc = 0.0;
+            for (int k = 0; k < N; ++k) acc += Mi[bx * N + k] * r[row * N + k];
+            t2[o] = acc;
+        }
+        __syncthreads();
+        for (int o = threadIdx.x; o < 5 * NB; o += blockDim.x) {  // along y, into r
+            const int bx = o % N, by = (o / N) % N, vz = o / (N * N);
+            double acc = 0.0;
+            for (int k = 0; k < N; ++k) acc += Mi[by * N + k] * t2[(vz * N + k) * N + bx];
+            r[o] = acc;
+        }
+        __syncthreads();
+        for (int o = threadIdx.x; o < 5 * NB; o += blockDim.x) {  // along z, / det J
+            const int byx = o % (N * N), bz = (o / (N * N)) % N, v = o / NB;
+            double acc = 0.0;
+            for (int k = 0; k < N; ++k) acc += Mi[bz * N + k] * r[(v * N + k) * N * N + byx];
+            a.U[(size_t)e * 5 * NB + o] = acc * inv_djac;
+        }
+    }
+}
+
+template <int P>
+int launch_project(dg_ctx* c, const ProjectArgs& a)
+{
+    constexpr size_t smem = project_smem_bytes<P>();
+    DG_CUDA(c, cudaFuncSetAttribute(project_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int n = a.e_end - a.e_begin;
+    int dev_sms = 0;
+    DG_CUDA(c, cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, c->device));
+    const int grid = std::max(1, std::min(n, 8 * dev_sms));
+    project_kernel<P><<<grid, 256, smem, c->stream>>>(a);
+    DG_CUDA(c, cudaGetLastError());
+    return DG_OK;
+}
+
+int project_ic_device(dg_ctx* c, int ic_type, const double* data, int ndata, double t, double gamma, double R, int e0,
+                      int ne)
+{
+    if (ne <= 0) return DG_OK;
+    ProjectArgs a{};
+    a.U = c->d_U0;
+    a.geo_class = c->d_geo_class;
+    a.geo = c->d_geo;
+    a.X0 = c->d_X0;
+    a.J = reinterpret_cast<const double*>(c->d_geo + c->pm.classes.size());
+    a.e_begin = e0;
+    a.e_end = e0 + ne;
+    a.ic_type = ic_type;
+    a.gamma = gamma;
+    a.R = R;
+    a.t = t;
+    for (int i = 0; i < ndata && i < 16; ++i) a.data[i] = data[i];
+    switch (c->p) {
+        case 0: return launch_project<0>(c, a);
+        case 1: return launch_project<1>(c, a);
+        case 2: return launch_project<2>(c, a);
+        case 3: return launch_project<3>(c, a);
+        case 4: return launch_project<4>(c, a);
+        case 5: return launch_project<5>(c, a);
+        default: return fail(c, DG_ERR_UNSUPPORTED, "order out of range");
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1068,13 +1214,24 @@ int dg_project_ic(dg_ctx* c, int ic_type, const double* data, int ndata, double 
     for (int i = 0; i < ndata && i < 16; ++i) d[i] = data[i];
     const int need[] = {5, 0, 0, 9, 1};
     if (ndata < need[ic_type]) return fail(c, DG_ERR_ARG, "initial condition needs more data values");
-    std::vector<double> U(static_cast<size_t>(c->ne) * c->nb * 5);
-    dgh::project_initial_condition(c->pm, c->tab, ic_type, d, c->gamma, c->R, t, U.data(), 0, c->ne);
-    if (Uc) std::memcpy(Uc, U.data(), U.size() * sizeof(double));
     DG_CUDA(c, cudaSetDevice(c->device));
-    const int rc = set_energy_reference(c, U.data());
+    int rc = project_ic_device(c, ic_type, d, 16, t, c->gamma, c->R, 0, c->ne);
     if (rc) return rc;
-    return upload_state_host_layout(c, U.data(), c->d_U0);
+    const bool mixed = c->precision == DG_PREC_MIXED_FP32;
+    if (!Uc && !mixed) {
+        DG_CUDA(c, cudaStreamSynchronize(c->stream));
+        return DG_OK;
+    }
+    // a host copy for the caller, and for the mixed residual's energy reference
+    std::vector<double> tmp;
+    double* host = Uc;
+    if (!host) {
+        tmp.resize(static_cast<size_t>(c->ne) * c->nb * 5);
+        host = tmp.data();
+    }
+    rc = download_range(c, c->d_U0, host, 0, c->ne);
+    if (rc) return rc;
+    return set_energy_reference(c, host);
 }
 
 int dg_l2_error(dg_ctx* c, int ic_type, const double* data, int ndata, double t, double* err)

@@ -88,6 +88,11 @@ int download_range(dg_ctx* c, const double* src, double* Uc, int e0, int ne);
 int run_reduce(dg_ctx* c, int kind, int ic_type, const double* data, int ndata, double t, double* out5, int e0, int ne,
                double gamma, double R);
 
+// L2 projection of an initial condition onto elements [e0, e0+ne) of d_U0, on
+// the device (queued on the context's stream)
+int project_ic_device(dg_ctx* c, int ic_type, const double* data, int ndata, double t, double gamma, double R, int e0,
+                      int ne);
+
 // uploads the geometry classes with class_dtf / class_eref
 int upload_geometry(dg_ctx* c, cudaStream_t s);
 

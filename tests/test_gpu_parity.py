@@ -125,12 +125,17 @@ def test_vortex3d_regression_on_gpu(golden):
     assert gpu.status() == 0
 
 
-@pytest.mark.parametrize("p", [0, 2, 5])
+@pytest.mark.parametrize("p", [0, 1, 2, 3, 4, 5])
 def test_initial_projection_and_error_match_oracle(p):
+    """The on-device L2 projection (one CTA per element) against the oracle's."""
     _, gpu, orc = make_pair((2, 2, 3), p, rotate_seed=9)
     U_gpu = gpu.project_ic("IsentropicVortexXY", VORTEX_XY)
     U_orc = orc.project_ic("IsentropicVortexXY", VORTEX_XY)
     assert rel_l2(U_gpu, U_orc).max() < 1e-13
+    tg_gpu = gpu.project_ic("TaylorGreen", [0.1])
+    tg_orc = orc.project_ic("TaylorGreen", [0.1])
+    assert rel_l2(tg_gpu, tg_orc).max() < 1e-13
+    gpu.project_ic("IsentropicVortexXY", VORTEX_XY)
     e_gpu = gpu.l2_error("IsentropicVortexXY", VORTEX_XY, 0.3)
     e_orc = orc.l2_error(U_orc, "IsentropicVortexXY", VORTEX_XY, 0.3)
     np.testing.assert_allclose(e_gpu[[0, 1, 2, 4]], e_orc[[0, 1, 2, 4]], rtol=1e-10)
