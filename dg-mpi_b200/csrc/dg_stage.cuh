@@ -214,8 +214,9 @@ __device__ __forceinline__ void interp2d(const T* __restrict__ Bt, const T (&s)[
         }
 }
 
-template <int P, int E, int NT, int G, typename T>
-__global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
+// MB: minimum resident CTAs per SM the register allocation must allow
+template <int P, int E, int NT, int G, typename T, int MB = 1>
+__global__ void __launch_bounds__(NT, MB) stage_kernel(StageArgs a)
 {
     using L = Lay<P, G, T>;
     constexpr int N = L::N, M = L::M, NB = L::NB, NF = L::NF, N2 = L::N2;
@@ -671,19 +672,20 @@ struct StageVariant {
     cudaError_t (*launch)(const StageArgs&, int grid, cudaStream_t);
 };
 
-template <int P, int E, int NT, int G, typename T>
+template <int P, int E, int NT, int G, typename T, int MB>
 cudaError_t launch_stage_variant(const StageArgs& a, int grid, cudaStream_t s)
 {
-    stage_kernel<P, E, NT, G, T><<<grid, NT, stage_smem_bytes<P, E, G, T>(), s>>>(a);
+    stage_kernel<P, E, NT, G, T, MB><<<grid, NT, stage_smem_bytes<P, E, G, T>(), s>>>(a);
     return cudaGetLastError();
 }
 
-template <int P, int E, int NT, int G, typename T = double>
+template <int P, int E, int NT, int G, typename T = double, int MB = 1>
 constexpr StageVariant make_variant()
 {
     static_assert(stage_smem_bytes<P, E, G, T>() <= 227 * 1024, "stage kernel shared memory exceeds 227 KB");
+    static_assert(MB * stage_smem_bytes<P, E, G, T>() <= 228 * 1024, "MB CTAs do not fit in shared memory");
     return StageVariant{E, NT, G, sizeof(T) == 4 ? 1 : 0, stage_smem_bytes<P, E, G, T>(),
-                        (const void*)stage_kernel<P, E, NT, G, T>, launch_stage_variant<P, E, NT, G, T>};
+                        (const void*)stage_kernel<P, E, NT, G, T, MB>, launch_stage_variant<P, E, NT, G, T, MB>};
 }
 
 // the variants compiled for order p (defined in dg_stage_p<p>.cu)
