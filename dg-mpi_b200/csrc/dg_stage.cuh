@@ -214,9 +214,8 @@ __device__ __forceinline__ void interp2d(const T* __restrict__ Bt, const T (&s)[
         }
 }
 
-// MB: minimum resident CTAs per SM the register allocation must allow
-template <int P, int E, int NT, int G, typename T, int MB = 1>
-__global__ void __launch_bounds__(NT, MB) stage_kernel(StageArgs a)
+template <int P, int E, int NT, int G, typename T>
+__global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
 {
     using L = Lay<P, G, T>;
     constexpr int N = L::N, M = L::M, NB = L::NB, NF = L::NF, N2 = L::N2;
@@ -447,23 +446,52 @@ __global__ void __launch_bounds__(NT, MB) stage_kernel(StageArgs a)
         //      coefficients may still be in flight) ----
         cp_async_wait_older();
         __syncthreads();
-        // own and neighbour traces: one task per (element, face, variable)
-        for (int t = tid; t < E * 30; t += NT) {
-            const int v = t % 5, f = (t / 5) % 6, e = t / 30;
-            T sn[N][N], so[N][N];
-            const double* nb = sOps + e * OPS + (f * 5 + v) * NS;
-            const double* own = sU + e * ES + v * VS;
-            // both sides in the own element's energy frame
-            const double sh = kShift && v == 4 ? a.geo[a.geo_class[min(e0 + e, a.ne - 1)]].eref : 0.0;
+        // own and neighbour traces: one task per (element, face, variable) doing
+        // both sides, or -- when the CTA has threads to spare (high orders) --
+        // one task per side
+        constexpr bool kSplitSides = 2 * E * 30 <= NT;
+        if constexpr (kSplitSides) {
+            for (int t = tid; t < E * 60; t += NT) {
+                const int v = t % 5, f = (t / 5) % 6, side = (t / 30) % 2, e = t / 60;
+                // both sides in the own element's energy frame
+                const double sh = kShift && v == 4 ? a.geo[a.geo_class[min(e0 + e, a.ne - 1)]].eref : 0.0;
+                T sl[N][N];
+                if (side == 0) {
+                    const double* own = sU + e * ES + v * VS;
 #pragma unroll
-            for (int b1 = 0; b1 < N; ++b1)
+                    for (int b1 = 0; b1 < N; ++b1)
 #pragma unroll
-                for (int b0 = 0; b0 < N; ++b0) {
-                    sn[b1][b0] = kShift ? T(nb[b1 * N + b0] - sh) : T(nb[b1 * N + b0]);
-                    so[b1][b0] = kShift ? T(own[slice_index<N>(f, b0, b1)] - sh) : T(own[slice_index<N>(f, b0, b1)]);
+                        for (int b0 = 0; b0 < N; ++b0)
+                            sl[b1][b0] =
+                                kShift ? T(own[slice_index<N>(f, b0, b1)] - sh) : T(own[slice_index<N>(f, b0, b1)]);
+                } else {
+                    const double* nb = sOps + e * OPS + (f * 5 + v) * NS;
+#pragma unroll
+                    for (int b1 = 0; b1 < N; ++b1)
+#pragma unroll
+                        for (int b0 = 0; b0 < N; ++b0)
+                            sl[b1][b0] = kShift ? T(nb[b1 * N + b0] - sh) : T(nb[b1 * N + b0]);
                 }
-            interp2d<N, M, T>(Bt, so, sW + e * W + (f * 5 + v) * FS);
-            interp2d<N, M, T>(Bt, sn, sW + e * W + 30 * FS + (f * 5 + v) * FS);
+                interp2d<N, M, T>(Bt, sl, sW + e * W + side * 30 * FS + (f * 5 + v) * FS);
+            }
+        } else {
+            for (int t = tid; t < E * 30; t += NT) {
+                const int v = t % 5, f = (t / 5) % 6, e = t / 30;
+                T sn[N][N], so[N][N];
+                const double* nb = sOps + e * OPS + (f * 5 + v) * NS;
+                const double* own = sU + e * ES + v * VS;
+                // both sides in the own element's energy frame
+                const double sh = kShift && v == 4 ? a.geo[a.geo_class[min(e0 + e, a.ne - 1)]].eref : 0.0;
+#pragma unroll
+                for (int b1 = 0; b1 < N; ++b1)
+#pragma unroll
+                    for (int b0 = 0; b0 < N; ++b0) {
+                        sn[b1][b0] = kShift ? T(nb[b1 * N + b0] - sh) : T(nb[b1 * N + b0]);
+                        so[b1][b0] = kShift ? T(own[slice_index<N>(f, b0, b1)] - sh) : T(own[slice_index<N>(f, b0, b1)]);
+                    }
+                interp2d<N, M, T>(Bt, so, sW + e * W + (f * 5 + v) * FS);
+                interp2d<N, M, T>(Bt, sn, sW + e * W + 30 * FS + (f * 5 + v) * FS);
+            }
         }
         __syncthreads();
         // the staging area is free: stream in this batch's RK operands
@@ -672,20 +700,19 @@ struct StageVariant {
     cudaError_t (*launch)(const StageArgs&, int grid, cudaStream_t);
 };
 
-template <int P, int E, int NT, int G, typename T, int MB>
+template <int P, int E, int NT, int G, typename T>
 cudaError_t launch_stage_variant(const StageArgs& a, int grid, cudaStream_t s)
 {
-    stage_kernel<P, E, NT, G, T, MB><<<grid, NT, stage_smem_bytes<P, E, G, T>(), s>>>(a);
+    stage_kernel<P, E, NT, G, T><<<grid, NT, stage_smem_bytes<P, E, G, T>(), s>>>(a);
     return cudaGetLastError();
 }
 
-template <int P, int E, int NT, int G, typename T = double, int MB = 1>
+template <int P, int E, int NT, int G, typename T = double>
 constexpr StageVariant make_variant()
 {
     static_assert(stage_smem_bytes<P, E, G, T>() <= 227 * 1024, "stage kernel shared memory exceeds 227 KB");
-    static_assert(MB * stage_smem_bytes<P, E, G, T>() <= 228 * 1024, "MB CTAs do not fit in shared memory");
     return StageVariant{E, NT, G, sizeof(T) == 4 ? 1 : 0, stage_smem_bytes<P, E, G, T>(),
-                        (const void*)stage_kernel<P, E, NT, G, T, MB>, launch_stage_variant<P, E, NT, G, T, MB>};
+                        (const void*)stage_kernel<P, E, NT, G, T>, launch_stage_variant<P, E, NT, G, T>};
 }
 
 // the variants compiled for order p (defined in dg_stage_p<p>.cu)
