@@ -610,9 +610,19 @@ double energy_reference(const dg_ctx* c, const double* Uc, int ne)
 {
     if (c->precision != DG_PREC_MIXED_FP32 || ne <= 0) return 0.0;
     const long long n = 1LL * ne * c->nb;
+    // fixed blocks summed in order: the same state gives the same bits for any
+    // thread count (a batch case and a context of that case must agree exactly)
+    constexpr int kBlocks = 256;
+    double part[kBlocks];
+#pragma omp parallel for schedule(static)
+    for (int b = 0; b < kBlocks; ++b) {
+        const long long i0 = n * b / kBlocks, i1 = n * (b + 1) / kBlocks;
+        double s = 0.0;
+        for (long long i = i0; i < i1; ++i) s += Uc[i * 5 + 4];
+        part[b] = s;
+    }
     double sum = 0.0;
-#pragma omp parallel for reduction(+ : sum)
-    for (long long i = 0; i < n; ++i) sum += Uc[i * 5 + 4];
+    for (int b = 0; b < kBlocks; ++b) sum += part[b];
     const double m = sum / static_cast<double>(n);
     return std::isfinite(m) ? m : 0.0;
 }

@@ -25,6 +25,7 @@
 // cp.async while the current batch computes.
 #pragma once
 #include <cstdint>
+#include <type_traits>
 
 #include "dg_physics.cuh"
 
@@ -109,11 +110,13 @@ __host__ __device__ constexpr int cmax(int a, int b) { return a > b ? a : b; }
 
 // G = number of variable groups of the fused pointwise phase (register budget);
 // T = arithmetic of the residual (the work area W holds T values, everything
-// else FP64)
-template <int P, int G, typename T = double>
+// else FP64); PZ: the groups' pencil tasks run in one phase (the z-contraction
+// output of all five variables is held at once)
+template <int P, int G, typename T = double, bool PZ = false>
 struct Lay {
     static constexpr int N = P + 1, M = P + 2, NB = N * N * N, NF = M * M, N2 = N * N;
     static constexpr int GV = G == 1 ? 5 : (G == 2 ? 3 : 2);  // variables per group (max)
+    static constexpr int GA = PZ ? 5 : GV;       // variables of the z-contraction buffers
     static constexpr int VS = odd(NB);           // per-variable stride of U / residual
     static constexpr int ES = 5 * VS;            // per-element stride of U / residual
     static constexpr int FS = odd(NF);           // per-(face, variable) stride of traces
@@ -121,9 +124,9 @@ struct Lay {
     static constexpr int X1S = odd(N2 * M);      // [bz][by][qx] block
     static constexpr int X2S = odd(N * NF);      // [bz][qy][qx] block
     // per-element work area: face phase {Tr[6][5], Tn[6][5]} x FS;
-    // volume phase X2[5] | (X1[5] or A[GV][3] + C[GV][2])
+    // volume phase X2[5] | (X1[5] or A[GA][3] + C[GA][2])
     static constexpr int face = 60 * FS;
-    static constexpr int vol = 5 * X2S + cmax(5 * X1S, GV * (3 * X2S + 2 * X1S));
+    static constexpr int vol = 5 * X2S + cmax(5 * X1S, GA * (3 * X2S + 2 * X1S));
     static constexpr int W = odd(cmax(face, vol));
     // FP64 operand region: first the neighbours' boundary slices [30][NS]
     // (streamed in during the volume phase), then the batch's U0 and RK
@@ -149,6 +152,16 @@ template <int P, int G>
 __host__ __device__ constexpr int group_size(int g)
 {
     return G == 1 ? 5 : (G == 2 ? (g == 0 ? 3 : 2) : (g == 2 ? 1 : 2));
+}
+
+// calls f(std::integral_constant<int, I>) for I = I0 .. I1-1
+template <int I0, int I1, typename F>
+__device__ __forceinline__ void static_for(F&& f)
+{
+    if constexpr (I0 < I1) {
+        f(std::integral_constant<int, I0>{});
+        static_for<I0 + 1, I1>(f);
+    }
 }
 
 __device__ __forceinline__ int face_axis(int f) { return f == 2 || f == 4 ? 0 : (f == 1 || f == 3 ? 1 : 2); }
@@ -214,10 +227,10 @@ __device__ __forceinline__ void interp2d(const T* __restrict__ Bt, const T (&s)[
         }
 }
 
-template <int P, int E, int NT, int G, typename T>
+template <int P, int E, int NT, int G, typename T, bool PZ>
 __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
 {
-    using L = Lay<P, G, T>;
+    using L = Lay<P, G, T, PZ>;
     constexpr int N = L::N, M = L::M, NB = L::NB, NF = L::NF, N2 = L::N2;
     constexpr int VS = L::VS, ES = L::ES, FS = L::FS, NS = L::NS, X1S = L::X1S, X2S = L::X2S, W = L::W, GV = L::GV;
     constexpr int OPS = L::OPS;
@@ -325,79 +338,76 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
 
         // ---- fused: z interpolation, Euler flux, contravariant transform and
         //      first (z) divergence contraction; then y and x contractions ----
+        T* Abuf = sW + 5 * X2S;                     // [GA][3][X2S] over X1
+        T* Cbuf = Abuf + L::GA * 3 * X2S;           // [GA][2][X1S]
+        // one (x,y) pencil of element e for variable group g; the buffers hold
+        // the group's variables from slot abase (0, or its first variable with PZ)
+        auto pencil = [&](auto gc, int e, int qxy) {
+            constexpr int g = decltype(gc)::value;
+            constexpr int gv0 = group_first<P, G>(g), gnv = group_size<P, G>(g), abase = PZ ? gv0 : 0;
+            const int qx = qxy % M, qy = qxy / M;
+            T xz[5][N];
 #pragma unroll
-        for (int g = 0; g < G; ++g) {
-            const int gv0 = group_first<P, G>(g), gnv = group_size<P, G>(g);
-            T* Abuf = sW + 5 * X2S;            // [GV][3][X2S] over X1
-            T* Cbuf = Abuf + GV * 3 * X2S;     // [GV][2][X1S]
-            for (int i = tid; i < E * NF; i += NT) {
-                const int e = i / NF, qxy = i % NF;
-                const int qx = qxy % M, qy = qxy / M;
-                T xz[5][N];
+            for (int v = 0; v < 5; ++v)
 #pragma unroll
-                for (int v = 0; v < 5; ++v)
+                for (int bz = 0; bz < N; ++bz) xz[v][bz] = X2[e * W + v * X2S + bz * NF + qxy];
+            const int ge = min(e0 + e, a.ne - 1);
+            const GeoDev* geo = a.geo + a.geo_class[ge];
+            const T hr = kShift ? T(a.gamma * geo->eref) : T(0);
+            const T pref = kShift ? T((a.gamma - 1.0) * geo->eref) : T(0);
+            T JD[9];
 #pragma unroll
-                    for (int bz = 0; bz < N; ++bz) xz[v][bz] = X2[e * W + v * X2S + bz * NF + qxy];
-                const int ge = min(e0 + e, a.ne - 1);
-                const GeoDev* geo = a.geo + a.geo_class[ge];
-                const T hr = kShift ? T(a.gamma * geo->eref) : T(0);
-                const T pref = kShift ? T((a.gamma - 1.0) * geo->eref) : T(0);
-                T JD[9];
+            for (int k = 0; k < 9; ++k) JD[k] = T(geo->JD[k]);
+            T acc[gnv][3][N];
 #pragma unroll
-                for (int k = 0; k < 9; ++k) JD[k] = T(geo->JD[k]);
-                T acc[GV][3][N];
+            for (int v = 0; v < gnv; ++v)
 #pragma unroll
-                for (int v = 0; v < GV; ++v)
+                for (int d = 0; d < 3; ++d)
 #pragma unroll
-                    for (int d = 0; d < 3; ++d)
+                    for (int bz = 0; bz < N; ++bz) acc[v][d][bz] = T(0);
+            const T wxy = Wt[qx] * Wt[qy];
 #pragma unroll
-                        for (int bz = 0; bz < N; ++bz) acc[v][d][bz] = T(0);
-                const T wxy = Wt[qx] * Wt[qy];
+            for (int qz = 0; qz < M; ++qz) {
+                T U[5];
 #pragma unroll
-                for (int qz = 0; qz < M; ++qz) {
-                    T U[5];
+                for (int v = 0; v < 5; ++v) {
+                    T s = T(0);
 #pragma unroll
-                    for (int v = 0; v < 5; ++v) {
-                        T s = T(0);
+                    for (int bz = 0; bz < N; ++bz) s += Bt[qz * N + bz] * xz[v][bz];
+                    U[v] = s;
+                }
+                T F[15];
+                const T p = dgp::interior_flux_r1<T, kShift>(gamma, U, F, hr);
+                if constexpr (g == 0) {
+                    if (!(U[0] > T(0))) status |= kStatusRho;
+                    if (!(p + pref > T(0))) status |= kStatusPressure;
+                    if (U[0] != U[0] || p != p) status |= kStatusNaN;
+                }
+                const T wq = wxy * Wt[qz];
 #pragma unroll
-                        for (int bz = 0; bz < N; ++bz) s += Bt[qz * N + bz] * xz[v][bz];
-                        U[v] = s;
-                    }
-                    T F[15];
-                    const T p = dgp::interior_flux_r1<T, kShift>(gamma, U, F, hr);
-                    if (g == 0) {
-                        if (!(U[0] > T(0))) status |= kStatusRho;
-                        if (!(p + pref > T(0))) status |= kStatusPressure;
-                        if (U[0] != U[0] || p != p) status |= kStatusNaN;
-                    }
-                    const T wq = wxy * Wt[qz];
+                for (int vv = 0; vv < gnv; ++vv) {
+                    const int v = gv0 + vv;
 #pragma unroll
-                    for (int vv = 0; vv < GV; ++vv) {
-                        if (vv < gnv) {
-                            const int v = gv0 + vv;
+                    for (int d = 0; d < 3; ++d) {
+                        const T Gd = (F[v] * JD[d * 3 + 0] + F[5 + v] * JD[d * 3 + 1] + F[10 + v] * JD[d * 3 + 2]) * wq;
 #pragma unroll
-                            for (int d = 0; d < 3; ++d) {
-                                const T Gd =
-                                    (F[v] * JD[d * 3 + 0] + F[5 + v] * JD[d * 3 + 1] + F[10 + v] * JD[d * 3 + 2]) * wq;
-#pragma unroll
-                                for (int bz = 0; bz < N; ++bz)
-                                    acc[vv][d][bz] += (d == 2 ? Dt[qz * N + bz] : Bt[qz * N + bz]) * Gd;
-                            }
-                        }
+                        for (int bz = 0; bz < N; ++bz) acc[vv][d][bz] += (d == 2 ? Dt[qz * N + bz] : Bt[qz * N + bz]) * Gd;
                     }
                 }
-#pragma unroll
-                for (int vv = 0; vv < GV; ++vv)
-                    if (vv < gnv)
-#pragma unroll
-                        for (int d = 0; d < 3; ++d)
-#pragma unroll
-                            for (int bz = 0; bz < N; ++bz) Abuf[e * W + (vv * 3 + d) * X2S + bz * NF + qxy] = acc[vv][d][bz];
             }
-            __syncthreads();
-            // y contraction: C0 = By^T A0 ; C12 = Dy^T A1 + By^T A2
-            for (int i = tid; i < E * gnv * N * M; i += NT) {
-                const int qx = i % M, bz = (i / M) % N, vv = (i / (M * N)) % gnv, e = i / (gnv * N * M);
+#pragma unroll
+            for (int vv = 0; vv < gnv; ++vv)
+#pragma unroll
+                for (int d = 0; d < 3; ++d)
+#pragma unroll
+                    for (int bz = 0; bz < N; ++bz)
+                        Abuf[e * W + ((abase + vv) * 3 + d) * X2S + bz * NF + qxy] = acc[vv][d][bz];
+        };
+        // y and x contractions of nv buffered variables into residual variables
+        // v0 .. v0+nv-1: C0 = By^T A0, C12 = Dy^T A1 + By^T A2; res = Dx^T C0 + Bx^T C12
+        auto contract_yx = [&](int nv, int v0) {
+            for (int i = tid; i < E * nv * N * M; i += NT) {
+                const int qx = i % M, bz = (i / M) % N, vv = (i / (M * N)) % nv, e = i / (nv * N * M);
                 const T* A0 = Abuf + e * W + (vv * 3 + 0) * X2S + bz * NF + qx;
                 const T* A1 = A0 + X2S;
                 const T* A2 = A1 + X2S;
@@ -421,9 +431,8 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
                 }
             }
             __syncthreads();
-            // x contraction into the (FP64) residual: res = Dx^T C0 + Bx^T C12
-            for (int i = tid; i < E * gnv * N2; i += NT) {
-                const int vv = i % gnv, byz = (i / gnv) % N2, e = i / (gnv * N2);
+            for (int i = tid; i < E * nv * N2; i += NT) {
+                const int vv = i % nv, byz = (i / nv) % N2, e = i / (nv * N2);
                 const T* C0 = Cbuf + e * W + (vv * 2) * X1S + byz * M;
                 const T* C12 = C0 + X1S;
                 T r[N];
@@ -435,11 +444,28 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
 #pragma unroll
                     for (int bx = 0; bx < N; ++bx) r[bx] += Dt[qx * N + bx] * c0 + Bt[qx * N + bx] * c12;
                 }
-                double* res = sRes + e * ES + (gv0 + vv) * VS + byz * N;
+                double* res = sRes + e * ES + (v0 + vv) * VS + byz * N;
 #pragma unroll
                 for (int bx = 0; bx < N; ++bx) res[bx] = double(r[bx]);
             }
             __syncthreads();
+        };
+        if constexpr (PZ) {
+            // every group's pencils in one phase, then all five variables at once
+            for (int i = tid; i < E * NF * G; i += NT) {
+                const int g = i / (E * NF), r = i - g * (E * NF);
+                static_for<0, G>([&](auto gc) {
+                    if (g == decltype(gc)::value) pencil(gc, r / NF, r % NF);
+                });
+            }
+            __syncthreads();
+            contract_yx(5, 0);
+        } else {
+            static_for<0, G>([&](auto gc) {
+                for (int i = tid; i < E * NF; i += NT) pencil(gc, i / NF, i % NF);
+                __syncthreads();
+                contract_yx(group_size<P, G>(decltype(gc)::value), group_first<P, G>(decltype(gc)::value));
+            });
         }
 
         // ---- faces: the neighbours' slices have landed (the next batch's
@@ -684,10 +710,10 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
     if (status) atomicOr(a.status, status);
 }
 
-template <int P, int E, int G, typename T>
+template <int P, int E, int G, typename T, bool PZ = false>
 constexpr size_t stage_smem_bytes()
 {
-    return ((E * Lay<P, G, T>::bytes_per_elem + 15) / 16) * 16 + E * Lay<P, G, T>::meta_bytes_per_elem;
+    return ((E * Lay<P, G, T, PZ>::bytes_per_elem + 15) / 16) * 16 + E * Lay<P, G, T, PZ>::meta_bytes_per_elem;
 }
 
 // ---- compiled launch variants (one translation unit per order) ----
@@ -700,19 +726,21 @@ struct StageVariant {
     cudaError_t (*launch)(const StageArgs&, int grid, cudaStream_t);
 };
 
-template <int P, int E, int NT, int G, typename T>
+template <int P, int E, int NT, int G, typename T, bool PZ>
 cudaError_t launch_stage_variant(const StageArgs& a, int grid, cudaStream_t s)
 {
-    stage_kernel<P, E, NT, G, T><<<grid, NT, stage_smem_bytes<P, E, G, T>(), s>>>(a);
+    stage_kernel<P, E, NT, G, T, PZ><<<grid, NT, stage_smem_bytes<P, E, G, T, PZ>(), s>>>(a);
     return cudaGetLastError();
 }
 
-template <int P, int E, int NT, int G, typename T = double>
+// PZ = true: the variable groups' pencil tasks in one phase (worth it when
+// E * (p+2)^2 * G tasks fill fewer rounds of NT threads than G sequential phases)
+template <int P, int E, int NT, int G, typename T = double, bool PZ = false>
 constexpr StageVariant make_variant()
 {
-    static_assert(stage_smem_bytes<P, E, G, T>() <= 227 * 1024, "stage kernel shared memory exceeds 227 KB");
-    return StageVariant{E, NT, G, sizeof(T) == 4 ? 1 : 0, stage_smem_bytes<P, E, G, T>(),
-                        (const void*)stage_kernel<P, E, NT, G, T>, launch_stage_variant<P, E, NT, G, T>};
+    static_assert(stage_smem_bytes<P, E, G, T, PZ>() <= 227 * 1024, "stage kernel shared memory exceeds 227 KB");
+    return StageVariant{E, NT, G, sizeof(T) == 4 ? 1 : 0, stage_smem_bytes<P, E, G, T, PZ>(),
+                        (const void*)stage_kernel<P, E, NT, G, T, PZ>, launch_stage_variant<P, E, NT, G, T, PZ>};
 }
 
 // the variants compiled for order p (defined in dg_stage_p<p>.cu)

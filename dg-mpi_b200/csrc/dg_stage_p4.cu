@@ -18,6 +18,7 @@ static const StageVariant kVariants4[] = {
     make_variant<4, 1, 128, 2, double>(),
     make_variant<4, 1, 64, 1, float>(),
     make_variant<4, 1, 128, 2, float>(),
+    make_variant<4, 1, 128, 2, float, true>(),
 };
 
 int stage_variants_p4(const StageVariant** out)

@@ -18,6 +18,7 @@ static const StageVariant kVariants5[] = {
     make_variant<5, 1, 128, 3, double>(),
     make_variant<5, 1, 128, 2, float>(),
     make_variant<5, 1, 64, 1, float>(),
+    make_variant<5, 1, 128, 3, double, true>(),
 };
 
 int stage_variants_p5(const StageVariant** out)
