@@ -132,6 +132,7 @@ int launch_stage(dg_ctx* c, int mode, const double* Us, const double* U0, double
     a.acc = c->d_acc;
     a.out = out;
     a.conn = c->d_conn;
+    a.frec = c->d_frec;
     a.geo_class = c->d_geo_class;
     a.geo = c->d_geo;
     a.cmap = c->d_cmap;
@@ -658,7 +659,7 @@ void release(dg_ctx* c)
     if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
     if (c->graph) cudaGraphDestroy(c->graph);
     cudaFree(c->d_U0); cudaFree(c->d_Ua); cudaFree(c->d_Ub); cudaFree(c->d_acc); cudaFree(c->d_out);
-    cudaFree(c->d_conn); cudaFree(c->d_geo_class); cudaFree(c->d_geo); cudaFree(c->d_cmap);
+    cudaFree(c->d_conn); cudaFree(c->d_frec); cudaFree(c->d_geo_class); cudaFree(c->d_geo); cudaFree(c->d_cmap);
     cudaFree(c->d_X0); cudaFree(c->d_partials); cudaFree(c->d_status);
     cudaFree(c->d_halo_send); cudaFree(c->d_halo_recv);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -801,6 +802,7 @@ int dgi::create_ctx(const dg_case_desc* cd, const dg_mesh_desc* md, const int* e
         {(void**)&c->d_acc, nstate * sizeof(double)},
         {(void**)&c->d_out, nstate * sizeof(double)},
         {(void**)&c->d_conn, static_cast<size_t>(c->ne_alloc) * 6 * sizeof(int2)},
+        {(void**)&c->d_frec, static_cast<size_t>(std::max(1, c->ne)) * 6 * sizeof(dgk::FaceRec)},
         {(void**)&c->d_geo_class, static_cast<size_t>(c->ne_alloc) * sizeof(int)},
         {(void**)&c->d_geo, ncls * (sizeof(GeoDev) + 9 * sizeof(double))},
         {(void**)&c->d_cmap, std::max<size_t>(1, c->pm.cmap.size())},
@@ -819,12 +821,31 @@ int dgi::create_ctx(const dg_case_desc* cd, const dg_mesh_desc* md, const int* e
     }
     std::vector<int2> conn(static_cast<size_t>(c->ne_alloc) * 6);
     for (size_t i = 0; i < conn.size(); ++i) conn[i] = make_int2(c->pm.conn[i * 2], c->pm.conn[i * 2 + 1]);
+    // the face records of the owned elements (see dgk::FaceRec)
+    std::vector<dgk::FaceRec> frec(static_cast<size_t>(std::max(1, c->ne)) * 6);
+    for (int e = 0; e < c->ne; ++e)
+        for (int f = 0; f < 6; ++f) {
+            const int nbr = c->pm.conn[(static_cast<size_t>(e) * 6 + f) * 2];
+            const int info = c->pm.conn[(static_cast<size_t>(e) * 6 + f) * 2 + 1];
+            const int isL = (info >> 3) & 1, fn = info & 7;
+            // the normal is the left element's (helpers.cpp:440-446)
+            const dgh::GeoClass& gL = c->pm.classes[c->pm.geo_class[isL ? e : nbr]];
+            const int fl = isL ? f : fn;
+            dgk::FaceRec& r = frec[static_cast<size_t>(e) * 6 + f];
+            for (int d = 0; d < 3; ++d) r.n[d] = c->flux == DG_FLUX_HLLC ? gL.nunit[fl][d] : gL.nhat[fl][d];
+            r.nmag = gL.nmag[fl];
+            r.nbr = nbr;
+            r.info = info;
+            r.cls = c->pm.geo_class[e];
+            r.pad = 0;
+        }
     std::vector<int2> hs(std::max(1, c->nslices)), hr(std::max(1, c->nslices));
     for (int i = 0; i < c->nslices; ++i) {
         hs[i] = make_int2(plan.send_elem[i], plan.send_face[i]);
         hr[i] = make_int2(plan.recv_elem[i], plan.recv_face[i]);
     }
     bool ok = cudaMemcpy(c->d_conn, conn.data(), conn.size() * sizeof(int2), cudaMemcpyHostToDevice) == cudaSuccess &&
+              cudaMemcpy(c->d_frec, frec.data(), frec.size() * sizeof(dgk::FaceRec), cudaMemcpyHostToDevice) == cudaSuccess &&
               cudaMemcpy(c->d_geo_class, c->pm.geo_class.data(), c->ne_alloc * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess &&
               cudaMemcpy(c->d_halo_send, hs.data(), hs.size() * sizeof(int2), cudaMemcpyHostToDevice) == cudaSuccess &&
               cudaMemcpy(c->d_halo_recv, hr.data(), hr.size() * sizeof(int2), cudaMemcpyHostToDevice) == cudaSuccess &&

@@ -29,6 +29,7 @@ struct dg_ctx {
     cudaStream_t stream = nullptr;
     double *d_U0 = nullptr, *d_Ua = nullptr, *d_Ub = nullptr, *d_acc = nullptr, *d_out = nullptr;
     int2* d_conn = nullptr;
+    dgk::FaceRec* d_frec = nullptr;    // [ne][6] face records of the owned elements
     int* d_geo_class = nullptr;
     dgk::GeoDev* d_geo = nullptr;
     uint8_t* d_cmap = nullptr;

@@ -70,6 +70,21 @@ struct GeoDev {
     double nunit[6][3];   // N * (1/|N|) (HLLC)
 };
 
+// One face of an owned element, built at context creation and prefetched with
+// the element's coefficients (48 bytes): the neighbour, the packed neighbour
+// face | left role << 3 | permutation code << 4 (as conn), the left element's
+// normal data (N/|N| for Lax-Friedrichs, N*(1/|N|) for HLLC, and |N|) and the
+// element's own geometry class.
+struct FaceRec {
+    double n[3];
+    double nmag;
+    int nbr;
+    int info;
+    int cls;
+    int pad;
+};
+static_assert(sizeof(FaceRec) == 48, "FaceRec is six 8-byte words");
+
 enum StageMode : int {
     kModeResidual = 0,  // out = R(Us)
     kModeMassInv = 1,   // out = dt * M^-1 R(Us)
@@ -93,6 +108,7 @@ struct StageArgs {
     double* acc;            // RK4 accumulator, [ne][5][nb]
     double* out;            // output, [ne][5][nb]
     const int2* conn;       // [ne][6]
+    const FaceRec* frec;    // [ne][6]
     const int* geo_class;   // [ne]
     const GeoDev* geo;      // [nclasses]
     const uint8_t* cmap;    // [ncodes][m*m]
@@ -136,11 +152,10 @@ struct Lay {
     static constexpr int per_elem_f64 = 2 * ES + ES + OPS;
     // bytes per element, work area in T
     static constexpr size_t bytes_per_elem = sizeof(double) * per_elem_f64 + sizeof(T) * W;
-    // face metadata of a batch, staged once per batch for the flux phase:
-    // per element its energy reference, per face the left element's normal
-    // data {n (LF: N/|N|, HLLC: N*(1/|N|)), |N|}, the role bit and the row of
-    // the face-point permutation
-    static constexpr size_t meta_bytes_per_elem = sizeof(double) + sizeof(T) * 24 + sizeof(int) * 6 + 6 * NF;
+    // face data of a batch: the six face records (the next batch's are
+    // prefetched once the flux phase has read them), the element's geometry
+    // class and the faces' rows of the face-point permutation
+    static constexpr size_t meta_bytes_per_elem = 6 * sizeof(FaceRec) + sizeof(int) + 6 * NF;
 };
 
 template <int P, int G>
@@ -186,6 +201,18 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 // all but the most recent group complete
 __device__ __forceinline__ void cp_async_wait_older() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+// queue the face records of batch e0 into dst [E][6]
+template <int E, int NT>
+__device__ __forceinline__ void prefetch_recs(const FaceRec* __restrict__ frec, int ne, int e0, FaceRec* dst)
+{
+    constexpr int W8 = 6 * sizeof(FaceRec) / 8;  // 8-byte words per element
+    for (int i = threadIdx.x; i < E * W8; i += NT) {
+        const int e = i / W8, r = i - e * W8;
+        const int ge = min(e0 + e, ne - 1);
+        cp_async8(reinterpret_cast<double*>(dst + e * 6) + r, reinterpret_cast<const double*>(frec + (size_t)ge * 6) + r);
+    }
+}
 
 // queue the coefficients of batch e0 of a global state into the padded
 // buffer dst (element stride estride)
@@ -239,12 +266,11 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
     double* sRes = sUbuf + 2 * E * ES;     // [E][ES]
     double* sOps = sRes + E * ES;          // [E][OPS] neighbour slices, then U0 | acc
     T* sW = reinterpret_cast<T*>(sOps + E * OPS);  // [E][W] in the residual's arithmetic
-    // face metadata (see Lay::meta_bytes_per_elem), 16-byte aligned after sW
+    // face data (see Lay::meta_bytes_per_elem), 16-byte aligned after sW
     unsigned char* meta = reinterpret_cast<unsigned char*>(smem) + ((E * L::bytes_per_elem + 15) / 16) * 16;
-    double* sEref = reinterpret_cast<double*>(meta);                  // [E]
-    T* sFn = reinterpret_cast<T*>(sEref + E);                          // [E*6][4]
-    int* sFi = reinterpret_cast<int*>(sFn + E * 24);                   // [E*6] left-role bit
-    unsigned char* sCm = reinterpret_cast<unsigned char*>(sFi + E * 6); // [E*6][NF]
+    FaceRec* sRec = reinterpret_cast<FaceRec*>(meta);                 // [E][6] this batch's face records
+    int* sCls = reinterpret_cast<int*>(sRec + E * 6);                  // [E] geometry classes
+    unsigned char* sCm = reinterpret_cast<unsigned char*>(sCls + E);  // [E*6][NF]
     const bool need_u0_acc = a.mode == kModeRK2 || a.mode == kModeRK3 || a.mode == kModeRK4;
     const T* __restrict__ Bt = TabSel<T>::B(a.tab);
     const T* __restrict__ Dt = TabSel<T>::D(a.tab);
@@ -259,7 +285,10 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
     const int e_first = a.e_begin + blockIdx.x * E;
 
     int buf = 0;
-    if (e_first < a.ne) prefetch_batch<P, G, E, NT>(a.Us, a.ne, e_first, sUbuf, ES);
+    if (e_first < a.ne) {
+        prefetch_batch<P, G, E, NT>(a.Us, a.ne, e_first, sUbuf, ES);
+        prefetch_recs<E, NT>(a.frec, a.ne, e_first, sRec);
+    }
     cp_async_commit();
 
     for (int e0 = e_first; e0 < a.ne; e0 += stride, buf ^= 1) {
@@ -270,29 +299,18 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
         // for the face phase, then the next batch's coefficients
         for (int t = tid; t < E * 30; t += NT) {
             const int fv = t % 30, e = t / 30, v = fv % 5, f = fv / 5;
-            const int ge = min(e0 + e, a.ne - 1);
-            const int2 c = a.conn[ge * 6 + f];
+            const FaceRec& rec = sRec[e * 6 + f];
+            const int2 c = make_int2(rec.nbr, rec.info);
             const double* src = a.Us + ((size_t)c.x * 5 + v) * NB;
             double* dst = sOps + e * OPS + fv * NS;
 #pragma unroll
             for (int b1 = 0; b1 < N; ++b1)
 #pragma unroll
                 for (int b0 = 0; b0 < N; ++b0) cp_async8(dst + b1 * N + b0, src + slice_index<N>(c.y & 7, b0, b1));
-            // this face's metadata for the flux phase, shared out over the five variable tasks
-            const int fm = e * 6 + f, isL = (c.y >> 3) & 1, code = c.y >> 4;
+            // this face's row of the face-point permutation, shared out over the five variable tasks
+            const int fm = e * 6 + f, code = c.y >> 4;
             for (int q = v; q < NF; q += 5) sCm[fm * NF + q] = a.cmap[code * NF + q];
-            if (v == 0) {
-                // the normal is the left element's (helpers.cpp:440-446)
-                const GeoDev* g = a.geo + (isL ? a.geo_class[ge] : a.geo_class[c.x]);
-                const int fl = isL ? f : (c.y & 7);
-                const double* n = a.flux == 1 ? g->nunit[fl] : g->nhat[fl];
-                sFn[fm * 4 + 0] = T(n[0]);
-                sFn[fm * 4 + 1] = T(n[1]);
-                sFn[fm * 4 + 2] = T(n[2]);
-                sFn[fm * 4 + 3] = T(g->nmag[fl]);
-                sFi[fm] = isL;
-                if (f == 0) sEref[e] = kShift ? a.geo[a.geo_class[ge]].eref : 0.0;
-            }
+            if (fv == 0) sCls[e] = rec.cls;
         }
         cp_async_commit();
         if (e0 + stride < a.ne) prefetch_batch<P, G, E, NT>(a.Us, a.ne, e0 + stride, sUbuf + (buf ^ 1) * E * ES, ES);
@@ -304,7 +322,7 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
         for (int i = tid; i < E * 5 * N2; i += NT) {
             const int v = i % 5, byz = (i / 5) % N2, e = i / (5 * N2);
             const double* u = sU + e * ES + v * VS + byz * N;
-            const double sh = kShift && v == 4 ? a.geo[a.geo_class[min(e0 + e, a.ne - 1)]].eref : 0.0;
+            const double sh = kShift && v == 4 ? a.geo[sRec[e * 6].cls].eref : 0.0;
             T row[N];
 #pragma unroll
             for (int bx = 0; bx < N; ++bx) row[bx] = kShift ? T(u[bx] - sh) : T(u[bx]);
@@ -351,8 +369,7 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
             for (int v = 0; v < 5; ++v)
 #pragma unroll
                 for (int bz = 0; bz < N; ++bz) xz[v][bz] = X2[e * W + v * X2S + bz * NF + qxy];
-            const int ge = min(e0 + e, a.ne - 1);
-            const GeoDev* geo = a.geo + a.geo_class[ge];
+            const GeoDev* geo = a.geo + sCls[e];
             const T hr = kShift ? T(a.gamma * geo->eref) : T(0);
             const T pref = kShift ? T((a.gamma - 1.0) * geo->eref) : T(0);
             T JD[9];
@@ -480,7 +497,7 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
             for (int t = tid; t < E * 60; t += NT) {
                 const int v = t % 5, f = (t / 5) % 6, side = (t / 30) % 2, e = t / 60;
                 // both sides in the own element's energy frame
-                const double sh = kShift && v == 4 ? a.geo[a.geo_class[min(e0 + e, a.ne - 1)]].eref : 0.0;
+                const double sh = kShift && v == 4 ? a.geo[sRec[e * 6].cls].eref : 0.0;
                 T sl[N][N];
                 if (side == 0) {
                     const double* own = sU + e * ES + v * VS;
@@ -507,7 +524,7 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
                 const double* nb = sOps + e * OPS + (f * 5 + v) * NS;
                 const double* own = sU + e * ES + v * VS;
                 // both sides in the own element's energy frame
-                const double sh = kShift && v == 4 ? a.geo[a.geo_class[min(e0 + e, a.ne - 1)]].eref : 0.0;
+                const double sh = kShift && v == 4 ? a.geo[sRec[e * 6].cls].eref : 0.0;
 #pragma unroll
                 for (int b1 = 0; b1 < N; ++b1)
 #pragma unroll
@@ -533,7 +550,9 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
             constexpr int total = E * 6 * NF;
             auto point = [&](int i, T (&Fo)[5], int& off) {
                 const int cidx = i % NF, f = (i / NF) % 6, e = i / (6 * NF);
-                const int fm = e * 6 + f, isL = sFi[fm];
+                const int fm = e * 6 + f;
+                const FaceRec& rec = sRec[fm];
+                const int isL = (rec.info >> 3) & 1;
                 const int cn = sCm[fm * NF + cidx];
                 const T* Tr = sW + e * W + f * 5 * FS;
                 const T* Tn = sW + e * W + 30 * FS + f * 5 * FS;
@@ -545,10 +564,10 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
                     UR[v] = isL ? un : uo;
                 }
                 // the left element's normal data, staged with the neighbour slices
-                const T nmag = sFn[fm * 4 + 3];
-                const double eref = kShift ? sEref[e] : 0.0;
+                const T nmag = T(rec.nmag);
+                const double eref = kShift ? a.geo[sRec[e * 6].cls].eref : 0.0;
                 if (a.flux == 1) {
-                    const T nu[3] = {sFn[fm * 4 + 0], sFn[fm * 4 + 1], sFn[fm * 4 + 2]};
+                    const T nu[3] = {T(rec.n[0]), T(rec.n[1]), T(rec.n[2])};
                     if (kShift) {  // HLLC takes the full energy
                         UL[4] += T(eref);
                         UR[4] += T(eref);
@@ -560,7 +579,7 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
                         for (int d = 0; d < 3; ++d) Fo[1 + d] -= pn * nu[d];
                     }
                 } else {
-                    const T nh[3] = {sFn[fm * 4 + 0], sFn[fm * 4 + 1], sFn[fm * 4 + 2]};
+                    const T nh[3] = {T(rec.n[0]), T(rec.n[1]), T(rec.n[2])};
                     dgp::flux_lax_friedrichs_fast<T, kShift>(gamma, UL, UR, nh, nmag, Fo, T(a.gamma * eref),
                                                              T((a.gamma - 1.0) * eref));
                 }
@@ -586,6 +605,10 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
         }
         __syncthreads();
 
+        // the face records have been read: queue the next batch's (they land
+        // before the inverse-mass pass, which waits for all copies)
+        if (e0 + stride < a.ne) prefetch_recs<E, NT>(a.frec, a.ne, e0 + stride, sRec);
+        cp_async_commit();
         // face lift per (element, face, variable) into Tn's space
         for (int t = tid; t < E * 30; t += NT) {
             const int v = t % 5, f = (t / 5) % 6, e = t / 30;
@@ -676,7 +699,7 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
             const int bxy = i % N2, ev = i / N2, e = ev / 5;
             if (e0 + e >= a.ne) continue;
             const int ge = e0 + e;
-            const GeoDev& gg = a.geo[a.geo_class[ge]];
+            const GeoDev& gg = a.geo[sCls[e]];
             const double scale = a.dt * gg.dtf * gg.inv_djac;
             const int v = ev % 5;
             const double* r = sRes + e * ES + v * VS + bxy;  // pencil along z
