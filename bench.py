@@ -321,7 +321,8 @@ def main():
                        "cfl": CFL, "dt": dt, "l2": "inputs larger than L2 (each state buffer %.0f MB > 126 MB)" % (state_bytes / 1e6),
                        "parallelism": "replicas" if world > 1 else "single-gpu",
                        "stage_variant": {"chosen": variants[best], "tuned_ms_per_launch": dict(
-                           ("E%d_NT%d_G%d_%s" % v, round(t, 4)) for v, t in zip(variants, tune_ms) if t >= 0)}},
+                           ("E%d_NT%d_G%d_%s" % v[:4] + ("_" + v[4] if v[4] else ""), round(t, 4))
+                           for v, t in zip(variants, tune_ms) if t >= 0)}},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
                          "peak_source": peak_kind,

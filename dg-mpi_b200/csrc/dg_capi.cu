@@ -1148,6 +1148,15 @@ int dg_stage_variant_info(int order, int v, int* elems_per_cta, int* threads_per
     return DG_OK;
 }
 
+int dg_stage_variant_flags(int order, int v, int* flags)
+{
+    const dgk::StageVariant* vs = nullptr;
+    const int nv = dgk::stage_variants(order, &vs);
+    if (v < 0 || v >= nv || !flags) return DG_ERR_ARG;
+    *flags = vs[v].flags;
+    return DG_OK;
+}
+
 int dg_set_stage_variant(dg_ctx* c, int v)
 {
     if (!c) return DG_ERR_ARG;

@@ -127,8 +127,9 @@ __host__ __device__ constexpr int cmax(int a, int b) { return a > b ? a : b; }
 // G = number of variable groups of the fused pointwise phase (register budget);
 // T = arithmetic of the residual (the work area W holds T values, everything
 // else FP64); PZ: the groups' pencil tasks run in one phase (the z-contraction
-// output of all five variables is held at once)
-template <int P, int G, typename T = double, bool PZ = false>
+// output of all five variables is held at once); SB: one coefficient buffer,
+// refilled with the next batch once the traces have read it (instead of two)
+template <int P, int G, typename T = double, bool PZ = false, bool SB = false>
 struct Lay {
     static constexpr int N = P + 1, M = P + 2, NB = N * N * N, NF = M * M, N2 = N * N;
     static constexpr int GV = G == 1 ? 5 : (G == 2 ? 3 : 2);  // variables per group (max)
@@ -148,8 +149,8 @@ struct Lay {
     // (streamed in during the volume phase), then the batch's U0 and RK
     // accumulator [2][ES] (streamed in during the face phase)
     static constexpr int OPS = cmax(2 * ES, 30 * NS);
-    // FP64: U (double-buffered prefetch), residual, operand region
-    static constexpr int per_elem_f64 = 2 * ES + ES + OPS;
+    // FP64: U (double-buffered prefetch, or single with SB), residual, operand region
+    static constexpr int per_elem_f64 = (SB ? 1 : 2) * ES + ES + OPS;
     // bytes per element, work area in T
     static constexpr size_t bytes_per_elem = sizeof(double) * per_elem_f64 + sizeof(T) * W;
     // face data of a batch: the six face records (the next batch's are
@@ -254,16 +255,16 @@ __device__ __forceinline__ void interp2d(const T* __restrict__ Bt, const T (&s)[
         }
 }
 
-template <int P, int E, int NT, int G, typename T, bool PZ>
+template <int P, int E, int NT, int G, typename T, bool PZ, bool SB>
 __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
 {
-    using L = Lay<P, G, T, PZ>;
+    using L = Lay<P, G, T, PZ, SB>;
     constexpr int N = L::N, M = L::M, NB = L::NB, NF = L::NF, N2 = L::N2;
     constexpr int VS = L::VS, ES = L::ES, FS = L::FS, NS = L::NS, X1S = L::X1S, X2S = L::X2S, W = L::W, GV = L::GV;
     constexpr int OPS = L::OPS;
     extern __shared__ double smem[];
-    double* sUbuf = smem;                  // [2][E][ES]
-    double* sRes = sUbuf + 2 * E * ES;     // [E][ES]
+    double* sUbuf = smem;                  // [2][E][ES] ([1][E][ES] with SB)
+    double* sRes = sUbuf + (SB ? 1 : 2) * E * ES;  // [E][ES]
     double* sOps = sRes + E * ES;          // [E][OPS] neighbour slices, then U0 | acc
     T* sW = reinterpret_cast<T*>(sOps + E * OPS);  // [E][W] in the residual's arithmetic
     // face data (see Lay::meta_bytes_per_elem), 16-byte aligned after sW
@@ -272,6 +273,9 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
     int* sCls = reinterpret_cast<int*>(sRec + E * 6);                  // [E] geometry classes
     unsigned char* sCm = reinterpret_cast<unsigned char*>(sCls + E);  // [E*6][NF]
     const bool need_u0_acc = a.mode == kModeRK2 || a.mode == kModeRK3 || a.mode == kModeRK4;
+    // with SB the coefficient buffer is refilled before the update, so the
+    // update's step-start state always comes from the operand region
+    const bool stage_u0 = need_u0_acc || (SB && (a.mode == kModeRK1 || a.mode == kModeFE));
     const T* __restrict__ Bt = TabSel<T>::B(a.tab);
     const T* __restrict__ Dt = TabSel<T>::D(a.tab);
     const T* __restrict__ Wt = TabSel<T>::W(a.tab);
@@ -295,7 +299,7 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
     cp_async_commit();
 
     for (int e0 = e_first; e0 < a.ne; e0 += stride, buf ^= 1) {
-        double* sU = sUbuf + buf * E * ES;
+        double* sU = sUbuf + (SB ? 0 : buf) * E * ES;
         cp_async_wait_all();
         __syncthreads();
         // stream in the neighbours' boundary slices (the periodic face gather)
@@ -316,7 +320,8 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
             if (fv == 0) sCls[e] = rec.cls;
         }
         cp_async_commit();
-        if (e0 + stride < a.ne) prefetch_batch<P, G, E, NT>(a.Us, a.ne, e0 + stride, sUbuf + (buf ^ 1) * E * ES, ES);
+        if (!SB && e0 + stride < a.ne)
+            prefetch_batch<P, G, E, NT>(a.Us, a.ne, e0 + stride, sUbuf + (buf ^ 1) * E * ES, ES);
         cp_async_commit();
 
         // ---- volume: interpolation passes x, y ----
@@ -490,7 +495,8 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
 
         // ---- faces: the neighbours' slices have landed (the next batch's
         //      coefficients may still be in flight) ----
-        cp_async_wait_older();
+        if constexpr (SB) cp_async_wait_all();  // only the slices are in flight
+        else cp_async_wait_older();
         __syncthreads();
         // own and neighbour traces: one task per (element, face, variable) doing
         // both sides, or -- when the CTA has threads to spare (high orders) --
@@ -540,11 +546,11 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
             }
         }
         __syncthreads();
-        // the staging area is free: stream in this batch's RK operands
-        if (need_u0_acc) {
-            prefetch_batch<P, G, E, NT>(a.U0, a.ne, e0, sOps, OPS);
-            prefetch_batch<P, G, E, NT>(a.acc, a.ne, e0, sOps + ES, OPS);
-        }
+        // the staging area is free: stream in this batch's RK operands (and,
+        // with SB, the next batch's coefficients: the traces were their last reader)
+        if (stage_u0) prefetch_batch<P, G, E, NT>(a.U0, a.ne, e0, sOps, OPS);
+        if (need_u0_acc) prefetch_batch<P, G, E, NT>(a.acc, a.ne, e0, sOps + ES, OPS);
+        if (SB && e0 + stride < a.ne) prefetch_batch<P, G, E, NT>(a.Us, a.ne, e0 + stride, sU, ES);
         cp_async_commit();
 
         // numerical flux at every face point, written over the own trace; two
@@ -712,7 +718,7 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
             const double* r = sRes + e * ES + v * VS + bxy;  // pencil along z
             // step-start state: the prefetched U0, or the stage state itself in
             // RK1 / FE where the two coincide
-            const double* u0 = (need_u0_acc ? sOps + e * OPS : sU + e * ES) + v * VS + bxy;
+            const double* u0 = (stage_u0 ? sOps + e * OPS : sU + e * ES) + v * VS + bxy;
             const double* ac = sOps + e * OPS + ES + v * VS + bxy;
             double t[N];
 #pragma unroll
@@ -740,10 +746,11 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
     if (status) atomicOr(a.status, status);
 }
 
-template <int P, int E, int G, typename T, bool PZ = false>
+template <int P, int E, int G, typename T, bool PZ = false, bool SB = false>
 constexpr size_t stage_smem_bytes()
 {
-    return ((E * Lay<P, G, T, PZ>::bytes_per_elem + 15) / 16) * 16 + E * Lay<P, G, T, PZ>::meta_bytes_per_elem;
+    using L = Lay<P, G, T, PZ, SB>;
+    return ((E * L::bytes_per_elem + 15) / 16) * 16 + E * L::meta_bytes_per_elem;
 }
 
 // ---- compiled launch variants (one translation unit per order) ----
@@ -751,26 +758,27 @@ constexpr size_t stage_smem_bytes()
 struct StageVariant {
     int E, NT, G;        // elements per CTA, threads per CTA, variable groups
     int fp32;            // 1: residual arithmetic in FP32 (mixed precision), 0: FP64
+    int flags;           // 1: groups' pencils in one phase (PZ), 2: single coefficient buffer (SB)
     size_t smem;         // dynamic shared memory per CTA
     const void* func;    // the kernel, for attributes / occupancy queries
     cudaError_t (*launch)(const StageArgs&, int grid, cudaStream_t);
 };
 
-template <int P, int E, int NT, int G, typename T, bool PZ>
+template <int P, int E, int NT, int G, typename T, bool PZ, bool SB>
 cudaError_t launch_stage_variant(const StageArgs& a, int grid, cudaStream_t s)
 {
-    stage_kernel<P, E, NT, G, T, PZ><<<grid, NT, stage_smem_bytes<P, E, G, T, PZ>(), s>>>(a);
+    stage_kernel<P, E, NT, G, T, PZ, SB><<<grid, NT, stage_smem_bytes<P, E, G, T, PZ, SB>(), s>>>(a);
     return cudaGetLastError();
 }
 
 // PZ = true: the variable groups' pencil tasks in one phase (worth it when
 // E * (p+2)^2 * G tasks fill fewer rounds of NT threads than G sequential phases)
-template <int P, int E, int NT, int G, typename T = double, bool PZ = false>
+template <int P, int E, int NT, int G, typename T = double, bool PZ = false, bool SB = false>
 constexpr StageVariant make_variant()
 {
-    static_assert(stage_smem_bytes<P, E, G, T, PZ>() <= 227 * 1024, "stage kernel shared memory exceeds 227 KB");
-    return StageVariant{E, NT, G, sizeof(T) == 4 ? 1 : 0, stage_smem_bytes<P, E, G, T, PZ>(),
-                        (const void*)stage_kernel<P, E, NT, G, T, PZ>, launch_stage_variant<P, E, NT, G, T, PZ>};
+    static_assert(stage_smem_bytes<P, E, G, T, PZ, SB>() <= 227 * 1024, "stage kernel shared memory exceeds 227 KB");
+    return StageVariant{E, NT, G, sizeof(T) == 4 ? 1 : 0, (PZ ? 1 : 0) | (SB ? 2 : 0), stage_smem_bytes<P, E, G, T, PZ, SB>(),
+                        (const void*)stage_kernel<P, E, NT, G, T, PZ, SB>, launch_stage_variant<P, E, NT, G, T, PZ, SB>};
 }
 
 // the variants compiled for order p (defined in dg_stage_p<p>.cu)

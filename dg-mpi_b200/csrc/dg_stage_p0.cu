@@ -1,7 +1,7 @@
 // dg_stage_p0.cu -- compiled launch variants of the stage kernel for order p = 0
-// (elements per CTA, threads per CTA, variable groups; FP64 residual first,
-// then the mixed-precision FP32 residual).  The first variant of each
-// precision is the default; the tuner (dg_tune_stage) may pick another.
+// (elements per CTA, threads per CTA, variable groups, residual arithmetic; then the
+// optional flags: all groups' pencils in one phase, single coefficient buffer).  The
+// first variant of each precision is the default (the measured best); dg_tune_stage may pick another.
 #include "dg_stage.cuh"
 
 namespace dgk {

@@ -1,19 +1,19 @@
 // dg_stage_p2.cu -- compiled launch variants of the stage kernel for order p = 2
-// (elements per CTA, threads per CTA, variable groups; FP64 residual first,
-// then the mixed-precision FP32 residual).  The first variant of each
-// precision is the default; the tuner (dg_tune_stage) may pick another.
+// (elements per CTA, threads per CTA, variable groups, residual arithmetic; then the
+// optional flags: all groups' pencils in one phase, single coefficient buffer).  The
+// first variant of each precision is the default (the measured best); dg_tune_stage may pick another.
 #include "dg_stage.cuh"
 
 namespace dgk {
 
 static const StageVariant kVariants2[] = {
-    make_variant<2, 6, 96, 1, double>(),
     make_variant<2, 1, 32, 1, double>(),
     make_variant<2, 2, 64, 1, double>(),
     make_variant<2, 1, 32, 2, double>(),
-    make_variant<2, 2, 64, 1, float>(),
+    make_variant<2, 6, 96, 1, double>(),
     make_variant<2, 1, 32, 1, float>(),
     make_variant<2, 4, 128, 1, float>(),
+    make_variant<2, 2, 64, 1, float>(),
 };
 
 int stage_variants_p2(const StageVariant** out)

@@ -1,20 +1,22 @@
 // dg_stage_p3.cu -- compiled launch variants of the stage kernel for order p = 3
-// (elements per CTA, threads per CTA, variable groups; FP64 residual first,
-// then the mixed-precision FP32 residual).  The first variant of each
-// precision is the default; the tuner (dg_tune_stage) may pick another.
+// (elements per CTA, threads per CTA, variable groups, residual arithmetic; then the
+// optional flags: all groups' pencils in one phase, single coefficient buffer).  The
+// first variant of each precision is the default (the measured best); dg_tune_stage may pick another.
 #include "dg_stage.cuh"
 
 namespace dgk {
 
 static const StageVariant kVariants3[] = {
-    make_variant<3, 1, 32, 2, double>(),
-    make_variant<3, 3, 96, 2, double>(),
-    make_variant<3, 1, 32, 1, double>(),
+    make_variant<3, 1, 32, 2, double, false, true>(),
     make_variant<3, 2, 64, 2, double>(),
-    make_variant<3, 1, 64, 2, double>(),
-    make_variant<3, 1, 32, 1, float>(),
-    make_variant<3, 2, 64, 1, float>(),
+    make_variant<3, 2, 64, 2, double, false, true>(),
+    make_variant<3, 1, 32, 2, double>(),
+    make_variant<3, 1, 32, 1, double>(),
+    make_variant<3, 3, 96, 2, double>(),
+    make_variant<3, 1, 32, 1, float, false, true>(),
+    make_variant<3, 2, 64, 2, float, false, true>(),
     make_variant<3, 2, 64, 2, float>(),
+    make_variant<3, 1, 32, 1, float>(),
     make_variant<3, 4, 128, 1, float>(),
 };
 

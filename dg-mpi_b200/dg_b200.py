@@ -100,6 +100,7 @@ def library(path: str | None = None) -> ctypes.CDLL:
         "dg_basis_tables": (ctypes.c_int, [ctypes.c_int, dp, dp, dp]),
         "dg_num_stage_variants": (ctypes.c_int, [ctypes.c_int]),
         "dg_stage_variant_info": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ip, ip, ip, ip]),
+        "dg_stage_variant_flags": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ip]),
         "dg_set_stage_variant": (ctypes.c_int, [vp, ctypes.c_int]),
         "dg_get_stage_variant": (ctypes.c_int, [vp]),
         "dg_tune_stage": (ctypes.c_int, [vp, ctypes.c_int, ip, dp]),
@@ -426,13 +427,17 @@ class Case:
 
     # -- launch variants ---------------------------------------------------
     def stage_variants(self):
-        """[(elements per CTA, threads per CTA, variable groups, precision)] compiled for this order."""
+        """[(elements per CTA, threads per CTA, variable groups, precision, options)] compiled for this
+        order; options is "" or a "+"-joined subset of "pz" (groups' pencils in one phase) and "sb"
+        (single coefficient buffer)."""
         out = []
         for v in range(self._lib.dg_num_stage_variants(self.order)):
-            E, NT, G, pr = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+            E, NT, G, pr, fl = (ctypes.c_int() for _ in range(5))
             self._lib.dg_stage_variant_info(self.order, v, ctypes.byref(E), ctypes.byref(NT), ctypes.byref(G),
                                             ctypes.byref(pr))
-            out.append((E.value, NT.value, G.value, "mixed_fp32" if pr.value == 1 else "fp64"))
+            self._lib.dg_stage_variant_flags(self.order, v, ctypes.byref(fl))
+            opts = "+".join(n for b, n in ((1, "pz"), (2, "sb")) if fl.value & b)
+            out.append((E.value, NT.value, G.value, "mixed_fp32" if pr.value == 1 else "fp64", opts))
         return out
 
     @property

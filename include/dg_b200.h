@@ -148,6 +148,10 @@ int dg_rk4_steps_timed(dg_ctx* ctx, double dt, int nsteps, double* device_ms);
 int dg_num_stage_variants(int order);
 int dg_stage_variant_info(int order, int variant, int* elems_per_cta, int* threads_per_cta, int* groups,
                           int* precision);
+/* Options of a variant: bit 0 -- the variable groups' pencil tasks run in one
+ * phase; bit 1 -- one coefficient buffer, refilled with the next batch once
+ * the face traces have read it (more resident CTAs, less prefetch overlap). */
+int dg_stage_variant_flags(int order, int variant, int* flags);
 int dg_set_stage_variant(dg_ctx* ctx, int variant);
 int dg_get_stage_variant(const dg_ctx* ctx);
 int dg_tune_stage(dg_ctx* ctx, int reps, int* best_variant, double* ms_per_variant);
