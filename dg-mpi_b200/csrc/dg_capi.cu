@@ -1190,12 +1190,14 @@ int dg_tune_stage(dg_ctx* c, int reps, int* best, double* ms_per_variant)
             continue;
         }
         c->variant = v;
-        // one untimed launch, then `reps` timed ones; the mass-inverse mode
-        // writes scratch output only, so the state is unchanged
-        rc = launch_stage(c, dgk::kModeMassInv, c->d_U0, c->d_U0, c->d_out, 1e-3);
+        // one untimed launch, then `reps` timed ones of an RK2 stage (reads the
+        // stage state, U0 and the accumulator, writes the accumulator and an
+        // output): the traffic of a real stage.  The output goes to scratch and
+        // the accumulator is dead between steps, so the state is unchanged.
+        rc = launch_stage(c, dgk::kModeRK2, c->d_U0, c->d_U0, c->d_out, 1e-3);
         if (rc) break;
         cudaEventRecord(ev[0], c->stream);
-        for (int r = 0; r < reps && rc == DG_OK; ++r) rc = launch_stage(c, dgk::kModeMassInv, c->d_U0, c->d_U0, c->d_out, 1e-3);
+        for (int r = 0; r < reps && rc == DG_OK; ++r) rc = launch_stage(c, dgk::kModeRK2, c->d_U0, c->d_U0, c->d_out, 1e-3);
         cudaEventRecord(ev[1], c->stream);
         if (cudaEventSynchronize(ev[1]) != cudaSuccess) { rc = fail(c, DG_ERR_CUDA, "tuning launch failed"); break; }
         float ms = 0.0f;

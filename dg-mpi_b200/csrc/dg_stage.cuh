@@ -126,11 +126,13 @@ __host__ __device__ constexpr int cmax(int a, int b) { return a > b ? a : b; }
 
 // G = number of variable groups of the fused pointwise phase (register budget);
 // T = arithmetic of the residual (the work area W holds T values, everything
-// else FP64); PZ: the groups' pencil tasks run in one phase (the z-contraction
-// output of all five variables is held at once); SB: one coefficient buffer,
-// refilled with the next batch once the traces have read it (instead of two)
-template <int P, int G, typename T = double, bool PZ = false, bool SB = false>
+// else FP64); FL: launch options, bit 1 (PZ) -- the groups' pencil tasks run in
+// one phase (the z-contraction output of all five variables is held at once);
+// bit 2 (SB) -- one coefficient buffer, refilled with the next batch once the
+// traces have read it (instead of two)
+template <int P, int G, typename T = double, int FL = 0>
 struct Lay {
+    static constexpr bool PZ = FL & 1, SB = FL & 2;
     static constexpr int N = P + 1, M = P + 2, NB = N * N * N, NF = M * M, N2 = N * N;
     static constexpr int GV = G == 1 ? 5 : (G == 2 ? 3 : 2);  // variables per group (max)
     static constexpr int GA = PZ ? 5 : GV;       // variables of the z-contraction buffers
@@ -255,10 +257,11 @@ __device__ __forceinline__ void interp2d(const T* __restrict__ Bt, const T (&s)[
         }
 }
 
-template <int P, int E, int NT, int G, typename T, bool PZ, bool SB>
+template <int P, int E, int NT, int G, typename T, int FL>
 __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
 {
-    using L = Lay<P, G, T, PZ, SB>;
+    using L = Lay<P, G, T, FL>;
+    constexpr bool PZ = L::PZ, SB = L::SB;
     constexpr int N = L::N, M = L::M, NB = L::NB, NF = L::NF, N2 = L::N2;
     constexpr int VS = L::VS, ES = L::ES, FS = L::FS, NS = L::NS, X1S = L::X1S, X2S = L::X2S, W = L::W, GV = L::GV;
     constexpr int OPS = L::OPS;
@@ -274,7 +277,7 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
     unsigned char* sCm = reinterpret_cast<unsigned char*>(sCls + E);  // [E*6][NF]
     const bool need_u0_acc = a.mode == kModeRK2 || a.mode == kModeRK3 || a.mode == kModeRK4;
     // with SB the coefficient buffer is refilled before the update, so the
-    // update's step-start state always comes from the operand region
+    // update's step-start state comes from the operand region in every mode
     const bool stage_u0 = need_u0_acc || (SB && (a.mode == kModeRK1 || a.mode == kModeFE));
     const T* __restrict__ Bt = TabSel<T>::B(a.tab);
     const T* __restrict__ Dt = TabSel<T>::D(a.tab);
@@ -746,10 +749,10 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
     if (status) atomicOr(a.status, status);
 }
 
-template <int P, int E, int G, typename T, bool PZ = false, bool SB = false>
+template <int P, int E, int G, typename T, int FL = 0>
 constexpr size_t stage_smem_bytes()
 {
-    using L = Lay<P, G, T, PZ, SB>;
+    using L = Lay<P, G, T, FL>;
     return ((E * L::bytes_per_elem + 15) / 16) * 16 + E * L::meta_bytes_per_elem;
 }
 
@@ -758,27 +761,29 @@ constexpr size_t stage_smem_bytes()
 struct StageVariant {
     int E, NT, G;        // elements per CTA, threads per CTA, variable groups
     int fp32;            // 1: residual arithmetic in FP32 (mixed precision), 0: FP64
-    int flags;           // 1: groups' pencils in one phase (PZ), 2: single coefficient buffer (SB)
+    int flags;           // 1: groups' pencils in one phase, 2: single coefficient buffer
     size_t smem;         // dynamic shared memory per CTA
     const void* func;    // the kernel, for attributes / occupancy queries
     cudaError_t (*launch)(const StageArgs&, int grid, cudaStream_t);
 };
 
-template <int P, int E, int NT, int G, typename T, bool PZ, bool SB>
+template <int P, int E, int NT, int G, typename T, int FL>
 cudaError_t launch_stage_variant(const StageArgs& a, int grid, cudaStream_t s)
 {
-    stage_kernel<P, E, NT, G, T, PZ, SB><<<grid, NT, stage_smem_bytes<P, E, G, T, PZ, SB>(), s>>>(a);
+    stage_kernel<P, E, NT, G, T, FL><<<grid, NT, stage_smem_bytes<P, E, G, T, FL>(), s>>>(a);
     return cudaGetLastError();
 }
 
-// PZ = true: the variable groups' pencil tasks in one phase (worth it when
-// E * (p+2)^2 * G tasks fill fewer rounds of NT threads than G sequential phases)
-template <int P, int E, int NT, int G, typename T = double, bool PZ = false, bool SB = false>
+// launch options FL (see Lay); one-phase groups pay off when E * (p+2)^2 * G
+// pencil tasks fill fewer rounds of NT threads than G sequential phases; the
+// single buffer trades prefetch overlap for occupancy
+constexpr int kPZ = 1, kSB = 2;
+template <int P, int E, int NT, int G, typename T = double, int FL = 0>
 constexpr StageVariant make_variant()
 {
-    static_assert(stage_smem_bytes<P, E, G, T, PZ, SB>() <= 227 * 1024, "stage kernel shared memory exceeds 227 KB");
-    return StageVariant{E, NT, G, sizeof(T) == 4 ? 1 : 0, (PZ ? 1 : 0) | (SB ? 2 : 0), stage_smem_bytes<P, E, G, T, PZ, SB>(),
-                        (const void*)stage_kernel<P, E, NT, G, T, PZ, SB>, launch_stage_variant<P, E, NT, G, T, PZ, SB>};
+    static_assert(stage_smem_bytes<P, E, G, T, FL>() <= 227 * 1024, "stage kernel shared memory exceeds 227 KB");
+    return StageVariant{E, NT, G, sizeof(T) == 4 ? 1 : 0, FL, stage_smem_bytes<P, E, G, T, FL>(),
+                        (const void*)stage_kernel<P, E, NT, G, T, FL>, launch_stage_variant<P, E, NT, G, T, FL>};
 }
 
 // the variants compiled for order p (defined in dg_stage_p<p>.cu)

@@ -7,16 +7,16 @@
 namespace dgk {
 
 static const StageVariant kVariants3[] = {
-    make_variant<3, 1, 32, 2, double, false, true>(),
+    make_variant<3, 1, 32, 2, double, kSB>(),
     make_variant<3, 2, 64, 2, double>(),
-    make_variant<3, 2, 64, 2, double, false, true>(),
+    make_variant<3, 2, 64, 2, double, kSB>(),
     make_variant<3, 1, 32, 2, double>(),
     make_variant<3, 1, 32, 1, double>(),
     make_variant<3, 3, 96, 2, double>(),
-    make_variant<3, 1, 32, 1, float, false, true>(),
-    make_variant<3, 2, 64, 2, float, false, true>(),
-    make_variant<3, 2, 64, 2, float>(),
+    make_variant<3, 1, 32, 1, float, kSB>(),
+    make_variant<3, 2, 64, 2, float, kSB>(),
     make_variant<3, 1, 32, 1, float>(),
+    make_variant<3, 2, 64, 2, float>(),
     make_variant<3, 4, 128, 1, float>(),
 };
 

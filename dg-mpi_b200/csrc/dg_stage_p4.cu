@@ -12,12 +12,11 @@ static const StageVariant kVariants4[] = {
     make_variant<4, 1, 128, 2, double>(),
     make_variant<4, 1, 32, 2, double>(),
     make_variant<4, 1, 32, 3, double>(),
-    make_variant<4, 1, 128, 2, float, true>(),
     make_variant<4, 1, 64, 1, float>(),
+    make_variant<4, 1, 128, 2, float, kPZ>(),
     make_variant<4, 1, 32, 2, float>(),
     make_variant<4, 1, 32, 1, float>(),
     make_variant<4, 2, 64, 1, float>(),
-    make_variant<4, 1, 128, 2, float>(),
 };
 
 int stage_variants_p4(const StageVariant** out)

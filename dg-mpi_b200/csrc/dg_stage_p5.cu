@@ -8,11 +8,11 @@ namespace dgk {
 
 static const StageVariant kVariants5[] = {
     make_variant<5, 1, 128, 3, double>(),
-    make_variant<5, 1, 128, 3, double, true>(),
+    make_variant<5, 1, 128, 3, double, kPZ>(),
     make_variant<5, 1, 64, 3, double>(),
     make_variant<5, 2, 128, 3, double>(),
     make_variant<5, 1, 32, 3, double>(),
-    make_variant<5, 1, 128, 2, float, false, true>(),
+    make_variant<5, 1, 128, 2, float, kSB>(),
     make_variant<5, 1, 128, 2, float>(),
     make_variant<5, 1, 64, 2, float>(),
     make_variant<5, 1, 64, 1, float>(),

@@ -141,8 +141,9 @@ int dg_rk4_steps_timed(dg_ctx* ctx, double dt, int nsteps, double* device_ms);
 /* ---- stage-kernel launch variants and their tuner ----
  * Each order has a few compiled variants of the fused stage kernel (elements
  * per CTA, threads per CTA, variable groups of the pointwise phase).  The
- * tuner times one stage of every variant of the context's precision on its
- * mesh and current state (the state is not modified) and selects the
+ * tuner times one RK stage of every variant of the context's precision on its
+ * mesh and current state (the state is not modified; the RK accumulator, dead
+ * between steps, serves as scratch, so call it between steps) and selects the
  * fastest (entries of other precision report -1 ms); callers cache the result
  * per (order, precision, GPU) and restore it with dg_set_stage_variant. */
 int dg_num_stage_variants(int order);
