@@ -301,8 +301,8 @@ void* dg_stream(dg_ctx* ctx);
  * dg_ctx on the same case).  Cases of the same (order, flux, gamma, gas
  * constant) share one group: their meshes are concatenated and one stage
  * launch per group and RK stage advances all of them, each element scaling its
- * update by its own case's dt.  dg_batch_rk4_steps replays a CUDA graph in
- * which the groups' launches are independent branches.  All cases must name
+ * update by its own case's dt.  dg_batch_rk4_steps replays a CUDA graph that
+ * runs the groups' launches one group after another (each fills the GPU).  All cases must name
  * the same device and precision.  Results per case are bit-identical to a
  * dg_ctx of that case running the same stage variant. */
 typedef struct dg_batch dg_batch;
