@@ -126,9 +126,9 @@ __host__ __device__ constexpr int cmax(int a, int b) { return a > b ? a : b; }
 
 // G = number of variable groups of the fused pointwise phase (register budget);
 // T = arithmetic of the residual (the work area W holds T values, everything
-// else FP64); FL: launch options, bit 1 (PZ) -- the groups' pencil tasks run in
+// else FP64); FL: launch options, flag 1 (PZ) -- the groups' pencil tasks run in
 // one phase (the z-contraction output of all five variables is held at once);
-// bit 2 (SB) -- one coefficient buffer, refilled with the next batch once the
+// flag 2 (SB) -- one coefficient buffer, refilled with the next batch once the
 // traces have read it (instead of two)
 template <int P, int G, typename T = double, int FL = 0>
 struct Lay {
