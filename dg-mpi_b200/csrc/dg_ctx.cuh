@@ -13,7 +13,7 @@
 #include "dg_stage.cuh"
 
 namespace dgi {
-constexpr int kMaxVariants = 16;  // launch variants per order (checked in prepare_variant)
+constexpr int kMaxVariants = 32;  // launch variants per order (checked in prepare_variant)
 }
 
 struct dg_ctx {

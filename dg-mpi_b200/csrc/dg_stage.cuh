@@ -129,10 +129,15 @@ __host__ __device__ constexpr int cmax(int a, int b) { return a > b ? a : b; }
 // else FP64); FL: launch options, flag 1 (PZ) -- the groups' pencil tasks run in
 // one phase (the z-contraction output of all five variables is held at once);
 // flag 2 (SB) -- one coefficient buffer, refilled with the next batch once the
-// traces have read it (instead of two)
+// traces have read it (instead of two); flag 4 (UF) -- unfused volume: the z
+// interpolation, the pointwise flux and each contraction are separate passes
+// over a point array holding all quadrature points (the flux is evaluated once
+// per point instead of once per variable group; G is unused); flag 8 (RS) --
+// traces and lifts as one task per output row instead of per face slice;
+// flag 16 (K1) -- one face-flux point per thread and iteration (registers)
 template <int P, int G, typename T = double, int FL = 0>
 struct Lay {
-    static constexpr bool PZ = FL & 1, SB = FL & 2;
+    static constexpr bool PZ = FL & 1, SB = FL & 2, UF = FL & 4, RS = FL & 8, K1 = FL & 16;
     static constexpr int N = P + 1, M = P + 2, NB = N * N * N, NF = M * M, N2 = N * N;
     static constexpr int GV = G == 1 ? 5 : (G == 2 ? 3 : 2);  // variables per group (max)
     static constexpr int GA = PZ ? 5 : GV;       // variables of the z-contraction buffers
@@ -142,10 +147,13 @@ struct Lay {
     static constexpr int NS = odd(N2);           // per-(face, variable) stride of neighbour slices
     static constexpr int X1S = odd(N2 * M);      // [bz][by][qx] block
     static constexpr int X2S = odd(N * NF);      // [bz][qy][qx] block
+    static constexpr int QS = odd(M * NF);       // [qz][qy][qx] block of the point array (UF)
     // per-element work area: face phase {Tr[6][5], Tn[6][5]} x FS;
-    // volume phase X2[5] | (X1[5] or A[GA][3] + C[GA][2])
+    // volume phase X2[5] | (X1[5] or A[GA][3] + C[GA][2]), or with UF the
+    // point array Q[15] (X2 in its first five rows, X1 after them)
     static constexpr int face = 60 * FS;
-    static constexpr int vol = 5 * X2S + cmax(5 * X1S, GA * (3 * X2S + 2 * X1S));
+    static constexpr int vol =
+        UF ? cmax(15 * QS, 5 * QS + 5 * X1S) : 5 * X2S + cmax(5 * X1S, GA * (3 * X2S + 2 * X1S));
     static constexpr int W = odd(cmax(face, vol));
     // FP64 operand region: first the neighbours' boundary slices [30][NS]
     // (streamed in during the volume phase), then the batch's U0 and RK
@@ -288,8 +296,8 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
     // the FP32 residual works on rE - E_ref (see dgp::interior_flux_r1)
     constexpr bool kShift = sizeof(T) == 4;
     // face-flux points per thread and iteration: measured best 3 at p = 2 and
-    // p = 5, 2 at the other orders (more points add registers)
-    constexpr int kFluxPoints = (P == 2 || P == 5) ? 3 : 2;
+    // p = 5, 2 at the other orders (more points add registers); 1 with K1
+    constexpr int kFluxPoints = L::K1 ? 1 : ((P == 2 || P == 5) ? 3 : 2);
     unsigned status = 0;
     const int stride = gridDim.x * E;
     const int e_first = a.e_begin + blockIdx.x * E;
@@ -328,8 +336,12 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
         cp_async_commit();
 
         // ---- volume: interpolation passes x, y ----
-        T* X2 = sW;               // per element: [5][X2S] with [bz][qy][qx]
-        T* X1 = sW + 5 * X2S;     // per element: [5][X1S] with [bz][by][qx]
+        // per element: X2 [5][X2V] with [bz][qy][qx] (with UF, the first five
+        // rows of the point array, where the z pass interpolates in place) and
+        // X1 [5][X1S] with [bz][by][qx] (with UF, in rows 5.. of the point array)
+        constexpr int X2V = L::UF ? L::QS : X2S;
+        T* X2 = sW;
+        T* X1 = sW + 5 * X2V;
         for (int i = tid; i < E * 5 * N2; i += NT) {
             const int v = i % 5, byz = (i / 5) % N2, e = i / (5 * N2);
             const double* u = sU + e * ES + v * VS + byz * N;
@@ -354,7 +366,7 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
             T col[N];
 #pragma unroll
             for (int by = 0; by < N; ++by) col[by] = x1[by * M];
-            T* o = X2 + e * W + v * X2S + bz * NF + qx;
+            T* o = X2 + e * W + v * X2V + bz * NF + qx;
 #pragma unroll
             for (int qy = 0; qy < M; ++qy) {
                 T s = T(0);
@@ -365,80 +377,88 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
         }
         __syncthreads();
 
-        // ---- fused: z interpolation, Euler flux, contravariant transform and
-        //      first (z) divergence contraction; then y and x contractions ----
-        T* Abuf = sW + 5 * X2S;                     // [GA][3][X2S] over X1
-        T* Cbuf = Abuf + L::GA * 3 * X2S;           // [GA][2][X1S]
-        // one (x,y) pencil of element e for variable group g; the buffers hold
-        // the group's variables from slot abase (0, or its first variable with PZ)
-        auto pencil = [&](auto gc, int e, int qxy) {
-            constexpr int g = decltype(gc)::value;
-            constexpr int gv0 = group_first<P, G>(g), gnv = group_size<P, G>(g), abase = PZ ? gv0 : 0;
-            const int qx = qxy % M, qy = qxy / M;
-            T xz[5][N];
+        if constexpr (L::UF) {
+            // ---- unfused: z interpolation in the point array, the flux at
+            //      every point, then z, y and x contractions (in place) ----
+            constexpr int QS = L::QS, NQ = M * NF;
+            T* Q = sW;  // per element: [15][QS], point index qz*NF + qy*M + qx
+            // z interpolation in place: each task owns one (variable, x-y point) column
+            for (int i = tid; i < E * 5 * NF; i += NT) {
+                const int qxy = i % NF, v = (i / NF) % 5, e = i / (5 * NF);
+                T* o = Q + e * W + v * QS + qxy;
+                T col[N];
 #pragma unroll
-            for (int v = 0; v < 5; ++v)
+                for (int bz = 0; bz < N; ++bz) col[bz] = o[bz * NF];
 #pragma unroll
-                for (int bz = 0; bz < N; ++bz) xz[v][bz] = X2[e * W + v * X2S + bz * NF + qxy];
-            const GeoDev* geo = a.geo + sCls[e];
-            const T hr = kShift ? T(a.gamma * geo->eref) : T(0);
-            const T pref = kShift ? T((a.gamma - 1.0) * geo->eref) : T(0);
-            T JD[9];
-#pragma unroll
-            for (int k = 0; k < 9; ++k) JD[k] = T(geo->JD[k]);
-            T acc[gnv][3][N];
-#pragma unroll
-            for (int v = 0; v < gnv; ++v)
-#pragma unroll
-                for (int d = 0; d < 3; ++d)
-#pragma unroll
-                    for (int bz = 0; bz < N; ++bz) acc[v][d][bz] = T(0);
-            const T wxy = Wt[qx] * Wt[qy];
-#pragma unroll
-            for (int qz = 0; qz < M; ++qz) {
-                T U[5];
-#pragma unroll
-                for (int v = 0; v < 5; ++v) {
+                for (int qz = 0; qz < M; ++qz) {
                     T s = T(0);
 #pragma unroll
-                    for (int bz = 0; bz < N; ++bz) s += Bt[qz * N + bz] * xz[v][bz];
-                    U[v] = s;
-                }
-                T F[15];
-                const T p = dgp::interior_flux_r1<T, kShift>(gamma, U, F, hr);
-                if constexpr (g == 0) {
-                    if (!(U[0] > T(0))) status |= kStatusRho;
-                    if (!(p + pref > T(0))) status |= kStatusPressure;
-                    if (U[0] != U[0] || p != p) status |= kStatusNaN;
-                }
-                const T wq = wxy * Wt[qz];
-#pragma unroll
-                for (int vv = 0; vv < gnv; ++vv) {
-                    const int v = gv0 + vv;
-#pragma unroll
-                    for (int d = 0; d < 3; ++d) {
-                        const T Gd = (F[v] * JD[d * 3 + 0] + F[5 + v] * JD[d * 3 + 1] + F[10 + v] * JD[d * 3 + 2]) * wq;
-#pragma unroll
-                        for (int bz = 0; bz < N; ++bz) acc[vv][d][bz] += (d == 2 ? Dt[qz * N + bz] : Bt[qz * N + bz]) * Gd;
-                    }
+                    for (int bz = 0; bz < N; ++bz) s += Bt[qz * N + bz] * col[bz];
+                    o[qz * NF] = s;
                 }
             }
+            __syncthreads();
+            // Euler flux and contravariant transform: point q's five states become
+            // its fifteen components (v, d) in row 3v+d (each thread owns column q)
+            for (int i = tid; i < E * NQ; i += NT) {
+                const int q = i % NQ, e = i / NQ;
+                const int qx = q % M, qy = (q / M) % M, qz = q / NF;
+                T* qp = Q + e * W + q;
+                T U[5];
 #pragma unroll
-            for (int vv = 0; vv < gnv; ++vv)
+                for (int v = 0; v < 5; ++v) U[v] = qp[v * QS];
+                const GeoDev* geo = a.geo + sCls[e];
+                const T hr = kShift ? T(a.gamma * geo->eref) : T(0);
+                const T pref = kShift ? T((a.gamma - 1.0) * geo->eref) : T(0);
+                T F[15];
+                const T p = dgp::interior_flux_r1<T, kShift>(gamma, U, F, hr);
+                if (!(U[0] > T(0))) status |= kStatusRho;
+                if (!(p + pref > T(0))) status |= kStatusPressure;
+                if (U[0] != U[0] || p != p) status |= kStatusNaN;
+                T JD[9];
 #pragma unroll
-                for (int d = 0; d < 3; ++d)
+                for (int k = 0; k < 9; ++k) JD[k] = T(geo->JD[k]);
+                const T wq = Wt[qx] * Wt[qy] * Wt[qz];
 #pragma unroll
-                    for (int bz = 0; bz < N; ++bz)
-                        Abuf[e * W + ((abase + vv) * 3 + d) * X2S + bz * NF + qxy] = acc[vv][d][bz];
-        };
-        // y and x contractions of nv buffered variables into residual variables
-        // v0 .. v0+nv-1: C0 = By^T A0, C12 = Dy^T A1 + By^T A2; res = Dx^T C0 + Bx^T C12
-        auto contract_yx = [&](int nv, int v0) {
-            for (int i = tid; i < E * nv * N * M; i += NT) {
-                const int qx = i % M, bz = (i / M) % N, vv = (i / (M * N)) % nv, e = i / (nv * N * M);
-                const T* A0 = Abuf + e * W + (vv * 3 + 0) * X2S + bz * NF + qx;
-                const T* A1 = A0 + X2S;
-                const T* A2 = A1 + X2S;
+                for (int v = 0; v < 5; ++v)
+#pragma unroll
+                    for (int d = 0; d < 3; ++d)
+                        qp[(v * 3 + d) * QS] = (F[v] * JD[d * 3 + 0] + F[5 + v] * JD[d * 3 + 1] + F[10 + v] * JD[d * 3 + 2]) * wq;
+            }
+            __syncthreads();
+            // z contraction per (variable, x-y point), the three directions together:
+            // A_d = Bz^T G_d (d = 0, 1), A_2 = Dz^T G_2, written over the column
+            for (int i = tid; i < E * 5 * NF; i += NT) {
+                const int qxy = i % NF, v = (i / NF) % 5, e = i / (5 * NF);
+                T* g = Q + e * W + (v * 3) * QS + qxy;
+                T a0[N], a1[N], a2[N];
+#pragma unroll
+                for (int bz = 0; bz < N; ++bz) { a0[bz] = T(0); a1[bz] = T(0); a2[bz] = T(0); }
+#pragma unroll
+                for (int qz = 0; qz < M; ++qz) {
+                    const T g0 = g[qz * NF], g1 = g[QS + qz * NF], g2 = g[2 * QS + qz * NF];
+#pragma unroll
+                    for (int bz = 0; bz < N; ++bz) {
+                        a0[bz] += Bt[qz * N + bz] * g0;
+                        a1[bz] += Bt[qz * N + bz] * g1;
+                        a2[bz] += Dt[qz * N + bz] * g2;
+                    }
+                }
+#pragma unroll
+                for (int bz = 0; bz < N; ++bz) {
+                    g[bz * NF] = a0[bz];
+                    g[QS + bz * NF] = a1[bz];
+                    g[2 * QS + bz * NF] = a2[bz];
+                }
+            }
+            __syncthreads();
+            // y contraction per (variable, bz, qx): C0 = By^T A0 into row 3v,
+            // C12 = Dy^T A1 + By^T A2 into row 3v+1
+            for (int i = tid; i < E * 5 * N * M; i += NT) {
+                const int qx = i % M, bz = (i / M) % N, v = (i / (M * N)) % 5, e = i / (5 * N * M);
+                T* A0 = Q + e * W + (v * 3) * QS + bz * NF + qx;
+                const T* A1 = A0 + QS;
+                const T* A2 = A1 + QS;
                 T c0[N], c12[N];
 #pragma unroll
                 for (int by = 0; by < N; ++by) { c0[by] = T(0); c12[by] = T(0); }
@@ -451,18 +471,18 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
                         c12[by] += Dt[qy * N + by] * a1 + Bt[qy * N + by] * a2;
                     }
                 }
-                T* C0 = Cbuf + e * W + (vv * 2) * X1S + bz * N * M + qx;
 #pragma unroll
                 for (int by = 0; by < N; ++by) {
-                    C0[by * M] = c0[by];
-                    C0[X1S + by * M] = c12[by];
+                    A0[by * M] = c0[by];
+                    A0[QS + by * M] = c12[by];
                 }
             }
             __syncthreads();
-            for (int i = tid; i < E * nv * N2; i += NT) {
-                const int vv = i % nv, byz = (i / nv) % N2, e = i / (nv * N2);
-                const T* C0 = Cbuf + e * W + (vv * 2) * X1S + byz * M;
-                const T* C12 = C0 + X1S;
+            // x contraction into the (FP64) residual: res = Dx^T C0 + Bx^T C12
+            for (int i = tid; i < E * 5 * N2; i += NT) {
+                const int v = i % 5, byz = (i / 5) % N2, e = i / (5 * N2);
+                const T* C0 = Q + e * W + (v * 3) * QS + (byz / N) * NF + (byz % N) * M;
+                const T* C12 = C0 + QS;
                 T r[N];
 #pragma unroll
                 for (int bx = 0; bx < N; ++bx) r[bx] = T(0);
@@ -472,28 +492,142 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
 #pragma unroll
                     for (int bx = 0; bx < N; ++bx) r[bx] += Dt[qx * N + bx] * c0 + Bt[qx * N + bx] * c12;
                 }
-                double* res = sRes + e * ES + (v0 + vv) * VS + byz * N;
+                double* res = sRes + e * ES + v * VS + byz * N;
 #pragma unroll
                 for (int bx = 0; bx < N; ++bx) res[bx] = double(r[bx]);
             }
             __syncthreads();
-        };
-        if constexpr (PZ) {
-            // every group's pencils in one phase, then all five variables at once
-            for (int i = tid; i < E * NF * G; i += NT) {
-                const int g = i / (E * NF), r = i - g * (E * NF);
+        } else {
+            // ---- fused: z interpolation, Euler flux, contravariant transform and
+            //      first (z) divergence contraction; then y and x contractions ----
+            T* Abuf = sW + 5 * X2S;                     // [GA][3][X2S] over X1
+            T* Cbuf = Abuf + L::GA * 3 * X2S;           // [GA][2][X1S]
+            // one (x,y) pencil of element e for variable group g; the buffers hold
+            // the group's variables from slot abase (0, or its first variable with PZ)
+            auto pencil = [&](auto gc, int e, int qxy) {
+                constexpr int g = decltype(gc)::value;
+                constexpr int gv0 = group_first<P, G>(g), gnv = group_size<P, G>(g), abase = PZ ? gv0 : 0;
+                const int qx = qxy % M, qy = qxy / M;
+                T xz[5][N];
+#pragma unroll
+                for (int v = 0; v < 5; ++v)
+#pragma unroll
+                    for (int bz = 0; bz < N; ++bz) xz[v][bz] = X2[e * W + v * X2S + bz * NF + qxy];
+                const GeoDev* geo = a.geo + sCls[e];
+                const T hr = kShift ? T(a.gamma * geo->eref) : T(0);
+                const T pref = kShift ? T((a.gamma - 1.0) * geo->eref) : T(0);
+                T JD[9];
+#pragma unroll
+                for (int k = 0; k < 9; ++k) JD[k] = T(geo->JD[k]);
+                T acc[gnv][3][N];
+#pragma unroll
+                for (int v = 0; v < gnv; ++v)
+#pragma unroll
+                    for (int d = 0; d < 3; ++d)
+#pragma unroll
+                        for (int bz = 0; bz < N; ++bz) acc[v][d][bz] = T(0);
+                const T wxy = Wt[qx] * Wt[qy];
+#pragma unroll
+                for (int qz = 0; qz < M; ++qz) {
+                    T U[5];
+#pragma unroll
+                    for (int v = 0; v < 5; ++v) {
+                        T s = T(0);
+#pragma unroll
+                        for (int bz = 0; bz < N; ++bz) s += Bt[qz * N + bz] * xz[v][bz];
+                        U[v] = s;
+                    }
+                    T F[15];
+                    const T p = dgp::interior_flux_r1<T, kShift>(gamma, U, F, hr);
+                    if constexpr (g == 0) {
+                        if (!(U[0] > T(0))) status |= kStatusRho;
+                        if (!(p + pref > T(0))) status |= kStatusPressure;
+                        if (U[0] != U[0] || p != p) status |= kStatusNaN;
+                    }
+                    const T wq = wxy * Wt[qz];
+#pragma unroll
+                    for (int vv = 0; vv < gnv; ++vv) {
+                        const int v = gv0 + vv;
+#pragma unroll
+                        for (int d = 0; d < 3; ++d) {
+                            const T Gd = (F[v] * JD[d * 3 + 0] + F[5 + v] * JD[d * 3 + 1] + F[10 + v] * JD[d * 3 + 2]) * wq;
+#pragma unroll
+                            for (int bz = 0; bz < N; ++bz) acc[vv][d][bz] += (d == 2 ? Dt[qz * N + bz] : Bt[qz * N + bz]) * Gd;
+                        }
+                    }
+                }
+#pragma unroll
+                for (int vv = 0; vv < gnv; ++vv)
+#pragma unroll
+                    for (int d = 0; d < 3; ++d)
+#pragma unroll
+                        for (int bz = 0; bz < N; ++bz)
+                            Abuf[e * W + ((abase + vv) * 3 + d) * X2S + bz * NF + qxy] = acc[vv][d][bz];
+            };
+            // y and x contractions of nv buffered variables into residual variables
+            // v0 .. v0+nv-1: C0 = By^T A0, C12 = Dy^T A1 + By^T A2; res = Dx^T C0 + Bx^T C12
+            auto contract_yx = [&](int nv, int v0) {
+                for (int i = tid; i < E * nv * N * M; i += NT) {
+                    const int qx = i % M, bz = (i / M) % N, vv = (i / (M * N)) % nv, e = i / (nv * N * M);
+                    const T* A0 = Abuf + e * W + (vv * 3 + 0) * X2S + bz * NF + qx;
+                    const T* A1 = A0 + X2S;
+                    const T* A2 = A1 + X2S;
+                    T c0[N], c12[N];
+#pragma unroll
+                    for (int by = 0; by < N; ++by) { c0[by] = T(0); c12[by] = T(0); }
+#pragma unroll
+                    for (int qy = 0; qy < M; ++qy) {
+                        const T a0 = A0[qy * M], a1 = A1[qy * M], a2 = A2[qy * M];
+#pragma unroll
+                        for (int by = 0; by < N; ++by) {
+                            c0[by] += Bt[qy * N + by] * a0;
+                            c12[by] += Dt[qy * N + by] * a1 + Bt[qy * N + by] * a2;
+                        }
+                    }
+                    T* C0 = Cbuf + e * W + (vv * 2) * X1S + bz * N * M + qx;
+#pragma unroll
+                    for (int by = 0; by < N; ++by) {
+                        C0[by * M] = c0[by];
+                        C0[X1S + by * M] = c12[by];
+                    }
+                }
+                __syncthreads();
+                for (int i = tid; i < E * nv * N2; i += NT) {
+                    const int vv = i % nv, byz = (i / nv) % N2, e = i / (nv * N2);
+                    const T* C0 = Cbuf + e * W + (vv * 2) * X1S + byz * M;
+                    const T* C12 = C0 + X1S;
+                    T r[N];
+#pragma unroll
+                    for (int bx = 0; bx < N; ++bx) r[bx] = T(0);
+#pragma unroll
+                    for (int qx = 0; qx < M; ++qx) {
+                        const T c0 = C0[qx], c12 = C12[qx];
+#pragma unroll
+                        for (int bx = 0; bx < N; ++bx) r[bx] += Dt[qx * N + bx] * c0 + Bt[qx * N + bx] * c12;
+                    }
+                    double* res = sRes + e * ES + (v0 + vv) * VS + byz * N;
+#pragma unroll
+                    for (int bx = 0; bx < N; ++bx) res[bx] = double(r[bx]);
+                }
+                __syncthreads();
+            };
+            if constexpr (PZ) {
+                // every group's pencils in one phase, then all five variables at once
+                for (int i = tid; i < E * NF * G; i += NT) {
+                    const int g = i / (E * NF), r = i - g * (E * NF);
+                    static_for<0, G>([&](auto gc) {
+                        if (g == decltype(gc)::value) pencil(gc, r / NF, r % NF);
+                    });
+                }
+                __syncthreads();
+                contract_yx(5, 0);
+            } else {
                 static_for<0, G>([&](auto gc) {
-                    if (g == decltype(gc)::value) pencil(gc, r / NF, r % NF);
+                    for (int i = tid; i < E * NF; i += NT) pencil(gc, i / NF, i % NF);
+                    __syncthreads();
+                    contract_yx(group_size<P, G>(decltype(gc)::value), group_first<P, G>(decltype(gc)::value));
                 });
             }
-            __syncthreads();
-            contract_yx(5, 0);
-        } else {
-            static_for<0, G>([&](auto gc) {
-                for (int i = tid; i < E * NF; i += NT) pencil(gc, i / NF, i % NF);
-                __syncthreads();
-                contract_yx(group_size<P, G>(decltype(gc)::value), group_first<P, G>(decltype(gc)::value));
-            });
         }
 
         // ---- faces: the neighbours' slices have landed (the next batch's
@@ -505,7 +639,47 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
         // both sides, or -- when the CTA has threads to spare (high orders) --
         // one task per side
         constexpr bool kSplitSides = 2 * E * 30 <= NT;
-        if constexpr (kSplitSides) {
+        if constexpr (L::RS) {
+            // one task per (element, side, face, variable, output row t1):
+            // r = sum_b1 B[t1][b1] s[b1][.], then row t1 = sum_b0 B[t0][b0] r[b0]
+            for (int t = tid; t < E * 60 * M; t += NT) {
+                const int t1 = t % M, r0 = t / M;
+                const int v = r0 % 5, f = (r0 / 5) % 6, side = (r0 / 30) % 2, e = r0 / 60;
+                // both sides in the own element's energy frame
+                const double sh = kShift && v == 4 ? a.geo[sRec[e * 6].cls].eref : 0.0;
+                // slice entry (b0, b1) at src[b0 * s0 + b1 * s1]
+                const double* src;
+                int s0 = 1, s1 = N;
+                if (side == 0) {
+                    const int ax = face_axis(f), sidx = face_side(f) ? N - 1 : 0;
+                    src = sU + e * ES + v * VS + (ax == 0 ? sidx : (ax == 1 ? sidx * N : sidx * N2));
+                    s0 = ax == 0 ? N : 1;
+                    s1 = ax == 2 ? N : N2;
+                } else {
+                    src = sOps + e * OPS + (f * 5 + v) * NS;
+                }
+                T r[N];
+#pragma unroll
+                for (int b0 = 0; b0 < N; ++b0) r[b0] = T(0);
+#pragma unroll
+                for (int b1 = 0; b1 < N; ++b1) {
+                    const T c = Bt[t1 * N + b1];
+#pragma unroll
+                    for (int b0 = 0; b0 < N; ++b0) {
+                        const double x = src[b0 * s0 + b1 * s1];
+                        r[b0] += c * (kShift ? T(x - sh) : T(x));
+                    }
+                }
+                T* o = sW + e * W + side * 30 * FS + (f * 5 + v) * FS + t1 * M;
+#pragma unroll
+                for (int t0 = 0; t0 < M; ++t0) {
+                    T sum = T(0);
+#pragma unroll
+                    for (int b0 = 0; b0 < N; ++b0) sum += Bt[t0 * N + b0] * r[b0];
+                    o[t0] = sum;
+                }
+            }
+        } else if constexpr (kSplitSides) {
             for (int t = tid; t < E * 60; t += NT) {
                 const int v = t % 5, f = (t / 5) % 6, side = (t / 30) % 2, e = t / 60;
                 // both sides in the own element's energy frame
@@ -626,29 +800,55 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
         if (e0 + stride < a.ne) prefetch_recs<E, NT>(a.frec, a.ne, e0 + stride, sRec);
         cp_async_commit();
         // face lift per (element, face, variable) into Tn's space
-        for (int t = tid; t < E * 30; t += NT) {
-            const int v = t % 5, f = (t / 5) % 6, e = t / 30;
-            const T* Fq = sW + e * W + (f * 5 + v) * FS;
-            T tmp[M][N];
+        if constexpr (L::RS) {
+            // one task per (element, face, variable, output row b1)
+            for (int t = tid; t < E * 30 * N; t += NT) {
+                const int b1 = t % N, r0 = t / N;
+                const int v = r0 % 5, f = (r0 / 5) % 6, e = r0 / 30;
+                const T* Fq = sW + e * W + (f * 5 + v) * FS;
+                T r[M];
 #pragma unroll
-            for (int t1 = 0; t1 < M; ++t1)
+                for (int t0 = 0; t0 < M; ++t0) r[t0] = T(0);
+#pragma unroll
+                for (int t1 = 0; t1 < M; ++t1) {
+                    const T c = Bt[t1 * N + b1];
+#pragma unroll
+                    for (int t0 = 0; t0 < M; ++t0) r[t0] += c * Fq[t1 * M + t0];
+                }
+                T* Lf = sW + e * W + 30 * FS + (f * 5 + v) * FS + b1 * N;
 #pragma unroll
                 for (int b0 = 0; b0 < N; ++b0) {
-                    T s = T(0);
+                    T sum = T(0);
 #pragma unroll
-                    for (int t0 = 0; t0 < M; ++t0) s += Bt[t0 * N + b0] * Fq[t1 * M + t0];
-                    tmp[t1][b0] = s;
+                    for (int t0 = 0; t0 < M; ++t0) sum += Bt[t0 * N + b0] * r[t0];
+                    Lf[b0] = sum;
                 }
-            T* Lf = sW + e * W + 30 * FS + (f * 5 + v) * FS;
+            }
+        } else {
+            for (int t = tid; t < E * 30; t += NT) {
+                const int v = t % 5, f = (t / 5) % 6, e = t / 30;
+                const T* Fq = sW + e * W + (f * 5 + v) * FS;
+                T tmp[M][N];
 #pragma unroll
-            for (int b1 = 0; b1 < N; ++b1)
+                for (int t1 = 0; t1 < M; ++t1)
 #pragma unroll
-                for (int b0 = 0; b0 < N; ++b0) {
-                    T s = T(0);
+                    for (int b0 = 0; b0 < N; ++b0) {
+                        T s = T(0);
 #pragma unroll
-                    for (int t1 = 0; t1 < M; ++t1) s += Bt[t1 * N + b1] * tmp[t1][b0];
-                    Lf[b1 * N + b0] = s;
-                }
+                        for (int t0 = 0; t0 < M; ++t0) s += Bt[t0 * N + b0] * Fq[t1 * M + t0];
+                        tmp[t1][b0] = s;
+                    }
+                T* Lf = sW + e * W + 30 * FS + (f * 5 + v) * FS;
+#pragma unroll
+                for (int b1 = 0; b1 < N; ++b1)
+#pragma unroll
+                    for (int b0 = 0; b0 < N; ++b0) {
+                        T s = T(0);
+#pragma unroll
+                        for (int t1 = 0; t1 < M; ++t1) s += Bt[t1 * N + b1] * tmp[t1][b0];
+                        Lf[b1 * N + b0] = s;
+                    }
+            }
         }
         __syncthreads();
         // add the six face contributions to the (FP64) residual
@@ -761,7 +961,9 @@ constexpr size_t stage_smem_bytes()
 struct StageVariant {
     int E, NT, G;        // elements per CTA, threads per CTA, variable groups
     int fp32;            // 1: residual arithmetic in FP32 (mixed precision), 0: FP64
-    int flags;           // 1: groups' pencils in one phase, 2: single coefficient buffer
+    int flags;           // 1: groups' pencils in one phase, 2: single coefficient buffer,
+                         // 4: unfused volume, 8: row-split traces and lifts,
+                         // 16: one face-flux point per thread
     size_t smem;         // dynamic shared memory per CTA
     const void* func;    // the kernel, for attributes / occupancy queries
     cudaError_t (*launch)(const StageArgs&, int grid, cudaStream_t);
@@ -776,8 +978,10 @@ cudaError_t launch_stage_variant(const StageArgs& a, int grid, cudaStream_t s)
 
 // launch options FL (see Lay); one-phase groups pay off when E * (p+2)^2 * G
 // pencil tasks fill fewer rounds of NT threads than G sequential phases; the
-// single buffer trades prefetch overlap for occupancy
-constexpr int kPZ = 1, kSB = 2;
+// single buffer trades prefetch overlap for occupancy; the unfused volume, the
+// row-split traces and the single flux point trade shared-memory traffic for
+// parallel tasks and registers (high orders)
+constexpr int kPZ = 1, kSB = 2, kUF = 4, kRS = 8, kK1 = 16;
 template <int P, int E, int NT, int G, typename T = double, int FL = 0>
 constexpr StageVariant make_variant()
 {

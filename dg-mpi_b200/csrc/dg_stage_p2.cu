@@ -1,6 +1,7 @@
 // dg_stage_p2.cu -- compiled launch variants of the stage kernel for order p = 2
 // (elements per CTA, threads per CTA, variable groups, residual arithmetic; then the
-// optional flags: all groups' pencils in one phase, single coefficient buffer).  The
+// optional flags: all groups' pencils in one phase, single coefficient buffer, unfused
+// volume, row-split traces and lifts, one face-flux point per thread).  The
 // first variant of each precision is the default (the measured best); dg_tune_stage may pick another.
 #include "dg_stage.cuh"
 
@@ -11,9 +12,15 @@ static const StageVariant kVariants2[] = {
     make_variant<2, 2, 64, 1, double>(),
     make_variant<2, 1, 32, 2, double>(),
     make_variant<2, 6, 96, 1, double>(),
+    make_variant<2, 1, 32, 1, double, kUF>(),
+    make_variant<2, 1, 64, 1, double, kUF | kSB>(),
+    make_variant<2, 2, 64, 1, double, kUF | kRS | kSB>(),
     make_variant<2, 1, 32, 1, float>(),
     make_variant<2, 4, 128, 1, float>(),
     make_variant<2, 2, 64, 1, float>(),
+    make_variant<2, 1, 32, 1, float, kUF>(),
+    make_variant<2, 2, 64, 1, float, kUF | kSB>(),
+    make_variant<2, 4, 128, 1, float, kUF | kRS | kSB>(),
 };
 
 int stage_variants_p2(const StageVariant** out)

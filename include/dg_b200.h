@@ -151,7 +151,11 @@ int dg_stage_variant_info(int order, int variant, int* elems_per_cta, int* threa
                           int* precision);
 /* Options of a variant: bit 0 -- the variable groups' pencil tasks run in one
  * phase; bit 1 -- one coefficient buffer, refilled with the next batch once
- * the face traces have read it (more resident CTAs, less prefetch overlap). */
+ * the face traces have read it (more resident CTAs, less prefetch overlap);
+ * bit 2 -- unfused volume (z interpolation, pointwise flux and contractions as
+ * separate passes over all quadrature points; the groups count is unused);
+ * bit 3 -- traces and lifts split into one task per output row; bit 4 -- one
+ * face-flux point per thread and iteration (fewer registers). */
 int dg_stage_variant_flags(int order, int variant, int* flags);
 int dg_set_stage_variant(dg_ctx* ctx, int variant);
 int dg_get_stage_variant(const dg_ctx* ctx);

@@ -202,18 +202,20 @@ def test_time_step_change_rebuilds_graph():
     assert rel_l2(gpu.get_state(), U_orc).max() < 1e-12
 
 
+@pytest.mark.parametrize("flux", ["LaxFriedrichs", "HLLC"])
 @pytest.mark.parametrize("p", [0, 1, 2, 3, 4, 5])
-def test_every_stage_variant_matches_oracle(p):
+def test_every_stage_variant_matches_oracle(p, flux):
     """Every compiled launch variant (elements and threads per CTA, variable
-    groups, one-phase groups, single coefficient buffer) -- the tuner may pick
-    any of them: FP64 variants against the oracle at 1e-12 after 3 RK4 steps,
-    mixed-precision variants against the FP64 result at 1e-6."""
+    groups and the launch options: one-phase groups, single coefficient
+    buffer, unfused volume, row-split traces, one flux point per thread) --
+    the tuner may pick any of them: FP64 variants against the oracle at 1e-12
+    after 3 RK4 steps, mixed-precision variants against the FP64 result at 1e-6."""
     mesh = dg_b200.periodic_box((3, 2, 3), (0.0, 0.0, 0.0), (10.0, 10.0, 10.0), rotate_seed=7)
-    orc = pyoracle.OracleCase.from_mesh(mesh, p, gas_constant=1.0)
+    orc = pyoracle.OracleCase.from_mesh(mesh, p, flux=flux, gas_constant=1.0)
     U = orc.project_ic("IsentropicVortexXY", VORTEX_XY)
     ref = None
     for precision in ("fp64", "mixed_fp32"):
-        case = dg_b200.Case(mesh, p, gas_constant=1.0, precision=precision)
+        case = dg_b200.Case(mesh, p, flux=flux, gas_constant=1.0, precision=precision)
         dt = case.cfl_time_step(U, 0.1)
         if ref is None:
             ref = orc.rk4(U, dt, 3)
