@@ -266,7 +266,7 @@ __device__ __forceinline__ void interp2d(const T* __restrict__ Bt, const T (&s)[
 }
 
 template <int P, int E, int NT, int G, typename T, int FL>
-__global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
+__device__ __forceinline__ void stage_body(const StageArgs& a)
 {
     using L = Lay<P, G, T, FL>;
     constexpr bool PZ = L::PZ, SB = L::SB;
@@ -314,21 +314,27 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
         cp_async_wait_all();
         __syncthreads();
         // stream in the neighbours' boundary slices (the periodic face gather)
-        // for the face phase, then the next batch's coefficients
-        for (int t = tid; t < E * 30; t += NT) {
-            const int fv = t % 30, e = t / 30, v = fv % 5, f = fv / 5;
+        // for the face phase, then the next batch's coefficients; one task per
+        // (element, face, variable), or per slice row when the CTA has threads
+        // to spare
+        constexpr int kSliceRows = NT > E * 30 ? N : 1;
+        for (int t = tid; t < E * 30 * kSliceRows; t += NT) {
+            const int row = t % kSliceRows, fv = (t / kSliceRows) % 30, e = t / (30 * kSliceRows);
+            const int v = fv % 5, f = fv / 5;
             const FaceRec& rec = sRec[e * 6 + f];
             const int2 c = make_int2(rec.nbr, rec.info);
             const double* src = a.Us + ((size_t)c.x * 5 + v) * NB;
             double* dst = sOps + e * OPS + fv * NS;
 #pragma unroll
-            for (int b1 = 0; b1 < N; ++b1)
+            for (int r = 0; r < N / kSliceRows; ++r) {
+                const int b1 = row + r;
 #pragma unroll
                 for (int b0 = 0; b0 < N; ++b0) cp_async8(dst + b1 * N + b0, src + slice_index<N>(c.y & 7, b0, b1));
-            // this face's row of the face-point permutation, shared out over the five variable tasks
+            }
+            // this face's row of the face-point permutation, shared out over the face's tasks
             const int fm = e * 6 + f, code = c.y >> 4;
-            for (int q = v; q < NF; q += 5) sCm[fm * NF + q] = a.cmap[code * NF + q];
-            if (fv == 0) sCls[e] = rec.cls;
+            for (int q = v * kSliceRows + row; q < NF; q += 5 * kSliceRows) sCm[fm * NF + q] = a.cmap[code * NF + q];
+            if (fv == 0 && row == 0) sCls[e] = rec.cls;
         }
         cp_async_commit();
         if (!SB && e0 + stride < a.ne)
@@ -949,6 +955,19 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
     if (status) atomicOr(a.status, status);
 }
 
+template <int P, int E, int NT, int G, typename T, int FL>
+__global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
+{
+    stage_body<P, E, NT, G, T, FL>(a);
+}
+// the same with at least MB resident CTAs per SM asked of the compiler (it then
+// keeps the registers within 64K / (NT * MB) per thread)
+template <int P, int E, int NT, int G, typename T, int FL, int MB>
+__global__ void __launch_bounds__(NT, MB) stage_kernel_mb(StageArgs a)
+{
+    stage_body<P, E, NT, G, T, FL>(a);
+}
+
 template <int P, int E, int G, typename T, int FL = 0>
 constexpr size_t stage_smem_bytes()
 {
@@ -963,16 +982,20 @@ struct StageVariant {
     int fp32;            // 1: residual arithmetic in FP32 (mixed precision), 0: FP64
     int flags;           // 1: groups' pencils in one phase, 2: single coefficient buffer,
                          // 4: unfused volume, 8: row-split traces and lifts,
-                         // 16: one face-flux point per thread
+                         // 16: one face-flux point per thread;
+                         // bits 8..11: minimum resident CTAs asked of the compiler (0: none)
     size_t smem;         // dynamic shared memory per CTA
     const void* func;    // the kernel, for attributes / occupancy queries
     cudaError_t (*launch)(const StageArgs&, int grid, cudaStream_t);
 };
 
-template <int P, int E, int NT, int G, typename T, int FL>
+template <int P, int E, int NT, int G, typename T, int FL, int MB>
 cudaError_t launch_stage_variant(const StageArgs& a, int grid, cudaStream_t s)
 {
-    stage_kernel<P, E, NT, G, T, FL><<<grid, NT, stage_smem_bytes<P, E, G, T, FL>(), s>>>(a);
+    if constexpr (MB > 0)
+        stage_kernel_mb<P, E, NT, G, T, FL, MB><<<grid, NT, stage_smem_bytes<P, E, G, T, FL>(), s>>>(a);
+    else
+        stage_kernel<P, E, NT, G, T, FL><<<grid, NT, stage_smem_bytes<P, E, G, T, FL>(), s>>>(a);
     return cudaGetLastError();
 }
 
@@ -982,12 +1005,17 @@ cudaError_t launch_stage_variant(const StageArgs& a, int grid, cudaStream_t s)
 // row-split traces and the single flux point trade shared-memory traffic for
 // parallel tasks and registers (high orders)
 constexpr int kPZ = 1, kSB = 2, kUF = 4, kRS = 8, kK1 = 16;
-template <int P, int E, int NT, int G, typename T = double, int FL = 0>
-constexpr StageVariant make_variant()
+// MB > 0: at least MB resident CTAs per SM asked of the compiler (a register cap)
+template <int P, int E, int NT, int G, typename T = double, int FL = 0, int MB = 0>
+StageVariant make_variant()
 {
     static_assert(stage_smem_bytes<P, E, G, T, FL>() <= 227 * 1024, "stage kernel shared memory exceeds 227 KB");
-    return StageVariant{E, NT, G, sizeof(T) == 4 ? 1 : 0, FL, stage_smem_bytes<P, E, G, T, FL>(),
-                        (const void*)stage_kernel<P, E, NT, G, T, FL>, launch_stage_variant<P, E, NT, G, T, FL>};
+    static_assert(MB >= 0 && MB < 16, "minimum resident CTAs out of range");
+    const void* func;
+    if constexpr (MB > 0) func = (const void*)stage_kernel_mb<P, E, NT, G, T, FL, MB>;
+    else func = (const void*)stage_kernel<P, E, NT, G, T, FL>;
+    return StageVariant{E, NT, G, sizeof(T) == 4 ? 1 : 0, FL | (MB << 8), stage_smem_bytes<P, E, G, T, FL>(),
+                        func, launch_stage_variant<P, E, NT, G, T, FL, MB>};
 }
 
 // the variants compiled for order p (defined in dg_stage_p<p>.cu)

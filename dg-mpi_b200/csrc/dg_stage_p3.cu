@@ -1,27 +1,28 @@
 // dg_stage_p3.cu -- compiled launch variants of the stage kernel for order p = 3
 // (elements per CTA, threads per CTA, variable groups, residual arithmetic; then the
 // optional flags: all groups' pencils in one phase, single coefficient buffer, unfused
-// volume, row-split traces and lifts, one face-flux point per thread).  The
+// volume, row-split traces and lifts, one face-flux point per thread; then the minimum of
+// resident CTAs per SM asked of the compiler).  The
 // first variant of each precision is the default (the measured best); dg_tune_stage may pick another.
 #include "dg_stage.cuh"
 
 namespace dgk {
 
 static const StageVariant kVariants3[] = {
+    make_variant<3, 1, 64, 1, double, kUF | kRS | kSB | kK1>(),
     make_variant<3, 1, 64, 1, double, kUF | kRS | kSB>(),
     make_variant<3, 1, 32, 2, double, kSB>(),
+    make_variant<3, 1, 96, 1, double, kUF | kRS | kSB | kK1>(),
+    make_variant<3, 1, 96, 1, double, kUF | kRS | kSB>(),
     make_variant<3, 1, 32, 1, double, kUF | kSB>(),
     make_variant<3, 2, 64, 2, double>(),
-    make_variant<3, 1, 96, 1, double, kUF | kRS | kSB>(),
-    make_variant<3, 1, 64, 1, double, kUF | kRS | kSB | kK1>(),
     make_variant<3, 1, 32, 2, double>(),
-    make_variant<3, 1, 32, 1, double>(),
+    make_variant<3, 1, 32, 1, float, kUF | kSB>(),
     make_variant<3, 1, 64, 1, float, kUF | kSB>(),
     make_variant<3, 2, 64, 1, float, kUF | kSB>(),
-    make_variant<3, 1, 32, 1, float, kSB>(),
-    make_variant<3, 1, 32, 1, float, kUF | kSB>(),
     make_variant<3, 2, 64, 2, float, kSB>(),
     make_variant<3, 1, 64, 1, float, kUF | kRS | kSB>(),
+    make_variant<3, 1, 32, 1, float, kSB>(),
     make_variant<3, 1, 32, 1, float>(),
 };
 

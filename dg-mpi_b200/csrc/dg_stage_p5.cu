@@ -1,13 +1,15 @@
 // dg_stage_p5.cu -- compiled launch variants of the stage kernel for order p = 5
 // (elements per CTA, threads per CTA, variable groups, residual arithmetic; then the
 // optional flags: all groups' pencils in one phase, single coefficient buffer, unfused
-// volume, row-split traces and lifts, one face-flux point per thread).  The
+// volume, row-split traces and lifts, one face-flux point per thread; then the minimum of
+// resident CTAs per SM asked of the compiler).  The
 // first variant of each precision is the default (the measured best); dg_tune_stage may pick another.
 #include "dg_stage.cuh"
 
 namespace dgk {
 
 static const StageVariant kVariants5[] = {
+    make_variant<5, 1, 256, 1, double, kUF | kRS | kSB | kK1, 2>(),
     make_variant<5, 1, 128, 1, double, kUF | kRS | kSB | kK1>(),
     make_variant<5, 1, 128, 1, double, kUF | kRS | kSB>(),
     make_variant<5, 1, 256, 1, double, kUF | kRS | kSB | kK1>(),
@@ -15,10 +17,11 @@ static const StageVariant kVariants5[] = {
     make_variant<5, 1, 128, 3, double, kRS>(),
     make_variant<5, 1, 128, 3, double>(),
     make_variant<5, 1, 128, 1, float, kUF | kRS | kSB | kK1>(),
-    make_variant<5, 1, 128, 1, float, kUF | kRS | kSB>(),
-    make_variant<5, 1, 128, 1, float, kUF | kSB>(),
     make_variant<5, 1, 256, 1, float, kUF | kRS | kSB>(),
+    make_variant<5, 1, 256, 1, float, kUF | kRS | kSB | kK1, 3>(),
+    make_variant<5, 1, 128, 1, float, kUF | kRS | kSB>(),
     make_variant<5, 1, 128, 2, float, kSB>(),
+    make_variant<5, 1, 128, 1, float, kUF | kSB>(),
     make_variant<5, 1, 64, 2, float>(),
 };
 

@@ -155,7 +155,8 @@ int dg_stage_variant_info(int order, int variant, int* elems_per_cta, int* threa
  * bit 2 -- unfused volume (z interpolation, pointwise flux and contractions as
  * separate passes over all quadrature points; the groups count is unused);
  * bit 3 -- traces and lifts split into one task per output row; bit 4 -- one
- * face-flux point per thread and iteration (fewer registers). */
+ * face-flux point per thread and iteration (fewer registers); bits 8..11 -- the minimum of resident CTAs per SM the kernel was compiled
+ * for (0: none; a register cap). */
 int dg_stage_variant_flags(int order, int variant, int* flags);
 int dg_set_stage_variant(dg_ctx* ctx, int variant);
 int dg_get_stage_variant(const dg_ctx* ctx);
