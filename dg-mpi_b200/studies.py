@@ -5,6 +5,8 @@
   python dg-mpi_b200/studies.py taylor_green # 96^3, p=4, Taylor-Green, 200 RK4 steps
   python dg-mpi_b200/studies.py ensemble     # 256 seeded vortex cases, p=1..5, 8^3..32^3, 100 steps
   python dg-mpi_b200/studies.py <name> --scale 0.25  # smaller mesh (fewer cases), same orders
+  python dg-mpi_b200/studies.py stage --nel 40 --order 3 --precision fp64 --variant 0
+                                             # one launch variant, 2 RK4 steps, no tuner (ncu captures)
 
 Each study runs the FP64 path and the mixed-precision path (FP32 residual,
 FP64 state) from the same projected initial condition and prints one JSON line:
@@ -153,13 +155,36 @@ def ensemble(scale: float, steps: int = 100, cfl: float = 0.1):
     return out
 
 
+def stage(nel: int, order: int, precision_: str, variant: int, steps: int):
+    """x-y vortex on an nel^3 box, one fixed stage-kernel launch variant (no tuner, so the
+    launch sequence is known: the projection, then four stage launches per step)."""
+    mesh = dg_b200.periodic_box((nel, nel, nel), (0.0, 0.0, 0.0), (10.0, 10.0, 10.0))
+    case = dg_b200.Case(mesh, order, gas_constant=1.0, precision=precision_)
+    U0 = case.project_ic("IsentropicVortexXY", VORTEX)
+    dt = case.cfl_time_step(U0, 0.1)
+    case.stage_variant = variant
+    case.rk4(dt, steps)
+    out = {"nel": nel, "order": order, "stage_variant": case.stage_variants()[variant], "steps": steps,
+           "status": case.status()}
+    case.close()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("study", choices=["precision", "taylor_green", "ensemble"])
+    ap.add_argument("study", choices=["precision", "taylor_green", "ensemble", "stage"])
     ap.add_argument("--scale", type=float, default=1.0)
+    ap.add_argument("--nel", type=int, default=40, help="stage: elements per direction")
+    ap.add_argument("--order", type=int, default=3, help="stage: polynomial order")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed_fp32"], help="stage: residual arithmetic")
+    ap.add_argument("--variant", type=int, default=0, help="stage: launch variant index")
+    ap.add_argument("--steps", type=int, default=2, help="stage: RK4 steps")
     args = ap.parse_args()
-    run = {"precision": precision, "taylor_green": taylor_green, "ensemble": ensemble}[args.study]
-    res = run(args.scale)
+    if args.study == "stage":
+        res = stage(args.nel, args.order, args.precision, args.variant, args.steps)
+    else:
+        run = {"precision": precision, "taylor_green": taylor_green, "ensemble": ensemble}[args.study]
+        res = run(args.scale)
     res["study"] = args.study
     print(json.dumps(res), flush=True)
 
