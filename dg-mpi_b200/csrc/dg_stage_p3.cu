@@ -10,19 +10,22 @@ namespace dgk {
 
 static const StageVariant kVariants3[] = {
     make_variant<3, 1, 64, 1, double, kUF | kRS | kSB | kK1>(),
+    make_variant<3, 1, 64, 1, double, kUF | kSB | kK1>(),
     make_variant<3, 1, 64, 1, double, kUF | kRS | kSB>(),
-    make_variant<3, 1, 32, 2, double, kSB>(),
     make_variant<3, 1, 96, 1, double, kUF | kRS | kSB | kK1>(),
-    make_variant<3, 1, 96, 1, double, kUF | kRS | kSB>(),
+    make_variant<3, 1, 32, 2, double, kSB>(),
     make_variant<3, 1, 32, 1, double, kUF | kSB>(),
+    make_variant<3, 1, 96, 1, double, kUF | kRS | kSB>(),
     make_variant<3, 2, 64, 2, double>(),
     make_variant<3, 1, 32, 2, double>(),
+    make_variant<3, 1, 32, 1, float, kUF | kSB | kK1>(),
     make_variant<3, 1, 32, 1, float, kUF | kSB>(),
+    make_variant<3, 2, 64, 1, float, kUF | kSB | kK1>(),
     make_variant<3, 1, 64, 1, float, kUF | kSB>(),
     make_variant<3, 2, 64, 1, float, kUF | kSB>(),
     make_variant<3, 2, 64, 2, float, kSB>(),
-    make_variant<3, 1, 64, 1, float, kUF | kRS | kSB>(),
     make_variant<3, 1, 32, 1, float, kSB>(),
+    make_variant<3, 1, 64, 1, float, kUF | kRS | kSB>(),
     make_variant<3, 1, 32, 1, float>(),
 };
 
