@@ -212,6 +212,8 @@ int dg_batch_create(int ncases, const dg_case_desc* cases, const dg_mesh_desc* m
         } catch (const std::exception& ex) {
             perr = std::string("mesh preparation failed: ") + ex.what();
         }
+        if (perr.empty() && pm.general)
+            perr = "unsupported: non-affine elements (general geometry runs in single-case contexts)";
         if (!perr.empty())
             return bfail(nullptr, perr.rfind("unsupported:", 0) == 0 ? DG_ERR_UNSUPPORTED : DG_ERR_ARG, tag + perr);
     }

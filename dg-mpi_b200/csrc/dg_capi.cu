@@ -99,7 +99,8 @@ bool variant_matches(const dg_ctx* c, int v)
 {
     const dgk::StageVariant* vs = nullptr;
     const int nv = dgk::stage_variants(c->p, &vs);
-    return v >= 0 && v < nv && (vs[v].fp32 != 0) == (c->precision == DG_PREC_MIXED_FP32);
+    return v >= 0 && v < nv && (vs[v].fp32 != 0) == (c->precision == DG_PREC_MIXED_FP32) &&
+           ((vs[v].flags & dgk::kGE) != 0) == c->pm.general;
 }
 
 // Sets the variant's shared-memory attribute and its persistent grid size
@@ -136,6 +137,10 @@ int launch_stage(dg_ctx* c, int mode, const double* Us, const double* U0, double
     a.geo_class = c->d_geo_class;
     a.geo = c->d_geo;
     a.cmap = c->d_cmap;
+    a.gjd = c->d_gjd;
+    a.gnrm = c->d_gnrm;
+    a.gimm = c->d_gimm;
+    a.gfsd = c->d_gfsd;
     a.status = c->d_status;
     a.e_begin = e_begin;
     a.ne = e_end;
@@ -215,12 +220,40 @@ __global__ void halo_unpack_kernel(double* __restrict__ U, const int2* __restric
 // reductions: one CTA per element (grid-stride), threads over points; per-CTA
 // partial sums land in a scratch array that the host adds in a fixed order.
 
+// Position and det J at reference point xi of a trilinear element with nodes
+// X [8][3] (the geometric basis of basis/tools.cpp:42-66; the same operations
+// as the host's dgh::trilinear_jacobian).
+__device__ void trilinear_point(const double* __restrict__ X, const double* xi, double* x, double* djac)
+{
+    double jac[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    x[0] = x[1] = x[2] = 0.0;
+    for (int n = 0; n < 8; ++n) {
+        double phi = 1.0, dphi[3];
+        for (int j = 0; j < 3; ++j) {
+            double g = 1.0;
+            for (int a = 0; a < 3; ++a) {
+                const double s = ((n >> a) & 1) ? 1.0 : -1.0;
+                g *= a == j ? 0.5 * s : 0.5 * (1.0 + s * xi[a]);
+            }
+            dphi[j] = g;
+            phi *= 0.5 * (1.0 + (((n >> j) & 1) ? 1.0 : -1.0) * xi[j]);
+        }
+        for (int i = 0; i < 3; ++i) {
+            x[i] += phi * X[n * 3 + i];
+            for (int j = 0; j < 3; ++j) jac[i * 3 + j] += X[n * 3 + i] * dphi[j];
+        }
+    }
+    *djac = jac[0] * jac[4] * jac[8] - jac[0] * jac[5] * jac[7] - jac[1] * jac[3] * jac[8] + jac[1] * jac[5] * jac[6] +
+            jac[2] * jac[3] * jac[7] - jac[2] * jac[4] * jac[6];
+}
+
 struct ReduceArgs {
     const double* U;        // device state [ne][5][nb]
     const int* geo_class;
     const GeoDev* geo;
     const double* X0;       // [ne][3]
     const double* J;        // [nclasses][9]
+    const double* gnodes;   // general geometry: element nodes [ne][8][3] (else null)
     double* partials;       // [gridDim.x][5]
     int ne, ic_type, kind;  // kind 0: L2 error, 1: kinetic energy
     double gamma, R, t;
@@ -263,12 +296,18 @@ __global__ void __launch_bounds__(256) reduce_kernel(ReduceArgs a)
                 }
                 Uq[v] = sz;
             }
-            const double w = (Wq[i] * Wq[j]) * Wq[k] * djac;
-            if (a.kind == 0) {
+            double x[3], dj = djac;
+            if (a.gnodes) {
+                const double xr[3] = {Xq[i], Xq[j], Xq[k]};
+                trilinear_point(a.gnodes + (size_t)e * 24, xr, x, &dj);
+            } else {
                 const double xi[3] = {Xq[i] + 1.0, Xq[j] + 1.0, Xq[k] + 1.0};
-                double x[3], Ue[5];
                 for (int d = 0; d < 3; ++d)
                     x[d] = a.X0[(size_t)e * 3 + d] + J[d * 3 + 0] * xi[0] + J[d * 3 + 1] * xi[1] + J[d * 3 + 2] * xi[2];
+            }
+            const double w = (Wq[i] * Wq[j]) * Wq[k] * dj;
+            if (a.kind == 0) {
+                double Ue[5];
                 dgp::initial_state(a.ic_type, a.data, a.gamma, a.R, x, a.t, Ue);
 #pragma unroll
                 for (int v = 0; v < 5; ++v) {
@@ -300,6 +339,7 @@ int run_reduce(dg_ctx* c, int kind, int ic_type, const double* data, int ndata, 
     a.geo_class = c->d_geo_class + e0;
     a.geo = c->d_geo;
     a.X0 = c->d_X0 + static_cast<size_t>(e0) * 3;
+    a.gnodes = c->pm.general ? c->d_gnodes + static_cast<size_t>(e0) * 24 : nullptr;
     a.partials = c->d_partials;
     a.ne = ne;
     a.ic_type = ic_type;
@@ -343,6 +383,10 @@ struct ProjectArgs {
     const GeoDev* geo;
     const double* X0;       // [ne][3]
     const double* J;        // [nclasses][9]
+    // general geometry (else null): element nodes [ne][8][3] and the inverse
+    // mass matrices, transposed [ne][nb][nb]
+    const double* gnodes;
+    const double* gimm;
     int e_begin, e_end, ic_type;
     double gamma, R, t;
     double data[16];
@@ -378,12 +422,17 @@ __global__ void __launch_bounds__(256) project_kernel(ProjectArgs a)
         __syncthreads();
         for (int q = threadIdx.x; q < Q; q += blockDim.x) {
             const int i = q % ME, j = (q / ME) % ME, k = q / (ME * ME);
-            const double xi[3] = {Xe[i] + 1.0, Xe[j] + 1.0, Xe[k] + 1.0};
-            double x[3], U[5];
-            for (int d = 0; d < 3; ++d)
-                x[d] = a.X0[(size_t)e * 3 + d] + J[d * 3 + 0] * xi[0] + J[d * 3 + 1] * xi[1] + J[d * 3 + 2] * xi[2];
+            double x[3], U[5], dj = djac;
+            if (a.gnodes) {
+                const double xr[3] = {Xe[i], Xe[j], Xe[k]};
+                trilinear_point(a.gnodes + (size_t)e * 24, xr, x, &dj);
+            } else {
+                const double xi[3] = {Xe[i] + 1.0, Xe[j] + 1.0, Xe[k] + 1.0};
+                for (int d = 0; d < 3; ++d)
+                    x[d] = a.X0[(size_t)e * 3 + d] + J[d * 3 + 0] * xi[0] + J[d * 3 + 1] * xi[1] + J[d * 3 + 2] * xi[2];
+            }
             dgp::initial_state(a.ic_type, a.data, a.gamma, a.R, x, a.t, U);
-            const double cw = (We[i] * We[j]) * We[k] * djac;
+            const double cw = (We[i] * We[j]) * We[k] * dj;
 #pragma unroll
             for (int v = 0; v < 5; ++v) f[v * Q + q] = U[v] * cw;
         }
@@ -409,6 +458,16 @@ __global__ void __launch_bounds__(256) project_kernel(ProjectArgs a)
             r[o] = acc;
         }
         __syncthreads();
+        if (a.gimm) {  // the element's dense inverse mass matrix
+            for (int o = threadIdx.x; o < 5 * NB; o += blockDim.x) {
+                const int j = o % NB, v = o / NB;
+                const double* im = a.gimm + (size_t)e * NB * NB + j;
+                double acc = 0.0;
+                for (int k = 0; k < NB; ++k) acc += im[(size_t)k * NB] * r[v * NB + k];
+                a.U[(size_t)e * 5 * NB + o] = acc;
+            }
+            continue;
+        }
         for (int o = threadIdx.x; o < 5 * NB; o += blockDim.x) {  // Minv along x, into t2
             const int bx = o % N, row = o / N;
             double acc = 0.0;
@@ -456,6 +515,8 @@ int project_ic_device(dg_ctx* c, int ic_type, const double* data, int ndata, dou
     a.geo = c->d_geo;
     a.X0 = c->d_X0;
     a.J = reinterpret_cast<const double*>(c->d_geo + c->pm.classes.size());
+    a.gnodes = c->pm.general ? c->d_gnodes : nullptr;
+    a.gimm = c->pm.general ? c->d_gimm : nullptr;
     a.e_begin = e0;
     a.e_end = e0 + ne;
     a.ic_type = ic_type;
@@ -652,6 +713,37 @@ int upload_geometry(dg_ctx* c, cudaStream_t s)
     return DG_OK;
 }
 
+// The FP64 residual of the uniform state (1, 0, 0, 0, 1/(gamma-1)) -- at rest,
+// unit pressure -- into d_gfsd, with the first FP64 general-geometry variant
+// (see dgk::StageArgs::gfsd); d_U0 is left zeroed.
+int unit_pressure_residual(dg_ctx* c)
+{
+    const int nv = dg_num_stage_variants(c->p);
+    const dgk::StageVariant* vs = nullptr;
+    dgk::stage_variants(c->p, &vs);
+    int v64 = -1;
+    for (int v = 0; v < nv && v64 < 0; ++v)
+        if (!vs[v].fp32 && (vs[v].flags & dgk::kGE)) v64 = v;
+    if (v64 < 0) return fail(c, DG_ERR_UNSUPPORTED, "no FP64 general-geometry stage kernel for this order");
+    const size_t nstate = static_cast<size_t>(c->ne) * c->nb * 5;
+    std::vector<double> U(nstate, 0.0);
+    for (size_t e = 0; e < static_cast<size_t>(c->ne); ++e)
+        for (int b = 0; b < c->nb; ++b) {
+            U[(e * 5 + 0) * c->nb + b] = 1.0;
+            U[(e * 5 + 4) * c->nb + b] = 1.0 / (c->gamma - 1.0);
+        }
+    DG_CUDA(c, cudaMemcpy(c->d_U0, U.data(), nstate * sizeof(double), cudaMemcpyHostToDevice));
+    const int keep = c->variant;
+    c->variant = v64;
+    int rc = launch_stage(c, dgk::kModeResidual, c->d_U0, c->d_U0, c->d_gfsd, 0.0);
+    c->variant = keep;
+    if (rc) return rc;
+    if ((rc = check_status(c)) != DG_OK) return rc;
+    DG_CUDA(c, cudaMemsetAsync(c->d_U0, 0, nstate * sizeof(double), c->stream));
+    DG_CUDA(c, cudaStreamSynchronize(c->stream));
+    return DG_OK;
+}
+
 void release(dg_ctx* c)
 {
     if (!c) return;
@@ -661,6 +753,7 @@ void release(dg_ctx* c)
     cudaFree(c->d_U0); cudaFree(c->d_Ua); cudaFree(c->d_Ub); cudaFree(c->d_acc); cudaFree(c->d_out);
     cudaFree(c->d_conn); cudaFree(c->d_frec); cudaFree(c->d_geo_class); cudaFree(c->d_geo); cudaFree(c->d_cmap);
     cudaFree(c->d_X0); cudaFree(c->d_partials); cudaFree(c->d_status);
+    cudaFree(c->d_gjd); cudaFree(c->d_gnrm); cudaFree(c->d_gimm); cudaFree(c->d_gnodes); cudaFree(c->d_gfsd);
     cudaFree(c->d_halo_send); cudaFree(c->d_halo_recv);
     if (c->stream) cudaStreamDestroy(c->stream);
 }
@@ -724,6 +817,8 @@ int dgi::create_ctx(const dg_case_desc* cd, const dg_mesh_desc* md, const int* e
     } catch (const std::exception& ex) {
         perr = std::string("mesh preparation failed: ") + ex.what();
     }
+    if (perr.empty() && part && c->pm.general)
+        perr = "unsupported: non-affine elements in a partitioned context (general geometry runs unpartitioned)";
     if (perr.empty() && part) {
         // the interior elements must not read a ghost: they run while the exchange is in flight
         for (int e = 0; e < part->ninterior && perr.empty(); ++e)
@@ -750,16 +845,54 @@ int dgi::create_ctx(const dg_case_desc* cd, const dg_mesh_desc* md, const int* e
     for (size_t i = 0; i < c->tab.B.size(); ++i) c->stage_tab.Bf[i] = static_cast<float>(c->tab.B[i]);
     for (size_t i = 0; i < c->tab.D.size(); ++i) c->stage_tab.Df[i] = static_cast<float>(c->tab.D[i]);
     for (size_t i = 0; i < c->tab.wq.size(); ++i) c->stage_tab.Wf[i] = static_cast<float>(c->tab.wq[i]);
-    {   // default launch variant: the first one compiled for the requested precision
-        const dgk::StageVariant* vs = nullptr;
-        const int nv = dgk::stage_variants(c->p, &vs);
+    {   // default launch variant: the first one compiled for the requested precision and geometry kind
+        const int nv = dg_num_stage_variants(c->p);
         c->variant = -1;
         for (int v = 0; v < nv && c->variant < 0; ++v)
-            if ((vs[v].fp32 != 0) == (c->precision == DG_PREC_MIXED_FP32)) c->variant = v;
+            if (variant_matches(c, v)) c->variant = v;
         if (c->variant < 0) {
             delete c;
-            return fail(nullptr, DG_ERR_UNSUPPORTED, "no stage kernel compiled for this order and precision");
+            return fail(nullptr, DG_ERR_UNSUPPORTED, "no stage kernel compiled for this order, precision and geometry");
         }
+    }
+    // general geometry: the dense inverse mass matrix of every element (host,
+    // once; nb^2 doubles per element) and the flux's normal data per face point
+    std::vector<double> gimm, gnrm;
+    if (c->pm.general) {
+        const int nb = c->nb, nf = (c->p + 2) * (c->p + 2);
+        gimm.resize(static_cast<size_t>(c->ne) * nb * nb);
+        int singular = -1;
+#pragma omp parallel for schedule(dynamic, 16)
+        for (int e = 0; e < c->ne; ++e)
+            if (!dgh::general_inverse_mass(c->tab, &c->pm.gnodes[static_cast<size_t>(e) * 24],
+                                           &gimm[static_cast<size_t>(e) * nb * nb])) {
+#pragma omp critical
+                singular = e;
+            }
+        if (singular >= 0) {
+            delete c;
+            return fail(nullptr, DG_ERR_ARG, "element " + std::to_string(singular) + " has a singular mass matrix");
+        }
+        // per face point: n (N/|N| for Lax-Friedrichs, N * (1/|N|) for HLLC, as
+        // in FaceRec), then |N| -- base/functions.cpp:40-49, euler/functions.cpp:309-311
+        gnrm.resize(static_cast<size_t>(c->ne) * 6 * 4 * nf);
+        for (size_t ef = 0; ef < static_cast<size_t>(c->ne) * 6; ++ef)
+            for (int q = 0; q < nf; ++q) {
+                const double* N = &c->pm.gN[ef * 3 * nf + q];
+                const double N0 = N[0], N1 = N[nf], N2 = N[2 * nf];
+                const double nm = std::sqrt(N0 * N0 + N1 * N1 + N2 * N2), inv = 1. / nm;
+                double* o = &gnrm[ef * 4 * nf + q];
+                if (c->flux == DG_FLUX_HLLC) {
+                    o[0] = N0 * inv;
+                    o[nf] = N1 * inv;
+                    o[2 * nf] = N2 * inv;
+                } else {
+                    o[0] = N0 / nm;
+                    o[nf] = N1 / nm;
+                    o[2 * nf] = N2 / nm;
+                }
+                o[3 * nf] = nm;
+            }
     }
 
     // the mesh is valid; now the device
@@ -811,6 +944,11 @@ int dgi::create_ctx(const dg_case_desc* cd, const dg_mesh_desc* md, const int* e
         {(void**)&c->d_halo_recv, std::max<size_t>(1, c->nslices) * sizeof(int2)},
         {(void**)&c->d_partials, static_cast<size_t>(c->red_grid) * 5 * sizeof(double)},
         {(void**)&c->d_status, sizeof(unsigned)},
+        {(void**)&c->d_gjd, std::max<size_t>(1, c->pm.gjd.size()) * sizeof(double)},
+        {(void**)&c->d_gnrm, std::max<size_t>(1, gnrm.size()) * sizeof(double)},
+        {(void**)&c->d_gimm, std::max<size_t>(1, gimm.size()) * sizeof(double)},
+        {(void**)&c->d_gnodes, std::max<size_t>(1, c->pm.gnodes.size()) * sizeof(double)},
+        {(void**)&c->d_gfsd, (c->pm.general && c->precision == DG_PREC_MIXED_FP32 ? nstate : 1) * sizeof(double)},
     };
     for (auto& al : allocs) {
         if (cudaMalloc(al.p, al.bytes) != cudaSuccess) {
@@ -851,6 +989,11 @@ int dgi::create_ctx(const dg_case_desc* cd, const dg_mesh_desc* md, const int* e
               cudaMemcpy(c->d_halo_recv, hr.data(), hr.size() * sizeof(int2), cudaMemcpyHostToDevice) == cudaSuccess &&
               cudaMemcpy(c->d_X0, c->pm.X0.data(), c->pm.X0.size() * sizeof(double), cudaMemcpyHostToDevice) == cudaSuccess &&
               (c->pm.cmap.empty() || cudaMemcpy(c->d_cmap, c->pm.cmap.data(), c->pm.cmap.size(), cudaMemcpyHostToDevice) == cudaSuccess) &&
+              (!c->pm.general ||
+               (cudaMemcpy(c->d_gjd, c->pm.gjd.data(), c->pm.gjd.size() * sizeof(double), cudaMemcpyHostToDevice) == cudaSuccess &&
+                cudaMemcpy(c->d_gnrm, gnrm.data(), gnrm.size() * sizeof(double), cudaMemcpyHostToDevice) == cudaSuccess &&
+                cudaMemcpy(c->d_gimm, gimm.data(), gimm.size() * sizeof(double), cudaMemcpyHostToDevice) == cudaSuccess &&
+                cudaMemcpy(c->d_gnodes, c->pm.gnodes.data(), c->pm.gnodes.size() * sizeof(double), cudaMemcpyHostToDevice) == cudaSuccess)) &&
               cudaMemset(c->d_status, 0, sizeof(unsigned)) == cudaSuccess &&
               cudaMemset(c->d_U0, 0, nstate * sizeof(double)) == cudaSuccess &&
               cudaMemset(c->d_acc, 0, nstate * sizeof(double)) == cudaSuccess;
@@ -861,6 +1004,7 @@ int dgi::create_ctx(const dg_case_desc* cd, const dg_mesh_desc* md, const int* e
     c->class_dtf.assign(ncls, 1.0);
     c->class_eref.assign(ncls, 0.0);
     if ((rc = upload_geometry(c, c->stream)) != DG_OK) return bail(rc);
+    if (c->pm.general && c->precision == DG_PREC_MIXED_FP32 && (rc = unit_pressure_residual(c)) != DG_OK) return bail(rc);
     *out = c;
     return DG_OK;
 }
@@ -1161,7 +1305,8 @@ int dg_set_stage_variant(dg_ctx* c, int v)
 {
     if (!c) return DG_ERR_ARG;
     if (v < 0 || v >= dg_num_stage_variants(c->p)) return fail(c, DG_ERR_ARG, "stage variant index out of range");
-    if (!variant_matches(c, v)) return fail(c, DG_ERR_ARG, "stage variant has the other residual precision");
+    if (!variant_matches(c, v))
+        return fail(c, DG_ERR_ARG, "stage variant has the other residual precision or geometry kind");
     if (v != c->variant) {
         c->variant = v;
         if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }

@@ -34,6 +34,10 @@ struct dg_ctx {
     dgk::GeoDev* d_geo = nullptr;
     uint8_t* d_cmap = nullptr;
     double* d_X0 = nullptr;
+    // general (trilinear) geometry (pm.general): the stage kernel's per-point
+    // tables (see dgk::StageArgs) and the element nodes [ne][8][3]
+    double *d_gjd = nullptr, *d_gnrm = nullptr, *d_gimm = nullptr, *d_gnodes = nullptr;
+    double* d_gfsd = nullptr;  // FP32 residual on general geometry: see dgk::StageArgs::gfsd
     double* d_partials = nullptr;
     unsigned* d_status = nullptr;
     int red_grid = 0;

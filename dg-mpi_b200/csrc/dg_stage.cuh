@@ -112,6 +112,20 @@ struct StageArgs {
     const int* geo_class;   // [ne]
     const GeoDev* geo;      // [nclasses]
     const uint8_t* cmap;    // [ncodes][m*m]
+    // general (trilinear) geometry, launch option GE: per element ijac * djac
+    // at the volume points [ne][9][(p+2)^3], the face normal data at the own
+    // face points [ne][6][4][(p+2)^2] (n as for FaceRec, then |N|), and the
+    // inverse mass matrix transposed [ne][nb][nb]
+    const double* gjd;
+    const double* gnrm;
+    const double* gimm;
+    // GE with the FP32 residual: the residual of a uniform state at rest with
+    // unit pressure [ne][5][nb] (FP64).  The FP32 residual leaves the constant
+    // pressure (gamma-1) E_ref out of the momentum fluxes; on affine meshes its
+    // volume and face terms cancel, on general meshes the reference's face
+    // normals (taken at reference face 0's points) leave a remainder, linear
+    // in the pressure, that this table restores.
+    const double* gfsd;
     unsigned* status;
     int e_begin, ne;        // the launch computes elements [e_begin, ne)
     int flux;               // 0 = Lax-Friedrichs, 1 = HLLC
@@ -134,10 +148,14 @@ __host__ __device__ constexpr int cmax(int a, int b) { return a > b ? a : b; }
 // over a point array holding all quadrature points (the flux is evaluated once
 // per point instead of once per variable group; G is unused); flag 8 (RS) --
 // traces and lifts as one task per output row instead of per face slice;
-// flag 16 (K1) -- one face-flux point per thread and iteration (registers)
+// flag 16 (K1) -- one face-flux point per thread and iteration (registers);
+// flag 32 (GE) -- general (trilinear) geometry: per-point metric terms and
+// normals and a dense per-element inverse mass matrix, read from global
+// memory (requires UF)
 template <int P, int G, typename T = double, int FL = 0>
 struct Lay {
-    static constexpr bool PZ = FL & 1, SB = FL & 2, UF = FL & 4, RS = FL & 8, K1 = FL & 16;
+    static constexpr bool PZ = FL & 1, SB = FL & 2, UF = FL & 4, RS = FL & 8, K1 = FL & 16, GE = FL & 32;
+    static_assert(!GE || UF, "general geometry needs the unfused volume");
     static constexpr int N = P + 1, M = P + 2, NB = N * N * N, NF = M * M, N2 = N * N;
     static constexpr int GV = G == 1 ? 5 : (G == 2 ? 3 : 2);  // variables per group (max)
     static constexpr int GA = PZ ? 5 : GV;       // variables of the z-contraction buffers
@@ -422,8 +440,14 @@ __device__ __forceinline__ void stage_body(const StageArgs& a)
                 if (!(p + pref > T(0))) status |= kStatusPressure;
                 if (U[0] != U[0] || p != p) status |= kStatusNaN;
                 T JD[9];
+                if constexpr (L::GE) {
+                    const double* gj = a.gjd + (size_t)min(e0 + e, a.ne - 1) * 9 * NQ + q;
 #pragma unroll
-                for (int k = 0; k < 9; ++k) JD[k] = T(geo->JD[k]);
+                    for (int k = 0; k < 9; ++k) JD[k] = T(gj[(size_t)k * NQ]);
+                } else {
+#pragma unroll
+                    for (int k = 0; k < 9; ++k) JD[k] = T(geo->JD[k]);
+                }
                 const T wq = Wt[qx] * Wt[qy] * Wt[qz];
 #pragma unroll
                 for (int v = 0; v < 5; ++v)
@@ -756,10 +780,22 @@ __device__ __forceinline__ void stage_body(const StageArgs& a)
                     UR[v] = isL ? un : uo;
                 }
                 // the left element's normal data, staged with the neighbour slices
-                const T nmag = T(rec.nmag);
+                // the left element's normal data: per face, or per face point (GE)
+                T nd[4];
+                if constexpr (L::GE) {
+                    const double* gn = a.gnrm + ((size_t)min(e0 + e, a.ne - 1) * 6 + f) * 4 * NF + cidx;
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) nd[k] = T(gn[k * NF]);
+                } else {
+                    nd[0] = T(rec.n[0]);
+                    nd[1] = T(rec.n[1]);
+                    nd[2] = T(rec.n[2]);
+                    nd[3] = T(rec.nmag);
+                }
+                const T nmag = nd[3];
                 const double eref = kShift ? a.geo[sRec[e * 6].cls].eref : 0.0;
                 if (a.flux == 1) {
-                    const T nu[3] = {T(rec.n[0]), T(rec.n[1]), T(rec.n[2])};
+                    const T nu[3] = {nd[0], nd[1], nd[2]};
                     if (kShift) {  // HLLC takes the full energy
                         UL[4] += T(eref);
                         UR[4] += T(eref);
@@ -771,7 +807,7 @@ __device__ __forceinline__ void stage_body(const StageArgs& a)
                         for (int d = 0; d < 3; ++d) Fo[1 + d] -= pn * nu[d];
                     }
                 } else {
-                    const T nh[3] = {T(rec.n[0]), T(rec.n[1]), T(rec.n[2])};
+                    const T nh[3] = {nd[0], nd[1], nd[2]};
                     dgp::flux_lax_friedrichs_fast<T, kShift>(gamma, UL, UR, nh, nmag, Fo, T(a.gamma * eref),
                                                              T((a.gamma - 1.0) * eref));
                 }
@@ -863,6 +899,10 @@ __device__ __forceinline__ void stage_body(const StageArgs& a)
             const int bc[3] = {b % N, (b / N) % N, b / N2};
             const T* Lf = sW + e * W + 30 * FS + v * FS;
             double s = 0.0;
+            if constexpr (L::GE && kShift) {
+                if (v >= 1 && v <= 3)
+                    s = (a.gamma - 1.0) * a.geo[sCls[e]].eref * a.gfsd[(size_t)min(e0 + e, a.ne - 1) * 5 * NB + v * NB + b];
+            }
 #pragma unroll
             for (int f = 0; f < 6; ++f) {
                 const int ax = face_axis(f), sidx = face_side(f) ? N - 1 : 0;
@@ -884,69 +924,108 @@ __device__ __forceinline__ void stage_body(const StageArgs& a)
             continue;
         }
 
-        // ---- inverse mass (FP64): x and y passes in place, z pass fused with the update ----
-        for (int i = tid; i < E * 5 * N2; i += NT) {
-            const int v = i % 5, byz = (i / 5) % N2, e = i / (5 * N2);
-            double* r = sRes + e * ES + v * VS + byz * N;  // pencil along x
-            double t[N];
+        if constexpr (L::GE) {
+            // ---- dense inverse mass (FP64, the element's own matrix) fused with
+            //      the update: one task per (element, basis function), the five
+            //      variables together; the matrix streams from global memory ----
+            cp_async_wait_all();  // this batch's U0 / accumulator have landed
+            __syncthreads();
+            for (int i = tid; i < E * NB; i += NT) {
+                const int j = i % NB, e = i / NB;
+                if (e0 + e >= a.ne) continue;
+                const int ge = e0 + e;
+                const double* im = a.gimm + (size_t)ge * NB * NB + j;  // iMM[j][k] at im[k * NB]
+                const double* r = sRes + e * ES;
+                double s[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll 4
+                for (int k = 0; k < NB; ++k) {
+                    const double mk = im[(size_t)k * NB];
 #pragma unroll
-            for (int k = 0; k < N; ++k) t[k] = r[k];
+                    for (int v = 0; v < 5; ++v) s[v] += mk * r[v * VS + k];
+                }
+                const double scale = a.dt * a.geo[sCls[e]].dtf;
 #pragma unroll
-            for (int j = 0; j < N; ++j) {
-                double s = 0.0;
-#pragma unroll
-                for (int k = 0; k < N; ++k) s += Mi[j * N + k] * t[k];
-                r[j] = s;
+                for (int v = 0; v < 5; ++v) {
+                    const double kk = scale * s[v];
+                    const size_t gi = (size_t)ge * 5 * NB + (size_t)v * NB + j;
+                    // step-start state: the prefetched U0, or the stage state itself in RK1 / FE
+                    const double u0 = stage_u0 ? sOps[e * OPS + v * VS + j] : sU[e * ES + v * VS + j];
+                    const double ac = sOps[e * OPS + ES + v * VS + j];
+                    switch (a.mode) {
+                        case kModeMassInv: a.out[gi] = kk; break;
+                        case kModeRK1: a.acc[gi] = kk; a.out[gi] = 0.5 * kk + u0; break;
+                        case kModeRK2: a.acc[gi] = ac + 2.0 * kk; a.out[gi] = 0.5 * kk + u0; break;
+                        case kModeRK3: a.acc[gi] = ac + 2.0 * kk; a.out[gi] = 1.0 * kk + u0; break;
+                        case kModeRK4: a.out[gi] = u0 + (1.0 / 6.0) * (ac + kk); break;
+                        default: a.out[gi] = u0 + 1.0 * kk; break;
+                    }
+                }
             }
-        }
-        __syncthreads();
-        for (int i = tid; i < E * 5 * N2; i += NT) {
-            // (element, variable) fastest: consecutive threads are VS apart (odd)
-            const int ev = i % (5 * E), bxz = i / (5 * E), bx = bxz % N, bz = bxz / N;
-            double* r = sRes + (ev / 5) * ES + (ev % 5) * VS + bz * N2 + bx;  // pencil along y
-            double t[N];
+        } else {
+            // ---- inverse mass (FP64): x and y passes in place, z pass fused with the update ----
+            for (int i = tid; i < E * 5 * N2; i += NT) {
+                const int v = i % 5, byz = (i / 5) % N2, e = i / (5 * N2);
+                double* r = sRes + e * ES + v * VS + byz * N;  // pencil along x
+                double t[N];
 #pragma unroll
-            for (int k = 0; k < N; ++k) t[k] = r[k * N];
+                for (int k = 0; k < N; ++k) t[k] = r[k];
 #pragma unroll
-            for (int j = 0; j < N; ++j) {
-                double s = 0.0;
+                for (int j = 0; j < N; ++j) {
+                    double s = 0.0;
 #pragma unroll
-                for (int k = 0; k < N; ++k) s += Mi[j * N + k] * t[k];
-                r[j * N] = s;
+                    for (int k = 0; k < N; ++k) s += Mi[j * N + k] * t[k];
+                    r[j] = s;
+                }
             }
-        }
-        cp_async_wait_all();  // this batch's U0 / accumulator have landed
-        __syncthreads();
-        for (int i = tid; i < E * 5 * N2; i += NT) {
-            const int bxy = i % N2, ev = i / N2, e = ev / 5;
-            if (e0 + e >= a.ne) continue;
-            const int ge = e0 + e;
-            const GeoDev& gg = a.geo[sCls[e]];
-            const double scale = a.dt * gg.dtf * gg.inv_djac;
-            const int v = ev % 5;
-            const double* r = sRes + e * ES + v * VS + bxy;  // pencil along z
-            // step-start state: the prefetched U0, or the stage state itself in
-            // RK1 / FE where the two coincide
-            const double* u0 = (stage_u0 ? sOps + e * OPS : sU + e * ES) + v * VS + bxy;
-            const double* ac = sOps + e * OPS + ES + v * VS + bxy;
-            double t[N];
+            __syncthreads();
+            for (int i = tid; i < E * 5 * N2; i += NT) {
+                // (element, variable) fastest: consecutive threads are VS apart (odd)
+                const int ev = i % (5 * E), bxz = i / (5 * E), bx = bxz % N, bz = bxz / N;
+                double* r = sRes + (ev / 5) * ES + (ev % 5) * VS + bz * N2 + bx;  // pencil along y
+                double t[N];
 #pragma unroll
-            for (int k = 0; k < N; ++k) t[k] = r[k * N2];
-            const size_t gbase = (size_t)e0 * 5 * NB + (size_t)ev * NB + bxy;
+                for (int k = 0; k < N; ++k) t[k] = r[k * N];
 #pragma unroll
-            for (int j = 0; j < N; ++j) {
-                double s = 0.0;
+                for (int j = 0; j < N; ++j) {
+                    double s = 0.0;
 #pragma unroll
-                for (int k = 0; k < N; ++k) s += Mi[j * N + k] * t[k];
-                const double kk = scale * s;
-                const size_t gi = gbase + (size_t)j * N2;
-                switch (a.mode) {
-                    case kModeMassInv: a.out[gi] = kk; break;
-                    case kModeRK1: a.acc[gi] = kk; a.out[gi] = 0.5 * kk + u0[j * N2]; break;
-                    case kModeRK2: a.acc[gi] = ac[j * N2] + 2.0 * kk; a.out[gi] = 0.5 * kk + u0[j * N2]; break;
-                    case kModeRK3: a.acc[gi] = ac[j * N2] + 2.0 * kk; a.out[gi] = 1.0 * kk + u0[j * N2]; break;
-                    case kModeRK4: a.out[gi] = u0[j * N2] + (1.0 / 6.0) * (ac[j * N2] + kk); break;
-                    default: a.out[gi] = u0[j * N2] + 1.0 * kk; break;
+                    for (int k = 0; k < N; ++k) s += Mi[j * N + k] * t[k];
+                    r[j * N] = s;
+                }
+            }
+            cp_async_wait_all();  // this batch's U0 / accumulator have landed
+            __syncthreads();
+            for (int i = tid; i < E * 5 * N2; i += NT) {
+                const int bxy = i % N2, ev = i / N2, e = ev / 5;
+                if (e0 + e >= a.ne) continue;
+                const int ge = e0 + e;
+                const GeoDev& gg = a.geo[sCls[e]];
+                const double scale = a.dt * gg.dtf * gg.inv_djac;
+                const int v = ev % 5;
+                const double* r = sRes + e * ES + v * VS + bxy;  // pencil along z
+                // step-start state: the prefetched U0, or the stage state itself in
+                // RK1 / FE where the two coincide
+                const double* u0 = (stage_u0 ? sOps + e * OPS : sU + e * ES) + v * VS + bxy;
+                const double* ac = sOps + e * OPS + ES + v * VS + bxy;
+                double t[N];
+#pragma unroll
+                for (int k = 0; k < N; ++k) t[k] = r[k * N2];
+                const size_t gbase = (size_t)e0 * 5 * NB + (size_t)ev * NB + bxy;
+#pragma unroll
+                for (int j = 0; j < N; ++j) {
+                    double s = 0.0;
+#pragma unroll
+                    for (int k = 0; k < N; ++k) s += Mi[j * N + k] * t[k];
+                    const double kk = scale * s;
+                    const size_t gi = gbase + (size_t)j * N2;
+                    switch (a.mode) {
+                        case kModeMassInv: a.out[gi] = kk; break;
+                        case kModeRK1: a.acc[gi] = kk; a.out[gi] = 0.5 * kk + u0[j * N2]; break;
+                        case kModeRK2: a.acc[gi] = ac[j * N2] + 2.0 * kk; a.out[gi] = 0.5 * kk + u0[j * N2]; break;
+                        case kModeRK3: a.acc[gi] = ac[j * N2] + 2.0 * kk; a.out[gi] = 1.0 * kk + u0[j * N2]; break;
+                        case kModeRK4: a.out[gi] = u0[j * N2] + (1.0 / 6.0) * (ac[j * N2] + kk); break;
+                        default: a.out[gi] = u0[j * N2] + 1.0 * kk; break;
+                    }
                 }
             }
         }
@@ -982,7 +1061,7 @@ struct StageVariant {
     int fp32;            // 1: residual arithmetic in FP32 (mixed precision), 0: FP64
     int flags;           // 1: groups' pencils in one phase, 2: single coefficient buffer,
                          // 4: unfused volume, 8: row-split traces and lifts,
-                         // 16: one face-flux point per thread;
+                         // 16: one face-flux point per thread, 32: general (trilinear) geometry;
                          // bits 8..11: minimum resident CTAs asked of the compiler (0: none)
     size_t smem;         // dynamic shared memory per CTA
     const void* func;    // the kernel, for attributes / occupancy queries
@@ -1003,8 +1082,10 @@ cudaError_t launch_stage_variant(const StageArgs& a, int grid, cudaStream_t s)
 // pencil tasks fill fewer rounds of NT threads than G sequential phases; the
 // single buffer trades prefetch overlap for occupancy; the unfused volume, the
 // row-split traces and the single flux point trade shared-memory traffic for
-// parallel tasks and registers (high orders)
-constexpr int kPZ = 1, kSB = 2, kUF = 4, kRS = 8, kK1 = 16;
+// parallel tasks and registers (high orders); general geometry is a property
+// of the mesh, not a tuning choice: contexts on non-affine meshes run GE
+// variants only, the others never do
+constexpr int kPZ = 1, kSB = 2, kUF = 4, kRS = 8, kK1 = 16, kGE = 32;
 // MB > 0: at least MB resident CTAs per SM asked of the compiler (a register cap)
 template <int P, int E, int NT, int G, typename T = double, int FL = 0, int MB = 0>
 StageVariant make_variant()

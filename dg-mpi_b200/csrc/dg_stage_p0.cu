@@ -2,7 +2,8 @@
 // (elements per CTA, threads per CTA, variable groups, residual arithmetic; then the
 // optional flags: all groups' pencils in one phase, single coefficient buffer, unfused
 // volume, row-split traces and lifts, one face-flux point per thread; then the minimum of
-// resident CTAs per SM asked of the compiler).  The
+// resident CTAs per SM asked of the compiler).  Contexts on non-affine meshes use the
+// general-geometry (kGE) entries only, the others never do.  The
 // first variant of each precision is the default (the measured best); dg_tune_stage may pick another.
 #include "dg_stage.cuh"
 
@@ -14,6 +15,9 @@ static const StageVariant kVariants0[] = {
     make_variant<0, 16, 64, 1, double>(),
     make_variant<0, 32, 128, 1, float>(),
     make_variant<0, 16, 64, 1, float>(),
+    // general (trilinear) geometry: the variants of non-affine meshes
+    make_variant<0, 4, 32, 1, double, kUF | kGE>(),
+    make_variant<0, 4, 32, 1, float, kUF | kGE>(),
 };
 
 int stage_variants_p0(const StageVariant** out)

@@ -2,7 +2,8 @@
 // (elements per CTA, threads per CTA, variable groups, residual arithmetic; then the
 // optional flags: all groups' pencils in one phase, single coefficient buffer, unfused
 // volume, row-split traces and lifts, one face-flux point per thread; then the minimum of
-// resident CTAs per SM asked of the compiler).  The
+// resident CTAs per SM asked of the compiler).  Contexts on non-affine meshes use the
+// general-geometry (kGE) entries only, the others never do.  The
 // first variant of each precision is the default (the measured best); dg_tune_stage may pick another.
 #include "dg_stage.cuh"
 
@@ -27,6 +28,9 @@ static const StageVariant kVariants3[] = {
     make_variant<3, 1, 32, 1, float, kSB>(),
     make_variant<3, 1, 64, 1, float, kUF | kRS | kSB>(),
     make_variant<3, 1, 32, 1, float>(),
+    // general (trilinear) geometry: the variants of non-affine meshes
+    make_variant<3, 1, 64, 1, double, kUF | kRS | kSB | kK1 | kGE>(),
+    make_variant<3, 1, 32, 1, float, kUF | kSB | kK1 | kGE>(),
 };
 
 int stage_variants_p3(const StageVariant** out)

@@ -102,8 +102,12 @@ double range_volume(const PreparedMesh& pm, int e_begin, int e_end)
 
 double range_hmin(const PreparedMesh& pm, int e_begin, int e_end)
 {
-    std::vector<char> seen(pm.classes.size(), 0);
     double h = 1e300;
+    if (pm.general) {
+        for (int e = e_begin; e < e_end; ++e) h = std::fmin(h, pm.elem_h[e]);
+        return h;
+    }
+    std::vector<char> seen(pm.classes.size(), 0);
     for (int e = e_begin; e < e_end; ++e) {
         const int k = pm.geo_class[e];
         if (seen[k]) continue;

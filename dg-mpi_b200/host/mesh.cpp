@@ -1,6 +1,7 @@
 // mesh.cpp -- see mesh.h.
 #include "mesh.h"
 
+#include <algorithm>
 #include <array>
 #include <cmath>
 #include <map>
@@ -176,6 +177,133 @@ BoxMesh make_periodic_box(const int n[3], const double x0[3], const double len[3
     return b;
 }
 
+// General geometry, volume part: node coordinates, ijac * djac at the volume
+// GL points (BasisTools::get_element_jacobian, basis/tools.cpp:42-66, with the
+// closed-form Math::det / Math::invA, linear_algebra.cpp:108-122, 243-259),
+// element volumes on that rule (MeshTools::get_element_volume,
+// mesh/tools.cpp:28-36) and shortest edges; one placeholder affine class.
+static std::string prepare_general_volume(const MeshView& mv, int m, PreparedMesh& out)
+{
+    const int ne = mv.nelem, nq = m * m * m;
+    std::vector<double> x, w;
+    gauss_legendre(m, x, w);
+    out.gnodes.resize(static_cast<size_t>(ne) * 24);
+    out.gjd.resize(static_cast<size_t>(ne) * 9 * nq);
+    out.elem_h.resize(ne);
+    std::vector<double> vol(ne, 0.0);
+    int bad = -1;
+#pragma omp parallel for schedule(static)
+    for (int e = 0; e < ne; ++e) {
+        double* X = &out.gnodes[static_cast<size_t>(e) * 24];
+        for (int l = 0; l < 8; ++l)
+            for (int a = 0; a < 3; ++a)
+                X[l * 3 + a] = mv.coords[static_cast<size_t>(mv.e2n[static_cast<size_t>(e) * 8 + l]) * 3 + a];
+        double v = 0.0;
+        for (int q = 0; q < nq; ++q) {
+            const int qx = q % m, qy = (q / m) % m, qz = q / (m * m);
+            const double xi[3] = {x[qx], x[qy], x[qz]};
+            double M[9];
+            trilinear_jacobian(X, xi, M);
+            const double det = det3(M);
+            if (!(det > 0.0)) {
+#pragma omp critical
+                bad = bad < 0 ? e : std::min(bad, e);
+                break;
+            }
+            double inv[9];
+            inv[0] = (M[4] * M[8] - M[5] * M[7]) / det;
+            inv[3] = -(M[3] * M[8] - M[5] * M[6]) / det;
+            inv[6] = (M[3] * M[7] - M[4] * M[6]) / det;
+            inv[1] = -(M[1] * M[8] - M[2] * M[7]) / det;
+            inv[4] = (M[0] * M[8] - M[2] * M[6]) / det;
+            inv[7] = -(M[0] * M[7] - M[1] * M[6]) / det;
+            inv[2] = (M[1] * M[5] - M[2] * M[4]) / det;
+            inv[5] = -(M[0] * M[5] - M[2] * M[3]) / det;
+            inv[8] = (M[0] * M[4] - M[1] * M[3]) / det;
+            for (int k = 0; k < 9; ++k) out.gjd[(static_cast<size_t>(e) * 9 + k) * nq + q] = inv[k] * det;
+            v += w[qx] * w[qy] * w[qz] * det;
+        }
+        vol[e] = v;
+        double h = 1e300;
+        for (int l = 0; l < 8; ++l)
+            for (int a = 0; a < 3; ++a)
+                if (!((l >> a) & 1)) {
+                    const int l2 = l | (1 << a);
+                    double d2 = 0.0;
+                    for (int c = 0; c < 3; ++c) d2 += (X[l2 * 3 + c] - X[l * 3 + c]) * (X[l2 * 3 + c] - X[l * 3 + c]);
+                    h = std::fmin(h, std::sqrt(d2));
+                }
+        out.elem_h[e] = h;
+    }
+    if (bad >= 0) return "element " + std::to_string(bad) + " has a non-positive Jacobian";
+    out.volume = 0.0;
+    out.hmin = 1e300;
+    for (int e = 0; e < out.nowned; ++e) {
+        out.volume += vol[e];
+        out.hmin = std::fmin(out.hmin, out.elem_h[e]);
+    }
+    GeoClass g{};
+    for (int i = 0; i < 3; ++i) g.J[i * 4] = g.JD[i * 4] = 1.0;
+    g.djac = g.inv_djac = 1.0;
+    for (int f = 0; f < 6; ++f) {
+        g.nmag[f] = 1.0;
+        g.N[f][face_axis(f)] = g.nhat[f][face_axis(f)] = g.nunit[f][face_axis(f)] = 1.0;
+    }
+    out.classes.assign(1, g);
+    out.geo_class.assign(ne, 0);
+    return "";
+}
+
+// General geometry, face part: the reference's face normals (precompute_normals,
+// helpers.cpp:380-500 with shape.cpp:482-532): at face-loop point q the cross
+// product of the tangents of the left element's bilinear face map (nodes in
+// get_local_nodes_on_face_hexahedron order) at the first two coordinates of
+// reference face 0's q-th point; each owned side stores it at its own
+// canonical point of loop index q.
+static void general_face_normals(const MeshView& mv, int m, const std::vector<int>* canon_inv,
+                                 const std::vector<int>* order_inv, PreparedMesh& out)
+{
+    const int nf = m * m, nowned = out.nowned;
+    std::vector<double> x, w;
+    gauss_legendre(m, x, w);
+    out.gN.assign(static_cast<size_t>(nowned) * 6 * 3 * nf, 0.0);
+    std::vector<double> Nq(static_cast<size_t>(nf) * 3);
+    for (int i = 0; i < mv.nface; ++i) {
+        const unsigned* r = &mv.faces[static_cast<size_t>(i) * 8];
+        const int eL = r[1], fL = r[2], oL = r[3], eR = r[5], fR = r[6], oR = r[7];
+        if (eL >= nowned && eR >= nowned) continue;
+        const auto nd = face_geometry_nodes(fL);
+        const double* X = &out.gnodes[static_cast<size_t>(eL) * 24];
+        for (int q = 0; q < nf; ++q) {
+            // face 0's point q = j*m + i is (x[j], x[i], -1) in the reference cube
+            const double s = x[q / m], t = x[q % m];
+            double a[3] = {0.0, 0.0, 0.0}, b[3] = {0.0, 0.0, 0.0};
+            for (int k = 0; k < 4; ++k) {
+                const int ii = k & 1, jj = k >> 1;
+                const double vs = ii ? 0.5 * (1.0 + s) : 0.5 * (1.0 - s), gs = ii ? 0.5 : -0.5;
+                const double vt = jj ? 0.5 * (1.0 + t) : 0.5 * (1.0 - t), gt = jj ? 0.5 : -0.5;
+                for (int d = 0; d < 3; ++d) {
+                    a[d] += X[nd[k] * 3 + d] * (gs * vt);
+                    b[d] += X[nd[k] * 3 + d] * (vs * gt);
+                }
+            }
+            Nq[q * 3 + 0] = a[1] * b[2] - a[2] * b[1];
+            Nq[q * 3 + 1] = a[2] * b[0] - a[0] * b[2];
+            Nq[q * 3 + 2] = a[0] * b[1] - a[1] * b[0];
+        }
+        const int side_e[2] = {eL, eR}, side_f[2] = {fL, fR}, side_o[2] = {oL, oR};
+        for (int sd = 0; sd < 2; ++sd) {
+            const int e = side_e[sd], f = side_f[sd], o = side_o[sd];
+            if (e >= nowned) continue;
+            for (int c = 0; c < nf; ++c) {
+                const int q = order_inv[o][canon_inv[f][c]];
+                for (int d = 0; d < 3; ++d)
+                    out.gN[((static_cast<size_t>(e) * 6 + f) * 3 + d) * nf + c] = Nq[static_cast<size_t>(q) * 3 + d];
+            }
+        }
+    }
+}
+
 std::string prepare_mesh(const MeshView& mv, int m, PreparedMesh& out)
 {
     if (mv.nelem <= 0) return "mesh has no elements";
@@ -192,6 +320,7 @@ std::string prepare_mesh(const MeshView& mv, int m, PreparedMesh& out)
     std::vector<double> Jall(static_cast<size_t>(ne) * 9);
     out.X0.resize(static_cast<size_t>(ne) * 3);
     double hs = 0.0;
+    bool nonaffine = false;
     for (int e = 0; e < ne; ++e) {
         double X[24];
         for (int l = 0; l < 8; ++l) {
@@ -212,85 +341,90 @@ std::string prepare_mesh(const MeshView& mv, int m, PreparedMesh& out)
             for (int i = 0; i < 3; ++i) {
                 double v = X[i];
                 for (int a = 0; a < 3; ++a) v += J[i * 3 + a] * (corner_sign(l, a) + 1);
-                if (std::fabs(v - X[l * 3 + i]) > 1e-9 * scale)
-                    return "unsupported: element " + std::to_string(e) + " is not affine";
+                if (std::fabs(v - X[l * 3 + i]) > 1e-9 * scale) nonaffine = true;
             }
         for (int a = 0; a < 3; ++a) out.X0[static_cast<size_t>(e) * 3 + a] = X[a];
     }
-    std::map<std::array<long long, 10>, int> class_of;
-    out.geo_class.resize(ne);
-    out.hmin = 1e300;
-    for (int e = 0; e < ne; ++e) {
-        const double* J = &Jall[static_cast<size_t>(e) * 9];
-        std::array<long long, 10> key{};
-        for (int i = 0; i < 9; ++i) key[i] = std::llround(J[i] / hs * 68719476736.0);  // 2^36
-        key[9] = mv.tag ? mv.tag[e] : 0;
-        auto it = class_of.find(key);
-        if (it != class_of.end()) {
-            out.geo_class[e] = it->second;
-            continue;
-        }
-        GeoClass g{};
-        for (int i = 0; i < 9; ++i) g.J[i] = J[i];
-        // Math::det / Math::invA closed forms (src/math/linear_algebra.cpp:108-122, 243-259)
-        const double* M = J;
-        const double det = M[0] * M[4] * M[8] - M[0] * M[5] * M[7] - M[1] * M[3] * M[8] +
-                           M[1] * M[5] * M[6] + M[2] * M[3] * M[7] - M[2] * M[4] * M[6];
-        if (!(det > 0.0)) return "element " + std::to_string(e) + " has a non-positive Jacobian";
-        double inv[9];
-        inv[0] = (M[4] * M[8] - M[5] * M[7]) / det;
-        inv[3] = -(M[3] * M[8] - M[5] * M[6]) / det;
-        inv[6] = (M[3] * M[7] - M[4] * M[6]) / det;
-        inv[1] = -(M[1] * M[8] - M[2] * M[7]) / det;
-        inv[4] = (M[0] * M[8] - M[2] * M[6]) / det;
-        inv[7] = -(M[0] * M[7] - M[1] * M[6]) / det;
-        inv[2] = (M[1] * M[5] - M[2] * M[4]) / det;
-        inv[5] = -(M[0] * M[5] - M[2] * M[3]) / det;
-        inv[8] = (M[0] * M[4] - M[1] * M[3]) / det;
-        for (int i = 0; i < 9; ++i) g.JD[i] = inv[i] * det;
-        g.djac = det;
-        g.inv_djac = 1.0 / det;
-        // face normals: cross product of the face map's tangent vectors built
-        // from the face's geometry nodes (shape.cpp:482-532; sign +1 = outward
-        // from the owning element, helpers.cpp:440-446)
-        for (int f = 0; f < 6; ++f) {
-            const auto nd = face_geometry_nodes(f);
-            double t1[3], t2[3];
-            for (int i = 0; i < 3; ++i) {
-                t1[i] = 0.0;
-                t2[i] = 0.0;
-                for (int a = 0; a < 3; ++a) {
-                    t1[i] += J[i * 3 + a] * 0.5 * (corner_sign(nd[1], a) - corner_sign(nd[0], a));
-                    t2[i] += J[i * 3 + a] * 0.5 * (corner_sign(nd[2], a) - corner_sign(nd[0], a));
+    out.general = nonaffine;
+    std::string gerr = out.general ? prepare_general_volume(mv, m, out) : std::string();
+    if (!gerr.empty()) return gerr;
+    if (!out.general) {
+        std::map<std::array<long long, 10>, int> class_of;
+        out.geo_class.resize(ne);
+        out.hmin = 1e300;
+        for (int e = 0; e < ne; ++e) {
+            const double* J = &Jall[static_cast<size_t>(e) * 9];
+            std::array<long long, 10> key{};
+            for (int i = 0; i < 9; ++i) key[i] = std::llround(J[i] / hs * 68719476736.0);  // 2^36
+            key[9] = mv.tag ? mv.tag[e] : 0;
+            auto it = class_of.find(key);
+            if (it != class_of.end()) {
+                out.geo_class[e] = it->second;
+                continue;
+            }
+            GeoClass g{};
+            for (int i = 0; i < 9; ++i) g.J[i] = J[i];
+            // Math::det / Math::invA closed forms (src/math/linear_algebra.cpp:108-122, 243-259)
+            const double* M = J;
+            const double det = M[0] * M[4] * M[8] - M[0] * M[5] * M[7] - M[1] * M[3] * M[8] +
+                               M[1] * M[5] * M[6] + M[2] * M[3] * M[7] - M[2] * M[4] * M[6];
+            if (!(det > 0.0)) return "element " + std::to_string(e) + " has a non-positive Jacobian";
+            double inv[9];
+            inv[0] = (M[4] * M[8] - M[5] * M[7]) / det;
+            inv[3] = -(M[3] * M[8] - M[5] * M[6]) / det;
+            inv[6] = (M[3] * M[7] - M[4] * M[6]) / det;
+            inv[1] = -(M[1] * M[8] - M[2] * M[7]) / det;
+            inv[4] = (M[0] * M[8] - M[2] * M[6]) / det;
+            inv[7] = -(M[0] * M[7] - M[1] * M[6]) / det;
+            inv[2] = (M[1] * M[5] - M[2] * M[4]) / det;
+            inv[5] = -(M[0] * M[5] - M[2] * M[3]) / det;
+            inv[8] = (M[0] * M[4] - M[1] * M[3]) / det;
+            for (int i = 0; i < 9; ++i) g.JD[i] = inv[i] * det;
+            g.djac = det;
+            g.inv_djac = 1.0 / det;
+            // face normals: cross product of the face map's tangent vectors built
+            // from the face's geometry nodes (shape.cpp:482-532; sign +1 = outward
+            // from the owning element, helpers.cpp:440-446)
+            for (int f = 0; f < 6; ++f) {
+                const auto nd = face_geometry_nodes(f);
+                double t1[3], t2[3];
+                for (int i = 0; i < 3; ++i) {
+                    t1[i] = 0.0;
+                    t2[i] = 0.0;
+                    for (int a = 0; a < 3; ++a) {
+                        t1[i] += J[i * 3 + a] * 0.5 * (corner_sign(nd[1], a) - corner_sign(nd[0], a));
+                        t2[i] += J[i * 3 + a] * 0.5 * (corner_sign(nd[2], a) - corner_sign(nd[0], a));
+                    }
+                }
+                g.N[f][0] = t1[1] * t2[2] - t1[2] * t2[1];
+                g.N[f][1] = t1[2] * t2[0] - t1[0] * t2[2];
+                g.N[f][2] = t1[0] * t2[1] - t1[1] * t2[0];
+                double nm = 0.0;
+                for (int d = 0; d < 3; ++d) nm += g.N[f][d] * g.N[f][d];
+                nm = std::sqrt(nm);
+                const double inv = 1. / nm;
+                g.nmag[f] = nm;
+                for (int d = 0; d < 3; ++d) {
+                    g.nhat[f][d] = g.N[f][d] / nm;
+                    g.nunit[f][d] = g.N[f][d] * inv;
                 }
             }
-            g.N[f][0] = t1[1] * t2[2] - t1[2] * t2[1];
-            g.N[f][1] = t1[2] * t2[0] - t1[0] * t2[2];
-            g.N[f][2] = t1[0] * t2[1] - t1[1] * t2[0];
-            double nm = 0.0;
-            for (int d = 0; d < 3; ++d) nm += g.N[f][d] * g.N[f][d];
-            nm = std::sqrt(nm);
-            const double inv = 1. / nm;
-            g.nmag[f] = nm;
-            for (int d = 0; d < 3; ++d) {
-                g.nhat[f][d] = g.N[f][d] / nm;
-                g.nunit[f][d] = g.N[f][d] * inv;
+            const int cid = static_cast<int>(out.classes.size());
+            out.classes.push_back(g);
+            class_of[key] = cid;
+            out.geo_class[e] = cid;
+        }
+        out.volume = 0.0;
+        for (int e = 0; e < (mv.nowned < 0 ? ne : std::min(mv.nowned, ne)); ++e) {  // owned elements
+            const GeoClass& g = out.classes[out.geo_class[e]];
+            out.volume += 8.0 * g.djac;
+            for (int a = 0; a < 3; ++a) {
+                const double len = 2.0 * std::sqrt(g.J[0 * 3 + a] * g.J[0 * 3 + a] + g.J[1 * 3 + a] * g.J[1 * 3 + a] +
+                                                   g.J[2 * 3 + a] * g.J[2 * 3 + a]);
+                out.hmin = std::fmin(out.hmin, len);
             }
         }
-        const int cid = static_cast<int>(out.classes.size());
-        out.classes.push_back(g);
-        class_of[key] = cid;
-        out.geo_class[e] = cid;
-    }
-    out.volume = 0.0;
-    for (int e = 0; e < (mv.nowned < 0 ? ne : std::min(mv.nowned, ne)); ++e) {  // owned elements
-        const GeoClass& g = out.classes[out.geo_class[e]];
-        out.volume += 8.0 * g.djac;
-        for (int a = 0; a < 3; ++a) {
-            const double len = 2.0 * std::sqrt(g.J[0 * 3 + a] * g.J[0 * 3 + a] + g.J[1 * 3 + a] * g.J[1 * 3 + a] +
-                                               g.J[2 * 3 + a] * g.J[2 * 3 + a]);
-            out.hmin = std::fmin(out.hmin, len);
-        }
+
     }
 
     // ---- face gather table ----
@@ -360,6 +494,7 @@ std::string prepare_mesh(const MeshView& mv, int m, PreparedMesh& out)
                 return "unsupported: face " + std::to_string(f) + " of element " + std::to_string(e) +
                        " is a boundary face (only periodic meshes are handled)";
     out.ncodes = static_cast<int>(code_of.size());
+    if (out.general) general_face_normals(mv, m, canon_inv, order_inv, out);
     return "";
 }
 

@@ -60,6 +60,15 @@ struct PreparedMesh {
     std::vector<double> X0;            // [ne][3] coordinates of local node 0
     double volume = 0.0;               // sum of element volumes
     double hmin = 0.0;                 // smallest element edge length
+    // General (trilinear, non-parallelepiped) geometry: set when some element
+    // is not affine.  Every element then carries per-point tables, as the
+    // reference's per-quadrature-point helpers do (helpers.cpp:5-51,
+    // 380-500), and the affine classes are unused (one placeholder class).
+    bool general = false;
+    std::vector<double> gnodes;        // [ne][8][3] node coordinates
+    std::vector<double> gjd;           // [ne][9][m^3] ijac(d, j) * djac at the volume GL points
+    std::vector<double> gN;            // [nowned][6][3][m*m] the left element's face normal N at each own face point
+    std::vector<double> elem_h;        // [ne] shortest edge of each element
 };
 
 // Validates the mesh and builds the tables for face grids of m x m points.

@@ -227,7 +227,114 @@ Tables1D make_tables(int p)
     gauss_legendre(t.me, t.xe, t.we);
     t.Be.assign(t.me * t.n, 0.0);
     for (int q = 0; q < t.me; ++q) lagrange_1d(t.xe[q], xn, &t.Be[q * t.n], nullptr);
+    // the inverse-mass rule's 1D tables, for general (trilinear) elements
+    t.mm = mm;
+    t.xm = xm;
+    t.wm = wm;
+    t.Bm.assign(t.mm * t.n, 0.0);
+    for (int q = 0; q < t.mm; ++q) lagrange_1d(t.xm[q], xn, &t.Bm[q * t.n], nullptr);
     return t;
+}
+
+void trilinear_jacobian(const double* X, const double* xi, double* jac)
+{
+    // geometric basis phi_n = prod_a (1 + s_a(n) xi_a) / 2, node n = i + 2j + 4k
+    double dphi[8][3];
+    for (int n = 0; n < 8; ++n)
+        for (int j = 0; j < 3; ++j) {
+            double g = 1.0;
+            for (int a = 0; a < 3; ++a) {
+                const double s = ((n >> a) & 1) ? 1.0 : -1.0;
+                g *= a == j ? 0.5 * s : 0.5 * (1.0 + s * xi[a]);
+            }
+            dphi[n][j] = g;
+        }
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            double s = 0.0;
+            for (int n = 0; n < 8; ++n) s += X[n * 3 + i] * dphi[n][j];
+            jac[i * 3 + j] = s;
+        }
+}
+
+double det3(const double* M)
+{
+    return M[0] * M[4] * M[8] - M[0] * M[5] * M[7] - M[1] * M[3] * M[8] + M[1] * M[5] * M[6] + M[2] * M[3] * M[7] -
+           M[2] * M[4] * M[6];
+}
+
+bool general_inverse_mass(const Tables1D& t, const double* X, double* out)
+{
+    const int n = t.n, mm = t.mm, nb = n * n * n;
+    // w * det J at the mass points, [z][y][x]
+    std::vector<double> D(static_cast<size_t>(mm) * mm * mm);
+    for (int z = 0; z < mm; ++z)
+        for (int y = 0; y < mm; ++y)
+            for (int x = 0; x < mm; ++x) {
+                const double xi[3] = {t.xm[x], t.xm[y], t.xm[z]};
+                double jac[9];
+                trilinear_jacobian(X, xi, jac);
+                D[(static_cast<size_t>(z) * mm + y) * mm + x] = t.wm[x] * t.wm[y] * t.wm[z] * det3(jac);
+            }
+    // sum-factorised B^T D B: contract x, then y, then z (basis index c*n*n + b*n + a)
+    std::vector<double> T1(static_cast<size_t>(n) * n * mm * mm);  // [a][a'][z][y]
+    for (int a = 0; a < n; ++a)
+        for (int a2 = 0; a2 < n; ++a2)
+            for (int z = 0; z < mm; ++z)
+                for (int y = 0; y < mm; ++y) {
+                    double s = 0.0;
+                    for (int x = 0; x < mm; ++x)
+                        s += t.Bm[x * n + a] * t.Bm[x * n + a2] * D[(static_cast<size_t>(z) * mm + y) * mm + x];
+                    T1[((static_cast<size_t>(a) * n + a2) * mm + z) * mm + y] = s;
+                }
+    std::vector<double> T2(static_cast<size_t>(n) * n * n * n * mm);  // [a][a'][b][b'][z]
+    for (int aa = 0; aa < n * n; ++aa)
+        for (int b = 0; b < n; ++b)
+            for (int b2 = 0; b2 < n; ++b2)
+                for (int z = 0; z < mm; ++z) {
+                    double s = 0.0;
+                    for (int y = 0; y < mm; ++y)
+                        s += t.Bm[y * n + b] * t.Bm[y * n + b2] * T1[(static_cast<size_t>(aa) * mm + z) * mm + y];
+                    T2[((static_cast<size_t>(aa) * n + b) * n + b2) * mm + z] = s;
+                }
+    std::vector<double> M(static_cast<size_t>(nb) * nb);
+    for (int a = 0; a < n; ++a)
+        for (int a2 = 0; a2 < n; ++a2)
+            for (int b = 0; b < n; ++b)
+                for (int b2 = 0; b2 < n; ++b2)
+                    for (int c = 0; c < n; ++c)
+                        for (int c2 = 0; c2 < n; ++c2) {
+                            double s = 0.0;
+                            const double* t2 = &T2[(((static_cast<size_t>(a) * n + a2) * n + b) * n + b2) * mm];
+                            for (int z = 0; z < mm; ++z) s += t.Bm[z * n + c] * t.Bm[z * n + c2] * t2[z];
+                            M[static_cast<size_t>((c * n + b) * n + a) * nb + (c2 * n + b2) * n + a2] = s;
+                        }
+    // unpivoted LU (Doolittle, unit lower L), then the inverse column by column
+    for (int k = 0; k < nb; ++k) {
+        const double piv = M[static_cast<size_t>(k) * nb + k];
+        if (!(std::fabs(piv) > 0.0)) return false;
+        for (int i = k + 1; i < nb; ++i) M[static_cast<size_t>(i) * nb + k] /= piv;
+        for (int i = k + 1; i < nb; ++i) {
+            const double lik = M[static_cast<size_t>(i) * nb + k];
+            for (int j = k + 1; j < nb; ++j) M[static_cast<size_t>(i) * nb + j] -= lik * M[static_cast<size_t>(k) * nb + j];
+        }
+    }
+    std::vector<double> col(nb);
+    for (int c = 0; c < nb; ++c) {
+        for (int i = 0; i < nb; ++i) {
+            double s = i == c ? 1.0 : 0.0;
+            for (int k = 0; k < i; ++k) s -= M[static_cast<size_t>(i) * nb + k] * col[k];
+            col[i] = s;
+        }
+        for (int i = nb - 1; i >= 0; --i) {
+            double s = col[i];
+            for (int k = i + 1; k < nb; ++k) s -= M[static_cast<size_t>(i) * nb + k] * col[k];
+            col[i] = s / M[static_cast<size_t>(i) * nb + i];
+        }
+        // column c of the inverse: iMM[i][c] = col[i], stored at out[c * nb + i]
+        for (int i = 0; i < nb; ++i) out[static_cast<size_t>(c) * nb + i] = col[i];
+    }
+    return true;
 }
 
 }  // namespace dgh

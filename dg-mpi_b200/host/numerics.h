@@ -57,7 +57,21 @@ struct Tables1D {
     std::vector<double> Minv;              // [n*n] inverse 1D mass matrix
     int me = 0;                            // IC / error rule: 2*max(p,1)+2 points
     std::vector<double> xe, we, Be;        // [me], [me], [me*n]
+    int mm = 0;                            // inverse-mass rule: 2p+2 points
+    std::vector<double> xm, wm, Bm;        // [mm], [mm], [mm*n]
 };
 Tables1D make_tables(int p);
+
+// Inverse mass matrix of one trilinear element with nodes X [8][3]
+// (helpers.cpp:54-100: the mass matrix B^T diag(w djac) B on the order-2p rule,
+// inverted by an unpivoted LU factorisation as BasisTools::get_inv_mass_matrices
+// does, basis/tools.cpp:86-110), written transposed: out[k * nb + j] = iMM[j][k].
+// Returns false for a singular factorisation.
+bool general_inverse_mass(const Tables1D& t, const double* X, double* out);
+
+// Jacobian of the trilinear map of nodes X [8][3] at reference point xi:
+// jac[i*3 + j] = sum_n X[n][i] dphi_n/dxi_j (basis/tools.cpp:42-66).
+void trilinear_jacobian(const double* X, const double* xi, double* jac);
+double det3(const double* M);
 
 }  // namespace dgh

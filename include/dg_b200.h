@@ -144,7 +144,7 @@ int dg_rk4_steps_timed(dg_ctx* ctx, double dt, int nsteps, double* device_ms);
  * tuner times one RK stage of every variant of the context's precision on its
  * mesh and current state (the state is not modified; the RK accumulator, dead
  * between steps, serves as scratch, so call it between steps) and selects the
- * fastest (entries of other precision report -1 ms); callers cache the result
+ * fastest (entries of the other precision or geometry kind report -1 ms); callers cache the result
  * per (order, precision, GPU) and restore it with dg_set_stage_variant. */
 int dg_num_stage_variants(int order);
 int dg_stage_variant_info(int order, int variant, int* elems_per_cta, int* threads_per_cta, int* groups,
@@ -155,7 +155,10 @@ int dg_stage_variant_info(int order, int variant, int* elems_per_cta, int* threa
  * bit 2 -- unfused volume (z interpolation, pointwise flux and contractions as
  * separate passes over all quadrature points; the groups count is unused);
  * bit 3 -- traces and lifts split into one task per output row; bit 4 -- one
- * face-flux point per thread and iteration (fewer registers); bits 8..11 -- the minimum of resident CTAs per SM the kernel was compiled
+ * face-flux point per thread and iteration (fewer registers); bit 5 -- general
+ * (trilinear) geometry: per-point metric terms and normals and a dense
+ * inverse mass matrix per element, the variants a context on a non-affine
+ * mesh runs (and the only ones it accepts); bits 8..11 -- the minimum of resident CTAs per SM the kernel was compiled
  * for (0: none; a register cap). */
 int dg_stage_variant_flags(int order, int variant, int* flags);
 int dg_set_stage_variant(dg_ctx* ctx, int variant);

@@ -66,7 +66,8 @@ def test_mixed_free_stream_and_tuner():
     best, ms = mix.tune_stage(reps=1)
     variants = mix.stage_variants()
     assert variants[best][3] == "mixed_fp32"
-    assert all((t < 0) == (v[3] != "mixed_fp32") for v, t in zip(variants, ms))
+    # variants of the other precision, and the general-geometry ones (this mesh is affine), are not timed
+    assert all((t < 0) == (v[3] != "mixed_fp32" or "ge" in v[4].split("+")) for v, t in zip(variants, ms))
     mix.rk4(1e-3, 5)
     assert np.abs(mix.get_state() - U).max() < 1e-6
 

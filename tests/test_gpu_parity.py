@@ -220,8 +220,8 @@ def test_every_stage_variant_matches_oracle(p, flux):
         if ref is None:
             ref = orc.rk4(U, dt, 3)
         for v, info in enumerate(case.stage_variants()):
-            if info[3] != precision:
-                continue
+            if info[3] != precision or "ge" in info[4].split("+"):
+                continue  # general-geometry variants run on non-affine meshes (test_gpu_general.py)
             case.stage_variant = v
             case.set_state(U)
             case.rk4(dt, 3)

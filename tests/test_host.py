@@ -126,13 +126,26 @@ def test_mesh_validation_rejects_boundary_faces_before_touching_the_gpu():
     assert ei.value.code == 5 and "boundary face" in str(ei.value)
 
 
-def test_mesh_validation_rejects_non_affine_elements():
+def test_non_affine_elements_pass_validation_and_folded_ones_do_not():
+    """Bent (trilinear) elements are accepted -- without a GPU creation then stops
+    at the device -- while an element with a non-positive Jacobian somewhere is
+    rejected on the host, as are non-affine cases in a batch."""
+    from conftest import gpu_available
     mesh = dg_b200.periodic_box((2, 2, 2))
     coords = mesh.node_coords.copy()
     coords[13] += [0.05, 0.0, 0.0]  # the centre node: every element around it bends
+    bent = dg_b200.Mesh(coords, mesh.elem_to_node_ids, mesh.interior_faces)
+    if not gpu_available():
+        with pytest.raises(dg_b200.DGError, match="DG_ERR_CUDA"):
+            dg_b200.Case(bent, 2)
+    folded = mesh.node_coords.copy()
+    folded[13] += [0.9, 0.0, 0.0]  # past the neighbouring nodes: elements fold
     with pytest.raises(dg_b200.DGError) as ei:
-        dg_b200.Case(dg_b200.Mesh(coords, mesh.elem_to_node_ids, mesh.interior_faces), 2)
-    assert ei.value.code == 5 and "not affine" in str(ei.value)
+        dg_b200.Case(dg_b200.Mesh(folded, mesh.elem_to_node_ids, mesh.interior_faces), 2)
+    assert ei.value.code == 1 and "non-positive Jacobian" in str(ei.value)
+    with pytest.raises(dg_b200.DGError) as ei:
+        dg_b200.Batch([(mesh, 2), (bent, 2)])
+    assert ei.value.code == 5 and "non-affine" in str(ei.value)
 
 
 def test_mesh_validation_rejects_out_of_range_entries():
