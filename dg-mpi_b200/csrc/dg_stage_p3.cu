@@ -31,6 +31,8 @@ static const StageVariant kVariants3[] = {
     // general (trilinear) geometry: the variants of non-affine meshes
     make_variant<3, 1, 64, 1, double, kUF | kRS | kSB | kK1 | kGE>(),
     make_variant<3, 1, 32, 1, float, kUF | kSB | kK1 | kGE>(),
+    make_variant<3, 1, 64, 1, float, kUF | kSB | kK1 | kGE>(),
+    make_variant<3, 1, 64, 1, float, kUF | kRS | kSB | kK1 | kGE>(),
 };
 
 int stage_variants_p3(const StageVariant** out)

@@ -5,6 +5,7 @@
   python dg-mpi_b200/studies.py taylor_green # 96^3, p=4, Taylor-Green, 200 RK4 steps
   python dg-mpi_b200/studies.py ensemble     # 256 seeded vortex cases, p=1..5, 8^3..32^3, 100 steps
   python dg-mpi_b200/studies.py <name> --scale 0.25  # smaller mesh (fewer cases), same orders
+  python dg-mpi_b200/studies.py general       # bent (non-affine) periodic boxes: 48^3 p=3, 24^3 p=5
   python dg-mpi_b200/studies.py stage --nel 40 --order 3 --precision fp64 --variant 0
                                              # one launch variant, 2 RK4 steps, no tuner (ncu captures)
 
@@ -155,6 +156,48 @@ def ensemble(scale: float, steps: int = 100, cfl: float = 0.1):
     return out
 
 
+def bent_box(n: int, amplitude: float):
+    """Periodic box on [0,10]^3 whose nodes move by a smooth periodic field
+    (products of sines and cosines of two coordinates, amplitude in cells):
+    every element becomes a general trilinear hexahedron."""
+    L = 10.0
+    mesh = dg_b200.periodic_box((n, n, n), (0.0, 0.0, 0.0), (L, L, L))
+    x = mesh.node_coords
+    s = [np.sin(2 * np.pi * x[:, d] / L + 0.7 * (d + 1)) for d in range(3)]
+    c = [np.cos(2 * np.pi * x[:, d] / L + 0.4 * (d + 1)) for d in range(3)]
+    disp = amplitude * (L / n) * np.stack([s[1] * c[2], s[2] * c[0], s[0] * c[1]], axis=1)
+    return dg_b200.Mesh(np.ascontiguousarray(x + disp), mesh.elem_to_node_ids, mesh.interior_faces)
+
+
+def general(scale: float):
+    """Non-affine meshes: the general-geometry stage kernel (per-point metric
+    terms and normals, a dense inverse mass matrix per element, all streamed
+    from HBM) on bent boxes, FP64 and mixed; rates, mixed vs FP64 after the
+    steps, and the achieved HBM rate of the streams the stage reads and writes."""
+    out = {"config": "x-y vortex on bent periodic boxes [0,10]^3 (5 % bend), LF flux, RK4 CFL 0.1"}
+    for n0, order, steps in ((48, 3, 40), (24, 5, 20)):
+        n = max(4, int(round(n0 * scale)))
+        mesh = bent_box(n, 0.05)
+        t0 = time.perf_counter()
+        cases, res = run_pair(mesh, order, "IsentropicVortexXY", VORTEX, steps, 0.1)
+        res["setup_s_both"] = time.perf_counter() - t0
+        nb, ne, m = (order + 1) ** 3, n ** 3, order + 2
+        # per element and stage: the five state streams (40 B/DOF), the metric
+        # terms, the face normal data and the inverse mass matrix (FP64)
+        bytes_elem = 40 * 5 * nb + 8 * (9 * m ** 3 + 6 * 4 * m * m + nb * nb)
+        for name in ("fp64", "mixed_fp32"):
+            r = res[name]
+            stages_per_s = r["dof_stage_per_s"] / (ne * nb * 5)
+            extra = 8 * 5 * nb if name == "mixed_fp32" else 0  # the FP32 residual's unit-pressure table
+            r["hbm_gbs_streams"] = stages_per_s * ne * (bytes_elem + extra) / 1e9
+        res["rel_l2_mixed_vs_fp64"] = [float(v) for v in res["rel_l2_mixed_vs_fp64"]]
+        res["bytes_per_element_stage"] = bytes_elem
+        for cs in cases.values():
+            cs.close()
+        out[f"{n}^3_p{order}"] = res
+    return out
+
+
 def stage(nel: int, order: int, precision_: str, variant: int, steps: int):
     """x-y vortex on an nel^3 box, one fixed stage-kernel launch variant (no tuner, so the
     launch sequence is known: the projection, then four stage launches per step)."""
@@ -172,7 +215,7 @@ def stage(nel: int, order: int, precision_: str, variant: int, steps: int):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("study", choices=["precision", "taylor_green", "ensemble", "stage"])
+    ap.add_argument("study", choices=["precision", "taylor_green", "ensemble", "general", "stage"])
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--nel", type=int, default=40, help="stage: elements per direction")
     ap.add_argument("--order", type=int, default=3, help="stage: polynomial order")
@@ -183,7 +226,7 @@ def main():
     if args.study == "stage":
         res = stage(args.nel, args.order, args.precision, args.variant, args.steps)
     else:
-        run = {"precision": precision, "taylor_green": taylor_green, "ensemble": ensemble}[args.study]
+        run = {"precision": precision, "taylor_green": taylor_green, "ensemble": ensemble, "general": general}[args.study]
         res = run(args.scale)
     res["study"] = args.study
     print(json.dumps(res), flush=True)
