@@ -937,7 +937,7 @@ __device__ __forceinline__ void stage_body(const StageArgs& a)
                 const double* im = a.gimm + (size_t)ge * NB * NB + j;  // iMM[j][k] at im[k * NB]
                 const double* r = sRes + e * ES;
                 double s[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-#pragma unroll 8
+#pragma unroll 16
                 for (int k = 0; k < NB; ++k) {
                     const double mk = im[(size_t)k * NB];
 #pragma unroll

@@ -69,8 +69,14 @@ typedef struct dg_ctx dg_ctx;
  * node_coords, elem_to_node_IDs, interior_faces).  interior_faces rows are
  * (rankL, elemL, faceL, orientL, rankR, elemR, faceR, orientR)
  * (src/mesh/mesh.h:280-284); on one GPU every rank entry must equal `rank`.
- * Elements must be affine (parallelepipeds); every face must be interior
- * (periodic meshes). */
+ * Every face must be interior (periodic meshes).  Elements may be general
+ * trilinear hexahedra: when one is not a parallelepiped, the context keeps,
+ * as the reference's helpers do, per-point metric terms and face normals and
+ * a dense inverse mass matrix per element (nb^2 doubles each: 32 KB at p = 3,
+ * 373 KB at p = 5) and runs the general-geometry kernel variants; such meshes
+ * are not accepted by dg_batch_create or dg_create_partitioned
+ * (DG_ERR_UNSUPPORTED), and an element whose Jacobian is not positive at a
+ * quadrature point is rejected (DG_ERR_ARG). */
 typedef struct dg_mesh_desc {
     int nnode;
     const double* node_coords;         /* [nnode][3] */
