@@ -361,6 +361,7 @@ int dg_batch_get_state(dg_batch* b, int c, double* Uc)
 
 int dg_batch_project_ic(dg_batch* b, int c, int ic_type, const double* data, int ndata, double t, double* Uc)
 {
+    dgi::NvtxRange nvtx_("dg_batch_project_ic");
     if (!case_ok(b, c)) return bfail(b, DG_ERR_ARG, "dg_batch_project_ic: case index out of range");
     if (ic_type < DG_IC_UNIFORM || ic_type > DG_IC_TAYLOR_GREEN) return bfail(b, DG_ERR_ARG, "unknown initial condition");
     const int need[] = {5, 0, 0, 9, 1};
@@ -416,6 +417,7 @@ int dg_batch_set_time_step(dg_batch* b, int c, double dt)
 
 int dg_batch_rk4_steps_timed(dg_batch* b, int nsteps, double* device_ms)
 {
+    dgi::NvtxRange nvtx_("dg_batch_rk4_steps_timed");
     if (!b || nsteps < 0) return bfail(b, DG_ERR_ARG, "dg_batch_rk4_steps: bad argument");
     if (cudaSetDevice(b->device) != cudaSuccess) return bfail(b, DG_ERR_CUDA, "cudaSetDevice failed");
     int rc = upload_time_steps(b);
@@ -441,6 +443,7 @@ int dg_batch_rk4_steps(dg_batch* b, int nsteps) { return dg_batch_rk4_steps_time
 
 int dg_batch_tune(dg_batch* b, int reps)
 {
+    dgi::NvtxRange nvtx_("dg_batch_tune");
     if (!b || reps < 1) return bfail(b, DG_ERR_ARG, "dg_batch_tune: bad argument");
     for (auto& g : b->groups) {
         const int keep = g.ctx->variant;

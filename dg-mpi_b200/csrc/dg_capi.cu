@@ -1137,18 +1137,21 @@ int halo_launch(dg_ctx* c, int buf, double* d_data, void* stream, bool pack)
 
 int dg_halo_pack(dg_ctx* c, int buf, double* d_send, void* stream)
 {
+    dgi::NvtxRange nvtx_("dg_halo_pack");
     if (!c) return DG_ERR_ARG;
     return halo_launch(c, buf, d_send, stream, true);
 }
 
 int dg_halo_unpack(dg_ctx* c, int buf, const double* d_recv, void* stream)
 {
+    dgi::NvtxRange nvtx_("dg_halo_unpack");
     if (!c) return DG_ERR_ARG;
     return halo_launch(c, buf, const_cast<double*>(d_recv), stream, false);
 }
 
 int dg_rk4_stage(dg_ctx* c, int stage, double dt, int range)
 {
+    dgi::NvtxRange nvtx_("dg_rk4_stage");
     if (!c || stage < 1 || stage > 4 || range < 0 || range > 2) return fail(c, DG_ERR_ARG, "dg_rk4_stage: bad argument");
     DG_CUDA(c, cudaSetDevice(c->device));
     const int e0 = range == 2 ? c->ninterior : 0, e1 = range == 1 ? c->ninterior : c->ne;
@@ -1189,6 +1192,7 @@ int set_energy_reference(dg_ctx* c, const double* Uc)
 
 int dg_set_state(dg_ctx* c, const double* Uc)
 {
+    dgi::NvtxRange nvtx_("dg_set_state");
     if (!c || !Uc) return fail(c, DG_ERR_ARG, "dg_set_state: null argument");
     DG_CUDA(c, cudaSetDevice(c->device));
     const int rc = set_energy_reference(c, Uc);
@@ -1198,6 +1202,7 @@ int dg_set_state(dg_ctx* c, const double* Uc)
 
 int dg_get_state(dg_ctx* c, double* Uc)
 {
+    dgi::NvtxRange nvtx_("dg_get_state");
     if (!c || !Uc) return fail(c, DG_ERR_ARG, "dg_get_state: null argument");
     DG_CUDA(c, cudaSetDevice(c->device));
     return download_host_layout(c, c->d_U0, Uc);
@@ -1205,6 +1210,7 @@ int dg_get_state(dg_ctx* c, double* Uc)
 
 int dg_residual(dg_ctx* c, double* res)
 {
+    dgi::NvtxRange nvtx_("dg_residual");
     if (!c || !res) return fail(c, DG_ERR_ARG, "dg_residual: null argument");
     DG_CUDA(c, cudaSetDevice(c->device));
     int rc = launch_stage(c, dgk::kModeResidual, c->d_U0, c->d_U0, c->d_acc, 0.0);
@@ -1216,6 +1222,7 @@ int dg_residual(dg_ctx* c, double* res)
 
 int dg_mass_inverse_residual(dg_ctx* c, double dt, double* dU)
 {
+    dgi::NvtxRange nvtx_("dg_mass_inverse_residual");
     if (!c || !dU) return fail(c, DG_ERR_ARG, "dg_mass_inverse_residual: null argument");
     DG_CUDA(c, cudaSetDevice(c->device));
     int rc = launch_stage(c, dgk::kModeMassInv, c->d_U0, c->d_U0, c->d_acc, dt);
@@ -1254,6 +1261,7 @@ int prepare_rk4_graph(dg_ctx* c, double dt)
 
 int dg_rk4_steps_timed(dg_ctx* c, double dt, int nsteps, double* device_ms)
 {
+    dgi::NvtxRange nvtx_("dg_rk4_steps_timed");
     if (!c || nsteps < 0 || !device_ms) return fail(c, DG_ERR_ARG, "dg_rk4_steps_timed: bad argument");
     DG_CUDA(c, cudaSetDevice(c->device));
     int rc = prepare_rk4_graph(c, dt);
@@ -1319,6 +1327,7 @@ int dg_get_stage_variant(const dg_ctx* c) { return c ? c->variant : -1; }
 
 int dg_tune_stage(dg_ctx* c, int reps, int* best, double* ms_per_variant)
 {
+    dgi::NvtxRange nvtx_("dg_tune_stage");
     if (!c || reps < 1) return fail(c, DG_ERR_ARG, "dg_tune_stage: bad argument");
     DG_CUDA(c, cudaSetDevice(c->device));
     const int nv = dg_num_stage_variants(c->p);
@@ -1363,6 +1372,7 @@ int dg_tune_stage(dg_ctx* c, int reps, int* best, double* ms_per_variant)
 
 int dg_rk4_steps(dg_ctx* c, double dt, int nsteps)
 {
+    dgi::NvtxRange nvtx_("dg_rk4_steps");
     if (!c || nsteps < 0) return fail(c, DG_ERR_ARG, "dg_rk4_steps: bad argument");
     if (nsteps == 0) return DG_OK;
     DG_CUDA(c, cudaSetDevice(c->device));
@@ -1375,6 +1385,7 @@ int dg_rk4_steps(dg_ctx* c, double dt, int nsteps)
 
 int dg_fe_steps(dg_ctx* c, double dt, int nsteps)
 {
+    dgi::NvtxRange nvtx_("dg_fe_steps");
     if (!c || nsteps < 0) return fail(c, DG_ERR_ARG, "dg_fe_steps: bad argument");
     DG_CUDA(c, cudaSetDevice(c->device));
     for (int s = 0; s < nsteps; ++s) {
@@ -1395,6 +1406,7 @@ int dg_fe_steps(dg_ctx* c, double dt, int nsteps)
 
 int dg_project_ic(dg_ctx* c, int ic_type, const double* data, int ndata, double t, double* Uc)
 {
+    dgi::NvtxRange nvtx_("dg_project_ic");
     if (!c) return fail(c, DG_ERR_ARG, "dg_project_ic: null context");
     if (ic_type < DG_IC_UNIFORM || ic_type > DG_IC_TAYLOR_GREEN) return fail(c, DG_ERR_ARG, "unknown initial condition");
     double d[16] = {0};
@@ -1423,6 +1435,7 @@ int dg_project_ic(dg_ctx* c, int ic_type, const double* data, int ndata, double 
 
 int dg_l2_error(dg_ctx* c, int ic_type, const double* data, int ndata, double t, double* err)
 {
+    dgi::NvtxRange nvtx_("dg_l2_error");
     if (!c || !err) return fail(c, DG_ERR_ARG, "dg_l2_error: null argument");
     if (ic_type < DG_IC_UNIFORM || ic_type > DG_IC_TAYLOR_GREEN) return fail(c, DG_ERR_ARG, "unknown exact solution");
     DG_CUDA(c, cudaSetDevice(c->device));
@@ -1435,6 +1448,7 @@ int dg_l2_error(dg_ctx* c, int ic_type, const double* data, int ndata, double t,
 
 int dg_kinetic_energy(dg_ctx* c, double* ke)
 {
+    dgi::NvtxRange nvtx_("dg_kinetic_energy");
     if (!c || !ke) return fail(c, DG_ERR_ARG, "dg_kinetic_energy: null argument");
     DG_CUDA(c, cudaSetDevice(c->device));
     double sums[5];
@@ -1578,6 +1592,7 @@ int dg_basis_tables(int p, double* B, double* D, double* Minv)
 
 int dg_cfl_time_step(dg_ctx* c, const double* Uc, double cfl, double* dt)
 {
+    dgi::NvtxRange nvtx_("dg_cfl_time_step");
     if (!c || !Uc || !dt || !(cfl > 0.0)) return fail(c, DG_ERR_ARG, "dg_cfl_time_step: bad argument");
     const double v = dgh::cfl_time_step(c->pm, c->p, c->gamma, Uc, cfl, 0, c->ne);
     if (!(v > 0.0)) return fail(c, DG_ERR_NONPHYSICAL, "state has non-positive density or pressure");

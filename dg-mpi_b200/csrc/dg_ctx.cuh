@@ -3,6 +3,7 @@
 // ensembles (dg_batch.cu).  Not part of the public interface.
 #pragma once
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <string>
 #include <vector>
@@ -14,6 +15,15 @@
 
 namespace dgi {
 constexpr int kMaxVariants = 32;  // launch variants per order (checked in prepare_variant)
+
+// NVTX range named after a C-ABI call, for timelines of Nsight tools (a no-op
+// when no tool is attached)
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 }
 
 struct dg_ctx {

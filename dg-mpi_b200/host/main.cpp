@@ -16,7 +16,12 @@
 //   [Physics]  name = "Euler", dim = 3, gamma = 1.4, GasConstant = 287.05,
 //              convective_flux_fcn = "LaxFriedrichs" | "HLLC"
 //   [InitialCondition] name, data
-//   [Output]   (extension) print_every = N, state_file = "path"
+//   [Output]   (extensions) print_every = N; state_file = "path" (binary
+//              checkpoint at the end: int64 ne, nb, 5, double time, then
+//              Uc [ne][nb][5]); restart_file = "path" (start from such a
+//              checkpoint instead of the initial condition; with `end` the
+//              run stops at that time, with `steps` it takes that many more);
+//              json = true (one JSON line of run metrics at the end)
 #include <cfloat>
 #include <chrono>
 #include <cstdio>
@@ -49,6 +54,7 @@ struct StepperBase {
 struct Solver {
     dg_ctx* ctx = nullptr;
     double time = 0.0;
+    std::vector<double> restart_state;  // [ne][nb][5] from a checkpoint, else empty
     long num_iterations = 0;
     int print_every = 0;
     std::unique_ptr<StepperBase> stepper;
@@ -154,6 +160,24 @@ int run(const dgh::Toml& deck, bool check_only)
     // Solver::init_state_from_fcn (L2 projection), base.cpp:113-223
     if (dg_project_ic(solver.ctx, ic, ic_data.data(), static_cast<int>(ic_data.size()), 0.0, Uc.data()))
         throw std::runtime_error(std::string("dg_project_ic: ") + dg_last_error(solver.ctx));
+    const bool restart = deck.has("Output", "restart_file");
+    if (restart) {
+        // the time step still comes from the deck (or the CFL on the initial
+        // condition), so a resumed run takes the same steps as an unbroken one
+        const std::string path = deck.str("Output", "restart_file");
+        std::ifstream f(path, std::ios::binary);
+        long long hdr[3] = {0, 0, 0};
+        double t = 0.0;
+        f.read(reinterpret_cast<char*>(hdr), sizeof(hdr));
+        f.read(reinterpret_cast<char*>(&t), sizeof(double));
+        if (!f || hdr[0] != ne || hdr[1] != nb || hdr[2] != 5)
+            throw std::runtime_error("restart_file " + path + " does not hold a state of this mesh and order");
+        std::vector<double> U0(Uc.size());
+        f.read(reinterpret_cast<char*>(U0.data()), static_cast<std::streamsize>(U0.size() * sizeof(double)));
+        if (!f) throw std::runtime_error("restart_file " + path + " is truncated");
+        solver.time = t;
+        solver.restart_state = std::move(U0);
+    }
 
     double dt = deck.num_or("Stepper", "timestep", 0.0);
     if (deck.has("Stepper", "cfl")) {
@@ -164,9 +188,14 @@ int run(const dgh::Toml& deck, bool check_only)
     if (deck.has("Stepper", "steps")) {
         solver.num_iterations = static_cast<long>(deck.num("Stepper", "steps"));
     } else {
-        // num_iterations = (int)(tfinal / dt), base.cpp:383
-        solver.num_iterations = static_cast<int>(deck.num("Stepper", "end") / dt);
+        // num_iterations = (int)(tfinal / dt), base.cpp:383; after a restart,
+        // the steps left to that end time
+        const double end = deck.num("Stepper", "end");
+        solver.num_iterations = static_cast<int>(end / dt) - (restart ? static_cast<long>(solver.time / dt + 0.5) : 0);
+        if (solver.num_iterations < 0) solver.num_iterations = 0;
     }
+    if (restart && dg_set_state(solver.ctx, solver.restart_state.data()))
+        throw std::runtime_error(std::string("dg_set_state: ") + dg_last_error(solver.ctx));
     if (stype == "RK4") solver.stepper = std::make_unique<RK4Gpu>();
     else solver.stepper = std::make_unique<FEGpu>();
     solver.stepper->set_time_step(dt);
@@ -175,8 +204,19 @@ int run(const dgh::Toml& deck, bool check_only)
     std::printf("timestep = %.17g, number of iterations = %ld, DOF = %lld\n", dt, solver.num_iterations,
                 static_cast<long long>(ne) * nb * 5);
 
+    const auto t0 = std::chrono::steady_clock::now();
     int rc = solver.solve();
     if (rc) throw std::runtime_error(std::string("solve: ") + dg_last_error(solver.ctx));
+    const double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    const double dof = static_cast<double>(ne) * nb * 5;
+    const int stages = stype == "RK4" ? 4 : 1;
+    std::string json = "{\"dof\": " + std::to_string(static_cast<long long>(dof)) +
+                       ", \"order\": " + std::to_string(order) + ", \"steps\": " + std::to_string(solver.num_iterations) +
+                       ", \"stages_per_step\": " + std::to_string(stages) + ", \"wall_s\": " + std::to_string(wall) +
+                       ", \"dof_stage_per_s\": " + std::to_string(wall > 0 ? dof * stages * solver.num_iterations / wall : 0.0);
+    char tbuf[64];
+    std::snprintf(tbuf, sizeof(tbuf), "%.17g", solver.time);
+    json += std::string(", \"time\": ") + tbuf;
 
     // post: volume-normalised L2 error against the exact solution
     // (get_error, src/post/main.cpp:30-201); TaylorGreen has none: kinetic energy instead
@@ -184,12 +224,21 @@ int run(const dgh::Toml& deck, bool check_only)
         double ke = 0.0;
         dg_kinetic_energy(solver.ctx, &ke);
         std::printf("kinetic_energy=%.*e\n", DECIMAL_DIG, ke);
+        std::snprintf(tbuf, sizeof(tbuf), "%.17g", ke);
+        json += std::string(", \"kinetic_energy\": ") + tbuf;
     } else {
         double err[5];
         if (dg_l2_error(solver.ctx, ic, ic_data.data(), static_cast<int>(ic_data.size()), solver.time, err))
             throw std::runtime_error(std::string("l2 error: ") + dg_last_error(solver.ctx));
         for (int s = 0; s < 5; ++s) std::printf("norm_total_error(%d)=%.*e\n", s, DECIMAL_DIG, err[s]);
+        json += ", \"l2_error\": [";
+        for (int s = 0; s < 5; ++s) {
+            std::snprintf(tbuf, sizeof(tbuf), "%s%.17g", s ? ", " : "", err[s]);
+            json += tbuf;
+        }
+        json += "]";
     }
+    if (deck.has("Output", "json") && deck.boolean("Output", "json")) std::printf("%s}\n", json.c_str());
     if (deck.has("Output", "state_file")) {
         dg_get_state(solver.ctx, Uc.data());
         std::ofstream f(deck.str("Output", "state_file"), std::ios::binary);

@@ -84,6 +84,12 @@ public:
         return v.num;
     }
     double num_or(const std::string& sec, const std::string& key, double d) const { return has(sec, key) ? num(sec, key) : d; }
+    bool boolean(const std::string& sec, const std::string& key) const
+    {
+        const TomlValue& v = at(sec, key);
+        if (v.kind != TomlValue::kBool) throw std::runtime_error("[" + sec + "] " + key + " must be true or false");
+        return v.b;
+    }
     std::vector<double> nums(const std::string& sec, const std::string& key) const
     {
         const TomlValue& v = at(sec, key);

@@ -49,3 +49,53 @@ def test_driver_reproduces_reference_regression(golden):
     assert "number of iterations = 1000" in r.stdout
     for s in (0, 1, 3, 4):
         assert abs(err[s] - ref[s]) <= 1e-12 * ref[s], (s, err[s], ref[s])
+
+
+def _deck(tmp_path, name, steps, output):
+    text = open(os.path.join(EXAMPLES, "vortex_xy_8cubed_p2.toml")).read()
+    text = re.sub(r"^steps\s*=.*$", "steps = %d" % steps, text, flags=re.M)
+    deck = tmp_path / name
+    deck.write_text(text + "\n[Output]\n" + output + "\n")
+    return str(deck)
+
+
+def test_driver_deck_with_output_extensions_parses(tmp_path):
+    r = run(["-input", _deck(tmp_path, "d.toml", 5, 'restart_file = "x.state"\njson = true'), "-check"])
+    assert r.returncode == 0, r.stderr
+
+
+@pytest.mark.gpu
+def test_driver_rejects_a_restart_file_of_another_mesh(tmp_path):
+    bad = tmp_path / "other.state"
+    np.array([7, 27, 5], np.int64).tofile(str(bad))
+    r = run(["-input", _deck(tmp_path, "d.toml", 5, 'restart_file = "%s"' % bad)])
+    assert r.returncode == 2 and "does not hold a state of this mesh" in r.stderr
+
+
+@pytest.mark.gpu
+def test_driver_checkpoint_resume_matches_unbroken_run(tmp_path):
+    """20 steps in one run against 12 steps, a checkpoint, and 8 more steps
+    from it: the states are bit for bit the same, and the JSON metrics line
+    reports the run."""
+    import json
+    full, part, rest = tmp_path / "full.state", tmp_path / "part.state", tmp_path / "rest.state"
+    r = run(["-input", _deck(tmp_path, "a.toml", 20, 'state_file = "%s"\njson = true' % full)])
+    assert r.returncode == 0, r.stderr
+    metrics = json.loads(r.stdout.strip().splitlines()[-1])
+    assert metrics["steps"] == 20 and metrics["stages_per_step"] == 4 and metrics["dof"] == 512 * 27 * 5
+    assert len(metrics["l2_error"]) == 5 and metrics["dof_stage_per_s"] > 0
+    r = run(["-input", _deck(tmp_path, "b.toml", 12, 'state_file = "%s"' % part)])
+    assert r.returncode == 0, r.stderr
+    r = run(["-input", _deck(tmp_path, "c.toml", 8, 'restart_file = "%s"\nstate_file = "%s"' % (part, rest))])
+    assert r.returncode == 0, r.stderr
+
+    def load(path):
+        raw = open(path, "rb").read()
+        hdr = np.frombuffer(raw[:24], np.int64)
+        t = np.frombuffer(raw[24:32], np.float64)[0]
+        return hdr, t, np.frombuffer(raw[32:], np.float64)
+    h1, t1, u1 = load(full)
+    h2, t2, u2 = load(rest)
+    assert list(h1) == list(h2) == [512, 27, 5]
+    assert t1 == t2 == metrics["time"]
+    assert np.array_equal(u1, u2)
