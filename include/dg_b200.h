@@ -309,10 +309,9 @@ void* dg_stream(dg_ctx* ctx);
 /* ---- batched ensembles ----
  *
  * Many independent cases (each its own periodic mesh, order and time step)
- * advanced together; the ensemble driver of the `dg_batch_*` entry points in
- * the survey's C ABI (the reference runs one case per process, so there is no
- * reference function it replaces; each case's arithmetic is exactly that of a
- * dg_ctx on the same case).  Cases of the same (order, flux, gamma, gas
+ * advanced together by the `dg_batch_*` entry points (the reference runs one
+ * case per process, so there is no reference function they replace; each
+ * case's arithmetic is exactly that of a dg_ctx on the same case).  Cases of the same (order, flux, gamma, gas
  * constant) share one group: their meshes are concatenated and one stage
  * launch per group and RK stage advances all of them, each element scaling its
  * update by its own case's dt.  dg_batch_rk4_steps replays a CUDA graph that
