@@ -100,7 +100,7 @@ bool variant_matches(const dg_ctx* c, int v)
     const dgk::StageVariant* vs = nullptr;
     const int nv = dgk::stage_variants(c->p, &vs);
     return v >= 0 && v < nv && (vs[v].fp32 != 0) == (c->precision == DG_PREC_MIXED_FP32) &&
-           ((vs[v].flags & dgk::kGE) != 0) == c->pm.general;
+           ((vs[v].flags & dgk::kGE) != 0) == c->pm.general && (!(vs[v].flags & dgk::kFX) || c->d_fflux);
 }
 
 // Sets the variant's shared-memory attribute and its persistent grid size
@@ -118,6 +118,15 @@ int prepare_variant(dg_ctx* c, int v)
     DG_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sv.func, sv.NT, sv.smem));
     if (per_sm < 1) return fail(c, DG_ERR_UNSUPPORTED, "stage kernel variant does not fit on an SM");
     const int batches = (c->ne + sv.E - 1) / sv.E;
+    if (sv.face_launch) {
+        if (!c->d_fflux) return fail(c, DG_ERR_UNSUPPORTED, "face-kernel variant on a context without a face list");
+        int face_per_sm = 0;
+        DG_CUDA(c, cudaFuncSetAttribute(sv.face_func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sv.face_smem));
+        DG_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&face_per_sm, sv.face_func, sv.face_threads, sv.face_smem));
+        if (face_per_sm < 1) return fail(c, DG_ERR_UNSUPPORTED, "face kernel does not fit on an SM");
+        const int fb = (c->p <= 2 ? 16 : (c->p == 3 ? 8 : 4));
+        c->variant_face_grid[v] = std::max(1, std::min((c->nface + fb - 1) / fb, dev_sms * face_per_sm));
+    }
     c->variant_grid[v] = std::max(1, std::min(batches, dev_sms * per_sm));
     return DG_OK;
 }
@@ -141,6 +150,9 @@ int launch_stage(dg_ctx* c, int mode, const double* Us, const double* U0, double
     a.gnrm = c->d_gnrm;
     a.gimm = c->d_gimm;
     a.gfsd = c->d_gfsd;
+    a.faces = c->d_faces;
+    a.nface = c->nface;
+    a.fflux = c->d_fflux;
     a.status = c->d_status;
     a.e_begin = e_begin;
     a.ne = e_end;
@@ -153,8 +165,15 @@ int launch_stage(dg_ctx* c, int mode, const double* Us, const double* U0, double
     if (rc) return rc;
     const dgk::StageVariant* vs = nullptr;
     dgk::stage_variants(c->p, &vs);
-    const int batches = (e_end - e_begin + vs[c->variant].E - 1) / vs[c->variant].E;
-    DG_CUDA(c, vs[c->variant].launch(a, std::min(c->variant_grid[c->variant], batches), c->stream));
+    const dgk::StageVariant& sv = vs[c->variant];
+    if (sv.face_launch) {
+        // every face's flux first (the stage kernel reads them); faces span the
+        // whole mesh, so face-kernel variants launch over all elements only
+        if (e_begin != 0 || e_end != c->ne) return fail(c, DG_ERR_ARG, "face-kernel variant on an element range");
+        DG_CUDA(c, sv.face_launch(a, c->variant_face_grid[c->variant], c->stream));
+    }
+    const int batches = (e_end - e_begin + sv.E - 1) / sv.E;
+    DG_CUDA(c, sv.launch(a, std::min(c->variant_grid[c->variant], batches), c->stream));
     return DG_OK;
 }
 
@@ -754,6 +773,7 @@ void release(dg_ctx* c)
     cudaFree(c->d_conn); cudaFree(c->d_frec); cudaFree(c->d_geo_class); cudaFree(c->d_geo); cudaFree(c->d_cmap);
     cudaFree(c->d_X0); cudaFree(c->d_partials); cudaFree(c->d_status);
     cudaFree(c->d_gjd); cudaFree(c->d_gnrm); cudaFree(c->d_gimm); cudaFree(c->d_gnodes); cudaFree(c->d_gfsd);
+    cudaFree(c->d_faces); cudaFree(c->d_fflux);
     cudaFree(c->d_halo_send); cudaFree(c->d_halo_recv);
     if (c->stream) cudaStreamDestroy(c->stream);
 }
@@ -975,8 +995,50 @@ int dgi::create_ctx(const dg_case_desc* cd, const dg_mesh_desc* md, const int* e
             r.nbr = nbr;
             r.info = info;
             r.cls = c->pm.geo_class[e];
-            r.pad = 0;
+            r.pad = -1;
         }
+    // launch option FX: number the interior faces by their left side; each
+    // side's record carries the face's number (unpartitioned affine contexts)
+    std::vector<int2> faces;
+    const bool face_list = !c->pm.general && c->ne == c->ne_alloc && c->ne > 0;
+    if (face_list) {
+        for (int e = 0; e < c->ne; ++e)
+            for (int f = 0; f < 6; ++f)
+                if ((frec[static_cast<size_t>(e) * 6 + f].info >> 3) & 1) {
+                    frec[static_cast<size_t>(e) * 6 + f].pad = static_cast<int>(faces.size());
+                    faces.push_back(make_int2(e, f));
+                }
+        for (int e = 0; e < c->ne; ++e)
+            for (int f = 0; f < 6; ++f) {
+                dgk::FaceRec& r = frec[static_cast<size_t>(e) * 6 + f];
+                if (!((r.info >> 3) & 1)) r.pad = frec[static_cast<size_t>(r.nbr) * 6 + (r.info & 7)].pad;
+            }
+        c->nface = static_cast<int>(faces.size());
+        // the face list and the flux buffer, when this order compiles a
+        // face-kernel variant (a failed allocation leaves those variants out)
+        const dgk::StageVariant* vs = nullptr;
+        const int nv = dgk::stage_variants(c->p, &vs);
+        bool has_fx = false;
+        for (int v = 0; v < nv; ++v) has_fx = has_fx || (vs[v].flags & dgk::kFX);
+        const size_t nflux = static_cast<size_t>(c->nface) * 5 * (c->p + 2) * (c->p + 2);
+        if (has_fx && c->nface > 0) {
+            if (cudaMalloc((void**)&c->d_faces, faces.size() * sizeof(int2)) != cudaSuccess ||
+                cudaMalloc((void**)&c->d_fflux, nflux * sizeof(double)) != cudaSuccess ||
+                cudaMemcpy(c->d_faces, faces.data(), faces.size() * sizeof(int2), cudaMemcpyHostToDevice) != cudaSuccess) {
+                cudaGetLastError();
+                cudaFree(c->d_faces);
+                cudaFree(c->d_fflux);
+                c->d_faces = nullptr;
+                c->d_fflux = nullptr;
+            }
+        }
+        // the default variant again, now that face-kernel variants may match
+        for (int v = 0; v < nv; ++v)
+            if (variant_matches(c, v)) {
+                c->variant = v;
+                break;
+            }
+    }
     std::vector<int2> hs(std::max(1, c->nslices)), hr(std::max(1, c->nslices));
     for (int i = 0; i < c->nslices; ++i) {
         hs[i] = make_int2(plan.send_elem[i], plan.send_face[i]);

@@ -14,7 +14,7 @@
 #include "dg_stage.cuh"
 
 namespace dgi {
-constexpr int kMaxVariants = 32;  // launch variants per order (checked in prepare_variant)
+constexpr int kMaxVariants = 48;  // launch variants per order (checked in prepare_variant)
 
 // NVTX range named after a C-ABI call, for timelines of Nsight tools (a no-op
 // when no tool is attached)
@@ -48,6 +48,13 @@ struct dg_ctx {
     // tables (see dgk::StageArgs) and the element nodes [ne][8][3]
     double *d_gjd = nullptr, *d_gnrm = nullptr, *d_gimm = nullptr, *d_gnodes = nullptr;
     double* d_gfsd = nullptr;  // FP32 residual on general geometry: see dgk::StageArgs::gfsd
+    // launch option FX (unpartitioned affine contexts of orders that compile
+    // FX variants): the interior faces (left element, left face) and the face
+    // kernel's fluxes [nface][5][(p+2)^2]
+    int nface = 0;
+    int2* d_faces = nullptr;
+    double* d_fflux = nullptr;
+    int variant_face_grid[dgi::kMaxVariants] = {};  // face kernel grid per FX variant
     double* d_partials = nullptr;
     unsigned* d_status = nullptr;
     int red_grid = 0;

@@ -126,6 +126,12 @@ struct StageArgs {
     // normals (taken at reference face 0's points) leave a remainder, linear
     // in the pressure, that this table restores.
     const double* gfsd;
+    // launch option FX: the interior faces as (left element, left face)
+    // [nface] and the face kernel's fluxes [nface][5][(p+2)^2] (T values, in
+    // the left element's canonical point order, weights applied, unsigned)
+    const int2* faces;
+    int nface;
+    void* fflux;
     unsigned* status;
     int e_begin, ne;        // the launch computes elements [e_begin, ne)
     int flux;               // 0 = Lax-Friedrichs, 1 = HLLC
@@ -151,11 +157,15 @@ __host__ __device__ constexpr int cmax(int a, int b) { return a > b ? a : b; }
 // flag 16 (K1) -- one face-flux point per thread and iteration (registers);
 // flag 32 (GE) -- general (trilinear) geometry: per-point metric terms and
 // normals and a dense per-element inverse mass matrix, read from global
-// memory (requires UF)
+// memory (requires UF); flag 64 (FX) -- face fluxes from the face kernel:
+// every interior face's flux is computed once (face_flux_kernel, launched
+// before the stage kernel) and each element stages its six faces' fluxes
+// instead of computing traces and fluxes (requires SB; not with GE)
 template <int P, int G, typename T = double, int FL = 0>
 struct Lay {
-    static constexpr bool PZ = FL & 1, SB = FL & 2, UF = FL & 4, RS = FL & 8, K1 = FL & 16, GE = FL & 32;
+    static constexpr bool PZ = FL & 1, SB = FL & 2, UF = FL & 4, RS = FL & 8, K1 = FL & 16, GE = FL & 32, FX = FL & 64;
     static_assert(!GE || UF, "general geometry needs the unfused volume");
+    static_assert(!FX || (SB && !GE), "face fluxes from the face kernel need the single buffer and affine geometry");
     static constexpr int N = P + 1, M = P + 2, NB = N * N * N, NF = M * M, N2 = N * N;
     static constexpr int GV = G == 1 ? 5 : (G == 2 ? 3 : 2);  // variables per group (max)
     static constexpr int GA = PZ ? 5 : GV;       // variables of the z-contraction buffers
@@ -174,9 +184,9 @@ struct Lay {
         UF ? cmax(15 * QS, 5 * QS + 5 * X1S) : 5 * X2S + cmax(5 * X1S, GA * (3 * X2S + 2 * X1S));
     static constexpr int W = odd(cmax(face, vol));
     // FP64 operand region: first the neighbours' boundary slices [30][NS]
-    // (streamed in during the volume phase), then the batch's U0 and RK
-    // accumulator [2][ES] (streamed in during the face phase)
-    static constexpr int OPS = cmax(2 * ES, 30 * NS);
+    // (with FX: the six faces' fluxes [30][FS] in T), streamed in during the
+    // volume phase, then the batch's U0 and RK accumulator [2][ES]
+    static constexpr int OPS = cmax(2 * ES, FX ? (30 * FS * (int)sizeof(T) + 7) / 8 : 30 * NS);
     // FP64: U (double-buffered prefetch, or single with SB), residual, operand region
     static constexpr int per_elem_f64 = (SB ? 1 : 2) * ES + ES + OPS;
     // bytes per element, work area in T
@@ -226,6 +236,13 @@ __device__ __forceinline__ void cp_async8(double* smem_dst, const double* gmem_s
     const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem_src) : "memory");
 }
+__device__ __forceinline__ void cp_async4(float* smem_dst, const float* gmem_src)
+{
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_t(double* d, const double* g) { cp_async8(d, g); }
+__device__ __forceinline__ void cp_async_t(float* d, const float* g) { cp_async4(d, g); }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 // all but the most recent group complete
@@ -254,6 +271,35 @@ __device__ __forceinline__ void prefetch_batch(const double* __restrict__ Us, in
         const int e = i / (5 * L::NB), r = i - e * (5 * L::NB), v = r / L::NB, b = r - v * L::NB;
         const int ge = min(e0 + e, ne - 1);
         cp_async8(dst + e * estride + v * L::VS + b, Us + (size_t)ge * 5 * L::NB + r);
+    }
+}
+
+// The numerical flux at one face point from the left and right states and
+// the left element's normal data nd = (n, |N|) (flux_functors_impl.h:168-264):
+// HLLC (euler/functions.cpp:298-399) or Lax-Friedrichs (base/functions.cpp:33-89).
+// With SHIFT (the FP32 residual) the states carry rE - eref and the constant
+// pressure (gamma-1) eref is left out of the momentum fluxes.
+template <typename T, bool SHIFT>
+__device__ __forceinline__ void numerical_flux(int flux, double gamma_d, T (&UL)[5], T (&UR)[5], const T (&nd)[4],
+                                               double eref, T (&Fo)[5], unsigned& status)
+{
+    const T gamma = T(gamma_d);
+    const T nmag = nd[3];
+    if (flux == 1) {
+        const T nu[3] = {nd[0], nd[1], nd[2]};
+        if (SHIFT) {  // HLLC takes the full energy
+            UL[4] += T(eref);
+            UR[4] += T(eref);
+        }
+        if (!dgp::flux_hllc_n(gamma, UL, UR, nu, nmag, Fo)) status |= kStatusHLLC;
+        if (SHIFT) {  // every HLLC branch carries P_side |N| n in the momenta: drop the constant part
+            const T pn = nmag * T((gamma_d - 1.0) * eref);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) Fo[1 + d] -= pn * nu[d];
+        }
+    } else {
+        const T nh[3] = {nd[0], nd[1], nd[2]};
+        dgp::flux_lax_friedrichs_fast<T, SHIFT>(gamma, UL, UR, nh, nmag, Fo, T(gamma_d * eref), T((gamma_d - 1.0) * eref));
     }
 }
 
@@ -335,24 +381,41 @@ __device__ __forceinline__ void stage_body(const StageArgs& a)
         // for the face phase, then the next batch's coefficients; one task per
         // (element, face, variable), or per slice row when the CTA has threads
         // to spare
-        constexpr int kSliceRows = NT > E * 30 ? N : 1;
-        for (int t = tid; t < E * 30 * kSliceRows; t += NT) {
-            const int row = t % kSliceRows, fv = (t / kSliceRows) % 30, e = t / (30 * kSliceRows);
-            const int v = fv % 5, f = fv / 5;
-            const FaceRec& rec = sRec[e * 6 + f];
-            const int2 c = make_int2(rec.nbr, rec.info);
-            const double* src = a.Us + ((size_t)c.x * 5 + v) * NB;
-            double* dst = sOps + e * OPS + fv * NS;
+        if constexpr (L::FX) {
+            // the six faces' fluxes, computed once per face by the face kernel:
+            // the left side reads them in its own point order, the right side
+            // through the face-point permutation (the lift applies the sign)
+            const T* gF = reinterpret_cast<const T*>(a.fflux);
+            for (int t = tid; t < E * 6 * NF; t += NT) {
+                const int c = t % NF, f = (t / NF) % 6, e = t / (6 * NF);
+                const FaceRec& rec = sRec[e * 6 + f];
+                const int pc = ((rec.info >> 3) & 1) ? c : a.cmap[(rec.info >> 4) * NF + c];
+                const T* src = gF + (size_t)rec.pad * 5 * NF + pc;
+                T* dst = reinterpret_cast<T*>(sOps + e * OPS) + f * 5 * FS + c;
 #pragma unroll
-            for (int r = 0; r < N / kSliceRows; ++r) {
-                const int b1 = row + r;
-#pragma unroll
-                for (int b0 = 0; b0 < N; ++b0) cp_async8(dst + b1 * N + b0, src + slice_index<N>(c.y & 7, b0, b1));
+                for (int v = 0; v < 5; ++v) cp_async_t(dst + v * FS, src + v * NF);
             }
-            // this face's row of the face-point permutation, shared out over the face's tasks
-            const int fm = e * 6 + f, code = c.y >> 4;
-            for (int q = v * kSliceRows + row; q < NF; q += 5 * kSliceRows) sCm[fm * NF + q] = a.cmap[code * NF + q];
-            if (fv == 0 && row == 0) sCls[e] = rec.cls;
+            for (int e = tid; e < E; e += NT) sCls[e] = sRec[e * 6].cls;
+        } else {
+            constexpr int kSliceRows = NT > E * 30 ? N : 1;
+            for (int t = tid; t < E * 30 * kSliceRows; t += NT) {
+                const int row = t % kSliceRows, fv = (t / kSliceRows) % 30, e = t / (30 * kSliceRows);
+                const int v = fv % 5, f = fv / 5;
+                const FaceRec& rec = sRec[e * 6 + f];
+                const int2 c = make_int2(rec.nbr, rec.info);
+                const double* src = a.Us + ((size_t)c.x * 5 + v) * NB;
+                double* dst = sOps + e * OPS + fv * NS;
+#pragma unroll
+                for (int r = 0; r < N / kSliceRows; ++r) {
+                    const int b1 = row + r;
+#pragma unroll
+                    for (int b0 = 0; b0 < N; ++b0) cp_async8(dst + b1 * N + b0, src + slice_index<N>(c.y & 7, b0, b1));
+                }
+                // this face's row of the face-point permutation, shared out over the face's tasks
+                const int fm = e * 6 + f, code = c.y >> 4;
+                for (int q = v * kSliceRows + row; q < NF; q += 5 * kSliceRows) sCm[fm * NF + q] = a.cmap[code * NF + q];
+                if (fv == 0 && row == 0) sCls[e] = rec.cls;
+            }
         }
         cp_async_commit();
         if (!SB && e0 + stride < a.ne)
@@ -383,6 +446,12 @@ __device__ __forceinline__ void stage_body(const StageArgs& a)
             }
         }
         __syncthreads();
+        // with FX the x pass was the coefficients' last reader: refill the
+        // single buffer with the next batch now
+        if constexpr (L::FX) {
+            if (e0 + stride < a.ne) prefetch_batch<P, G, E, NT>(a.Us, a.ne, e0 + stride, sU, ES);
+            cp_async_commit();
+        }
         for (int i = tid; i < E * 5 * N * M; i += NT) {
             const int v = i % 5, r = i / 5;
             const int qx = r % M, bz = (r / M) % N, e = r / (M * N);
@@ -660,194 +729,194 @@ __device__ __forceinline__ void stage_body(const StageArgs& a)
             }
         }
 
-        // ---- faces: the neighbours' slices have landed (the next batch's
-        //      coefficients may still be in flight) ----
-        if constexpr (SB) cp_async_wait_all();  // only the slices are in flight
-        else cp_async_wait_older();
-        __syncthreads();
-        // own and neighbour traces: one task per (element, face, variable) doing
-        // both sides, or -- when the CTA has threads to spare (high orders) --
-        // one task per side
-        constexpr bool kSplitSides = 2 * E * 30 <= NT;
-        if constexpr (L::RS) {
-            // one task per (element, side, face, variable, output row t1):
-            // r = sum_b1 B[t1][b1] s[b1][.], then row t1 = sum_b0 B[t0][b0] r[b0]
-            for (int t = tid; t < E * 60 * M; t += NT) {
-                const int t1 = t % M, r0 = t / M;
-                const int v = r0 % 5, f = (r0 / 5) % 6, side = (r0 / 30) % 2, e = r0 / 60;
-                // both sides in the own element's energy frame
-                const double sh = kShift && v == 4 ? a.geo[sRec[e * 6].cls].eref : 0.0;
-                // slice entry (b0, b1) at src[b0 * s0 + b1 * s1]
-                const double* src;
-                int s0 = 1, s1 = N;
-                if (side == 0) {
-                    const int ax = face_axis(f), sidx = face_side(f) ? N - 1 : 0;
-                    src = sU + e * ES + v * VS + (ax == 0 ? sidx : (ax == 1 ? sidx * N : sidx * N2));
-                    s0 = ax == 0 ? N : 1;
-                    s1 = ax == 2 ? N : N2;
-                } else {
-                    src = sOps + e * OPS + (f * 5 + v) * NS;
-                }
-                T r[N];
+        if constexpr (!L::FX) {
+            // ---- faces: the neighbours' slices have landed (the next batch's
+            //      coefficients may still be in flight) ----
+            if constexpr (SB) cp_async_wait_all();  // only the slices are in flight
+            else cp_async_wait_older();
+            __syncthreads();
+            // own and neighbour traces: one task per (element, face, variable) doing
+            // both sides, or -- when the CTA has threads to spare (high orders) --
+            // one task per side
+            constexpr bool kSplitSides = 2 * E * 30 <= NT;
+            if constexpr (L::RS) {
+                // one task per (element, side, face, variable, output row t1):
+                // r = sum_b1 B[t1][b1] s[b1][.], then row t1 = sum_b0 B[t0][b0] r[b0]
+                for (int t = tid; t < E * 60 * M; t += NT) {
+                    const int t1 = t % M, r0 = t / M;
+                    const int v = r0 % 5, f = (r0 / 5) % 6, side = (r0 / 30) % 2, e = r0 / 60;
+                    // both sides in the own element's energy frame
+                    const double sh = kShift && v == 4 ? a.geo[sRec[e * 6].cls].eref : 0.0;
+                    // slice entry (b0, b1) at src[b0 * s0 + b1 * s1]
+                    const double* src;
+                    int s0 = 1, s1 = N;
+                    if (side == 0) {
+                        const int ax = face_axis(f), sidx = face_side(f) ? N - 1 : 0;
+                        src = sU + e * ES + v * VS + (ax == 0 ? sidx : (ax == 1 ? sidx * N : sidx * N2));
+                        s0 = ax == 0 ? N : 1;
+                        s1 = ax == 2 ? N : N2;
+                    } else {
+                        src = sOps + e * OPS + (f * 5 + v) * NS;
+                    }
+                    T r[N];
 #pragma unroll
-                for (int b0 = 0; b0 < N; ++b0) r[b0] = T(0);
+                    for (int b0 = 0; b0 < N; ++b0) r[b0] = T(0);
 #pragma unroll
-                for (int b1 = 0; b1 < N; ++b1) {
-                    const T c = Bt[t1 * N + b1];
+                    for (int b1 = 0; b1 < N; ++b1) {
+                        const T c = Bt[t1 * N + b1];
 #pragma unroll
-                    for (int b0 = 0; b0 < N; ++b0) {
-                        const double x = src[b0 * s0 + b1 * s1];
-                        r[b0] += c * (kShift ? T(x - sh) : T(x));
+                        for (int b0 = 0; b0 < N; ++b0) {
+                            const double x = src[b0 * s0 + b1 * s1];
+                            r[b0] += c * (kShift ? T(x - sh) : T(x));
+                        }
+                    }
+                    T* o = sW + e * W + side * 30 * FS + (f * 5 + v) * FS + t1 * M;
+#pragma unroll
+                    for (int t0 = 0; t0 < M; ++t0) {
+                        T sum = T(0);
+#pragma unroll
+                        for (int b0 = 0; b0 < N; ++b0) sum += Bt[t0 * N + b0] * r[b0];
+                        o[t0] = sum;
                     }
                 }
-                T* o = sW + e * W + side * 30 * FS + (f * 5 + v) * FS + t1 * M;
+            } else if constexpr (kSplitSides) {
+                for (int t = tid; t < E * 60; t += NT) {
+                    const int v = t % 5, f = (t / 5) % 6, side = (t / 30) % 2, e = t / 60;
+                    // both sides in the own element's energy frame
+                    const double sh = kShift && v == 4 ? a.geo[sRec[e * 6].cls].eref : 0.0;
+                    T sl[N][N];
+                    if (side == 0) {
+                        const double* own = sU + e * ES + v * VS;
 #pragma unroll
-                for (int t0 = 0; t0 < M; ++t0) {
-                    T sum = T(0);
+                        for (int b1 = 0; b1 < N; ++b1)
 #pragma unroll
-                    for (int b0 = 0; b0 < N; ++b0) sum += Bt[t0 * N + b0] * r[b0];
-                    o[t0] = sum;
+                            for (int b0 = 0; b0 < N; ++b0)
+                                sl[b1][b0] =
+                                    kShift ? T(own[slice_index<N>(f, b0, b1)] - sh) : T(own[slice_index<N>(f, b0, b1)]);
+                    } else {
+                        const double* nb = sOps + e * OPS + (f * 5 + v) * NS;
+#pragma unroll
+                        for (int b1 = 0; b1 < N; ++b1)
+#pragma unroll
+                            for (int b0 = 0; b0 < N; ++b0)
+                                sl[b1][b0] = kShift ? T(nb[b1 * N + b0] - sh) : T(nb[b1 * N + b0]);
+                    }
+                    interp2d<N, M, T>(Bt, sl, sW + e * W + side * 30 * FS + (f * 5 + v) * FS);
                 }
-            }
-        } else if constexpr (kSplitSides) {
-            for (int t = tid; t < E * 60; t += NT) {
-                const int v = t % 5, f = (t / 5) % 6, side = (t / 30) % 2, e = t / 60;
-                // both sides in the own element's energy frame
-                const double sh = kShift && v == 4 ? a.geo[sRec[e * 6].cls].eref : 0.0;
-                T sl[N][N];
-                if (side == 0) {
-                    const double* own = sU + e * ES + v * VS;
-#pragma unroll
-                    for (int b1 = 0; b1 < N; ++b1)
-#pragma unroll
-                        for (int b0 = 0; b0 < N; ++b0)
-                            sl[b1][b0] =
-                                kShift ? T(own[slice_index<N>(f, b0, b1)] - sh) : T(own[slice_index<N>(f, b0, b1)]);
-                } else {
+            } else {
+                for (int t = tid; t < E * 30; t += NT) {
+                    const int v = t % 5, f = (t / 5) % 6, e = t / 30;
+                    T sn[N][N], so[N][N];
                     const double* nb = sOps + e * OPS + (f * 5 + v) * NS;
+                    const double* own = sU + e * ES + v * VS;
+                    // both sides in the own element's energy frame
+                    const double sh = kShift && v == 4 ? a.geo[sRec[e * 6].cls].eref : 0.0;
 #pragma unroll
                     for (int b1 = 0; b1 < N; ++b1)
 #pragma unroll
-                        for (int b0 = 0; b0 < N; ++b0)
-                            sl[b1][b0] = kShift ? T(nb[b1 * N + b0] - sh) : T(nb[b1 * N + b0]);
+                        for (int b0 = 0; b0 < N; ++b0) {
+                            sn[b1][b0] = kShift ? T(nb[b1 * N + b0] - sh) : T(nb[b1 * N + b0]);
+                            so[b1][b0] = kShift ? T(own[slice_index<N>(f, b0, b1)] - sh) : T(own[slice_index<N>(f, b0, b1)]);
+                        }
+                    interp2d<N, M, T>(Bt, so, sW + e * W + (f * 5 + v) * FS);
+                    interp2d<N, M, T>(Bt, sn, sW + e * W + 30 * FS + (f * 5 + v) * FS);
                 }
-                interp2d<N, M, T>(Bt, sl, sW + e * W + side * 30 * FS + (f * 5 + v) * FS);
             }
+            __syncthreads();
+            // the staging area is free: stream in this batch's RK operands (and,
+            // with SB, the next batch's coefficients: the traces were their last reader)
+            if (stage_u0) prefetch_batch<P, G, E, NT>(a.U0, a.ne, e0, sOps, OPS);
+            if (need_u0_acc) prefetch_batch<P, G, E, NT>(a.acc, a.ne, e0, sOps + ES, OPS);
+            if (SB && e0 + stride < a.ne) prefetch_batch<P, G, E, NT>(a.Us, a.ne, e0 + stride, sU, ES);
+            cp_async_commit();
+
+            // numerical flux at every face point, written over the own trace; two
+            // points per thread and iteration for instruction-level parallelism
+            {
+                constexpr int total = E * 6 * NF;
+                auto point = [&](int i, T (&Fo)[5], int& off) {
+                    const int cidx = i % NF, f = (i / NF) % 6, e = i / (6 * NF);
+                    const int fm = e * 6 + f;
+                    const FaceRec& rec = sRec[fm];
+                    const int isL = (rec.info >> 3) & 1;
+                    const int cn = sCm[fm * NF + cidx];
+                    const T* Tr = sW + e * W + f * 5 * FS;
+                    const T* Tn = sW + e * W + 30 * FS + f * 5 * FS;
+                    T UL[5], UR[5];
+#pragma unroll
+                    for (int v = 0; v < 5; ++v) {
+                        const T uo = Tr[v * FS + cidx], un = Tn[v * FS + cn];
+                        UL[v] = isL ? uo : un;  // element-wise selects keep both in registers
+                        UR[v] = isL ? un : uo;
+                    }
+                    // the left element's normal data: per face, or per face point (GE)
+                    T nd[4];
+                    if constexpr (L::GE) {
+                        const double* gn = a.gnrm + ((size_t)min(e0 + e, a.ne - 1) * 6 + f) * 4 * NF + cidx;
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) nd[k] = T(gn[k * NF]);
+                    } else {
+                        nd[0] = T(rec.n[0]);
+                        nd[1] = T(rec.n[1]);
+                        nd[2] = T(rec.n[2]);
+                        nd[3] = T(rec.nmag);
+                    }
+                    const double eref = kShift ? a.geo[sRec[e * 6].cls].eref : 0.0;
+                    numerical_flux<T, kShift>(a.flux, a.gamma, UL, UR, nd, eref, Fo, status);
+                    const T w = Wt[cidx % M] * Wt[cidx / M];
+                    const T sgn = isL ? T(-1.0) : T(1.0);
+#pragma unroll
+                    for (int v = 0; v < 5; ++v) Fo[v] = sgn * (Fo[v] * w);
+                    off = e * W + f * 5 * FS + cidx;
+                };
+                // KP independent points per thread and iteration (latency hiding)
+                constexpr int KP = kFluxPoints;
+                for (int i0 = tid; i0 < total; i0 += KP * NT) {
+                    T Fk[KP][5];
+                    int ok[KP];
+#pragma unroll
+                    for (int k = 0; k < KP; ++k) {
+                        const int ik = i0 + k * NT;
+                        point(ik < total ? ik : i0, Fk[k], ok[k]);
+                    }
+#pragma unroll
+                    for (int k = 0; k < KP; ++k)
+                        if (k == 0 || i0 + k * NT < total) {
+#pragma unroll
+                            for (int v = 0; v < 5; ++v) sW[ok[k] + v * FS] = Fk[k][v];
+                        }
+                }
+            }
+            __syncthreads();
+
+            // the face records have been read: queue the next batch's (they land
+            // before the inverse-mass pass, which waits for all copies)
+            if (e0 + stride < a.ne) prefetch_recs<E, NT>(a.frec, a.ne, e0 + stride, sRec);
+            cp_async_commit();
         } else {
-            for (int t = tid; t < E * 30; t += NT) {
-                const int v = t % 5, f = (t / 5) % 6, e = t / 30;
-                T sn[N][N], so[N][N];
-                const double* nb = sOps + e * OPS + (f * 5 + v) * NS;
-                const double* own = sU + e * ES + v * VS;
-                // both sides in the own element's energy frame
-                const double sh = kShift && v == 4 ? a.geo[sRec[e * 6].cls].eref : 0.0;
-#pragma unroll
-                for (int b1 = 0; b1 < N; ++b1)
-#pragma unroll
-                    for (int b0 = 0; b0 < N; ++b0) {
-                        sn[b1][b0] = kShift ? T(nb[b1 * N + b0] - sh) : T(nb[b1 * N + b0]);
-                        so[b1][b0] = kShift ? T(own[slice_index<N>(f, b0, b1)] - sh) : T(own[slice_index<N>(f, b0, b1)]);
-                    }
-                interp2d<N, M, T>(Bt, so, sW + e * W + (f * 5 + v) * FS);
-                interp2d<N, M, T>(Bt, sn, sW + e * W + 30 * FS + (f * 5 + v) * FS);
-            }
+            // the face fluxes have landed (the next batch's coefficients may
+            // still be in flight)
+            cp_async_wait_older();
+            __syncthreads();
         }
-        __syncthreads();
-        // the staging area is free: stream in this batch's RK operands (and,
-        // with SB, the next batch's coefficients: the traces were their last reader)
-        if (stage_u0) prefetch_batch<P, G, E, NT>(a.U0, a.ne, e0, sOps, OPS);
-        if (need_u0_acc) prefetch_batch<P, G, E, NT>(a.acc, a.ne, e0, sOps + ES, OPS);
-        if (SB && e0 + stride < a.ne) prefetch_batch<P, G, E, NT>(a.Us, a.ne, e0 + stride, sU, ES);
-        cp_async_commit();
-
-        // numerical flux at every face point, written over the own trace; two
-        // points per thread and iteration for instruction-level parallelism
-        {
-            constexpr int total = E * 6 * NF;
-            auto point = [&](int i, T (&Fo)[5], int& off) {
-                const int cidx = i % NF, f = (i / NF) % 6, e = i / (6 * NF);
-                const int fm = e * 6 + f;
-                const FaceRec& rec = sRec[fm];
-                const int isL = (rec.info >> 3) & 1;
-                const int cn = sCm[fm * NF + cidx];
-                const T* Tr = sW + e * W + f * 5 * FS;
-                const T* Tn = sW + e * W + 30 * FS + f * 5 * FS;
-                T UL[5], UR[5];
-#pragma unroll
-                for (int v = 0; v < 5; ++v) {
-                    const T uo = Tr[v * FS + cidx], un = Tn[v * FS + cn];
-                    UL[v] = isL ? uo : un;  // element-wise selects keep both in registers
-                    UR[v] = isL ? un : uo;
-                }
-                // the left element's normal data, staged with the neighbour slices
-                // the left element's normal data: per face, or per face point (GE)
-                T nd[4];
-                if constexpr (L::GE) {
-                    const double* gn = a.gnrm + ((size_t)min(e0 + e, a.ne - 1) * 6 + f) * 4 * NF + cidx;
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) nd[k] = T(gn[k * NF]);
-                } else {
-                    nd[0] = T(rec.n[0]);
-                    nd[1] = T(rec.n[1]);
-                    nd[2] = T(rec.n[2]);
-                    nd[3] = T(rec.nmag);
-                }
-                const T nmag = nd[3];
-                const double eref = kShift ? a.geo[sRec[e * 6].cls].eref : 0.0;
-                if (a.flux == 1) {
-                    const T nu[3] = {nd[0], nd[1], nd[2]};
-                    if (kShift) {  // HLLC takes the full energy
-                        UL[4] += T(eref);
-                        UR[4] += T(eref);
-                    }
-                    if (!dgp::flux_hllc_n(gamma, UL, UR, nu, nmag, Fo)) status |= kStatusHLLC;
-                    if (kShift) {  // every HLLC branch carries P_side |N| n in the momenta: drop the constant part
-                        const T pn = nmag * T((a.gamma - 1.0) * eref);
-#pragma unroll
-                        for (int d = 0; d < 3; ++d) Fo[1 + d] -= pn * nu[d];
-                    }
-                } else {
-                    const T nh[3] = {nd[0], nd[1], nd[2]};
-                    dgp::flux_lax_friedrichs_fast<T, kShift>(gamma, UL, UR, nh, nmag, Fo, T(a.gamma * eref),
-                                                             T((a.gamma - 1.0) * eref));
-                }
-                const T w = Wt[cidx % M] * Wt[cidx / M];
-                const T sgn = isL ? T(-1.0) : T(1.0);
-#pragma unroll
-                for (int v = 0; v < 5; ++v) Fo[v] = sgn * (Fo[v] * w);
-                off = e * W + f * 5 * FS + cidx;
-            };
-            // KP independent points per thread and iteration (latency hiding)
-            constexpr int KP = kFluxPoints;
-            for (int i0 = tid; i0 < total; i0 += KP * NT) {
-                T Fk[KP][5];
-                int ok[KP];
-#pragma unroll
-                for (int k = 0; k < KP; ++k) {
-                    const int ik = i0 + k * NT;
-                    point(ik < total ? ik : i0, Fk[k], ok[k]);
-                }
-#pragma unroll
-                for (int k = 0; k < KP; ++k)
-                    if (k == 0 || i0 + k * NT < total) {
-#pragma unroll
-                        for (int v = 0; v < 5; ++v) sW[ok[k] + v * FS] = Fk[k][v];
-                    }
-            }
-        }
-        __syncthreads();
-
-        // the face records have been read: queue the next batch's (they land
-        // before the inverse-mass pass, which waits for all copies)
-        if (e0 + stride < a.ne) prefetch_recs<E, NT>(a.frec, a.ne, e0 + stride, sRec);
-        cp_async_commit();
         // face lift per (element, face, variable) into Tn's space
+        // the face flux of (element e, face f): in the trace area, or with FX the
+        // face kernel's flux staged in the operand region, negated for the left side
+        auto face_flux_in = [&](int e, int f) -> const T* {
+            if constexpr (L::FX) return reinterpret_cast<const T*>(sOps + e * OPS) + f * 5 * FS;
+            else return sW + e * W + f * 5 * FS;
+        };
+        auto face_sign = [&](int e, int f) -> T {
+            if constexpr (L::FX) return ((sRec[e * 6 + f].info >> 3) & 1) ? T(-1.0) : T(1.0);
+            else return T(1.0);
+        };
         if constexpr (L::RS) {
             // one task per (element, face, variable, output row b1)
             for (int t = tid; t < E * 30 * N; t += NT) {
                 const int b1 = t % N, r0 = t / N;
                 const int v = r0 % 5, f = (r0 / 5) % 6, e = r0 / 30;
-                const T* Fq = sW + e * W + (f * 5 + v) * FS;
+                const T* Fq = face_flux_in(e, f) + v * FS;
+                const T sgn = face_sign(e, f);
                 T r[M];
 #pragma unroll
                 for (int t0 = 0; t0 < M; ++t0) r[t0] = T(0);
@@ -863,13 +932,14 @@ __device__ __forceinline__ void stage_body(const StageArgs& a)
                     T sum = T(0);
 #pragma unroll
                     for (int t0 = 0; t0 < M; ++t0) sum += Bt[t0 * N + b0] * r[t0];
-                    Lf[b0] = sum;
+                    Lf[b0] = L::FX ? sgn * sum : sum;
                 }
             }
         } else {
             for (int t = tid; t < E * 30; t += NT) {
                 const int v = t % 5, f = (t / 5) % 6, e = t / 30;
-                const T* Fq = sW + e * W + (f * 5 + v) * FS;
+                const T* Fq = face_flux_in(e, f) + v * FS;
+                const T sgn = face_sign(e, f);
                 T tmp[M][N];
 #pragma unroll
                 for (int t1 = 0; t1 < M; ++t1)
@@ -888,11 +958,19 @@ __device__ __forceinline__ void stage_body(const StageArgs& a)
                         T s = T(0);
 #pragma unroll
                         for (int t1 = 0; t1 < M; ++t1) s += Bt[t1 * N + b1] * tmp[t1][b0];
-                        Lf[b1 * N + b0] = s;
+                        Lf[b1 * N + b0] = L::FX ? sgn * s : s;
                     }
             }
         }
         __syncthreads();
+        if constexpr (L::FX) {
+            // the staged fluxes and the face records have been read: stream in this
+            // batch's RK operands and the next batch's records
+            if (stage_u0) prefetch_batch<P, G, E, NT>(a.U0, a.ne, e0, sOps, OPS);
+            if (need_u0_acc) prefetch_batch<P, G, E, NT>(a.acc, a.ne, e0, sOps + ES, OPS);
+            if (e0 + stride < a.ne) prefetch_recs<E, NT>(a.frec, a.ne, e0 + stride, sRec);
+            cp_async_commit();
+        }
         // add the six face contributions to the (FP64) residual
         for (int i = tid; i < E * 5 * NB; i += NT) {
             const int b = i % NB, v = (i / NB) % 5, e = i / (5 * NB);
@@ -1034,6 +1112,109 @@ __device__ __forceinline__ void stage_body(const StageArgs& a)
     if (status) atomicOr(a.status, status);
 }
 
+// ---- launch option FX: the face kernel ----
+// Every interior face's numerical flux, once: per batch of FB faces, both
+// sides' boundary slices (cp.async), their traces (2D interpolation), and at
+// each point of the left element's face grid the flux with the left element's
+// normal (both states in the left element's energy frame), times the point's
+// quadrature weight, written to fflux[face][5][(p+2)^2] in the left element's
+// canonical point order.  The same operations as the stage kernel's own face
+// phase (flux_functors_impl.h:168-264), done once per face instead of once per
+// side.
+template <int P>
+__host__ __device__ constexpr int face_batch() { return P <= 2 ? 16 : (P == 3 ? 8 : 4); }
+
+template <int P, typename T>
+constexpr size_t face_smem_bytes()
+{
+    using L = Lay<P, 1, T>;
+    constexpr int FB = face_batch<P>();
+    return sizeof(double) * FB * 10 * L::NS + ((sizeof(T) * FB * 10 * L::FS + 15) / 16) * 16 + FB * sizeof(FaceRec) +
+           2 * FB * sizeof(int);
+}
+
+template <int P, typename T>
+__global__ void __launch_bounds__(128) face_flux_kernel(StageArgs a)
+{
+    using L = Lay<P, 1, T>;
+    constexpr int FB = face_batch<P>(), NT = 128;
+    constexpr int N = L::N, M = L::M, NB = L::NB, NF = L::NF, NS = L::NS, FS = L::FS;
+    constexpr bool kShift = sizeof(T) == 4;
+    extern __shared__ double fsm[];
+    double* sSl = fsm;                                                              // [FB][2][5][NS]
+    T* sTr = reinterpret_cast<T*>(sSl + FB * 10 * NS);                              // [FB][2][5][FS]
+    unsigned char* tail = reinterpret_cast<unsigned char*>(sTr) + ((sizeof(T) * FB * 10 * FS + 15) / 16) * 16;
+    FaceRec* sRecL = reinterpret_cast<FaceRec*>(tail);                              // [FB] left side's record
+    int* sEL = reinterpret_cast<int*>(sRecL + FB);                                  // [FB] left element
+    int* sFL = sEL + FB;                                                            // [FB] left face
+    const T* __restrict__ Bt = TabSel<T>::B(a.tab);
+    const T* __restrict__ Wt = TabSel<T>::W(a.tab);
+    T* out = reinterpret_cast<T*>(a.fflux);
+    const int tid = threadIdx.x;
+    unsigned status = 0;
+    for (int f0 = blockIdx.x * FB; f0 < a.nface; f0 += gridDim.x * FB) {
+        __syncthreads();
+        for (int j = tid; j < FB; j += NT) {
+            const int2 fe = a.faces[min(f0 + j, a.nface - 1)];
+            sRecL[j] = a.frec[(size_t)fe.x * 6 + fe.y];
+            sEL[j] = fe.x;
+            sFL[j] = fe.y;
+        }
+        __syncthreads();
+        // both sides' boundary slices, one task per slice row
+        for (int t = tid; t < FB * 10 * N; t += NT) {
+            const int row = t % N, r0 = t / N;
+            const int v = r0 % 5, side = (r0 / 5) % 2, j = r0 / 10;
+            const FaceRec& rec = sRecL[j];
+            const int el = side == 0 ? sEL[j] : rec.nbr;
+            const int fc = side == 0 ? sFL[j] : (rec.info & 7);
+            const double* src = a.Us + ((size_t)el * 5 + v) * NB;
+            double* dst = sSl + ((j * 2 + side) * 5 + v) * NS + row * N;
+#pragma unroll
+            for (int b0 = 0; b0 < N; ++b0) cp_async8(dst + b0, src + slice_index<N>(fc, b0, row));
+        }
+        cp_async_commit();
+        cp_async_wait_all();
+        __syncthreads();
+        // traces of both sides, in the left element's energy frame
+        for (int t = tid; t < FB * 10; t += NT) {
+            const int v = t % 5, sj = t / 5;
+            const double sh = kShift && v == 4 ? a.geo[sRecL[sj / 2].cls].eref : 0.0;
+            const double* sl0 = sSl + (sj * 5 + v) * NS;
+            T sl[N][N];
+#pragma unroll
+            for (int b1 = 0; b1 < N; ++b1)
+#pragma unroll
+                for (int b0 = 0; b0 < N; ++b0) sl[b1][b0] = kShift ? T(sl0[b1 * N + b0] - sh) : T(sl0[b1 * N + b0]);
+            interp2d<N, M, T>(Bt, sl, sTr + (sj * 5 + v) * FS);
+        }
+        __syncthreads();
+        // the flux at the left element's face points
+        for (int i = tid; i < FB * NF; i += NT) {
+            const int c = i % NF, j = i / NF;
+            if (f0 + j >= a.nface) continue;
+            const FaceRec& rec = sRecL[j];
+            const int cn = a.cmap[(rec.info >> 4) * NF + c];
+            const T* TL = sTr + (j * 2) * 5 * FS;
+            const T* TR = TL + 5 * FS;
+            T UL[5], UR[5], Fo[5];
+#pragma unroll
+            for (int v = 0; v < 5; ++v) {
+                UL[v] = TL[v * FS + c];
+                UR[v] = TR[v * FS + cn];
+            }
+            const T nd[4] = {T(rec.n[0]), T(rec.n[1]), T(rec.n[2]), T(rec.nmag)};
+            const double eref = kShift ? a.geo[rec.cls].eref : 0.0;
+            numerical_flux<T, kShift>(a.flux, a.gamma, UL, UR, nd, eref, Fo, status);
+            const T w = Wt[c % M] * Wt[c / M];
+            T* o = out + (size_t)(f0 + j) * 5 * NF + c;
+#pragma unroll
+            for (int v = 0; v < 5; ++v) o[v * NF] = Fo[v] * w;
+        }
+    }
+    if (status) atomicOr(a.status, status);
+}
+
 template <int P, int E, int NT, int G, typename T, int FL>
 __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
 {
@@ -1061,12 +1242,25 @@ struct StageVariant {
     int fp32;            // 1: residual arithmetic in FP32 (mixed precision), 0: FP64
     int flags;           // 1: groups' pencils in one phase, 2: single coefficient buffer,
                          // 4: unfused volume, 8: row-split traces and lifts,
-                         // 16: one face-flux point per thread, 32: general (trilinear) geometry;
+                         // 16: one face-flux point per thread, 32: general (trilinear) geometry,
+                         // 64: face fluxes from the face kernel;
                          // bits 8..11: minimum resident CTAs asked of the compiler (0: none)
     size_t smem;         // dynamic shared memory per CTA
     const void* func;    // the kernel, for attributes / occupancy queries
     cudaError_t (*launch)(const StageArgs&, int grid, cudaStream_t);
+    // FX variants: the face kernel launched before the stage kernel (else null)
+    const void* face_func;
+    size_t face_smem;
+    int face_threads;
+    cudaError_t (*face_launch)(const StageArgs&, int grid, cudaStream_t);
 };
+
+template <int P, typename T>
+cudaError_t launch_face_kernel(const StageArgs& a, int grid, cudaStream_t s)
+{
+    face_flux_kernel<P, T><<<grid, 128, face_smem_bytes<P, T>(), s>>>(a);
+    return cudaGetLastError();
+}
 
 template <int P, int E, int NT, int G, typename T, int FL, int MB>
 cudaError_t launch_stage_variant(const StageArgs& a, int grid, cudaStream_t s)
@@ -1085,7 +1279,7 @@ cudaError_t launch_stage_variant(const StageArgs& a, int grid, cudaStream_t s)
 // parallel tasks and registers (high orders); general geometry is a property
 // of the mesh, not a tuning choice: contexts on non-affine meshes run GE
 // variants only, the others never do
-constexpr int kPZ = 1, kSB = 2, kUF = 4, kRS = 8, kK1 = 16, kGE = 32;
+constexpr int kPZ = 1, kSB = 2, kUF = 4, kRS = 8, kK1 = 16, kGE = 32, kFX = 64;
 // MB > 0: at least MB resident CTAs per SM asked of the compiler (a register cap)
 template <int P, int E, int NT, int G, typename T = double, int FL = 0, int MB = 0>
 StageVariant make_variant()
@@ -1095,8 +1289,16 @@ StageVariant make_variant()
     const void* func;
     if constexpr (MB > 0) func = (const void*)stage_kernel_mb<P, E, NT, G, T, FL, MB>;
     else func = (const void*)stage_kernel<P, E, NT, G, T, FL>;
-    return StageVariant{E, NT, G, sizeof(T) == 4 ? 1 : 0, FL | (MB << 8), stage_smem_bytes<P, E, G, T, FL>(),
-                        func, launch_stage_variant<P, E, NT, G, T, FL, MB>};
+    StageVariant v{E, NT, G, sizeof(T) == 4 ? 1 : 0, FL | (MB << 8), stage_smem_bytes<P, E, G, T, FL>(),
+                   func, launch_stage_variant<P, E, NT, G, T, FL, MB>, nullptr, 0, 0, nullptr};
+    if constexpr ((FL & 64) != 0) {
+        static_assert(face_smem_bytes<P, T>() <= 227 * 1024, "face kernel shared memory exceeds 227 KB");
+        v.face_func = (const void*)face_flux_kernel<P, T>;
+        v.face_smem = face_smem_bytes<P, T>();
+        v.face_threads = 128;
+        v.face_launch = launch_face_kernel<P, T>;
+    }
+    return v;
 }
 
 // the variants compiled for order p (defined in dg_stage_p<p>.cu)

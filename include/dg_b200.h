@@ -164,7 +164,10 @@ int dg_stage_variant_info(int order, int variant, int* elems_per_cta, int* threa
  * face-flux point per thread and iteration (fewer registers); bit 5 -- general
  * (trilinear) geometry: per-point metric terms and normals and a dense
  * inverse mass matrix per element, the variants a context on a non-affine
- * mesh runs (and the only ones it accepts); bits 8..11 -- the minimum of resident CTAs per SM the kernel was compiled
+ * mesh runs (and the only ones it accepts); bit 6 -- every interior face's
+ * flux computed once by a face kernel launched before the stage kernel (the
+ * elements read their six faces' fluxes; unpartitioned affine contexts);
+ * bits 8..11 -- the minimum of resident CTAs per SM the kernel was compiled
  * for (0: none; a register cap). */
 int dg_stage_variant_flags(int order, int variant, int* flags);
 int dg_set_stage_variant(dg_ctx* ctx, int variant);
