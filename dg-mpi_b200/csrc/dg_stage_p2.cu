@@ -10,25 +10,20 @@
 namespace dgk {
 
 static const StageVariant kVariants2[] = {
+    make_variant<2, 1, 32, 1, double, kUF | kSB | kFX>(),
+    make_variant<2, 2, 64, 1, double, kUF | kSB | kFX>(),
+    make_variant<2, 1, 64, 1, double, kUF | kRS | kSB | kFX>(),
     make_variant<2, 1, 32, 1, double, kUF>(),
     make_variant<2, 2, 64, 1, double, kUF | kRS | kSB>(),
-    make_variant<2, 1, 64, 1, double, kUF | kSB>(),
     make_variant<2, 1, 32, 1, double>(),
     make_variant<2, 2, 64, 1, double>(),
-    make_variant<2, 1, 32, 2, double>(),
-    make_variant<2, 6, 96, 1, double>(),
-    make_variant<2, 1, 32, 1, double, kUF | kSB | kFX>(),
-    make_variant<2, 1, 64, 1, double, kUF | kRS | kSB | kFX>(),
-    make_variant<2, 2, 64, 1, double, kUF | kSB | kFX>(),
+    make_variant<2, 1, 32, 1, float, kUF | kSB | kFX>(),
+    make_variant<2, 2, 64, 1, float, kUF | kSB | kFX>(),
+    make_variant<2, 1, 64, 1, float, kUF | kRS | kSB | kFX>(),
     make_variant<2, 1, 32, 1, float, kUF>(),
     make_variant<2, 2, 64, 1, float, kUF | kSB>(),
     make_variant<2, 4, 128, 1, float>(),
     make_variant<2, 1, 32, 1, float>(),
-    make_variant<2, 2, 64, 1, float>(),
-    make_variant<2, 4, 128, 1, float, kUF | kRS | kSB>(),
-    make_variant<2, 1, 32, 1, float, kUF | kSB | kFX>(),
-    make_variant<2, 1, 64, 1, float, kUF | kRS | kSB | kFX>(),
-    make_variant<2, 2, 64, 1, float, kUF | kSB | kFX>(),
     // general (trilinear) geometry: the variants of non-affine meshes
     make_variant<2, 1, 32, 1, double, kUF | kGE>(),
     make_variant<2, 1, 32, 1, float, kUF | kGE>(),

@@ -10,33 +10,26 @@
 namespace dgk {
 
 static const StageVariant kVariants3[] = {
+    make_variant<3, 1, 128, 1, double, kUF | kRS | kSB | kFX>(),
+    make_variant<3, 1, 128, 1, double, kUF | kRS | kSB | kFX, 8>(),
+    make_variant<3, 1, 96, 1, double, kUF | kRS | kSB | kFX>(),
+    make_variant<3, 1, 64, 1, double, kUF | kRS | kSB | kFX>(),
+    make_variant<3, 2, 128, 1, double, kUF | kRS | kSB | kFX>(),
+    make_variant<3, 1, 32, 1, double, kUF | kSB | kFX>(),
     make_variant<3, 1, 64, 1, double, kUF | kRS | kSB | kK1>(),
     make_variant<3, 1, 64, 1, double, kUF | kSB | kK1>(),
-    make_variant<3, 1, 64, 1, double, kUF | kRS | kSB>(),
-    make_variant<3, 1, 96, 1, double, kUF | kRS | kSB | kK1>(),
     make_variant<3, 1, 32, 2, double, kSB>(),
-    make_variant<3, 1, 32, 1, double, kUF | kSB>(),
-    make_variant<3, 1, 96, 1, double, kUF | kRS | kSB>(),
     make_variant<3, 2, 64, 2, double>(),
-    make_variant<3, 1, 32, 2, double>(),
-    make_variant<3, 1, 64, 1, double, kUF | kRS | kSB | kFX>(),
-    make_variant<3, 1, 32, 1, double, kUF | kSB | kFX>(),
-    make_variant<3, 1, 128, 1, double, kUF | kRS | kSB | kFX>(),
-    make_variant<3, 1, 96, 1, double, kUF | kRS | kSB | kFX>(),
-    make_variant<3, 2, 128, 1, double, kUF | kRS | kSB | kFX>(),
+    make_variant<3, 1, 64, 1, float, kUF | kSB | kFX>(),
+    make_variant<3, 1, 128, 1, float, kUF | kRS | kSB | kFX>(),
+    make_variant<3, 1, 64, 1, float, kUF | kRS | kSB | kFX>(),
+    make_variant<3, 1, 32, 1, float, kUF | kSB | kFX>(),
+    make_variant<3, 1, 128, 1, float, kUF | kSB | kFX>(),
     make_variant<3, 1, 32, 1, float, kUF | kSB | kK1>(),
     make_variant<3, 1, 32, 1, float, kUF | kSB>(),
     make_variant<3, 2, 64, 1, float, kUF | kSB | kK1>(),
-    make_variant<3, 1, 64, 1, float, kUF | kSB>(),
-    make_variant<3, 2, 64, 1, float, kUF | kSB>(),
-    make_variant<3, 2, 64, 2, float, kSB>(),
     make_variant<3, 1, 32, 1, float, kSB>(),
-    make_variant<3, 1, 64, 1, float, kUF | kRS | kSB>(),
     make_variant<3, 1, 32, 1, float>(),
-    make_variant<3, 1, 32, 1, float, kUF | kSB | kFX>(),
-    make_variant<3, 1, 64, 1, float, kUF | kRS | kSB | kFX>(),
-    make_variant<3, 1, 64, 1, float, kUF | kSB | kFX>(),
-    make_variant<3, 1, 128, 1, float, kUF | kRS | kSB | kFX>(),
     // general (trilinear) geometry: the variants of non-affine meshes
     make_variant<3, 1, 64, 1, double, kUF | kRS | kSB | kK1 | kGE>(),
     make_variant<3, 1, 32, 1, float, kUF | kSB | kK1 | kGE>(),

@@ -10,28 +10,21 @@
 namespace dgk {
 
 static const StageVariant kVariants4[] = {
+    make_variant<4, 1, 96, 1, double, kUF | kRS | kSB | kFX>(),
+    make_variant<4, 1, 128, 1, double, kUF | kRS | kSB | kFX>(),
+    make_variant<4, 1, 128, 1, double, kUF | kRS | kSB | kFX, 4>(),
+    make_variant<4, 1, 64, 1, double, kUF | kSB | kFX>(),
     make_variant<4, 1, 128, 1, double, kUF | kRS | kSB | kK1, 4>(),
     make_variant<4, 1, 128, 1, double, kUF | kRS | kSB | kK1>(),
     make_variant<4, 1, 96, 1, double, kUF | kRS | kSB | kK1>(),
-    make_variant<4, 1, 96, 1, double, kUF | kRS | kSB>(),
-    make_variant<4, 1, 64, 1, double, kUF | kSB>(),
-    make_variant<4, 1, 64, 1, double, kUF | kRS | kSB | kK1>(),
-    make_variant<4, 1, 128, 1, double, kUF | kRS | kSB>(),
     make_variant<4, 1, 64, 2, double>(),
-    make_variant<4, 1, 128, 1, double, kUF | kRS | kSB | kFX>(),
-    make_variant<4, 1, 96, 1, double, kUF | kRS | kSB | kFX>(),
-    make_variant<4, 1, 64, 1, double, kUF | kSB | kFX>(),
-    make_variant<4, 1, 128, 1, float, kUF | kSB>(),
-    make_variant<4, 1, 128, 1, float, kUF | kSB, 5>(),
-    make_variant<4, 1, 128, 1, float, kUF | kRS | kSB>(),
-    make_variant<4, 1, 128, 1, float, kUF | kSB | kK1>(),
-    make_variant<4, 1, 96, 1, float, kUF | kRS | kSB>(),
-    make_variant<4, 1, 64, 1, float, kUF | kSB>(),
-    make_variant<4, 1, 128, 2, float, kPZ>(),
-    make_variant<4, 1, 64, 1, float>(),
     make_variant<4, 1, 128, 1, float, kUF | kSB | kFX>(),
     make_variant<4, 1, 128, 1, float, kUF | kRS | kSB | kFX>(),
     make_variant<4, 1, 64, 1, float, kUF | kSB | kFX>(),
+    make_variant<4, 1, 128, 1, float, kUF | kSB>(),
+    make_variant<4, 1, 128, 1, float, kUF | kRS | kSB>(),
+    make_variant<4, 1, 128, 2, float, kPZ>(),
+    make_variant<4, 1, 64, 1, float>(),
     // general (trilinear) geometry: the variants of non-affine meshes
     make_variant<4, 1, 128, 1, double, kUF | kRS | kSB | kK1 | kGE>(),
     make_variant<4, 1, 128, 1, float, kUF | kSB | kGE>(),

@@ -10,25 +10,18 @@
 namespace dgk {
 
 static const StageVariant kVariants5[] = {
+    make_variant<5, 1, 256, 1, double, kUF | kRS | kSB | kFX, 2>(),
+    make_variant<5, 1, 192, 1, double, kUF | kRS | kSB | kFX>(),
+    make_variant<5, 1, 128, 1, double, kUF | kRS | kSB | kFX>(),
     make_variant<5, 1, 256, 1, double, kUF | kRS | kSB | kK1, 2>(),
     make_variant<5, 1, 128, 1, double, kUF | kRS | kSB | kK1>(),
-    make_variant<5, 1, 128, 1, double, kUF | kRS | kSB>(),
-    make_variant<5, 1, 256, 1, double, kUF | kRS | kSB | kK1>(),
-    make_variant<5, 1, 128, 1, double, kUF | kSB | kK1>(),
-    make_variant<5, 1, 128, 3, double, kRS>(),
     make_variant<5, 1, 128, 3, double>(),
-    make_variant<5, 1, 256, 1, double, kUF | kRS | kSB | kFX, 2>(),
-    make_variant<5, 1, 128, 1, double, kUF | kRS | kSB | kFX>(),
-    make_variant<5, 1, 192, 1, double, kUF | kRS | kSB | kFX>(),
-    make_variant<5, 1, 128, 1, float, kUF | kRS | kSB | kK1>(),
-    make_variant<5, 1, 256, 1, float, kUF | kRS | kSB>(),
-    make_variant<5, 1, 256, 1, float, kUF | kRS | kSB | kK1, 3>(),
-    make_variant<5, 1, 128, 1, float, kUF | kRS | kSB>(),
-    make_variant<5, 1, 128, 2, float, kSB>(),
-    make_variant<5, 1, 128, 1, float, kUF | kSB>(),
-    make_variant<5, 1, 64, 2, float>(),
-    make_variant<5, 1, 128, 1, float, kUF | kRS | kSB | kFX>(),
     make_variant<5, 1, 256, 1, float, kUF | kRS | kSB | kFX, 3>(),
+    make_variant<5, 1, 128, 1, float, kUF | kRS | kSB | kFX>(),
+    make_variant<5, 1, 256, 1, float, kUF | kRS | kSB | kK1, 3>(),
+    make_variant<5, 1, 128, 1, float, kUF | kRS | kSB | kK1>(),
+    make_variant<5, 1, 128, 2, float, kSB>(),
+    make_variant<5, 1, 64, 2, float>(),
     // general (trilinear) geometry: the variants of non-affine meshes
     make_variant<5, 1, 256, 1, double, kUF | kRS | kSB | kK1 | kGE, 2>(),
     make_variant<5, 1, 128, 1, float, kUF | kRS | kSB | kK1 | kGE>(),
