@@ -124,7 +124,7 @@ int prepare_variant(dg_ctx* c, int v)
         DG_CUDA(c, cudaFuncSetAttribute(sv.face_func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sv.face_smem));
         DG_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&face_per_sm, sv.face_func, sv.face_threads, sv.face_smem));
         if (face_per_sm < 1) return fail(c, DG_ERR_UNSUPPORTED, "face kernel does not fit on an SM");
-        const int fb = (c->p <= 2 ? 16 : (c->p == 3 ? 8 : 4));
+        const int fb = dgk::face_batch_of(c->p);
         c->variant_face_grid[v] = std::max(1, std::min((c->nface + fb - 1) / fb, dev_sms * face_per_sm));
     }
     c->variant_grid[v] = std::max(1, std::min(batches, dev_sms * per_sm));

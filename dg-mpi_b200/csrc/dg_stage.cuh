@@ -1121,8 +1121,11 @@ __device__ __forceinline__ void stage_body(const StageArgs& a)
 // canonical point order.  The same operations as the stage kernel's own face
 // phase (flux_functors_impl.h:168-264), done once per face instead of once per
 // side.
+// faces per batch and threads of the face kernel
+__host__ __device__ constexpr int face_batch_of(int p) { return p <= 2 ? 16 : (p == 3 ? 8 : 4); }
 template <int P>
-__host__ __device__ constexpr int face_batch() { return P <= 2 ? 16 : (P == 3 ? 8 : 4); }
+__host__ __device__ constexpr int face_batch() { return face_batch_of(P); }
+constexpr int kFaceThreads = 128;
 
 template <int P, typename T>
 constexpr size_t face_smem_bytes()
@@ -1134,10 +1137,10 @@ constexpr size_t face_smem_bytes()
 }
 
 template <int P, typename T>
-__global__ void __launch_bounds__(128) face_flux_kernel(StageArgs a)
+__global__ void __launch_bounds__(kFaceThreads) face_flux_kernel(StageArgs a)
 {
     using L = Lay<P, 1, T>;
-    constexpr int FB = face_batch<P>(), NT = 128;
+    constexpr int FB = face_batch<P>(), NT = kFaceThreads;
     constexpr int N = L::N, M = L::M, NB = L::NB, NF = L::NF, NS = L::NS, FS = L::FS;
     constexpr bool kShift = sizeof(T) == 4;
     extern __shared__ double fsm[];
@@ -1258,7 +1261,7 @@ struct StageVariant {
 template <int P, typename T>
 cudaError_t launch_face_kernel(const StageArgs& a, int grid, cudaStream_t s)
 {
-    face_flux_kernel<P, T><<<grid, 128, face_smem_bytes<P, T>(), s>>>(a);
+    face_flux_kernel<P, T><<<grid, kFaceThreads, face_smem_bytes<P, T>(), s>>>(a);
     return cudaGetLastError();
 }
 
@@ -1295,7 +1298,7 @@ StageVariant make_variant()
         static_assert(face_smem_bytes<P, T>() <= 227 * 1024, "face kernel shared memory exceeds 227 KB");
         v.face_func = (const void*)face_flux_kernel<P, T>;
         v.face_smem = face_smem_bytes<P, T>();
-        v.face_threads = 128;
+        v.face_threads = kFaceThreads;
         v.face_launch = launch_face_kernel<P, T>;
     }
     return v;
