@@ -998,9 +998,9 @@ int dgi::create_ctx(const dg_case_desc* cd, const dg_mesh_desc* md, const int* e
             r.pad = -1;
         }
     // launch option FX: number the interior faces by their left side; each
-    // side's record carries the face's number (unpartitioned affine contexts)
+    // side's record carries the face's number (unpartitioned contexts)
     std::vector<int2> faces;
-    const bool face_list = !c->pm.general && c->ne == c->ne_alloc && c->ne > 0;
+    const bool face_list = c->ne == c->ne_alloc && c->ne > 0;
     if (face_list) {
         for (int e = 0; e < c->ne; ++e)
             for (int f = 0; f < 6; ++f)

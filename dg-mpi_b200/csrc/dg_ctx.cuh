@@ -48,8 +48,8 @@ struct dg_ctx {
     // tables (see dgk::StageArgs) and the element nodes [ne][8][3]
     double *d_gjd = nullptr, *d_gnrm = nullptr, *d_gimm = nullptr, *d_gnodes = nullptr;
     double* d_gfsd = nullptr;  // FP32 residual on general geometry: see dgk::StageArgs::gfsd
-    // launch option FX (unpartitioned affine contexts of orders that compile
-    // FX variants): the interior faces (left element, left face) and the face
+    // launch option FX (unpartitioned contexts of orders that compile FX
+    // variants): the interior faces (left element, left face) and the face
     // kernel's fluxes [nface][5][(p+2)^2]
     int nface = 0;
     int2* d_faces = nullptr;

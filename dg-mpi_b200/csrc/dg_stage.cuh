@@ -160,12 +160,12 @@ __host__ __device__ constexpr int cmax(int a, int b) { return a > b ? a : b; }
 // memory (requires UF); flag 64 (FX) -- face fluxes from the face kernel:
 // every interior face's flux is computed once (face_flux_kernel, launched
 // before the stage kernel) and each element stages its six faces' fluxes
-// instead of computing traces and fluxes (requires SB; not with GE)
+// instead of computing traces and fluxes (requires SB)
 template <int P, int G, typename T = double, int FL = 0>
 struct Lay {
     static constexpr bool PZ = FL & 1, SB = FL & 2, UF = FL & 4, RS = FL & 8, K1 = FL & 16, GE = FL & 32, FX = FL & 64;
     static_assert(!GE || UF, "general geometry needs the unfused volume");
-    static_assert(!FX || (SB && !GE), "face fluxes from the face kernel need the single buffer and affine geometry");
+    static_assert(!FX || SB, "face fluxes from the face kernel need the single buffer");
     static constexpr int N = P + 1, M = P + 2, NB = N * N * N, NF = M * M, N2 = N * N;
     static constexpr int GV = G == 1 ? 5 : (G == 2 ? 3 : 2);  // variables per group (max)
     static constexpr int GA = PZ ? 5 : GV;       // variables of the z-contraction buffers
@@ -1136,7 +1136,8 @@ constexpr size_t face_smem_bytes()
            2 * FB * sizeof(int);
 }
 
-template <int P, typename T>
+// GEO: general geometry, the left element's normal data per face point
+template <int P, typename T, bool GEO>
 __global__ void __launch_bounds__(kFaceThreads) face_flux_kernel(StageArgs a)
 {
     using L = Lay<P, 1, T>;
@@ -1206,7 +1207,17 @@ __global__ void __launch_bounds__(kFaceThreads) face_flux_kernel(StageArgs a)
                 UL[v] = TL[v * FS + c];
                 UR[v] = TR[v * FS + cn];
             }
-            const T nd[4] = {T(rec.n[0]), T(rec.n[1]), T(rec.n[2]), T(rec.nmag)};
+            T nd[4];
+            if constexpr (GEO) {
+                const double* gn = a.gnrm + ((size_t)sEL[j] * 6 + sFL[j]) * 4 * NF + c;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) nd[k] = T(gn[k * NF]);
+            } else {
+                nd[0] = T(rec.n[0]);
+                nd[1] = T(rec.n[1]);
+                nd[2] = T(rec.n[2]);
+                nd[3] = T(rec.nmag);
+            }
             const double eref = kShift ? a.geo[rec.cls].eref : 0.0;
             numerical_flux<T, kShift>(a.flux, a.gamma, UL, UR, nd, eref, Fo, status);
             const T w = Wt[c % M] * Wt[c / M];
@@ -1258,10 +1269,10 @@ struct StageVariant {
     cudaError_t (*face_launch)(const StageArgs&, int grid, cudaStream_t);
 };
 
-template <int P, typename T>
+template <int P, typename T, bool GEO>
 cudaError_t launch_face_kernel(const StageArgs& a, int grid, cudaStream_t s)
 {
-    face_flux_kernel<P, T><<<grid, kFaceThreads, face_smem_bytes<P, T>(), s>>>(a);
+    face_flux_kernel<P, T, GEO><<<grid, kFaceThreads, face_smem_bytes<P, T>(), s>>>(a);
     return cudaGetLastError();
 }
 
@@ -1296,10 +1307,11 @@ StageVariant make_variant()
                    func, launch_stage_variant<P, E, NT, G, T, FL, MB>, nullptr, 0, 0, nullptr};
     if constexpr ((FL & 64) != 0) {
         static_assert(face_smem_bytes<P, T>() <= 227 * 1024, "face kernel shared memory exceeds 227 KB");
-        v.face_func = (const void*)face_flux_kernel<P, T>;
+        constexpr bool geo = (FL & 32) != 0;
+        v.face_func = (const void*)face_flux_kernel<P, T, geo>;
         v.face_smem = face_smem_bytes<P, T>();
         v.face_threads = kFaceThreads;
-        v.face_launch = launch_face_kernel<P, T>;
+        v.face_launch = launch_face_kernel<P, T, geo>;
     }
     return v;
 }

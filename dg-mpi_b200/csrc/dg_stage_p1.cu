@@ -14,6 +14,8 @@ static const StageVariant kVariants1[] = {
     make_variant<1, 4, 64, 1, double>(),
     make_variant<1, 2, 64, 1, double>(),
     make_variant<1, 1, 32, 1, double>(),
+    make_variant<1, 8, 128, 1, float, kUF | kSB | kFX>(),
+    make_variant<1, 4, 64, 1, float, kUF | kSB | kFX>(),
     make_variant<1, 8, 128, 1, float>(),
     make_variant<1, 4, 64, 1, float>(),
     make_variant<1, 2, 64, 1, float>(),

@@ -27,6 +27,8 @@ static const StageVariant kVariants2[] = {
     // general (trilinear) geometry: the variants of non-affine meshes
     make_variant<2, 1, 32, 1, double, kUF | kGE>(),
     make_variant<2, 1, 32, 1, float, kUF | kGE>(),
+    make_variant<2, 1, 32, 1, double, kUF | kSB | kGE | kFX>(),
+    make_variant<2, 1, 32, 1, float, kUF | kSB | kGE | kFX>(),
 };
 
 int stage_variants_p2(const StageVariant** out)

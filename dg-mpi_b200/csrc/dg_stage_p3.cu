@@ -35,6 +35,8 @@ static const StageVariant kVariants3[] = {
     make_variant<3, 1, 32, 1, float, kUF | kSB | kK1 | kGE>(),
     make_variant<3, 1, 64, 1, float, kUF | kSB | kK1 | kGE>(),
     make_variant<3, 1, 64, 1, float, kUF | kRS | kSB | kK1 | kGE>(),
+    make_variant<3, 1, 128, 1, double, kUF | kRS | kSB | kGE | kFX>(),
+    make_variant<3, 1, 128, 1, float, kUF | kSB | kGE | kFX>(),
 };
 
 int stage_variants_p3(const StageVariant** out)

@@ -29,6 +29,8 @@ static const StageVariant kVariants4[] = {
     make_variant<4, 1, 128, 1, double, kUF | kRS | kSB | kK1 | kGE>(),
     make_variant<4, 1, 128, 1, float, kUF | kSB | kGE>(),
     make_variant<4, 1, 96, 1, double, kUF | kRS | kSB | kK1 | kGE>(),
+    make_variant<4, 1, 128, 1, double, kUF | kRS | kSB | kGE | kFX>(),
+    make_variant<4, 1, 128, 1, float, kUF | kSB | kGE | kFX>(),
 };
 
 int stage_variants_p4(const StageVariant** out)

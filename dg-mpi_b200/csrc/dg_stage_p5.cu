@@ -27,6 +27,8 @@ static const StageVariant kVariants5[] = {
     make_variant<5, 1, 128, 1, float, kUF | kRS | kSB | kK1 | kGE>(),
     make_variant<5, 1, 128, 1, double, kUF | kRS | kSB | kK1 | kGE>(),
     make_variant<5, 1, 256, 1, float, kUF | kRS | kSB | kK1 | kGE, 3>(),
+    make_variant<5, 1, 256, 1, double, kUF | kRS | kSB | kGE | kFX, 2>(),
+    make_variant<5, 1, 256, 1, float, kUF | kRS | kSB | kGE | kFX, 3>(),
 };
 
 int stage_variants_p5(const StageVariant** out)
