@@ -10,9 +10,11 @@
 namespace dgk {
 
 static const StageVariant kVariants3[] = {
+    make_variant<3, 1, 128, 1, double, kUF | kSB | kFX>(),
     make_variant<3, 1, 128, 1, double, kUF | kRS | kSB | kFX>(),
     make_variant<3, 1, 128, 1, double, kUF | kRS | kSB | kFX, 8>(),
     make_variant<3, 1, 96, 1, double, kUF | kRS | kSB | kFX>(),
+    make_variant<3, 1, 96, 1, double, kUF | kSB | kFX>(),
     make_variant<3, 1, 64, 1, double, kUF | kRS | kSB | kFX>(),
     make_variant<3, 2, 128, 1, double, kUF | kRS | kSB | kFX>(),
     make_variant<3, 1, 32, 1, double, kUF | kSB | kFX>(),

@@ -10,6 +10,8 @@
 namespace dgk {
 
 static const StageVariant kVariants4[] = {
+    make_variant<4, 1, 128, 1, double, kUF | kSB | kFX, 4>(),
+    make_variant<4, 1, 96, 1, double, kUF | kSB | kFX>(),
     make_variant<4, 1, 96, 1, double, kUF | kRS | kSB | kFX>(),
     make_variant<4, 1, 128, 1, double, kUF | kRS | kSB | kFX>(),
     make_variant<4, 1, 128, 1, double, kUF | kRS | kSB | kFX, 4>(),
