@@ -13,12 +13,12 @@ static const StageVariant kVariants5[] = {
     make_variant<5, 1, 256, 1, double, kUF | kRS | kSB | kFX, 2>(),
     make_variant<5, 1, 192, 1, double, kUF | kRS | kSB | kFX>(),
     make_variant<5, 1, 128, 1, double, kUF | kRS | kSB | kFX>(),
-    make_variant<5, 1, 256, 1, float, kUF | kSB | kFX, 3>(),
     make_variant<5, 1, 256, 1, double, kUF | kRS | kSB | kK1, 2>(),
     make_variant<5, 1, 128, 1, double, kUF | kRS | kSB | kK1>(),
     make_variant<5, 1, 128, 3, double>(),
     make_variant<5, 1, 256, 1, float, kUF | kRS | kSB | kFX, 3>(),
     make_variant<5, 1, 128, 1, float, kUF | kRS | kSB | kFX>(),
+    make_variant<5, 1, 256, 1, float, kUF | kSB | kFX, 3>(),
     make_variant<5, 1, 256, 1, float, kUF | kRS | kSB | kK1, 3>(),
     make_variant<5, 1, 128, 1, float, kUF | kRS | kSB | kK1>(),
     make_variant<5, 1, 128, 2, float, kSB>(),
