@@ -167,10 +167,17 @@ int launch_stage(dg_ctx* c, int mode, const double* Us, const double* U0, double
     dgk::stage_variants(c->p, &vs);
     const dgk::StageVariant& sv = vs[c->variant];
     if (sv.face_launch) {
-        // every face's flux first (the stage kernel reads them); faces span the
-        // whole mesh, so face-kernel variants launch over all elements only
-        if (e_begin != 0 || e_end != c->ne) return fail(c, DG_ERR_ARG, "face-kernel variant on an element range");
-        DG_CUDA(c, sv.face_launch(a, c->variant_face_grid[c->variant], c->stream));
+        // the fluxes of the faces this element range is the first to need (the
+        // stage kernel reads them): all faces, the faces touching an interior
+        // element, or the rest
+        int f0 = 0, f1 = c->nface;
+        if (e_begin == 0 && e_end == c->ninterior && e_end < c->ne) f1 = c->nface_inner;
+        else if (e_begin == c->ninterior && e_begin > 0 && e_end == c->ne) f0 = c->nface_inner;
+        else if (e_begin != 0 || e_end != c->ne) return fail(c, DG_ERR_ARG, "face-kernel variant on an element range");
+        a.face_begin = f0;
+        a.nface = f1;
+        const int fb = dgk::face_batch_of(c->p);
+        if (f1 > f0) DG_CUDA(c, sv.face_launch(a, std::min(c->variant_face_grid[c->variant], (f1 - f0 + fb - 1) / fb), c->stream));
     }
     const int batches = (e_end - e_begin + sv.E - 1) / sv.E;
     DG_CUDA(c, sv.launch(a, std::min(c->variant_grid[c->variant], batches), c->stream));
@@ -997,21 +1004,35 @@ int dgi::create_ctx(const dg_case_desc* cd, const dg_mesh_desc* md, const int* e
             r.cls = c->pm.geo_class[e];
             r.pad = -1;
         }
-    // launch option FX: number the interior faces by their left side; each
-    // side's record carries the face's number (unpartitioned contexts)
+    // launch option FX: the face list.  A face between owned elements is
+    // listed by its left side, a face next to a ghost by its owned side; the
+    // faces touching an interior element come first (the interior range's
+    // launch computes them while the halo exchange is in flight), the others
+    // after.  Each owned side's record carries the face's number, with bit 30
+    // set on the listed side (it reads the flux in its own point order).
     std::vector<int2> faces;
-    const bool face_list = c->ne == c->ne_alloc && c->ne > 0;
+    const bool face_list = c->ne > 0;
     if (face_list) {
-        for (int e = 0; e < c->ne; ++e)
-            for (int f = 0; f < 6; ++f)
-                if ((frec[static_cast<size_t>(e) * 6 + f].info >> 3) & 1) {
-                    frec[static_cast<size_t>(e) * 6 + f].pad = static_cast<int>(faces.size());
-                    faces.push_back(make_int2(e, f));
-                }
+        auto rec = [&](int e, int f) -> dgk::FaceRec& { return frec[static_cast<size_t>(e) * 6 + f]; };
+        auto listed = [&](int e, int f) {
+            rec(e, f).pad = static_cast<int>(faces.size()) | (1 << 30);
+            faces.push_back(make_int2(e, f));
+        };
         for (int e = 0; e < c->ne; ++e)
             for (int f = 0; f < 6; ++f) {
-                dgk::FaceRec& r = frec[static_cast<size_t>(e) * 6 + f];
-                if (!((r.info >> 3) & 1)) r.pad = frec[static_cast<size_t>(r.nbr) * 6 + (r.info & 7)].pad;
+                const dgk::FaceRec& r = rec(e, f);
+                if (r.nbr < c->ne && ((r.info >> 3) & 1) && (e < c->ninterior || r.nbr < c->ninterior)) listed(e, f);
+            }
+        c->nface_inner = static_cast<int>(faces.size());
+        for (int e = 0; e < c->ne; ++e)
+            for (int f = 0; f < 6; ++f) {
+                const dgk::FaceRec& r = rec(e, f);
+                if (r.nbr >= c->ne || (((r.info >> 3) & 1) && e >= c->ninterior && r.nbr >= c->ninterior)) listed(e, f);
+            }
+        for (int e = 0; e < c->ne; ++e)
+            for (int f = 0; f < 6; ++f) {
+                dgk::FaceRec& r = rec(e, f);
+                if (r.nbr < c->ne && !((r.info >> 3) & 1)) r.pad = rec(r.nbr, r.info & 7).pad & 0x3fffffff;
             }
         c->nface = static_cast<int>(faces.size());
         // the face list and the flux buffer, when this order compiles a

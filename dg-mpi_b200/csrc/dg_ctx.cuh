@@ -48,10 +48,12 @@ struct dg_ctx {
     // tables (see dgk::StageArgs) and the element nodes [ne][8][3]
     double *d_gjd = nullptr, *d_gnrm = nullptr, *d_gimm = nullptr, *d_gnodes = nullptr;
     double* d_gfsd = nullptr;  // FP32 residual on general geometry: see dgk::StageArgs::gfsd
-    // launch option FX (unpartitioned contexts of orders that compile FX
-    // variants): the interior faces (left element, left face) and the face
-    // kernel's fluxes [nface][5][(p+2)^2]
-    int nface = 0;
+    // launch option FX (orders that compile FX variants): the faces, listed by
+    // the side whose point order their flux is stored in -- first the nface_inner
+    // faces that touch an interior element (computed with the interior
+    // elements, before the halo exchange ends), then the others -- and the
+    // face kernel's fluxes [nface][5][(p+2)^2]
+    int nface = 0, nface_inner = 0;
     int2* d_faces = nullptr;
     double* d_fflux = nullptr;
     int variant_face_grid[dgi::kMaxVariants] = {};  // face kernel grid per FX variant

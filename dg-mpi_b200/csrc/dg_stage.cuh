@@ -73,8 +73,9 @@ struct GeoDev {
 // One face of an owned element, built at context creation and prefetched with
 // the element's coefficients (48 bytes): the neighbour, the packed neighbour
 // face | left role << 3 | permutation code << 4 (as conn), the left element's
-// normal data (N/|N| for Lax-Friedrichs, N*(1/|N|) for HLLC, and |N|) and the
-// element's own geometry class.
+// normal data (N/|N| for Lax-Friedrichs, N*(1/|N|) for HLLC, and |N|), the
+// element's own geometry class, and (launch option FX) the face's number in
+// the face list | 1 << 30 when the flux is stored in this side's point order.
 struct FaceRec {
     double n[3];
     double nmag;
@@ -126,11 +127,12 @@ struct StageArgs {
     // normals (taken at reference face 0's points) leave a remainder, linear
     // in the pressure, that this table restores.
     const double* gfsd;
-    // launch option FX: the interior faces as (left element, left face)
-    // [nface] and the face kernel's fluxes [nface][5][(p+2)^2] (T values, in
-    // the left element's canonical point order, weights applied, unsigned)
+    // launch option FX: the faces as (element, face) of the side whose point
+    // order the flux is stored in [nface], the range [face_begin, nface) one
+    // face-kernel launch computes, and the fluxes [nface][5][(p+2)^2] (T
+    // values, weights applied, unsigned)
     const int2* faces;
-    int nface;
+    int face_begin, nface;
     void* fflux;
     unsigned* status;
     int e_begin, ne;        // the launch computes elements [e_begin, ne)
@@ -383,14 +385,15 @@ __device__ __forceinline__ void stage_body(const StageArgs& a)
         // to spare
         if constexpr (L::FX) {
             // the six faces' fluxes, computed once per face by the face kernel:
-            // the left side reads them in its own point order, the right side
-            // through the face-point permutation (the lift applies the sign)
+            // the side the flux was computed for reads it in its own point
+            // order, the other through the face-point permutation (the lift
+            // applies the sign of the element's side)
             const T* gF = reinterpret_cast<const T*>(a.fflux);
             for (int t = tid; t < E * 6 * NF; t += NT) {
                 const int c = t % NF, f = (t / NF) % 6, e = t / (6 * NF);
                 const FaceRec& rec = sRec[e * 6 + f];
-                const int pc = ((rec.info >> 3) & 1) ? c : a.cmap[(rec.info >> 4) * NF + c];
-                const T* src = gF + (size_t)rec.pad * 5 * NF + pc;
+                const int pc = ((rec.pad >> 30) & 1) ? c : a.cmap[(rec.info >> 4) * NF + c];
+                const T* src = gF + (size_t)(rec.pad & 0x3fffffff) * 5 * NF + pc;
                 T* dst = reinterpret_cast<T*>(sOps + e * OPS) + f * 5 * FS + c;
 #pragma unroll
                 for (int v = 0; v < 5; ++v) cp_async_t(dst + v * FS, src + v * NF);
@@ -1115,10 +1118,11 @@ __device__ __forceinline__ void stage_body(const StageArgs& a)
 // ---- launch option FX: the face kernel ----
 // Every interior face's numerical flux, once: per batch of FB faces, both
 // sides' boundary slices (cp.async), their traces (2D interpolation), and at
-// each point of the left element's face grid the flux with the left element's
-// normal (both states in the left element's energy frame), times the point's
-// quadrature weight, written to fflux[face][5][(p+2)^2] in the left element's
-// canonical point order.  The same operations as the stage kernel's own face
+// each point of the listed side's face grid (the left side, or an owned right
+// side facing a ghost) the flux in the reference's L/R convention with the
+// left element's normal (both states in the listed side's energy frame),
+// times the point's quadrature weight, written to fflux[face][5][(p+2)^2] in
+// the listed side's canonical point order.  The same operations as the stage kernel's own face
 // phase (flux_functors_impl.h:168-264), done once per face instead of once per
 // side.
 // faces per batch and threads of the face kernel
@@ -1148,15 +1152,15 @@ __global__ void __launch_bounds__(kFaceThreads) face_flux_kernel(StageArgs a)
     double* sSl = fsm;                                                              // [FB][2][5][NS]
     T* sTr = reinterpret_cast<T*>(sSl + FB * 10 * NS);                              // [FB][2][5][FS]
     unsigned char* tail = reinterpret_cast<unsigned char*>(sTr) + ((sizeof(T) * FB * 10 * FS + 15) / 16) * 16;
-    FaceRec* sRecL = reinterpret_cast<FaceRec*>(tail);                              // [FB] left side's record
-    int* sEL = reinterpret_cast<int*>(sRecL + FB);                                  // [FB] left element
-    int* sFL = sEL + FB;                                                            // [FB] left face
+    FaceRec* sRecL = reinterpret_cast<FaceRec*>(tail);                              // [FB] listed side's record
+    int* sEL = reinterpret_cast<int*>(sRecL + FB);                                  // [FB] listed element
+    int* sFL = sEL + FB;                                                            // [FB] listed face
     const T* __restrict__ Bt = TabSel<T>::B(a.tab);
     const T* __restrict__ Wt = TabSel<T>::W(a.tab);
     T* out = reinterpret_cast<T*>(a.fflux);
     const int tid = threadIdx.x;
     unsigned status = 0;
-    for (int f0 = blockIdx.x * FB; f0 < a.nface; f0 += gridDim.x * FB) {
+    for (int f0 = a.face_begin + blockIdx.x * FB; f0 < a.nface; f0 += gridDim.x * FB) {
         __syncthreads();
         for (int j = tid; j < FB; j += NT) {
             const int2 fe = a.faces[min(f0 + j, a.nface - 1)];
@@ -1193,19 +1197,21 @@ __global__ void __launch_bounds__(kFaceThreads) face_flux_kernel(StageArgs a)
             interp2d<N, M, T>(Bt, sl, sTr + (sj * 5 + v) * FS);
         }
         __syncthreads();
-        // the flux at the left element's face points
+        // the flux at the listed side's face points
         for (int i = tid; i < FB * NF; i += NT) {
             const int c = i % NF, j = i / NF;
             if (f0 + j >= a.nface) continue;
             const FaceRec& rec = sRecL[j];
             const int cn = a.cmap[(rec.info >> 4) * NF + c];
-            const T* TL = sTr + (j * 2) * 5 * FS;
-            const T* TR = TL + 5 * FS;
+            const int isL = (rec.info >> 3) & 1;
+            const T* To = sTr + (j * 2) * 5 * FS;  // the listed side
+            const T* Tn = To + 5 * FS;             // the other side
             T UL[5], UR[5], Fo[5];
 #pragma unroll
             for (int v = 0; v < 5; ++v) {
-                UL[v] = TL[v * FS + c];
-                UR[v] = TR[v * FS + cn];
+                const T uo = To[v * FS + c], un = Tn[v * FS + cn];
+                UL[v] = isL ? uo : un;
+                UR[v] = isL ? un : uo;
             }
             T nd[4];
             if constexpr (GEO) {
