@@ -432,8 +432,7 @@ class Case:
         (single coefficient buffer), "uf" (unfused volume), "rs" (row-split traces and lifts),
         "k1" (one face-flux point per thread), "ge" (general trilinear geometry: the variants that
         non-affine meshes run), "fx" (each face's flux once, from a face kernel launched before the
-        stage kernel; unpartitioned affine contexts), and "mb<n>" when the variant asks the compiler
-        for n resident CTAs per SM."""
+        stage kernel), and "mb<n>" when the variant asks the compiler for n resident CTAs per SM."""
         out = []
         for v in range(self._lib.dg_num_stage_variants(self.order)):
             E, NT, G, pr, fl = (ctypes.c_int() for _ in range(5))

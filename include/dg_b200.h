@@ -166,7 +166,7 @@ int dg_stage_variant_info(int order, int variant, int* elems_per_cta, int* threa
  * inverse mass matrix per element, the variants a context on a non-affine
  * mesh runs (and the only ones it accepts); bit 6 -- every interior face's
  * flux computed once by a face kernel launched before the stage kernel (the
- * elements read their six faces' fluxes; unpartitioned affine contexts);
+ * elements read their six faces' fluxes);
  * bits 8..11 -- the minimum of resident CTAs per SM the kernel was compiled
  * for (0: none; a register cap). */
 int dg_stage_variant_flags(int order, int variant, int* flags);
