@@ -1,4 +1,4 @@
-// dg_stage.cuh -- the fused DG stage kernel (sm_100a; FP64, or FP32 residual with FP64 state).
+// dg_stage.cuh -- the DG stage kernel and the face-flux kernel (sm_100a; FP64, or FP32 residual with FP64 state).
 //
 // One launch evaluates, for batches of E elements per CTA (grid-stride):
 //   face traces of the element and of its six neighbours (2D sum-factorised
@@ -13,16 +13,21 @@
 //   contravariant transform and grad-basis^T contraction
 //   (helpers.cpp:185-198, flux_functors_impl.h:46-115, tools.cpp:7-35),
 //   the inverse mass (Kronecker product of 1D inverses / det J for affine
-//   elements, replacing the dense per-element iMM of tools.cpp:124-139),
+//   elements, replacing the dense per-element iMM of tools.cpp:124-139; the
+//   dense per-element inverse itself on general trilinear elements),
 //   and the RK4 / forward-Euler stage update (stepper.cpp:23-142).
+// With the face-flux launch option a second kernel, face_flux_kernel, runs
+// before it and computes the traces and the flux of every face once; the
+// stage kernel then stages its six faces' fluxes instead.
 //
-// Every 3D contraction is sum-factorised into 1D passes over shared memory;
-// the last interpolation pass, the pointwise flux and the first divergence
-// pass are fused per (x,y) pencil in registers; traces and lifts are 2D
-// interpolations done per (element, face, variable) in registers.  Shared
-// strides are odd so that FP64 accesses of consecutive tasks avoid bank
-// conflicts.  The coefficients of the next batch are prefetched with
-// cp.async while the current batch computes.
+// Every 3D contraction is sum-factorised into 1D passes over shared memory:
+// either the last interpolation pass, the pointwise flux and the first
+// divergence pass fused per (x,y) pencil in registers, or (unfused volume)
+// separate passes over a point array holding every quadrature point; traces
+// and lifts are 2D interpolations per (element, face, variable) or per output
+// row.  Shared strides are odd so that FP64 accesses of consecutive tasks
+// avoid bank conflicts.  The coefficients of the next batch are prefetched
+// with cp.async while the current batch computes.
 #pragma once
 #include <cstdint>
 #include <type_traits>
