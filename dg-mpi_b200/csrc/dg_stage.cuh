@@ -151,6 +151,66 @@ struct StageArgs {
 __host__ __device__ constexpr int odd(int x) { return x | 1; }
 __host__ __device__ constexpr int cmax(int a, int b) { return a > b ? a : b; }
 
+// Shared-memory bank layout. A warp's FP64 access is served per half-warp
+// (16 lanes, bank pair = word % 16), an FP32 access per warp (bank = word % 32);
+// distinct words on one bank cost one wavefront each. The point-array row
+// stride and the task order of every pass below were chosen together by
+// counting the wavefronts of each pass's addresses over all strides up to 16
+// past the block size and all task orders (per order and arithmetic width).
+//
+// point-array row stride of the unfused volume
+__host__ __device__ constexpr int qs_stride(int P, int bytes)
+{
+    return P == 2 ? 79
+         : P == 3 ? (bytes == 8 ? 127 : 126)
+         : P == 4 ? (bytes == 8 ? 223 : 231)
+         : P == 5 ? (bytes == 8 ? 349 : 343)
+                  : odd((P + 2) * (P + 2) * (P + 2));
+}
+// Task orders. Two coordinates: 0 = the first one varies fastest, 1 = the
+// second. Three coordinates (c0, c1, c2): O = f + 3 m + 9 s names the fastest,
+// middle and slowest one.
+template <int P, int BYTES>
+struct TaskOrd {
+    static constexpr bool W8 = BYTES == 8;
+    static constexpr int x = P >= 3 || (P == 2 && !W8) ? 1 : 0;                                 // (v, byz)
+    static constexpr int y = P == 2 ? 11 : P == 3 ? 5 : P == 4 ? (W8 ? 5 : 21) : P == 5 ? (W8 ? 21 : 11) : 21;  // (v, qx, bz)
+    static constexpr int z = P == 5 && W8 ? 1 : 0;                                              // (qxy, v)
+    static constexpr int zc = P == 2 ? (W8 ? 0 : 1) : P == 3 ? 1 : P == 4 ? (W8 ? 1 : 0) : 0;  // (qxy, v)
+    static constexpr int yc = P == 2 ? (W8 ? 21 : 11) : P == 3 ? (W8 ? 21 : 5) : P == 4 ? (W8 ? 21 : 11)
+                            : P == 5 ? (W8 ? 19 : 21) : 7;                                      // (v, qx, bz)
+    static constexpr int xc = P >= 3 || (P == 2 && !W8) ? 1 : 0;                                // (v, byz)
+    static constexpr int gather = P == 4 ? 1 : 0;                                               // (b, v)
+    static constexpr int minvx = P >= 2 ? 1 : 0;                                                // (v, byz)
+    static constexpr int minvy = P == 2 || P == 4 ? 11 : P == 3 || P == 5 ? 7 : 21;             // (v, bx, bz)
+};
+template <int O, int n0, int n1>
+__device__ __forceinline__ void task2(int r, int& c0, int& c1)
+{
+    if constexpr (O == 0) {
+        c0 = r % n0;
+        c1 = r / n0;
+    } else {
+        c1 = r % n1;
+        c0 = r / n1;
+    }
+}
+template <int O, int n0, int n1, int n2>
+__device__ __forceinline__ void task3(int r, int& c0, int& c1, int& c2)
+{
+    constexpr int f = O % 3, m = (O / 3) % 3, s = O / 9;
+    static_assert(f != m && m != s && f != s, "task order must name three coordinates");
+    constexpr int n[3] = {n0, n1, n2};
+    constexpr int nf = n[f], nm = n[m];
+    int c[3];
+    c[f] = r % nf;
+    c[m] = (r / nf) % nm;
+    c[s] = r / (nf * nm);
+    c0 = c[0];
+    c1 = c[1];
+    c2 = c[2];
+}
+
 // G = number of variable groups of the fused pointwise phase (register budget);
 // T = arithmetic of the residual (the work area W holds T values, everything
 // else FP64); FL: launch options, flag 1 (PZ) -- the groups' pencil tasks run in
@@ -182,7 +242,18 @@ struct Lay {
     static constexpr int NS = odd(N2);           // per-(face, variable) stride of neighbour slices
     static constexpr int X1S = odd(N2 * M);      // [bz][by][qx] block
     static constexpr int X2S = odd(N * NF);      // [bz][qy][qx] block
-    static constexpr int QS = odd(M * NF);       // [qz][qy][qx] block of the point array (UF)
+    static constexpr int QS = qs_stride(P, sizeof(T));  // [qz][qy][qx] block of the point array (UF)
+    // word of coefficient (bx, by, bz) in a variable's block of U / residual /
+    // U0 / accumulator: at p = 3 the rows are rotated so that every axis-aligned
+    // plane of the 4x4x4 block falls on 16 distinct bank pairs (the x, y and z
+    // pencils of a variable, 16 to a half-warp, are then conflict-free);
+    // otherwise x fastest
+    static constexpr bool SWZ = N == 4;
+    __host__ __device__ static constexpr int cw(int bx, int by, int bz)
+    {
+        return SWZ ? 16 * by + 4 * ((bx + by) & 3) + ((bz + bx) & 3) : (bz * N + by) * N + bx;
+    }
+    __host__ __device__ static constexpr int cwl(int b) { return SWZ ? cw(b % N, (b / N) % N, b / N2) : b; }
     // per-element work area: face phase {Tr[6][5], Tn[6][5]} x FS;
     // volume phase X2[5] | (X1[5] or A[GA][3] + C[GA][2]), or with UF the
     // point array Q[15] (X2 in its first five rows, X1 after them)
@@ -277,7 +348,7 @@ __device__ __forceinline__ void prefetch_batch(const double* __restrict__ Us, in
     for (int i = threadIdx.x; i < E * 5 * L::NB; i += NT) {
         const int e = i / (5 * L::NB), r = i - e * (5 * L::NB), v = r / L::NB, b = r - v * L::NB;
         const int ge = min(e0 + e, ne - 1);
-        cp_async8(dst + e * estride + v * L::VS + b, Us + (size_t)ge * 5 * L::NB + r);
+        cp_async8(dst + e * estride + v * L::VS + L::cwl(b), Us + (size_t)ge * 5 * L::NB + r);
     }
 }
 
@@ -344,6 +415,7 @@ __device__ __forceinline__ void stage_body(const StageArgs& a)
     constexpr int N = L::N, M = L::M, NB = L::NB, NF = L::NF, N2 = L::N2;
     constexpr int VS = L::VS, ES = L::ES, FS = L::FS, NS = L::NS, X1S = L::X1S, X2S = L::X2S, W = L::W, GV = L::GV;
     constexpr int OPS = L::OPS;
+    using TO = TaskOrd<P, sizeof(T)>;
     extern __shared__ double smem[];
     double* sUbuf = smem;                  // [2][E][ES] ([1][E][ES] with SB)
     double* sRes = sUbuf + (SB ? 1 : 2) * E * ES;  // [E][ES]
@@ -438,12 +510,18 @@ __device__ __forceinline__ void stage_body(const StageArgs& a)
         T* X2 = sW;
         T* X1 = sW + 5 * X2V;
         for (int i = tid; i < E * 5 * N2; i += NT) {
-            const int v = i % 5, byz = (i / 5) % N2, e = i / (5 * N2);
-            const double* u = sU + e * ES + v * VS + byz * N;
+            const int e = i / (5 * N2);
+            int v, byz;
+            task2<TO::x, 5, N2>(i - e * 5 * N2, v, byz);
+            const double* u = sU + e * ES + v * VS;
+            const int by = byz % N, bz = byz / N;
             const double sh = kShift && v == 4 ? a.geo[sRec[e * 6].cls].eref : 0.0;
             T row[N];
 #pragma unroll
-            for (int bx = 0; bx < N; ++bx) row[bx] = kShift ? T(u[bx] - sh) : T(u[bx]);
+            for (int bx = 0; bx < N; ++bx) {
+                const double ub = u[L::cw(bx, by, bz)];
+                row[bx] = kShift ? T(ub - sh) : T(ub);
+            }
             T* o = X1 + e * W + v * X1S + byz * M;
 #pragma unroll
             for (int qx = 0; qx < M; ++qx) {
@@ -461,8 +539,9 @@ __device__ __forceinline__ void stage_body(const StageArgs& a)
             cp_async_commit();
         }
         for (int i = tid; i < E * 5 * N * M; i += NT) {
-            const int v = i % 5, r = i / 5;
-            const int qx = r % M, bz = (r / M) % N, e = r / (M * N);
+            const int e = i / (5 * N * M);
+            int v, qx, bz;
+            task3<TO::y, 5, M, N>(i - e * 5 * N * M, v, qx, bz);
             const T* x1 = X1 + e * W + v * X1S + bz * N * M + qx;
             T col[N];
 #pragma unroll
@@ -485,7 +564,9 @@ __device__ __forceinline__ void stage_body(const StageArgs& a)
             T* Q = sW;  // per element: [15][QS], point index qz*NF + qy*M + qx
             // z interpolation in place: each task owns one (variable, x-y point) column
             for (int i = tid; i < E * 5 * NF; i += NT) {
-                const int qxy = i % NF, v = (i / NF) % 5, e = i / (5 * NF);
+                const int e = i / (5 * NF);
+                int qxy, v;
+                task2<TO::z, NF, 5>(i - e * 5 * NF, qxy, v);
                 T* o = Q + e * W + v * QS + qxy;
                 T col[N];
 #pragma unroll
@@ -536,7 +617,9 @@ __device__ __forceinline__ void stage_body(const StageArgs& a)
             // z contraction per (variable, x-y point), the three directions together:
             // A_d = Bz^T G_d (d = 0, 1), A_2 = Dz^T G_2, written over the column
             for (int i = tid; i < E * 5 * NF; i += NT) {
-                const int qxy = i % NF, v = (i / NF) % 5, e = i / (5 * NF);
+                const int e = i / (5 * NF);
+                int qxy, v;
+                task2<TO::zc, NF, 5>(i - e * 5 * NF, qxy, v);
                 T* g = Q + e * W + (v * 3) * QS + qxy;
                 T a0[N], a1[N], a2[N];
 #pragma unroll
@@ -562,7 +645,9 @@ __device__ __forceinline__ void stage_body(const StageArgs& a)
             // y contraction per (variable, bz, qx): C0 = By^T A0 into row 3v,
             // C12 = Dy^T A1 + By^T A2 into row 3v+1
             for (int i = tid; i < E * 5 * N * M; i += NT) {
-                const int qx = i % M, bz = (i / M) % N, v = (i / (M * N)) % 5, e = i / (5 * N * M);
+                const int e = i / (5 * N * M);
+                int v, qx, bz;
+                task3<TO::yc, 5, M, N>(i - e * 5 * N * M, v, qx, bz);
                 T* A0 = Q + e * W + (v * 3) * QS + bz * NF + qx;
                 const T* A1 = A0 + QS;
                 const T* A2 = A1 + QS;
@@ -587,7 +672,9 @@ __device__ __forceinline__ void stage_body(const StageArgs& a)
             __syncthreads();
             // x contraction into the (FP64) residual: res = Dx^T C0 + Bx^T C12
             for (int i = tid; i < E * 5 * N2; i += NT) {
-                const int v = i % 5, byz = (i / 5) % N2, e = i / (5 * N2);
+                const int e = i / (5 * N2);
+                int v, byz;
+                task2<TO::xc, 5, N2>(i - e * 5 * N2, v, byz);
                 const T* C0 = Q + e * W + (v * 3) * QS + (byz / N) * NF + (byz % N) * M;
                 const T* C12 = C0 + QS;
                 T r[N];
@@ -599,9 +686,9 @@ __device__ __forceinline__ void stage_body(const StageArgs& a)
 #pragma unroll
                     for (int bx = 0; bx < N; ++bx) r[bx] += Dt[qx * N + bx] * c0 + Bt[qx * N + bx] * c12;
                 }
-                double* res = sRes + e * ES + v * VS + byz * N;
+                double* res = sRes + e * ES + v * VS;
 #pragma unroll
-                for (int bx = 0; bx < N; ++bx) res[bx] = double(r[bx]);
+                for (int bx = 0; bx < N; ++bx) res[L::cw(bx, byz % N, byz / N)] = double(r[bx]);
             }
             __syncthreads();
         } else {
@@ -712,9 +799,9 @@ __device__ __forceinline__ void stage_body(const StageArgs& a)
 #pragma unroll
                         for (int bx = 0; bx < N; ++bx) r[bx] += Dt[qx * N + bx] * c0 + Bt[qx * N + bx] * c12;
                     }
-                    double* res = sRes + e * ES + (v0 + vv) * VS + byz * N;
+                    double* res = sRes + e * ES + (v0 + vv) * VS;
 #pragma unroll
-                    for (int bx = 0; bx < N; ++bx) res[bx] = double(r[bx]);
+                    for (int bx = 0; bx < N; ++bx) res[L::cw(bx, byz % N, byz / N)] = double(r[bx]);
                 }
                 __syncthreads();
             };
@@ -756,11 +843,13 @@ __device__ __forceinline__ void stage_body(const StageArgs& a)
                     // both sides in the own element's energy frame
                     const double sh = kShift && v == 4 ? a.geo[sRec[e * 6].cls].eref : 0.0;
                     // slice entry (b0, b1) at src[b0 * s0 + b1 * s1]
+                    // (own side: coefficient index o0 + b0 * s0 + b1 * s1 in the block's layout)
                     const double* src;
-                    int s0 = 1, s1 = N;
+                    int s0 = 1, s1 = N, o0 = 0;
                     if (side == 0) {
                         const int ax = face_axis(f), sidx = face_side(f) ? N - 1 : 0;
-                        src = sU + e * ES + v * VS + (ax == 0 ? sidx : (ax == 1 ? sidx * N : sidx * N2));
+                        src = sU + e * ES + v * VS;
+                        o0 = ax == 0 ? sidx : (ax == 1 ? sidx * N : sidx * N2);
                         s0 = ax == 0 ? N : 1;
                         s1 = ax == 2 ? N : N2;
                     } else {
@@ -774,7 +863,8 @@ __device__ __forceinline__ void stage_body(const StageArgs& a)
                         const T c = Bt[t1 * N + b1];
 #pragma unroll
                         for (int b0 = 0; b0 < N; ++b0) {
-                            const double x = src[b0 * s0 + b1 * s1];
+                            const int k = o0 + b0 * s0 + b1 * s1;
+                            const double x = src[side == 0 ? L::cwl(k) : k];
                             r[b0] += c * (kShift ? T(x - sh) : T(x));
                         }
                     }
@@ -800,7 +890,7 @@ __device__ __forceinline__ void stage_body(const StageArgs& a)
 #pragma unroll
                             for (int b0 = 0; b0 < N; ++b0)
                                 sl[b1][b0] =
-                                    kShift ? T(own[slice_index<N>(f, b0, b1)] - sh) : T(own[slice_index<N>(f, b0, b1)]);
+                                    kShift ? T(own[L::cwl(slice_index<N>(f, b0, b1))] - sh) : T(own[L::cwl(slice_index<N>(f, b0, b1))]);
                     } else {
                         const double* nb = sOps + e * OPS + (f * 5 + v) * NS;
 #pragma unroll
@@ -824,7 +914,7 @@ __device__ __forceinline__ void stage_body(const StageArgs& a)
 #pragma unroll
                         for (int b0 = 0; b0 < N; ++b0) {
                             sn[b1][b0] = kShift ? T(nb[b1 * N + b0] - sh) : T(nb[b1 * N + b0]);
-                            so[b1][b0] = kShift ? T(own[slice_index<N>(f, b0, b1)] - sh) : T(own[slice_index<N>(f, b0, b1)]);
+                            so[b1][b0] = kShift ? T(own[L::cwl(slice_index<N>(f, b0, b1))] - sh) : T(own[L::cwl(slice_index<N>(f, b0, b1))]);
                         }
                     interp2d<N, M, T>(Bt, so, sW + e * W + (f * 5 + v) * FS);
                     interp2d<N, M, T>(Bt, sn, sW + e * W + 30 * FS + (f * 5 + v) * FS);
@@ -981,7 +1071,9 @@ __device__ __forceinline__ void stage_body(const StageArgs& a)
         }
         // add the six face contributions to the (FP64) residual
         for (int i = tid; i < E * 5 * NB; i += NT) {
-            const int b = i % NB, v = (i / NB) % 5, e = i / (5 * NB);
+            const int e = i / (5 * NB);
+            int b, v;
+            task2<TO::gather, NB, 5>(i - e * 5 * NB, b, v);
             const int bc[3] = {b % N, (b / N) % N, b / N2};
             const T* Lf = sW + e * W + 30 * FS + v * FS;
             double s = 0.0;
@@ -998,14 +1090,14 @@ __device__ __forceinline__ void stage_body(const StageArgs& a)
                     s += double(Lf[f * 5 * FS + b1 * N + b0]);
                 }
             }
-            sRes[e * ES + v * VS + b] += s;
+            sRes[e * ES + v * VS + L::cw(bc[0], bc[1], bc[2])] += s;
         }
         __syncthreads();
 
         if (a.mode == kModeResidual) {
             for (int i = tid; i < E * 5 * NB; i += NT) {
                 const int e = i / (5 * NB), r = i - e * (5 * NB), v = r / NB, b = r - v * NB;
-                if (e0 + e < a.ne) a.out[(size_t)e0 * 5 * NB + i] = sRes[e * ES + v * VS + b];
+                if (e0 + e < a.ne) a.out[(size_t)e0 * 5 * NB + i] = sRes[e * ES + v * VS + L::cwl(b)];
             }
             continue;
         }
@@ -1023,20 +1115,25 @@ __device__ __forceinline__ void stage_body(const StageArgs& a)
                 const double* im = a.gimm + (size_t)ge * NB * NB + j;  // iMM[j][k] at im[k * NB]
                 const double* r = sRes + e * ES;
                 double s[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-#pragma unroll 16
-                for (int k = 0; k < NB; ++k) {
-                    const double mk = im[(size_t)k * NB];
+                for (int kz = 0; kz < N; ++kz)
 #pragma unroll
-                    for (int v = 0; v < 5; ++v) s[v] += mk * r[v * VS + k];
-                }
+                    for (int ky = 0; ky < N; ++ky)
+#pragma unroll
+                        for (int kx = 0; kx < N; ++kx) {
+                            const double mk = im[(size_t)((kz * N + ky) * N + kx) * NB];
+                            const int kw = L::cw(kx, ky, kz);
+#pragma unroll
+                            for (int v = 0; v < 5; ++v) s[v] += mk * r[v * VS + kw];
+                        }
                 const double scale = a.dt * a.geo[sCls[e]].dtf;
 #pragma unroll
                 for (int v = 0; v < 5; ++v) {
                     const double kk = scale * s[v];
                     const size_t gi = (size_t)ge * 5 * NB + (size_t)v * NB + j;
                     // step-start state: the prefetched U0, or the stage state itself in RK1 / FE
-                    const double u0 = stage_u0 ? sOps[e * OPS + v * VS + j] : sU[e * ES + v * VS + j];
-                    const double ac = sOps[e * OPS + ES + v * VS + j];
+                    const int jw = L::cwl(j);
+                    const double u0 = stage_u0 ? sOps[e * OPS + v * VS + jw] : sU[e * ES + v * VS + jw];
+                    const double ac = sOps[e * OPS + ES + v * VS + jw];
                     switch (a.mode) {
                         case kModeMassInv: a.out[gi] = kk; break;
                         case kModeRK1: a.acc[gi] = kk; a.out[gi] = 0.5 * kk + u0; break;
@@ -1050,33 +1147,37 @@ __device__ __forceinline__ void stage_body(const StageArgs& a)
         } else {
             // ---- inverse mass (FP64): x and y passes in place, z pass fused with the update ----
             for (int i = tid; i < E * 5 * N2; i += NT) {
-                const int v = i % 5, byz = (i / 5) % N2, e = i / (5 * N2);
-                double* r = sRes + e * ES + v * VS + byz * N;  // pencil along x
+                const int e = i / (5 * N2);
+                int v, byz;
+                task2<TO::minvx, 5, N2>(i - e * 5 * N2, v, byz);
+                const int by = byz % N, bz = byz / N;
+                double* r = sRes + e * ES + v * VS;  // pencil along x
                 double t[N];
 #pragma unroll
-                for (int k = 0; k < N; ++k) t[k] = r[k];
+                for (int k = 0; k < N; ++k) t[k] = r[L::cw(k, by, bz)];
 #pragma unroll
                 for (int j = 0; j < N; ++j) {
                     double s = 0.0;
 #pragma unroll
                     for (int k = 0; k < N; ++k) s += Mi[j * N + k] * t[k];
-                    r[j] = s;
+                    r[L::cw(j, by, bz)] = s;
                 }
             }
             __syncthreads();
             for (int i = tid; i < E * 5 * N2; i += NT) {
-                // (element, variable) fastest: consecutive threads are VS apart (odd)
-                const int ev = i % (5 * E), bxz = i / (5 * E), bx = bxz % N, bz = bxz / N;
-                double* r = sRes + (ev / 5) * ES + (ev % 5) * VS + bz * N2 + bx;  // pencil along y
+                const int e = i / (5 * N2);
+                int v, bx, bz;
+                task3<TO::minvy, 5, N, N>(i - e * 5 * N2, v, bx, bz);
+                double* r = sRes + e * ES + v * VS;  // pencil along y
                 double t[N];
 #pragma unroll
-                for (int k = 0; k < N; ++k) t[k] = r[k * N];
+                for (int k = 0; k < N; ++k) t[k] = r[L::cw(bx, k, bz)];
 #pragma unroll
                 for (int j = 0; j < N; ++j) {
                     double s = 0.0;
 #pragma unroll
                     for (int k = 0; k < N; ++k) s += Mi[j * N + k] * t[k];
-                    r[j * N] = s;
+                    r[L::cw(bx, j, bz)] = s;
                 }
             }
             cp_async_wait_all();  // this batch's U0 / accumulator have landed
@@ -1088,14 +1189,16 @@ __device__ __forceinline__ void stage_body(const StageArgs& a)
                 const GeoDev& gg = a.geo[sCls[e]];
                 const double scale = a.dt * gg.dtf * gg.inv_djac;
                 const int v = ev % 5;
-                const double* r = sRes + e * ES + v * VS + bxy;  // pencil along z
+                // pencil along z: (bx, by, k) at word L::cw(bx, by, k) of each block
+                const int bx = bxy % N, by = bxy / N;
+                const double* r = sRes + e * ES + v * VS;
                 // step-start state: the prefetched U0, or the stage state itself in
                 // RK1 / FE where the two coincide
-                const double* u0 = (stage_u0 ? sOps + e * OPS : sU + e * ES) + v * VS + bxy;
-                const double* ac = sOps + e * OPS + ES + v * VS + bxy;
+                const double* u0 = (stage_u0 ? sOps + e * OPS : sU + e * ES) + v * VS;
+                const double* ac = sOps + e * OPS + ES + v * VS;
                 double t[N];
 #pragma unroll
-                for (int k = 0; k < N; ++k) t[k] = r[k * N2];
+                for (int k = 0; k < N; ++k) t[k] = r[L::cw(bx, by, k)];
                 const size_t gbase = (size_t)e0 * 5 * NB + (size_t)ev * NB + bxy;
 #pragma unroll
                 for (int j = 0; j < N; ++j) {
@@ -1104,13 +1207,14 @@ __device__ __forceinline__ void stage_body(const StageArgs& a)
                     for (int k = 0; k < N; ++k) s += Mi[j * N + k] * t[k];
                     const double kk = scale * s;
                     const size_t gi = gbase + (size_t)j * N2;
+                    const int jw = L::cw(bx, by, j);
                     switch (a.mode) {
                         case kModeMassInv: a.out[gi] = kk; break;
-                        case kModeRK1: a.acc[gi] = kk; a.out[gi] = 0.5 * kk + u0[j * N2]; break;
-                        case kModeRK2: a.acc[gi] = ac[j * N2] + 2.0 * kk; a.out[gi] = 0.5 * kk + u0[j * N2]; break;
-                        case kModeRK3: a.acc[gi] = ac[j * N2] + 2.0 * kk; a.out[gi] = 1.0 * kk + u0[j * N2]; break;
-                        case kModeRK4: a.out[gi] = u0[j * N2] + (1.0 / 6.0) * (ac[j * N2] + kk); break;
-                        default: a.out[gi] = u0[j * N2] + 1.0 * kk; break;
+                        case kModeRK1: a.acc[gi] = kk; a.out[gi] = 0.5 * kk + u0[jw]; break;
+                        case kModeRK2: a.acc[gi] = ac[jw] + 2.0 * kk; a.out[gi] = 0.5 * kk + u0[jw]; break;
+                        case kModeRK3: a.acc[gi] = ac[jw] + 2.0 * kk; a.out[gi] = 1.0 * kk + u0[jw]; break;
+                        case kModeRK4: a.out[gi] = u0[jw] + (1.0 / 6.0) * (ac[jw] + kk); break;
+                        default: a.out[gi] = u0[jw] + 1.0 * kk; break;
                     }
                 }
             }
