@@ -25,8 +25,9 @@
 // divergence pass fused per (x,y) pencil in registers, or (unfused volume)
 // separate passes over a point array holding every quadrature point; traces
 // and lifts are 2D interpolations per (element, face, variable) or per output
-// row.  Shared strides are odd so that FP64 accesses of consecutive tasks
-// avoid bank conflicts.  The coefficients of the next batch are prefetched
+// row.  Shared strides, task orders and (at p = 3) a row rotation of the
+// coefficient blocks are chosen against bank conflicts (see qs_stride,
+// TaskOrd and Lay::cw).  The coefficients of the next batch are prefetched
 // with cp.async while the current batch computes.
 #pragma once
 #include <cstdint>
@@ -254,6 +255,30 @@ struct Lay {
         return SWZ ? 16 * by + 4 * ((bx + by) & 3) + ((bz + bx) & 3) : (bz * N + by) * N + bx;
     }
     __host__ __device__ static constexpr int cwl(int b) { return SWZ ? cw(b % N, (b / N) % N, b / N2) : b; }
+    // cw is a bijection of the block onto words 0 .. NB-1 and, rotated, every
+    // axis-aligned plane covers all 16 bank pairs
+    static constexpr bool cw_ok()
+    {
+        bool word[NB] = {};
+        for (int b = 0; b < NB; ++b) {
+            const int w = cwl(b);
+            if (w < 0 || w >= NB || word[w]) return false;
+            word[w] = true;
+        }
+        if (SWZ)
+            for (int ax = 0; ax < 3; ++ax)
+                for (int k = 0; k < N; ++k) {
+                    bool bank[16] = {};
+                    for (int i = 0; i < N; ++i)
+                        for (int j = 0; j < N; ++j) {
+                            const int w = ax == 0 ? cw(k, i, j) : (ax == 1 ? cw(i, k, j) : cw(i, j, k));
+                            if (bank[w % 16]) return false;
+                            bank[w % 16] = true;
+                        }
+                }
+        return true;
+    }
+    static_assert(cw_ok(), "coefficient block layout must be a bijection (and plane-conflict-free when rotated)");
     // per-element work area: face phase {Tr[6][5], Tn[6][5]} x FS;
     // volume phase X2[5] | (X1[5] or A[GA][3] + C[GA][2]), or with UF the
     // point array Q[15] (X2 in its first five rows, X1 after them)
@@ -1226,7 +1251,8 @@ __device__ __forceinline__ void stage_body(const StageArgs& a)
 
 // ---- launch option FX: the face kernel ----
 // Every interior face's numerical flux, once: per batch of FB faces, both
-// sides' boundary slices (cp.async), their traces (2D interpolation), and at
+// sides' boundary slices (gathered from the state into registers, one task per
+// face side and variable), their traces (2D interpolation), and at
 // each point of the listed side's face grid (the left side, or an owned right
 // side facing a ghost) the flux in the reference's L/R convention with the
 // left element's normal (both states in the listed side's energy frame),
@@ -1235,7 +1261,7 @@ __device__ __forceinline__ void stage_body(const StageArgs& a)
 // phase (flux_functors_impl.h:168-264), done once per face instead of once per
 // side.
 // faces per batch and threads of the face kernel
-__host__ __device__ constexpr int face_batch_of(int p) { return p <= 2 ? 16 : (p == 3 ? 8 : 4); }
+__host__ __device__ constexpr int face_batch_of(int p) { return p <= 3 ? 16 : 8; }
 template <int P>
 __host__ __device__ constexpr int face_batch() { return face_batch_of(P); }
 constexpr int kFaceThreads = 128;
@@ -1245,8 +1271,7 @@ constexpr size_t face_smem_bytes()
 {
     using L = Lay<P, 1, T>;
     constexpr int FB = face_batch<P>();
-    return sizeof(double) * FB * 10 * L::NS + ((sizeof(T) * FB * 10 * L::FS + 15) / 16) * 16 + FB * sizeof(FaceRec) +
-           2 * FB * sizeof(int);
+    return ((sizeof(T) * FB * 10 * L::FS + 15) / 16) * 16 + FB * sizeof(FaceRec) + 2 * FB * sizeof(int);
 }
 
 // GEO: general geometry, the left element's normal data per face point
@@ -1255,11 +1280,10 @@ __global__ void __launch_bounds__(kFaceThreads) face_flux_kernel(StageArgs a)
 {
     using L = Lay<P, 1, T>;
     constexpr int FB = face_batch<P>(), NT = kFaceThreads;
-    constexpr int N = L::N, M = L::M, NB = L::NB, NF = L::NF, NS = L::NS, FS = L::FS;
+    constexpr int N = L::N, M = L::M, NB = L::NB, NF = L::NF, N2 = L::N2, FS = L::FS;
     constexpr bool kShift = sizeof(T) == 4;
     extern __shared__ double fsm[];
-    double* sSl = fsm;                                                              // [FB][2][5][NS]
-    T* sTr = reinterpret_cast<T*>(sSl + FB * 10 * NS);                              // [FB][2][5][FS]
+    T* sTr = reinterpret_cast<T*>(fsm);                                             // [FB][2][5][FS]
     unsigned char* tail = reinterpret_cast<unsigned char*>(sTr) + ((sizeof(T) * FB * 10 * FS + 15) / 16) * 16;
     FaceRec* sRecL = reinterpret_cast<FaceRec*>(tail);                              // [FB] listed side's record
     int* sEL = reinterpret_cast<int*>(sRecL + FB);                                  // [FB] listed element
@@ -1278,31 +1302,29 @@ __global__ void __launch_bounds__(kFaceThreads) face_flux_kernel(StageArgs a)
             sFL[j] = fe.y;
         }
         __syncthreads();
-        // both sides' boundary slices, one task per slice row
-        for (int t = tid; t < FB * 10 * N; t += NT) {
-            const int row = t % N, r0 = t / N;
-            const int v = r0 % 5, side = (r0 / 5) % 2, j = r0 / 10;
+        // traces of both sides, in the left element's energy frame: one task per
+        // (face, side, variable) gathers its boundary slice from the state into
+        // registers (entry (b0, b1) at coefficient o0 + b0 s0 + b1 s1)
+        for (int t = tid; t < FB * 10; t += NT) {
+            const int v = t % 5, sj = t / 5, j = sj / 2, side = sj % 2;
             const FaceRec& rec = sRecL[j];
             const int el = side == 0 ? sEL[j] : rec.nbr;
             const int fc = side == 0 ? sFL[j] : (rec.info & 7);
-            const double* src = a.Us + ((size_t)el * 5 + v) * NB;
-            double* dst = sSl + ((j * 2 + side) * 5 + v) * NS + row * N;
+            const int ax = face_axis(fc), sidx = face_side(fc) ? N - 1 : 0;
+            const int o0 = ax == 0 ? sidx : (ax == 1 ? sidx * N : sidx * N2);
+            const int s0 = ax == 0 ? N : 1, s1 = ax == 2 ? N : N2;
+            const double* src = a.Us + ((size_t)el * 5 + v) * NB + o0;
+            const double sh = kShift && v == 4 ? a.geo[rec.cls].eref : 0.0;
+            double x[N][N];
 #pragma unroll
-            for (int b0 = 0; b0 < N; ++b0) cp_async8(dst + b0, src + slice_index<N>(fc, b0, row));
-        }
-        cp_async_commit();
-        cp_async_wait_all();
-        __syncthreads();
-        // traces of both sides, in the left element's energy frame
-        for (int t = tid; t < FB * 10; t += NT) {
-            const int v = t % 5, sj = t / 5;
-            const double sh = kShift && v == 4 ? a.geo[sRecL[sj / 2].cls].eref : 0.0;
-            const double* sl0 = sSl + (sj * 5 + v) * NS;
+            for (int b1 = 0; b1 < N; ++b1)
+#pragma unroll
+                for (int b0 = 0; b0 < N; ++b0) x[b1][b0] = __ldg(src + b0 * s0 + b1 * s1);
             T sl[N][N];
 #pragma unroll
             for (int b1 = 0; b1 < N; ++b1)
 #pragma unroll
-                for (int b0 = 0; b0 < N; ++b0) sl[b1][b0] = kShift ? T(sl0[b1 * N + b0] - sh) : T(sl0[b1 * N + b0]);
+                for (int b0 = 0; b0 < N; ++b0) sl[b1][b0] = kShift ? T(x[b1][b0] - sh) : T(x[b1][b0]);
             interp2d<N, M, T>(Bt, sl, sTr + (sj * 5 + v) * FS);
         }
         __syncthreads();
