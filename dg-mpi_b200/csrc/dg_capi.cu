@@ -124,7 +124,7 @@ int prepare_variant(dg_ctx* c, int v)
         DG_CUDA(c, cudaFuncSetAttribute(sv.face_func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sv.face_smem));
         DG_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&face_per_sm, sv.face_func, sv.face_threads, sv.face_smem));
         if (face_per_sm < 1) return fail(c, DG_ERR_UNSUPPORTED, "face kernel does not fit on an SM");
-        const int fb = dgk::face_batch_of(c->p);
+        const int fb = sv.face_batch;
         c->variant_face_grid[v] = std::max(1, std::min((c->nface + fb - 1) / fb, dev_sms * face_per_sm));
     }
     c->variant_grid[v] = std::max(1, std::min(batches, dev_sms * per_sm));
@@ -176,7 +176,7 @@ int launch_stage(dg_ctx* c, int mode, const double* Us, const double* U0, double
         else if (e_begin != 0 || e_end != c->ne) return fail(c, DG_ERR_ARG, "face-kernel variant on an element range");
         a.face_begin = f0;
         a.nface = f1;
-        const int fb = dgk::face_batch_of(c->p);
+        const int fb = sv.face_batch;
         if (f1 > f0) DG_CUDA(c, sv.face_launch(a, std::min(c->variant_face_grid[c->variant], (f1 - f0 + fb - 1) / fb), c->stream));
     }
     const int batches = (e_end - e_begin + sv.E - 1) / sv.E;

@@ -1260,17 +1260,18 @@ __device__ __forceinline__ void stage_body(const StageArgs& a)
 // the listed side's canonical point order.  The same operations as the stage kernel's own face
 // phase (flux_functors_impl.h:168-264), done once per face instead of once per
 // side.
-// faces per batch and threads of the face kernel
-__host__ __device__ constexpr int face_batch_of(int p) { return p <= 3 ? 16 : 8; }
-template <int P>
-__host__ __device__ constexpr int face_batch() { return face_batch_of(P); }
+// faces per batch (measured best: 16 up to p = 3; above, 12 for the FP64
+// kernel and 8 for the FP32 one) and threads of the face kernel
+__host__ __device__ constexpr int face_batch_of(int p, int bytes) { return p <= 3 ? 16 : (bytes == 8 ? 12 : 8); }
+template <int P, typename T>
+__host__ __device__ constexpr int face_batch() { return face_batch_of(P, sizeof(T)); }
 constexpr int kFaceThreads = 128;
 
 template <int P, typename T>
 constexpr size_t face_smem_bytes()
 {
     using L = Lay<P, 1, T>;
-    constexpr int FB = face_batch<P>();
+    constexpr int FB = face_batch<P, T>();
     return ((sizeof(T) * FB * 10 * L::FS + 15) / 16) * 16 + FB * sizeof(FaceRec) + 2 * FB * sizeof(int);
 }
 
@@ -1279,7 +1280,7 @@ template <int P, typename T, bool GEO>
 __global__ void __launch_bounds__(kFaceThreads) face_flux_kernel(StageArgs a)
 {
     using L = Lay<P, 1, T>;
-    constexpr int FB = face_batch<P>(), NT = kFaceThreads;
+    constexpr int FB = face_batch<P, T>(), NT = kFaceThreads;
     constexpr int N = L::N, M = L::M, NB = L::NB, NF = L::NF, N2 = L::N2, FS = L::FS;
     constexpr bool kShift = sizeof(T) == 4;
     extern __shared__ double fsm[];
@@ -1404,6 +1405,7 @@ struct StageVariant {
     size_t face_smem;
     int face_threads;
     cudaError_t (*face_launch)(const StageArgs&, int grid, cudaStream_t);
+    int face_batch;      // faces per CTA batch of the face kernel
 };
 
 template <int P, typename T, bool GEO>
@@ -1441,7 +1443,7 @@ StageVariant make_variant()
     if constexpr (MB > 0) func = (const void*)stage_kernel_mb<P, E, NT, G, T, FL, MB>;
     else func = (const void*)stage_kernel<P, E, NT, G, T, FL>;
     StageVariant v{E, NT, G, sizeof(T) == 4 ? 1 : 0, FL | (MB << 8), stage_smem_bytes<P, E, G, T, FL>(),
-                   func, launch_stage_variant<P, E, NT, G, T, FL, MB>, nullptr, 0, 0, nullptr};
+                   func, launch_stage_variant<P, E, NT, G, T, FL, MB>, nullptr, 0, 0, nullptr, 0};
     if constexpr ((FL & 64) != 0) {
         static_assert(face_smem_bytes<P, T>() <= 227 * 1024, "face kernel shared memory exceeds 227 KB");
         constexpr bool geo = (FL & 32) != 0;
@@ -1449,6 +1451,7 @@ StageVariant make_variant()
         v.face_smem = face_smem_bytes<P, T>();
         v.face_threads = kFaceThreads;
         v.face_launch = launch_face_kernel<P, T, geo>;
+        v.face_batch = face_batch<P, T>();
     }
     return v;
 }
