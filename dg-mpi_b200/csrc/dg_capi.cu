@@ -1556,6 +1556,25 @@ int dg_kinetic_energy_noalloc(int order, int nelem, const double* d_state, const
     cudaError_t ce = cudaGetDevice(&dev);
     if (ce != cudaSuccess) return fail(nullptr, DG_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(ce));
     if (dev < 0 || dev >= 64) return fail(nullptr, DG_ERR_UNSUPPORTED, "device ordinal above 63");
+    // every buffer must be memory of the current device: a pointer of another
+    // device (or a host pointer) would fault asynchronously, after DG_OK
+    const void* bufs[3] = {d_state, d_djac, d_ke};
+    const char* names[3] = {"d_state", "d_djac", "d_ke"};
+    for (int i = 0; i < 3; ++i) {
+        cudaPointerAttributes at{};
+        ce = cudaPointerGetAttributes(&at, bufs[i]);
+        if (ce != cudaSuccess) {
+            (void)cudaGetLastError();
+            return fail(nullptr, DG_ERR_ARG, std::string("dg_kinetic_energy_noalloc: ") + names[i] +
+                                                  " is not a CUDA pointer: " + cudaGetErrorString(ce));
+        }
+        if (at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged)
+            return fail(nullptr, DG_ERR_ARG, std::string("dg_kinetic_energy_noalloc: ") + names[i] + " is not device memory");
+        if (at.device != dev)
+            return fail(nullptr, DG_ERR_ARG, std::string("dg_kinetic_energy_noalloc: ") + names[i] + " is memory of device " +
+                                                  std::to_string(at.device) + ", not of the current device " +
+                                                  std::to_string(dev));
+    }
     double* scratch = nullptr;
     {
         // one-time set-up per device, with that device current: basis tables

@@ -158,7 +158,7 @@ __host__ __device__ constexpr int cmax(int a, int b) { return a > b ? a : b; }
 // stride and the task order of every pass below were chosen together by
 // counting the wavefronts of each pass's addresses over all strides up to 16
 // past the block size and all task orders (per order and arithmetic width);
-// bank_model.py beside this directory reproduces them. The update pass keeps
+// tests/bank_model.py reproduces them. The update pass keeps
 // its z-pencil order (consecutive threads write consecutive global words).
 //
 // point-array row stride of the unfused volume

@@ -201,7 +201,19 @@ int dg_kinetic_energy(dg_ctx* ctx, double* ke);
  * the result, (1/V) * integral of |rho u|^2 / (2 rho) over the mesh with
  * V = sum of 8 * djac, is written to the device double d_ke.  Work is queued
  * on `stream` (a cudaStream_t, NULL for the default stream) and the call does
- * not wait for it.
+ * not wait for it.  d_state must be complete on `stream` when the call is
+ * made: a state written by a context's calls is written on dg_stream(ctx),
+ * which does not wait for other streams, so record an event on dg_stream(ctx)
+ * and make `stream` wait on it (or synchronise) first.
+ *
+ * Affine meshes only: one det J per element is applied at every quadrature
+ * point, which is exact for parallelepiped elements (every mesh of
+ * dg_mesh_periodic_box).  On a trilinear (non-affine) mesh the Jacobian varies
+ * inside an element and the result differs from dg_kinetic_energy, which
+ * evaluates it per point.  For an affine mesh, d_djac[e] is the constant
+ * Jacobian determinant of element e (for a uniform box with element size
+ * h, (hx/2)(hy/2)(hz/2)).  d_state, d_djac and d_ke must be memory of the
+ * current device (checked; DG_ERR_ARG otherwise).
  *
  * Scratch lives in a static device array of 32768 doubles (256 KB) that every
  * GPU loading this library holds until the process exits; it holds two
@@ -213,7 +225,10 @@ int dg_kinetic_energy(dg_ctx* ctx, double* ke);
  * it reads, so nothing is carried over from an earlier call.  The first call on a device
  * does a one-time set-up (loads the basis tables and looks up the array's
  * device address with that device current); make that first call before any
- * stream capture. */
+ * stream capture.  That set-up is cached per device for the life of the
+ * process: a cudaDeviceReset between calls invalidates it (the tables and
+ * the array's address belong to the reset context), so do not reset a device
+ * that this call has used. */
 int dg_kinetic_energy_noalloc(int order, int nelem, const double* d_state, const double* d_djac,
                               double* d_ke, void* stream);
 

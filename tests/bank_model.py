@@ -22,8 +22,8 @@ interpolation in place, pointwise flux (5 rows -> 15 rows), z / y / x
 contractions, lift, lift gather into the residual, inverse-mass x and y
 passes and the update (z pencils).
 
-    python dg-mpi_b200/bank_model.py 3 8      # p = 3, FP64 work area
-    python dg-mpi_b200/bank_model.py 5 4 --search
+    python tests/bank_model.py 3 8      # p = 3, FP64 work area
+    python tests/bank_model.py 5 4 --search
 
 Design tool only: nothing in the library imports it.
 """

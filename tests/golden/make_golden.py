@@ -12,7 +12,7 @@ executed) and records the numbers its tests and tables pin:
     (test/numerics/basis/test_basis.cpp:264-272) and the equidistant-node
     expectations (test/numerics/test_nodes.cpp, test/numerics/basis/test_tools.cpp).
 
-Usage: python tests/golden/make_golden.py [reference_root]
+Usage: python tests/golden/make_golden.py <reference root>
 """
 from __future__ import annotations
 
@@ -88,4 +88,6 @@ def main(root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <reference root>")
+    main(sys.argv[1])

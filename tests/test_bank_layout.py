@@ -1,6 +1,6 @@
 """The stage kernel's shared-memory layout constants against the bank model.
 
-dg-mpi_b200/bank_model.py counts the shared-memory wavefronts of the stage
+tests/bank_model.py (beside this file) counts the shared-memory wavefronts of the stage
 kernel's passes; csrc/dg_stage.cuh holds the point-array strides
 (qs_stride), the per-pass task orders (TaskOrd) and the rotated coefficient
 rows at p = 3 (Lay::cw). These CPU tests compile a host probe of the header
@@ -8,6 +8,7 @@ with nvcc (no GPU needed), check that the model's copy of the constants is the
 header's, and that the committed choice is the model's optimum.
 """
 import json
+import os
 import shutil
 import subprocess
 
@@ -44,7 +45,7 @@ def header(tmp_path_factory):
     d = tmp_path_factory.mktemp("probe")
     src, exe = d / "probe.cu", d / "probe"
     src.write_text(PROBE)
-    root = bm.__file__.rsplit("/", 1)[0]
+    root = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "dg-mpi_b200")
     subprocess.run(["nvcc", "-std=c++17", "--expt-relaxed-constexpr", "-Wno-deprecated-gpu-targets",
                     "-I" + root + "/csrc", "-I" + root + "/../include", "-o", str(exe), str(src)],
                    check=True, capture_output=True)

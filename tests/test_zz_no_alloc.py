@@ -31,19 +31,37 @@ def test_noalloc_kinetic_energy_matches_context_entry_point():
     djac = torch.full((ne,), float(np.prod(h / 2.0)), dtype=torch.float64, device="cuda")
     out = torch.zeros(1, dtype=torch.float64, device="cuda")
 
+    # the caller's stream, ordered after the context's stream (which wrote the
+    # state) by an event, as the header asks
+    ctx_stream = torch.cuda.ExternalStream(case.stream_ptr())
+    stream = torch.cuda.Stream()
     results = []
     for call in range(2):
         if call == 1:
             case.rk4(case.cfl_time_step(U0, 0.1), 3)  # a different state for the second call
-        ke_ref = case.kinetic_energy()
-        out.fill_(-1.0)
+        written = torch.cuda.Event()
+        written.record(ctx_stream)
+        with torch.cuda.stream(stream):
+            out.fill_(-1.0)
+        stream.wait_event(written)
         dg_b200.kinetic_energy_noalloc(p, ne, case.device_state_ptr(), djac.data_ptr(), out.data_ptr(),
-                                       torch.cuda.current_stream().cuda_stream)
-        torch.cuda.synchronize()
+                                       stream.cuda_stream)
+        stream.synchronize()
+        ke_ref = case.kinetic_energy()
         ke = float(out.item())
         assert abs(ke - ke_ref) <= TOL * abs(ke_ref), (call, ke, ke_ref)
         results.append(ke)
     assert results[0] != results[1]
+
+
+def test_noalloc_kinetic_energy_rejects_host_pointers():
+    import torch
+
+    ok = torch.zeros(8, dtype=torch.float64, device="cuda")
+    host = np.zeros(8)
+    with pytest.raises(dg_b200.DGError) as ei:
+        dg_b200.kinetic_energy_noalloc(1, 1, host.ctypes.data, ok.data_ptr(), ok.data_ptr())
+    assert ei.value.code == 1 and "d_state" in str(ei.value)
 
 
 def test_noalloc_kinetic_energy_rejects_meshes_beyond_its_scratch():
