@@ -245,6 +245,78 @@ DG_HD bool flux_hllc_n(T gam, const T* UL, const T* UR, const T* n, T djac, T* F
     return true;
 }
 
+// HLLC of flux_hllc_n on states whose energy is stored relative to a constant
+// (U[4] = rE - eref), for the FP32 residual.  The pressure enters in its
+// shifted form P' = P - pref, pref = (gamma-1) eref, wherever only differences
+// of pressures or the momentum fluxes need it: the PVRS estimate and sStar use
+// P'R - P'L, the compression test pStar > P_K becomes p'Star > P'_K, and the
+// momentum fluxes carry P' n (the constant pref n is left out, as in
+// interior_flux_r1: its volume and face terms cancel).  The full pressure
+// P' + pref enters only the sound speeds, the shock factor's denominator and
+// the energy fluxes, where FP32's relative rounding is harmless.  So the
+// momenta never see the rounding of the large energy at low Mach.  In exact
+// arithmetic this is flux_hllc_n with pref n subtracted from the momenta.
+template <typename T>
+DG_HD bool flux_hllc_shift(T gam, const T* UL, const T* UR, const T* n, T djac, T eref, T* F)
+{
+    const T pref = (gam - T(1.)) * eref;
+    const T rhoL = UL[0], rhoL1 = T(1.) / rhoL;
+    const T unL = (UL[1] * n[0] + UL[2] * n[1] + UL[3] * n[2]) * rhoL1;
+    const T PsL = pressure(gam, UL);  // shifted
+    const T PL = PsL + pref;
+    const T aL = sqrt(gam * PL * rhoL1);
+    const T rhoR = UR[0], rhoR1 = T(1.) / rhoR;
+    const T unR = (UR[1] * n[0] + UR[2] * n[1] + UR[3] * n[2]) * rhoR1;
+    const T PsR = pressure(gam, UR);
+    const T PR = PsR + pref;
+    const T aR = sqrt(gam * PR * rhoR1);
+    const T rAvg = T(0.5) * (rhoL + rhoR);
+    const T aAvg = T(0.5) * (aL + aR);
+    // shifted PVRS estimate, clamped where the full estimate is negative
+    T psStar = T(0.5) * (PsL + PsR - (unR - unL) * rAvg * aAvg);
+    if (psStar + pref < T(0.)) psStar = -pref;
+    const T dL = psStar - PsL, dR = psStar - PsR;  // pStar - P_K
+    T qL = T(1.0), qR = T(1.0);
+    if (dL > T(0.)) qL = sqrt(T(1.) + (gam + T(1.)) / (T(2.) * gam) * (dL / PL));
+    if (dR > T(0.)) qR = sqrt(T(1.) + (gam + T(1.)) / (T(2.) * gam) * (dR / PR));
+    const T sL = unL - aL * qL;
+    const T sR = unR + aR * qR;
+    const T sStar = (PsR - PsL + rhoL * unL * (sL - unL) - rhoR * unR * (sR - unR)) /
+                    (rhoL * (sL - unL) - rhoR * (sR - unR));
+    const T hr = gam * eref;  // rE + P = U[4] + P' + gamma eref
+    if (sL >= T(0.)) {
+        F[0] = djac * rhoL * unL;
+        for (int i = 0; i < 3; ++i) F[1 + i] = djac * (UL[1 + i] * unL + PsL * n[i]);
+        F[4] = djac * ((UL[4] + PsL + hr) * unL);
+    } else if (sR <= T(0.)) {
+        F[0] = djac * rhoR * unR;
+        for (int i = 0; i < 3; ++i) F[1 + i] = djac * (UR[1 + i] * unR + PsR * n[i]);
+        F[4] = djac * ((UR[4] + PsR + hr) * unR);
+    } else if ((sL < T(0.)) && (sStar >= T(0.))) {
+        const T f1 = sStar - unL;
+        const T cm1 = f1 / (sL - sStar);  // c - 1, c = (sL - unL) / (sL - sStar)
+        const T c = T(1.) + cm1;
+        const T f2 = sStar + PL / (rhoL * (sL - unL));
+        F[0] = djac * (rhoL * unL + rhoL * sL * cm1);
+        for (int i = 0; i < 3; ++i)
+            F[1 + i] = djac * (UL[1 + i] * unL + PsL * n[i] + sL * (UL[1 + i] * cm1 + rhoL * c * f1 * n[i]));
+        F[4] = djac * ((UL[4] + PsL + hr) * unL + sL * ((UL[4] + eref) * cm1 + rhoL * c * f1 * f2));
+    } else if ((sStar < T(0.)) && (sR > T(0.))) {
+        const T f1 = sStar - unR;
+        const T cm1 = f1 / (sR - sStar);
+        const T c = T(1.) + cm1;
+        const T f2 = sStar + PR / (rhoR * (sR - unR));
+        F[0] = djac * (rhoR * unR + rhoR * sR * cm1);
+        for (int i = 0; i < 3; ++i)
+            F[1 + i] = djac * (UR[1 + i] * unR + PsR * n[i] + sR * (UR[1 + i] * cm1 + rhoR * c * f1 * n[i]));
+        F[4] = djac * ((UR[4] + PsR + hr) * unR + sR * ((UR[4] + eref) * cm1 + rhoR * c * f1 * f2));
+    } else {
+        for (int s = 0; s < 5; ++s) F[s] = T(0.0);
+        return false;
+    }
+    return true;
+}
+
 // Initial conditions / exact solutions, Physics<3>::call_IC and
 // call_exact_solution (src/physics/base/base.cpp:90-137) plus the advected
 // xy vortex and Taylor-Green families.  Type codes match DG_IC_* in dg_b200.h.

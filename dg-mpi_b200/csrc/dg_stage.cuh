@@ -392,16 +392,11 @@ __device__ __forceinline__ void numerical_flux(int flux, double gamma_d, T (&UL)
     const T nmag = nd[3];
     if (flux == 1) {
         const T nu[3] = {nd[0], nd[1], nd[2]};
-        if (SHIFT) {  // HLLC takes the full energy
-            UL[4] += T(eref);
-            UR[4] += T(eref);
-        }
-        if (!dgp::flux_hllc_n(gamma, UL, UR, nu, nmag, Fo)) status |= kStatusHLLC;
-        if (SHIFT) {  // every HLLC branch carries P_side |N| n in the momenta: drop the constant part
-            const T pn = nmag * T((gamma_d - 1.0) * eref);
-#pragma unroll
-            for (int d = 0; d < 3; ++d) Fo[1 + d] -= pn * nu[d];
-        }
+        // the FP32 residual keeps the shifted energy and leaves the constant
+        // pressure out of the momenta (dgp::flux_hllc_shift)
+        const bool ok = SHIFT ? dgp::flux_hllc_shift(gamma, UL, UR, nu, nmag, T(eref), Fo)
+                              : dgp::flux_hllc_n(gamma, UL, UR, nu, nmag, Fo);
+        if (!ok) status |= kStatusHLLC;
     } else {
         const T nh[3] = {nd[0], nd[1], nd[2]};
         dgp::flux_lax_friedrichs_fast<T, SHIFT>(gamma, UL, UR, nh, nmag, Fo, T(gamma_d * eref), T((gamma_d - 1.0) * eref));
