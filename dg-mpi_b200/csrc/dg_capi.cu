@@ -15,6 +15,7 @@
 #include "../host/case.h"
 #include "../host/partition.h"
 #include "dg_ctx.cuh"
+#include "dg_tc.cuh"
 
 using dgk::GeoDev;
 using dgk::StageArgs;
@@ -30,6 +31,14 @@ int dgk::stage_variants(int p, const StageVariant** out)
         case 5: return stage_variants_p5(out);
         default: *out = nullptr; return 0;
     }
+}
+
+bool dgk::tc_operator(int p, const double* B1, std::vector<float>& out)
+{
+    if (p != 3) return false;
+    out.assign(4 * TcCfg<3>::kBopAtom / sizeof(float), 0.f);
+    tc_operator_table<3>(B1, out.data());
+    return true;
 }
 
 namespace {
@@ -100,7 +109,8 @@ bool variant_matches(const dg_ctx* c, int v)
     const dgk::StageVariant* vs = nullptr;
     const int nv = dgk::stage_variants(c->p, &vs);
     return v >= 0 && v < nv && (vs[v].fp32 != 0) == (c->precision == DG_PREC_MIXED_FP32) &&
-           ((vs[v].flags & dgk::kGE) != 0) == c->pm.general && (!(vs[v].flags & dgk::kFX) || c->d_fflux);
+           ((vs[v].flags & dgk::kGE) != 0) == c->pm.general && (!(vs[v].flags & dgk::kFX) || c->d_fflux) &&
+           (!(vs[v].flags & dgk::kTC) || c->d_tcop);
 }
 
 // Sets the variant's shared-memory attribute and its persistent grid size
@@ -153,6 +163,7 @@ int launch_stage(dg_ctx* c, int mode, const double* Us, const double* U0, double
     a.faces = c->d_faces;
     a.nface = c->nface;
     a.fflux = c->d_fflux;
+    a.tcop = c->d_tcop;
     a.status = c->d_status;
     a.e_begin = e_begin;
     a.ne = e_end;
@@ -662,6 +673,10 @@ int check_status(dg_ctx* c)
         DG_CUDA(c, cudaMemsetAsync(c->d_status, 0, sizeof(unsigned), c->stream));
         DG_CUDA(c, cudaStreamSynchronize(c->stream));
         char buf[160];
+        if (st & dgk::kStatusTimeout) {
+            snprintf(buf, sizeof(buf), "a bounded device wait gave up (status 0x%x)", st);
+            return fail(c, DG_ERR_TIMEOUT, buf);
+        }
         snprintf(buf, sizeof(buf), "non-physical state detected on the device (status 0x%x)", st);
         return fail(c, DG_ERR_NONPHYSICAL, buf);
     }
@@ -780,7 +795,7 @@ void release(dg_ctx* c)
     cudaFree(c->d_conn); cudaFree(c->d_frec); cudaFree(c->d_geo_class); cudaFree(c->d_geo); cudaFree(c->d_cmap);
     cudaFree(c->d_X0); cudaFree(c->d_partials); cudaFree(c->d_status);
     cudaFree(c->d_gjd); cudaFree(c->d_gnrm); cudaFree(c->d_gimm); cudaFree(c->d_gnodes); cudaFree(c->d_gfsd);
-    cudaFree(c->d_faces); cudaFree(c->d_fflux);
+    cudaFree(c->d_faces); cudaFree(c->d_fflux); cudaFree(c->d_tcop);
     cudaFree(c->d_halo_send); cudaFree(c->d_halo_recv);
     if (c->stream) cudaStreamDestroy(c->stream);
 }
@@ -872,6 +887,15 @@ int dgi::create_ctx(const dg_case_desc* cd, const dg_mesh_desc* md, const int* e
     for (size_t i = 0; i < c->tab.B.size(); ++i) c->stage_tab.Bf[i] = static_cast<float>(c->tab.B[i]);
     for (size_t i = 0; i < c->tab.D.size(); ++i) c->stage_tab.Df[i] = static_cast<float>(c->tab.D[i]);
     for (size_t i = 0; i < c->tab.wq.size(); ++i) c->stage_tab.Wf[i] = static_cast<float>(c->tab.wq[i]);
+    {   // nodal derivative of the 1D basis: Dn[i*n + j] = l_j'(xi_i) at the equidistant nodes
+        const int n = c->p + 1;
+        const std::vector<double> xn = dgh::equidistant_nodes(n);
+        std::vector<double> val(n), grad(n);
+        for (int i = 0; i < n; ++i) {
+            dgh::lagrange_1d(xn[i], xn, val.data(), grad.data());
+            for (int j = 0; j < n; ++j) c->stage_tab.Dn[i * n + j] = static_cast<float>(grad[j]);
+        }
+    }
     {   // default launch variant: the first one compiled for the requested precision and geometry kind
         const int nv = dg_num_stage_variants(c->p);
         c->variant = -1;
@@ -1051,6 +1075,19 @@ int dgi::create_ctx(const dg_case_desc* cd, const dg_mesh_desc* md, const int* e
                 cudaFree(c->d_fflux);
                 c->d_faces = nullptr;
                 c->d_fflux = nullptr;
+            }
+        }
+        // the tensor-core variants' operator table (FP32 residual on affine meshes)
+        bool has_tc = false;
+        for (int v = 0; v < nv; ++v) has_tc = has_tc || (vs[v].flags & dgk::kTC);
+        if (has_tc && c->d_fflux && c->precision == DG_PREC_MIXED_FP32 && !c->pm.general) {
+            std::vector<float> op;
+            if (dgk::tc_operator(c->p, c->tab.B.data(), op) &&
+                (cudaMalloc((void**)&c->d_tcop, op.size() * sizeof(float)) != cudaSuccess ||
+                 cudaMemcpy(c->d_tcop, op.data(), op.size() * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess)) {
+                cudaGetLastError();
+                cudaFree(c->d_tcop);
+                c->d_tcop = nullptr;
             }
         }
         // the default variant again, now that face-kernel variants may match

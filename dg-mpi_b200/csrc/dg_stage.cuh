@@ -32,6 +32,7 @@
 #pragma once
 #include <cstdint>
 #include <type_traits>
+#include <vector>
 
 #include "dg_physics.cuh"
 
@@ -51,6 +52,9 @@ struct StageTables {
     float Bf[kTabB];                           // FP32 copies for the mixed-precision residual
     float Df[kTabB];
     float Wf[kMaxP + 2];
+    // derivative of the 1D Lagrange basis at its own equidistant nodes,
+    // Dn[i*N + j] = l_j'(xi_i) (the tensor-core kernel's nodal derivative)
+    float Dn[(kMaxP + 1) * (kMaxP + 1)];
 };
 
 template <typename T> struct TabSel;
@@ -140,6 +144,9 @@ struct StageArgs {
     const int2* faces;
     int face_begin, nface;
     void* fflux;
+    // tensor-core kernel: the basis operator B[q][b] as TF32 hi / lo in its
+    // shared-memory layout (dgk::tc_operator_table)
+    const float* tcop;
     unsigned* status;
     int e_begin, ne;        // the launch computes elements [e_begin, ne)
     int flux;               // 0 = Lax-Friedrichs, 1 = HLLC
@@ -1392,7 +1399,7 @@ struct StageVariant {
     int flags;           // 1: groups' pencils in one phase, 2: single coefficient buffer,
                          // 4: unfused volume, 8: row-split traces and lifts,
                          // 16: one face-flux point per thread, 32: general (trilinear) geometry,
-                         // 64: face fluxes from the face kernel;
+                         // 64: face fluxes from the face kernel, 128: the tensor-core kernel;
                          // bits 8..11: minimum resident CTAs asked of the compiler (0: none)
     size_t smem;         // dynamic shared memory per CTA
     const void* func;    // the kernel, for attributes / occupancy queries
@@ -1430,6 +1437,8 @@ cudaError_t launch_stage_variant(const StageArgs& a, int grid, cudaStream_t s)
 // of the mesh, not a tuning choice: contexts on non-affine meshes run GE
 // variants only, the others never do
 constexpr int kPZ = 1, kSB = 2, kUF = 4, kRS = 8, kK1 = 16, kGE = 32, kFX = 64;
+// the tensor-core stage kernel (dg_tc.cuh): a kernel of its own, not an option of stage_kernel
+constexpr int kTC = 128;
 // MB > 0: at least MB resident CTAs per SM asked of the compiler (a register cap)
 template <int P, int E, int NT, int G, typename T = double, int FL = 0, int MB = 0>
 StageVariant make_variant()
@@ -1455,6 +1464,9 @@ StageVariant make_variant()
 
 // the variants compiled for order p (defined in dg_stage_p<p>.cu)
 int stage_variants(int p, const StageVariant** out);
+// the tensor-core kernel's operator table of order p from the 1D basis
+// B1[q * (p+1) + b] at the GL points (false: no tensor-core kernel for p)
+bool tc_operator(int p, const double* B1, std::vector<float>& out);
 int stage_variants_p0(const StageVariant** out);
 int stage_variants_p1(const StageVariant** out);
 int stage_variants_p2(const StageVariant** out);

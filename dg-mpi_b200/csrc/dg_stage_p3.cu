@@ -6,6 +6,7 @@
 // general-geometry (kGE) entries only, the others never do.  The
 // first variant of each precision is the default (the measured best); dg_tune_stage may pick another.
 #include "dg_stage.cuh"
+#include "dg_tc.cuh"
 
 namespace dgk {
 
@@ -39,6 +40,8 @@ static const StageVariant kVariants3[] = {
     make_variant<3, 1, 64, 1, float, kUF | kRS | kSB | kK1 | kGE>(),
     make_variant<3, 1, 128, 1, double, kUF | kRS | kSB | kGE | kFX>(),
     make_variant<3, 1, 128, 1, float, kUF | kSB | kGE | kFX>(),
+    // the tensor-core kernel (split-TF32 volume integral)
+    make_tc_variant<3>(),
 };
 
 int stage_variants_p3(const StageVariant** out)

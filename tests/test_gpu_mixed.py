@@ -112,5 +112,9 @@ def test_precision_config_p5_500_steps(flux):
     e64 = f64.l2_error("IsentropicVortexXY", VORTEX_XY, t)
     emx = mix.l2_error("IsentropicVortexXY", VORTEX_XY, t)
     print(f"p=5 16^3 500 steps {flux}: mixed vs FP64 {d}, L2 error FP64 {e64}, mixed {emx}")
-    np.testing.assert_allclose(emx[[0, 1, 2, 4]], e64[[0, 1, 2, 4]], rtol=1e-2)
+    # at p = 5 the discretisation error (~5e-7 in rho) is as small as the FP32
+    # residual's rounding, so the two errors against the exact vortex differ by
+    # at most the distance between the solutions (triangle inequality; the
+    # states are O(1), rho E ~ 3)
+    assert np.all(np.abs(emx - e64) <= 3.0 * TOL), (emx, e64)
     assert mix.status() == 0 and f64.status() == 0
