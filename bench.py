@@ -19,7 +19,13 @@ roofline : one RK stage (the face-flux kernel + the stage kernel when the tuner
 cpu_baseline / --impl reference : the CPU oracle (restatement of the
            reference's dense Kokkos algorithm, OpenMP over elements) on a
            16^3 sample of the same workload (same order, same per-element work)
-N > 1    : one independent replica of the workload per GPU (weak scaling)
+N > 1    : slab decomposition (weak scaling): rank r owns a 64^3 slab of a
+           periodic 64 x 64 x 64N box, the boundary coefficient slices travel
+           per RK stage over NCCL (dg_dist.HaloExchange) while the interior
+           elements compute, then the boundary elements; --replicas runs one
+           independent replica of the workload per GPU instead.  (--transport
+           host stages the exchange through pinned host buffers over gloo: the
+           same stage order, for several ranks sharing one GPU.)
 """
 from __future__ import annotations
 
@@ -223,6 +229,115 @@ def run_reference(args, rank: int):
     print(json.dumps(line), flush=True)
 
 
+def slab_main(args, world, rank, local):
+    """The slab-decomposed workload over `world` ranks: device-timed steps (CUDA
+    events on each rank's stream, max over ranks) and end to end through the
+    public API (each rank's slab from pinned host memory in and out)."""
+    import datetime
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    import dg_dist
+    ndev = max(1, torch.cuda.device_count())
+    device = local % ndev
+    torch.cuda.set_device(device)
+    backend = "nccl" if args.transport == "device" else "gloo"
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    K, W = args.steps, args.warmup
+    dc = dg_dist.DistributedCase((NEL, NEL, NEL * world), (0.0, 0.0, 0.0), (10.0, 10.0, 10.0 * world), ORDER,
+                                 gas_constant=1.0, transport=args.transport)
+    case = dc.case
+    U0 = case.project_ic("IsentropicVortexXY", VORTEX)
+    dt = dc.cfl_time_step(U0, CFL)
+    if args.variant is None:
+        best, tune_ms = case.tune_stage(reps=2)
+    else:
+        case.stage_variant = best = args.variant
+        tune_ms = [-1.0] * len(case.stage_variants())
+    # every rank runs rank 0's choice
+    v = torch.tensor([best], dtype=torch.int64, device="cuda" if backend == "nccl" else "cpu")
+    dist.broadcast(v, 0)
+    case.stage_variant = best = int(v.item())
+    variants = case.stage_variants()
+    dof = case.ne * case.nb * 5
+    red_dev = "cuda" if backend == "nccl" else "cpu"
+
+    def max_over_ranks(x):
+        t = torch.tensor([x], dtype=torch.float64, device=red_dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    case.set_state(U0)
+    with ClockSampler(device) as clocks:
+        time.sleep(0.3)
+        dc.rk4(dt, W)
+        dc.sync()
+        dist.barrier()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        ev[0].record(dc.stream)
+        dc.rk4(dt, K)
+        ev[1].record(dc.stream)
+        ev[1].synchronize()
+        device_ms = max_over_ranks(ev[0].elapsed_time(ev[1]))
+    status = case.status()
+    value = world * dof * 4 * K / (device_ms / 1e3)
+    e2e = None
+    host_in = host_out = None
+    if not args.no_e2e:
+        host_in = torch.from_numpy(U0).pin_memory()
+        host_out = torch.empty_like(host_in).pin_memory()
+        dist.barrier()
+        t0 = time.perf_counter()
+        case.set_state_ptr(host_in.data_ptr())
+        for _ in range(K):
+            dc.rk4(dt, 1)
+        dc.sync()
+        case.get_state_ptr(host_out.data_ptr())
+        e2e_s = max_over_ranks(time.perf_counter() - t0)
+        e2e = world * dof * 4 * K / e2e_s
+        if not torch.isfinite(host_out).all():
+            raise RuntimeError("non-finite state after the e2e run")
+    if rank == 0:
+        peaks, peak_kind = measured_peaks()
+        launch_s = device_ms / 1e3 / (4 * K)
+        achieved = BYTES_PER_DOF_STAGE * dof / launch_s / 1e9
+        state_bytes = dof * 8
+        face_split = "fx" in variants[best][4].split("+")
+        per_stage = 2 * (2 if face_split else 1) + (2 if dc.exchange.peers else 0)
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+            "ms_per_step": device_ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (analytic isentropic vortex IC, in-memory periodic mesh)",
+            "config": {"workload": f"vortex_xy_{NEL}cubed_p{ORDER}_fp64_per_rank_slab",
+                       "mesh": f"{NEL}x{NEL}x{NEL * world} periodic hex on [0,10]x[0,10]x[0,{10 * world}], "
+                               f"one {NEL}^3 slab per rank",
+                       "order": ORDER, "dof_per_rank": dof, "flux": "LaxFriedrichs", "cfl": CFL, "dt": dt,
+                       "parallelism": f"slab decomposition over {world} ranks, halo exchange per RK stage "
+                                      f"({args.transport} transport, {backend}) overlapped with the interior elements",
+                       "halo_peers": len(dc.exchange.peers),
+                       "halo_slices": sum(c for _, _, c in dc.exchange.peers),
+                       "interior_elements": dc.part.ninterior,
+                       "l2": "inputs larger than L2 (each state buffer %.0f MB > 126 MB)" % (state_bytes / 1e6),
+                       "stage_variant": {"chosen": variants[best]}},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                         "frac": achieved / peaks["hbm_gbs"], "traffic": profile_traffic(),
+                         "peak_source": peak_kind, "kernel": "per rank: stage + face kernels over the interior "
+                         "and boundary element ranges (one RK stage)", "bytes_per_launch": BYTES_PER_DOF_STAGE * dof},
+            "e2e": None if e2e is None else {
+                "value": e2e, "unit": UNIT, "h2d_bytes_per_step": state_bytes / K,
+                "d2h_bytes_per_step": state_bytes / K,
+                "timing": "host clock around the public API (set_state, K x DistributedCase.rk4, get_state), max over ranks"},
+            "gpu_launches": 4 * K * per_stage,
+            "clocks": clocks.summary(),
+            "status": status,
+        }
+        print(json.dumps(line), flush=True)
+    dist.barrier()
+    del host_in, host_out
+    dc.close()
+    dist.destroy_process_group()
+
+
 def main():
     global NEL
     ap = argparse.ArgumentParser()
@@ -236,6 +351,10 @@ def main():
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision leg")
     ap.add_argument("--variant", type=int, default=None, help="fixed FP64 launch variant instead of the tuner's pick")
     ap.add_argument("--mixed-variant", type=int, default=None, help="fixed mixed-precision launch variant")
+    ap.add_argument("--replicas", action="store_true", help="N > 1: independent replicas instead of the slab decomposition")
+    ap.add_argument("--slab", action="store_true", help="the slab decomposition also at N = 1")
+    ap.add_argument("--transport", default="device", choices=["device", "host"],
+                    help="slab halo exchange: device buffers over NCCL, or pinned host buffers over gloo")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -247,6 +366,9 @@ def main():
 
     if args.impl == "reference":
         run_reference(args, rank)
+        return
+    if (world > 1 and not args.replicas) or args.slab:
+        slab_main(args, world, rank, local)
         return
 
     import torch

@@ -36,7 +36,7 @@ int dgk::stage_variants(int p, const StageVariant** out)
 bool dgk::tc_operator(int p, const double* B1, std::vector<float>& out)
 {
     if (p != 3) return false;
-    out.assign(4 * TcCfg<3>::kBopAtom / sizeof(float), 0.f);
+    out.assign(TcCfg<3>::kOpBytes / sizeof(float), 0.f);
     tc_operator_table<3>(B1, out.data());
     return true;
 }

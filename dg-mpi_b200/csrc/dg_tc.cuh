@@ -186,27 +186,32 @@ struct TcCfg<3> {
     static constexpr int C = 5 * E;        // (element, variable) columns of a tile (30)
     static constexpr int N1 = 32;          // GEMM1 N: the columns, padded to 32
     static constexpr int MQ = 128;         // GEMM1 M = GEMM2 K: the points, padded
+    static constexpr int KC = 64;          // GEMM2 K per chunk (two chunks through one G buffer)
     static constexpr int NT = 256;         // threads (eight warps, two per TMEM lane quarter)
     static constexpr int kTmemCols = 128;  // D1 at columns [0, 32), D2 at [64, 128)
     static constexpr int kD2 = 64;
-    // shared memory (bytes from a 1024-aligned base)
-    static constexpr int kBopAtom = MQ * 128;           // 16384: one 32-wide k atom of B over 128 rows
-    static constexpr int kBopHi = 0, kBopLo = 2 * kBopAtom;  // [128 q][64 b] each
+    // shared memory (bytes from a 1024-aligned base).  The operator twice, as
+    // K-major 128-byte swizzled operands (TF32 MN-major operands would need the
+    // 32-byte-granule swizzle instead, so GEMM2 gets its own copy, B^T):
+    //   Bop [128 q][64 b] (GEMM1's A), Bt [64 b][128 q] (GEMM2's B), hi and lo each
+    static constexpr int kBopAtom = MQ * 128;           // 16384: a 32-wide k atom of Bop over 128 rows
+    static constexpr int kBtAtom = NB * 128;            // 8192: a 32-wide k atom of Bt over 64 rows
+    static constexpr int kBopHi = 0, kBopLo = 2 * kBopAtom;
+    static constexpr int kBtHi = 4 * kBopAtom, kBtLo = kBtHi + 4 * kBtAtom;
+    static constexpr int kOpBytes = 4 * kBopAtom + 8 * kBtAtom;  // 131072: one bulk copy
     static constexpr int kUopAtom = N1 * 128;           // 4096
-    static constexpr int kUopHi = 4 * kBopAtom, kUopLo = kUopHi + 2 * kUopAtom;  // [32 c][64 b] each
-    // G: [128 rows][128 q]; rows 96..127 are never written (their outputs are
-    // ignored), so the k atoms are packed at 12 row groups (12288 bytes) and
-    // those rows read into the next atom (or, past the last one, into Ust)
+    static constexpr int kUopHi = kOpBytes, kUopLo = kUopHi + 2 * kUopAtom;  // [32 c][64 b] each
+    // G: [128 rows][KC points] per chunk; rows 96..127 are never written (their
+    // outputs are ignored), so the k atoms are packed at 12 row groups (12288
+    // bytes) and those rows read into the next atom (past the last one, into Fh)
     static constexpr int kGAtom = 12 * 1024;
-    static constexpr int kGHi = kUopLo + 2 * kUopAtom, kGLo = kGHi + 4 * kGAtom;
-    static constexpr int kUst = kGLo + 4 * kGAtom;      // FP64 state of the next tile [E][5][nb]
-    static constexpr int kUstBytes = E * 5 * NB * 8;
-    static constexpr int kFh = kUst + kUstBytes;        // face fluxes [E][6][5][FS] FP32
+    static constexpr int kGHi = kUopLo + 2 * kUopAtom, kGLo = kGHi + 2 * kGAtom;
+    static constexpr int kFh = kGLo + 2 * kGAtom;       // face fluxes [E][6][5][FS] FP32
     static constexpr int kFhBytes = ((E * 30 * FS * 4 + 15) / 16) * 16;
     static constexpr int kRec = kFh + kFhBytes;         // face records [E][6]
     static constexpr int kMeta = kRec + E * 6 * 48;     // per element: JD[9], eref, hr, pref (FP32) [E][12]
     static constexpr int kCls = kMeta + E * 12 * 4;     // geometry class [E]
-    static constexpr int kBar = ((kCls + E * 4 + 7) / 8) * 8;  // mbarriers: U, GEMM1, GEMM2
+    static constexpr int kBar = ((kCls + E * 4 + 7) / 8) * 8;  // mbarriers: operator, GEMM1, GEMM2
     static constexpr int kSlot = kBar + 3 * 8;          // TMEM base address
     static constexpr int kBytes = kSlot + 16;
     static constexpr size_t kSmem = kBytes + 1024;      // + alignment slack
@@ -215,9 +220,9 @@ struct TcCfg<3> {
     static constexpr int PS = NB + 1;
     static constexpr int kRes = kPart + ((3 * C * PS * 4 + 15) / 16) * 16;  // FP64 [C][PS] residual
     static constexpr int kLift = kUopHi;                // FP32 [E][6][5][N*N] face lifts (Uop is dead)
-    static_assert(kRes + C * PS * 8 <= kUst, "epilogue buffers must fit in the G region");
+    static_assert(kRes + C * PS * 8 <= kFh, "epilogue buffers must fit in the G region");
     static_assert(kLift + E * 30 * N * N * 4 <= kGHi, "lift buffer must fit in the Uop region");
-    static_assert(kGLo + 3 * kGAtom + 16 * 1024 <= kBytes, "the last G atom's unused rows must stay inside shared memory");
+    static_assert(kGLo + kGAtom + 16 * 1024 <= kBytes, "the last G atom's unused rows must stay inside shared memory");
     static_assert(kSmem <= 227 * 1024, "tensor-core stage kernel exceeds 227 KB of shared memory");
 };
 
@@ -235,23 +240,25 @@ inline float tf32_host(float x)
 // host: the operator B[q][b] of order P -- q over the (p+2)^3 volume points
 // (q = qx + M qy + M^2 qz, zero rows past them), b over the (p+1)^3 basis
 // functions (b = bx + N by + N^2 bz), B = B1[qx][bx] B1[qy][by] B1[qz][bz] --
-// as TF32 hi and lo in the swizzled layout of TcCfg (kBopHi then kBopLo), for
-// one bulk copy.  B1[q * N + b] is the 1D basis at the GL points.
+// as TF32 hi and lo, in the swizzled layouts of TcCfg: Bop [q][b] then
+// Bt [b][q] (kOpBytes, one bulk copy).  B1[q * N + b] is the 1D basis at the
+// GL points.
 template <int P>
 void tc_operator_table(const double* B1, float* out)
 {
     using K = TcCfg<P>;
     constexpr int N = K::N, M = K::M;
-    const int half = 2 * K::kBopAtom / 4;  // floats of the hi table
-    for (int i = 0; i < 2 * half; ++i) out[i] = 0.f;
+    for (int i = 0; i < K::kOpBytes / 4; ++i) out[i] = 0.f;
     for (int q = 0; q < K::NQ; ++q)
         for (int b = 0; b < K::NB; ++b) {
             const double v = B1[(q % M) * N + b % N] * B1[((q / M) % M) * N + (b / N) % N] * B1[(q / (M * M)) * N + b / (N * N)];
             const float hi = tf32_host(static_cast<float>(v));
             const float lo = tf32_host(static_cast<float>(v - static_cast<double>(hi)));
-            const uint32_t off = tc::sw128(q, b, K::kBopAtom) / 4;
-            out[off] = hi;
-            out[half + off] = lo;
+            const uint32_t o1 = tc::sw128(q, b, K::kBopAtom), o2 = tc::sw128(b, q, K::kBtAtom);
+            out[(K::kBopHi + o1) / 4] = hi;
+            out[(K::kBopLo + o1) / 4] = lo;
+            out[(K::kBtHi + o2) / 4] = hi;
+            out[(K::kBtLo + o2) / 4] = lo;
         }
 }
 
@@ -271,11 +278,10 @@ __global__ void __launch_bounds__(TcCfg<P>::NT, 1) tc_stage_kernel(StageArgs a)
     FaceRec* sRec = reinterpret_cast<FaceRec*>(sm + K::kRec);
     float* sMeta = reinterpret_cast<float*>(sm + K::kMeta);
     int* sCls = reinterpret_cast<int*>(sm + K::kCls);
-    const double* Ust = reinterpret_cast<const double*>(sm + K::kUst);
     float* Part = reinterpret_cast<float*>(sm + K::kPart);
     double* Res = reinterpret_cast<double*>(sm + K::kRes);
     float* Lift = reinterpret_cast<float*>(sm + K::kLift);
-    const uint32_t barU = sbase + K::kBar, bar1 = barU + 8, bar2 = barU + 16;
+    const uint32_t barOp = sbase + K::kBar, bar1 = barOp + 8, bar2 = barOp + 16;
     uint32_t* slot = reinterpret_cast<uint32_t*>(sm + K::kSlot);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const float* __restrict__ Bt = a.tab.Bf;
@@ -284,6 +290,8 @@ __global__ void __launch_bounds__(TcCfg<P>::NT, 1) tc_stage_kernel(StageArgs a)
     const double* __restrict__ Mi = a.tab.Minv;
     const float gamma = float(a.gamma);
     const int ntiles = (a.ne - a.e_begin + E - 1) / E;
+    const bool need_acc = a.mode == kModeRK2 || a.mode == kModeRK3 || a.mode == kModeRK4;
+    const bool need_u0 = a.mode >= kModeRK1;
     unsigned status = 0;
 
     if (warp == 0) {
@@ -291,7 +299,7 @@ __global__ void __launch_bounds__(TcCfg<P>::NT, 1) tc_stage_kernel(StageArgs a)
         tc::tmem_relinquish();
     }
     if (tid == 0) {
-        tc::mbar_init(barU, 1);
+        tc::mbar_init(barOp, 1);
         tc::mbar_init(bar1, 1);
         tc::mbar_init(bar2, 1);
         tc::mbar_fence_init();
@@ -301,26 +309,30 @@ __global__ void __launch_bounds__(TcCfg<P>::NT, 1) tc_stage_kernel(StageArgs a)
     tc::tc_fence_after();
     const uint32_t tmem = *slot;
     const uint32_t d1 = tmem, d2 = tmem + K::kD2;
-    auto tile_elems = [&](int t) { return min(E, a.ne - (a.e_begin + t * E)); };
     if (tid == 0 && (int)blockIdx.x < ntiles) {
-        // the operator (hi and lo) and the first tile's state, on one transaction
-        const int t = blockIdx.x;
-        const uint32_t ub = tile_elems(t) * 5 * NB * 8;
-        tc::mbar_expect_tx(barU, 4 * K::kBopAtom + ub);
-        tc::bulk_g2s(sbase + K::kBopHi, a.tcop, 4 * K::kBopAtom, barU);
-        tc::bulk_g2s(sbase + K::kUst, a.Us + (size_t)(a.e_begin + t * E) * 5 * NB, ub, barU);
+        tc::mbar_expect_tx(barOp, K::kOpBytes);
+        tc::bulk_g2s(sbase, a.tcop, K::kOpBytes, barOp);
     }
-    uint32_t phU = 0, ph1 = 0, ph2 = 0;
-    bool alive = true;
-    for (int t = blockIdx.x; t < ntiles && alive; t += gridDim.x) {
-        const int e0 = a.e_begin + t * E, nel = tile_elems(t);
-        // ---- the tile's state has landed; face records and geometry ----
-        if (!__syncthreads_and(tc::mbar_wait(barU, phU, kWait))) {
-            status |= kStatusTimeout;
-            alive = false;
-            break;
+    // the state (and the RK operands) of tile t into L2 ahead of their plain loads
+    auto prefetch_tile = [&](int t) {
+        if (t >= ntiles) return;
+        const int e0 = a.e_begin + t * E, nel = min(E, a.ne - e0);
+        const int lines = nel * 5 * NB * 8 / 128;  // 20 per element
+        const size_t off = (size_t)e0 * 5 * NB;
+        for (int i = tid; i < 3 * lines; i += K::NT) {
+            const int k = i / lines, l = i - k * lines;
+            const double* src = k == 0 ? a.Us : (k == 1 ? (need_u0 ? a.U0 : nullptr) : (need_acc ? a.acc : nullptr));
+            if (src) asm volatile("prefetch.global.L2 [%0];\n" ::"l"(src + off + l * 16));
         }
-        phU ^= 1;
+    };
+    prefetch_tile(blockIdx.x);
+    bool alive = __syncthreads_and(tc::mbar_wait(barOp, 0, kWait));
+    if (!alive) status |= kStatusTimeout;
+    uint32_t ph1 = 0, ph2 = 0;
+    for (int t = blockIdx.x; t < ntiles && alive; t += gridDim.x) {
+        const int e0 = a.e_begin + t * E, nel = min(E, a.ne - e0);
+        prefetch_tile(t + gridDim.x);
+        // ---- face records and geometry of the tile ----
         for (int i = tid; i < E * 6 * 3; i += K::NT) {  // 16-byte pieces of the records
             const int e = i / 18;
             const int ge = min(e0 + e, a.ne - 1);
@@ -344,7 +356,7 @@ __global__ void __launch_bounds__(TcCfg<P>::NT, 1) tc_stage_kernel(StageArgs a)
             const int c = i / NB, b = i - c * NB, e = c / 5, v = c - 5 * e;
             float hi = 0.f, lo = 0.f;
             if (c < C && e < nel) {
-                const double x = Ust[(e * 5 + v) * NB + b] - (v == 4 ? a.geo[sCls[e]].eref : 0.0);
+                const double x = a.Us[(size_t)e0 * 5 * NB + i] - (v == 4 ? a.geo[sCls[e]].eref : 0.0);
                 hi = tc::tf32(float(x));
                 lo = tc::tf32(float(x - double(hi)));
             }
@@ -357,13 +369,6 @@ __global__ void __launch_bounds__(TcCfg<P>::NT, 1) tc_stage_kernel(StageArgs a)
         __syncthreads();
         if (tid == 0) {
             tc::tc_fence_after();
-            // the next tile's state streams in while this one computes
-            const int tn = t + gridDim.x;
-            if (tn < ntiles) {
-                const uint32_t ub = tile_elems(tn) * 5 * NB * 8;
-                tc::mbar_expect_tx(barU, ub);
-                tc::bulk_g2s(sbase + K::kUst, a.Us + (size_t)(a.e_begin + tn * E) * 5 * NB, ub, barU);
-            }
             // GEMM1: D1[q][c] = sum_b B[q][b] U[c][b]; lo*hi, hi*lo, hi*hi
             constexpr uint32_t id1 = tc::idesc_tf32(128, K::N1, 0);
 #pragma unroll
@@ -403,23 +408,27 @@ __global__ void __launch_bounds__(TcCfg<P>::NT, 1) tc_stage_kernel(StageArgs a)
         }
         ph1 ^= 1;
         tc::tc_fence_after();
+        const int qt = warp & 3, fhalf = warp >> 2;
+        const int q = qt * 32 + lane;
+        const int chunk = qt >> 1;        // this warp's points fall in GEMM2's K chunk 0 (q < 64) or 1
+        const int ql = q - chunk * K::KC;  // point within the chunk
+        float G[3][15];                    // this thread's fluxes: 3 elements x (d, v)
         {
-            const int qt = warp & 3, half = warp >> 2;
-            const int q = qt * 32 + lane;
-            float u[16];
-            tc::tmem_ld16(d1 + (static_cast<uint32_t>(qt * 32) << 16) + static_cast<uint32_t>(half * 15), u);
+            float u[32];  // all 32 columns (aligned loads); this half's elements start at column 15 fhalf
+            const uint32_t lrow = d1 + (static_cast<uint32_t>(qt * 32) << 16);
+            tc::tmem_ld16(lrow, u);
+            tc::tmem_ld16(lrow + 16, u + 16);
             tc::tmem_wait_ld();
             const int qx = q % M, qy = (q / M) % M, qz = q / (M * M);
             const float wq = q < NQ ? Wt[qx] * Wt[qy] * Wt[qz] : 0.f;
 #pragma unroll
             for (int ee = 0; ee < 3; ++ee) {
-                const int e = half * 3 + ee;
-                float G[15];
+                const int e = fhalf * 3 + ee;
                 if (q < NQ && e < nel) {
                     const float* mt = sMeta + e * 12;
                     float U[5], F[15];
 #pragma unroll
-                    for (int v = 0; v < 5; ++v) U[v] = u[ee * 5 + v];
+                    for (int v = 0; v < 5; ++v) U[v] = fhalf ? u[15 + ee * 5 + v] : u[ee * 5 + v];
                     const float p = dgp::interior_flux_r1<float, true>(gamma, U, F, mt[10]);
                     if (!(U[0] > 0.f)) status |= kStatusRho;
                     if (!(p + mt[11] > 0.f)) status |= kStatusPressure;
@@ -428,42 +437,70 @@ __global__ void __launch_bounds__(TcCfg<P>::NT, 1) tc_stage_kernel(StageArgs a)
                     for (int v = 0; v < 5; ++v)
 #pragma unroll
                         for (int d = 0; d < 3; ++d)
-                            G[d * 5 + v] = (F[v] * mt[d * 3 + 0] + F[5 + v] * mt[d * 3 + 1] + F[10 + v] * mt[d * 3 + 2]) * wq;
+                            G[ee][d * 5 + v] = (F[v] * mt[d * 3 + 0] + F[5 + v] * mt[d * 3 + 1] + F[10 + v] * mt[d * 3 + 2]) * wq;
                 } else {
 #pragma unroll
-                    for (int k = 0; k < 15; ++k) G[k] = 0.f;
+                    for (int k = 0; k < 15; ++k) G[ee][k] = 0.f;
                 }
+            }
+        }
+        // G of one chunk into the buffer: rows 32 d + 5 e + v, K = the point within the chunk
+        auto store_G = [&]() {
+#pragma unroll
+            for (int ee = 0; ee < 3; ++ee) {
+                const int e = fhalf * 3 + ee;
 #pragma unroll
                 for (int d = 0; d < 3; ++d)
 #pragma unroll
                     for (int v = 0; v < 5; ++v) {
-                        const float g = G[d * 5 + v];
+                        const float g = G[ee][d * 5 + v];
                         const float hi = tc::tf32(g), lo = tc::tf32(g - hi);
-                        const uint32_t off = tc::sw128(32 * d + 5 * e + v, q, K::kGAtom);
+                        const uint32_t off = tc::sw128(32 * d + 5 * e + v, ql, K::kGAtom);
                         *reinterpret_cast<float*>(sm + K::kGHi + off) = hi;
                         *reinterpret_cast<float*>(sm + K::kGLo + off) = lo;
                     }
             }
-        }
+        };
+        // GEMM2 over chunk ch: H[r][b] += sum_{q in chunk} G[r][q] Bt[b][q]
+        auto issue_gemm2 = [&](int ch) {
+            constexpr uint32_t id2 = tc::idesc_tf32(128, NB, 0);
+#pragma unroll
+            for (int s = 0; s < 3; ++s) {
+                const uint32_t ab = sbase + (s == 0 ? K::kGLo : K::kGHi);
+                const uint32_t bb = sbase + (s == 1 ? K::kBtLo : K::kBtHi);
+#pragma unroll
+                for (int kl = 0; kl < K::KC / 8; ++kl) {
+                    const int kk = ch * (K::KC / 8) + kl;
+                    const uint64_t ad = tc::sdesc(ab + (kl >> 2) * K::kGAtom + (kl & 3) * 32, 16, 1024);
+                    const uint64_t bd = tc::sdesc(bb + (kk >> 2) * K::kBtAtom + (kk & 3) * 32, 16, 1024);
+                    tc::mma_tf32(d2, ad, bd, id2, (ch > 0 || s > 0 || kl > 0) ? 1u : 0u);
+                }
+            }
+            tc::mma_commit(bar2);
+        };
+        if (chunk == 0) store_G();
         tc::fence_proxy_async();
         tc::tc_fence_before();
         __syncthreads();
         if (tid == 0) {
             tc::tc_fence_after();
-            // GEMM2: H[r][b] = sum_q G[r][q] B[q][b] (B read MN-major from the same table)
-            constexpr uint32_t id2 = tc::idesc_tf32(128, NB, 1);
-#pragma unroll
-            for (int s = 0; s < 3; ++s) {
-                const uint32_t ab = sbase + (s == 0 ? K::kGLo : K::kGHi);
-                const uint32_t bb = sbase + (s == 1 ? K::kBopLo : K::kBopHi);
-#pragma unroll
-                for (int kk = 0; kk < K::MQ / 8; ++kk) {
-                    const uint64_t ad = tc::sdesc(ab + (kk >> 2) * K::kGAtom + (kk & 3) * 32, 16, 1024);
-                    const uint64_t bd = tc::sdesc(bb + kk * 1024, K::kBopAtom, 1024);
-                    tc::mma_tf32(d2, ad, bd, id2, (s > 0 || kk > 0) ? 1u : 0u);
-                }
-            }
-            tc::mma_commit(bar2);
+            issue_gemm2(0);
+        }
+        // the first chunk must be consumed before the second overwrites the buffer
+        if (!__syncthreads_and(tc::mbar_wait(bar2, ph2, kWait))) {
+            status |= kStatusTimeout;
+            alive = false;
+            break;
+        }
+        ph2 ^= 1;
+        tc::tc_fence_after();
+        if (chunk == 1) store_G();
+        tc::fence_proxy_async();
+        tc::tc_fence_before();
+        __syncthreads();
+        if (tid == 0) {
+            tc::tc_fence_after();
+            issue_gemm2(1);
         }
         // ---- face lifts (FP32) while GEMM2 runs, into the Uop region ----
         cp_async_wait_all();
@@ -649,9 +686,9 @@ __global__ void __launch_bounds__(TcCfg<P>::NT, 1) tc_stage_kernel(StageArgs a)
         }
         __syncthreads();
     }
-    // a CTA that stopped early may still have its next tile's copy in flight:
-    // wait for it (bounded) before the shared memory goes away
-    if (!alive && tid == 0) (void)tc::mbar_wait(barU, phU, kWait);
+    // a CTA that gave up waiting for the operator may still have its copy in
+    // flight: wait for it (bounded) before the shared memory goes away
+    if (!alive && tid == 0) (void)tc::mbar_wait(barOp, 0, kWait);
     cp_async_wait_all();
     tc::tc_fence_before();
     __syncthreads();

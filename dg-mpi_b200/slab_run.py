@@ -78,6 +78,7 @@ def main():
                        "interior_elements": dc.part.ninterior, "owned_elements": dc.part.nowned},
             "status": status}), flush=True)
     dist.barrier()
+    dc.close()
     dist.destroy_process_group()
 
 
