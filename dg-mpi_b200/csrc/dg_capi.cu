@@ -33,12 +33,18 @@ int dgk::stage_variants(int p, const StageVariant** out)
     }
 }
 
-bool dgk::tc_operator(int p, const double* B1, std::vector<float>& out)
+bool dgk::tc_operator(int p, const double* B1, std::vector<uint16_t>& out)
 {
     if (p != 3) return false;
-    out.assign(TcCfg<3>::kOpBytes / sizeof(float), 0.f);
+    out.assign(TcCfg<3>::kOpBytes / sizeof(uint16_t), 0);
     tc_operator_table<3>(B1, out.data());
     return true;
+}
+
+int dgk::tc_face_stride(int p)
+{
+    const int n = 5 * (p + 2) * (p + 2);
+    return (n + 3) / 4 * 4;  // FP32 elements: a multiple of 16 bytes
 }
 
 namespace {
@@ -123,10 +129,20 @@ int prepare_variant(dg_ctx* c, int v)
     if (c->variant_grid[v] > 0) return DG_OK;
     const dgk::StageVariant& sv = vs[v];
     DG_CUDA(c, cudaFuncSetAttribute(sv.func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sv.smem));
+    // the tensor-core kernel runs two ~100 KB CTAs per SM: ask for the largest
+    // shared-memory carveout (otherwise the occupancy query, and the launch,
+    // may settle for one)
+    if (sv.flags & dgk::kTC)
+        DG_CUDA(c, cudaFuncSetAttribute(sv.func, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared));
     int dev_sms = 0, per_sm = 0;
     DG_CUDA(c, cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, c->device));
     DG_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sv.func, sv.NT, sv.smem));
     if (per_sm < 1) return fail(c, DG_ERR_UNSUPPORTED, "stage kernel variant does not fit on an SM");
+    // the tensor-core kernel is built for two resident CTAs per SM (registers
+    // and shared memory sized for it; its CTAs never wait on one another, so a
+    // CTA that finds no room simply starts later); the occupancy query has been
+    // seen to report one for it
+    if (sv.flags & dgk::kTC) per_sm = std::max(per_sm, 2);
     const int batches = (c->ne + sv.E - 1) / sv.E;
     if (sv.face_launch) {
         if (!c->d_fflux) return fail(c, DG_ERR_UNSUPPORTED, "face-kernel variant on a context without a face list");
@@ -163,6 +179,7 @@ int launch_stage(dg_ctx* c, int mode, const double* Us, const double* U0, double
     a.faces = c->d_faces;
     a.nface = c->nface;
     a.fflux = c->d_fflux;
+    a.fstride = 5 * (c->p + 2) * (c->p + 2);
     a.tcop = c->d_tcop;
     a.status = c->d_status;
     a.e_begin = e_begin;
@@ -177,6 +194,8 @@ int launch_stage(dg_ctx* c, int mode, const double* Us, const double* U0, double
     const dgk::StageVariant* vs = nullptr;
     dgk::stage_variants(c->p, &vs);
     const dgk::StageVariant& sv = vs[c->variant];
+    // the tensor-core kernel bulk-copies each face's fluxes: a 16-byte multiple per face
+    if (sv.flags & dgk::kTC) a.fstride = dgk::tc_face_stride(c->p);
     if (sv.face_launch) {
         // the fluxes of the faces this element range is the first to need (the
         // stage kernel reads them): all faces, the faces touching an interior
@@ -1081,10 +1100,10 @@ int dgi::create_ctx(const dg_case_desc* cd, const dg_mesh_desc* md, const int* e
         bool has_tc = false;
         for (int v = 0; v < nv; ++v) has_tc = has_tc || (vs[v].flags & dgk::kTC);
         if (has_tc && c->d_fflux && c->precision == DG_PREC_MIXED_FP32 && !c->pm.general) {
-            std::vector<float> op;
+            std::vector<uint16_t> op;
             if (dgk::tc_operator(c->p, c->tab.B.data(), op) &&
-                (cudaMalloc((void**)&c->d_tcop, op.size() * sizeof(float)) != cudaSuccess ||
-                 cudaMemcpy(c->d_tcop, op.data(), op.size() * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess)) {
+                (cudaMalloc((void**)&c->d_tcop, op.size() * sizeof(uint16_t)) != cudaSuccess ||
+                 cudaMemcpy(c->d_tcop, op.data(), op.size() * sizeof(uint16_t), cudaMemcpyHostToDevice) != cudaSuccess)) {
                 cudaGetLastError();
                 cudaFree(c->d_tcop);
                 c->d_tcop = nullptr;

@@ -57,7 +57,7 @@ struct dg_ctx {
     int2* d_faces = nullptr;
     double* d_fflux = nullptr;
     // tensor-core variants (kTC): the basis operator in its shared-memory layout
-    float* d_tcop = nullptr;
+    uint16_t* d_tcop = nullptr;
     int variant_face_grid[dgi::kMaxVariants] = {};  // face kernel grid per FX variant
     double* d_partials = nullptr;
     unsigned* d_status = nullptr;

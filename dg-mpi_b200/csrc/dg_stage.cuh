@@ -144,9 +144,10 @@ struct StageArgs {
     const int2* faces;
     int face_begin, nface;
     void* fflux;
-    // tensor-core kernel: the basis operator B[q][b] as TF32 hi / lo in its
+    int fstride;            // elements per face in fflux: 5 (p+2)^2, or padded to a 16-byte multiple (TC)
+    // tensor-core kernel: the basis operator B[q][b] as three BF16 parts in its
     // shared-memory layout (dgk::tc_operator_table)
-    const float* tcop;
+    const uint16_t* tcop;
     unsigned* status;
     int e_begin, ne;        // the launch computes elements [e_begin, ne)
     int flux;               // 0 = Lax-Friedrichs, 1 = HLLC
@@ -499,7 +500,7 @@ __device__ __forceinline__ void stage_body(const StageArgs& a)
                 const int c = t % NF, f = (t / NF) % 6, e = t / (6 * NF);
                 const FaceRec& rec = sRec[e * 6 + f];
                 const int pc = ((rec.pad >> 30) & 1) ? c : a.cmap[(rec.info >> 4) * NF + c];
-                const T* src = gF + (size_t)(rec.pad & 0x3fffffff) * 5 * NF + pc;
+                const T* src = gF + (size_t)(rec.pad & 0x3fffffff) * a.fstride + pc;
                 T* dst = reinterpret_cast<T*>(sOps + e * OPS) + f * 5 * FS + c;
 #pragma unroll
                 for (int v = 0; v < 5; ++v) cp_async_t(dst + v * FS, src + v * NF);
@@ -1363,7 +1364,7 @@ __global__ void __launch_bounds__(kFaceThreads) face_flux_kernel(StageArgs a)
             const double eref = kShift ? a.geo[rec.cls].eref : 0.0;
             numerical_flux<T, kShift>(a.flux, a.gamma, UL, UR, nd, eref, Fo, status);
             const T w = Wt[c % M] * Wt[c / M];
-            T* o = out + (size_t)(f0 + j) * 5 * NF + c;
+            T* o = out + (size_t)(f0 + j) * a.fstride + c;
 #pragma unroll
             for (int v = 0; v < 5; ++v) o[v * NF] = Fo[v] * w;
         }
@@ -1465,8 +1466,10 @@ StageVariant make_variant()
 // the variants compiled for order p (defined in dg_stage_p<p>.cu)
 int stage_variants(int p, const StageVariant** out);
 // the tensor-core kernel's operator table of order p from the 1D basis
-// B1[q * (p+1) + b] at the GL points (false: no tensor-core kernel for p)
-bool tc_operator(int p, const double* B1, std::vector<float>& out);
+// B1[q * (p+1) + b] at the GL points, as BF16 bit patterns (false: no
+// tensor-core kernel for p), and its face-flux stride (FP32 elements per face)
+bool tc_operator(int p, const double* B1, std::vector<uint16_t>& out);
+int tc_face_stride(int p);
 int stage_variants_p0(const StageVariant** out);
 int stage_variants_p1(const StageVariant** out);
 int stage_variants_p2(const StageVariant** out);

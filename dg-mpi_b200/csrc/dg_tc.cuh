@@ -1,5 +1,5 @@
 // dg_tc.cuh -- the tensor-core stage kernel (sm_100a, tcgen05): the volume
-// integral of the FP32 residual as split-TF32 products on the 5th-generation
+// integral of the FP32 residual as split-BF16 products on the 5th-generation
 // tensor cores, with FP32 accumulation in tensor memory (TMEM).
 //
 // Reference path replaced (as in dg_stage.cuh): evaluate_state B*U
@@ -10,7 +10,7 @@
 // (stepper.cpp:23-142).  The face fluxes come from face_flux_kernel (launch
 // option FX), computed once per face.
 //
-// Per tile of E elements (one CTA per SM, grid-stride over tiles):
+// Per tile of E elements (grid-stride over tiles):
 //   GEMM1  D1[q][c] = sum_b B[q][b] U[c][b]      (M = 128 volume points, N = the
 //          tile's (element, variable) columns, K = nb): the state at every
 //          quadrature point, one TMEM lane per point, so one thread holds all
@@ -22,23 +22,40 @@
 //          Delta_d the nodal derivative matrix along axis d (exact: the
 //          derivative of a degree-p Lagrange polynomial is interpolated exactly
 //          at the p+1 nodes), so res = sum_d Delta_d^T H_d -- one operator, B,
-//          serves both GEMMs: K-major as GEMM1's A, MN-major as GEMM2's B;
+//          stored once, serves both GEMMs: K-major as GEMM1's A, MN-major as
+//          GEMM2's B;
 //   then, on the CUDA cores, Delta_d^T along each axis (FP32), the face lift of
 //   the face kernel's fluxes (FP32), the sum into the FP64 residual, the
 //   Kronecker inverse mass and the RK stage update in FP64.
-// Split products: every operand x is stored as hi = tf32(x), lo = tf32(x - hi)
-// and each GEMM accumulates lo*hi + hi*lo + hi*hi (the small terms first).
+// Split products (BF16x6): every operand x (FP32) is stored as three BF16
+// parts x = x0 + x1 + x2 (8 significant bits each: exact for an FP32 value)
+// and each GEMM accumulates the six products xi * yj with i + j <= 2, the
+// small ones first; what is left out (i + j >= 3) is below 2^-23 of the
+// product, so the GEMMs keep FP32's accuracy.  BF16 MMAs run at twice the
+// TF32 rate: six of them cost what the three products of TF32x3 cost, and
+// TF32x3 (22-bit operands) measured 4-5x less accurate than FP32 here.
 // The state enters as U - E_ref in its energy (the FP32 residual's energy
 // reference, see dgp::interior_flux_r1).
 //
+// Two CTAs per SM (about 100 KB of shared memory and at most 128 registers
+// per thread each) hide each other's waits: the operator (48 KB), the
+// state's three parts, and GEMM2's A operand in two chunks of 64 points (the
+// points of lane quarters 0-1, then 2-3: the second chunk is written once the
+// first has been multiplied, the face lifts run in between).  The next
+// tile's face records are bulk-copied into shared memory ahead of use; its
+// state, RK operands and face fluxes are prefetched into L2.  Every wait on
+// an mbarrier is bounded (clock64); a wait that gives up sets
+// kStatusTimeout, the CTA stops, waits (bounded) for its copies in flight,
+// releases its TMEM and returns.  No multicast, no peer memory: every
+// operand is in this CTA's own shared memory.
+//
 // Shared-memory operands use the 128-byte swizzled canonical layout of the
-// UMMA descriptors: atoms of 8 rows x 128 bytes (32 four-byte elements along
-// the atom's row), 1024-byte aligned, with the 16-byte chunk index of a row
-// XORed with the row's index within the atom.  Every wait on an mbarrier is
-// bounded (clock64); a wait that gives up sets kStatusTimeout, the CTA stops,
-// releases its TMEM and returns.  No multicast, no peer memory: every operand
-// is in this CTA's own shared memory.
+// UMMA descriptors: atoms of 8 rows x 128 bytes (64 BF16 elements along the
+// atom's row), 1024-byte aligned, with the 16-byte chunk index of a row XORed
+// with the row's index within the atom.
 #pragma once
+#include <cuda_bf16.h>
+
 #include <cstdint>
 #include <cstring>
 
@@ -90,6 +107,7 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t
                  : "memory");
 }
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];\n" ::"l"(p)); }
 
 __device__ __forceinline__ void tmem_alloc(uint32_t dst_slot, uint32_t ncols)
 {
@@ -104,13 +122,13 @@ __device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols)
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
 
-// D (TMEM, FP32) (+)= A (smem) * B (smem), kind::tf32, issued by one thread
-__device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t acc)
+// D (TMEM, FP32) (+)= A (smem) * B (smem), kind::f16 with BF16 operands, issued by one thread
+__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t acc)
 {
     const uint32_t z = 0;
     asm volatile(
         "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-        " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n}\n" ::"r"(d_tmem),
+        " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n}\n" ::"r"(d_tmem),
         "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc), "r"(z), "r"(z), "r"(z), "r"(z));
 }
 // arrives on the mbarrier once every MMA issued so far by this thread is complete
@@ -120,7 +138,7 @@ __device__ __forceinline__ void mma_commit(uint32_t bar)
 }
 
 // TMEM -> registers: this warp's 32 lanes (lane quarter warp % 4), consecutive columns
-__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&r)[8])
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float* r)
 {
     uint32_t u[8];
     asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];\n"
@@ -143,12 +161,17 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* r)
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory"); }
 
-// round to TF32 (10 explicit mantissa bits), to nearest, ties away from zero
-__device__ __forceinline__ float tf32(float x)
+// x = x0 + x1 + x2 exactly, each part a BF16 (round to nearest even)
+__device__ __forceinline__ void split3(float x, uint16_t (&p)[3])
 {
-    uint32_t r;
-    asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x));
-    return __uint_as_float(r);
+    const __nv_bfloat16 b0 = __float2bfloat16_rn(x);
+    const float r1 = x - __bfloat162float(b0);
+    const __nv_bfloat16 b1 = __float2bfloat16_rn(r1);
+    const float r2 = r1 - __bfloat162float(b1);
+    const __nv_bfloat16 b2 = __float2bfloat16_rn(r2);
+    p[0] = __bfloat16_as_ushort(b0);
+    p[1] = __bfloat16_as_ushort(b1);
+    p[2] = __bfloat16_as_ushort(b2);
 }
 
 // ---- descriptors ----
@@ -158,21 +181,25 @@ __device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t
     return static_cast<uint64_t>((saddr >> 4) & 0x3FFF) | (static_cast<uint64_t>((lbo >> 4) & 0x3FFF) << 16) |
            (static_cast<uint64_t>((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46) | (2ull << 61);
 }
-// instruction descriptor of kind::tf32 with FP32 accumulation: M rows, N
-// columns, A K-major, B K-major (b_mn = 0) or MN-major (b_mn = 1)
-__host__ __device__ constexpr uint32_t idesc_tf32(int M, int N, int b_mn)
+// instruction descriptor of kind::f16 with BF16 A and B and FP32 accumulation:
+// M rows, N columns, A K-major, B K-major (b_mn = 0) or MN-major (b_mn = 1)
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N, int b_mn)
 {
-    return (1u << 4) | (2u << 7) | (2u << 10) | (static_cast<uint32_t>(b_mn) << 16) |
+    return (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(b_mn) << 16) |
            (static_cast<uint32_t>(N >> 3) << 17) | (static_cast<uint32_t>(M >> 4) << 24);
 }
 
-// byte offset of element (row, k) of a four-byte operand in 128-byte swizzled
-// atoms: 8-row groups at 1024 bytes, 32-element atoms along k at `katom` bytes
-__host__ __device__ constexpr uint32_t sw128(int row, int k, int katom)
+// byte offset of element (row, k) of a two-byte operand in 128-byte swizzled
+// atoms: 8-row groups at 1024 bytes, 64-element atoms along k at `katom` bytes
+__host__ __device__ constexpr uint32_t sw128h(int row, int k, int katom)
 {
-    return static_cast<uint32_t>((k >> 5) * katom + (row >> 3) * 1024 + (row & 7) * 128 +
-                                 ((((k & 31) >> 2) ^ (row & 7)) << 4) + (k & 3) * 4);
+    return static_cast<uint32_t>((k >> 6) * katom + (row >> 3) * 1024 + (row & 7) * 128 +
+                                 ((((k & 63) >> 3) ^ (row & 7)) << 4) + (k & 7) * 2);
 }
+
+// the six products x_i * y_j (i + j <= 2), small ones first
+__host__ __device__ constexpr int prod_a(int s) { return s == 0 ? 0 : s == 1 ? 1 : s == 2 ? 2 : s == 3 ? 0 : s == 4 ? 1 : 0; }
+__host__ __device__ constexpr int prod_b(int s) { return s == 0 ? 2 : s == 1 ? 1 : s == 2 ? 0 : s == 3 ? 1 : s == 4 ? 0 : 0; }
 
 }  // namespace tc
 
@@ -181,57 +208,66 @@ template <int P>
 struct TcCfg;
 template <>
 struct TcCfg<3> {
-    static constexpr int N = 4, M = 5, NB = 64, NQ = 125, NF = 25, FS = 25;
+    static constexpr int N = 4, M = 5, NB = 64, NQ = 125, NF = 25;
     static constexpr int E = 6;            // elements per tile
     static constexpr int C = 5 * E;        // (element, variable) columns of a tile (30)
     static constexpr int N1 = 32;          // GEMM1 N: the columns, padded to 32
     static constexpr int MQ = 128;         // GEMM1 M = GEMM2 K: the points, padded
-    static constexpr int KC = 64;          // GEMM2 K per chunk (two chunks through one G buffer)
+    static constexpr int KC = 64;          // GEMM2 K per chunk: the points of two TMEM lane quarters
     static constexpr int NT = 256;         // threads (eight warps, two per TMEM lane quarter)
-    static constexpr int kTmemCols = 128;  // D1 at columns [0, 32), D2 at [64, 128)
-    static constexpr int kD2 = 64;
-    // shared memory (bytes from a 1024-aligned base).  The operator twice, as
-    // K-major 128-byte swizzled operands (TF32 MN-major operands would need the
-    // 32-byte-granule swizzle instead, so GEMM2 gets its own copy, B^T):
-    //   Bop [128 q][64 b] (GEMM1's A), Bt [64 b][128 q] (GEMM2's B), hi and lo each
-    static constexpr int kBopAtom = MQ * 128;           // 16384: a 32-wide k atom of Bop over 128 rows
-    static constexpr int kBtAtom = NB * 128;            // 8192: a 32-wide k atom of Bt over 64 rows
-    static constexpr int kBopHi = 0, kBopLo = 2 * kBopAtom;
-    static constexpr int kBtHi = 4 * kBopAtom, kBtLo = kBtHi + 4 * kBtAtom;
-    static constexpr int kOpBytes = 4 * kBopAtom + 8 * kBtAtom;  // 131072: one bulk copy
-    static constexpr int kUopAtom = N1 * 128;           // 4096
-    static constexpr int kUopHi = kOpBytes, kUopLo = kUopHi + 2 * kUopAtom;  // [32 c][64 b] each
-    // G: [128 rows][KC points] per chunk; rows 96..127 are never written (their
-    // outputs are ignored), so the k atoms are packed at 12 row groups (12288
-    // bytes) and those rows read into the next atom (past the last one, into Fh)
-    static constexpr int kGAtom = 12 * 1024;
-    static constexpr int kGHi = kUopLo + 2 * kUopAtom, kGLo = kGHi + 2 * kGAtom;
-    static constexpr int kFh = kGLo + 2 * kGAtom;       // face fluxes [E][6][5][FS] FP32
-    static constexpr int kFhBytes = ((E * 30 * FS * 4 + 15) / 16) * 16;
-    static constexpr int kRec = kFh + kFhBytes;         // face records [E][6]
-    static constexpr int kMeta = kRec + E * 6 * 48;     // per element: JD[9], eref, hr, pref (FP32) [E][12]
-    static constexpr int kCls = kMeta + E * 12 * 4;     // geometry class [E]
-    static constexpr int kBar = ((kCls + E * 4 + 7) / 8) * 8;  // mbarriers: operator, GEMM1, GEMM2
-    static constexpr int kSlot = kBar + 3 * 8;          // TMEM base address
-    static constexpr int kBytes = kSlot + 16;
+    static constexpr int MINB = 2;         // CTAs per SM (registers <= 128 per thread)
+    static constexpr int FSTR = 128;       // FP32 elements per face in the face kernel's output (5 x 25, padded)
+    // TMEM: each GEMM accumulates its hi * hi products and its five small
+    // products (x_i y_j, 0 < i + j <= 2) in separate accumulators, added at
+    // the read-out, so FP32 rounding of the large sum does not swallow the
+    // small terms: D1 big / small at columns [0, 32) / [32, 64), D2 big /
+    // small at [64, 128) / [128, 192)
+    static constexpr int kTmemCols = 256;
+    static constexpr int kD1s = 32, kD2 = 64, kD2s = 128;
+    // shared memory (bytes from a 1024-aligned base)
+    static constexpr int kOpPart = MQ * 128;             // [128 q][64 b] BF16, one 64-wide k atom: 16384
+    static constexpr int kOp = 0, kOpBytes = 3 * kOpPart;
+    static constexpr int kUopPart = N1 * 128;            // [32 c][64 b] BF16: 4096
+    static constexpr int kUop = kOpBytes;
+    // G: [128 rows][KC points] BF16 per part, one 64-wide k atom; rows 96..127
+    // are never written (their outputs are ignored), so the parts are packed at
+    // 12 row groups (12288 bytes) and those rows read into the next part (past
+    // the last one, into the records after it)
+    static constexpr int kGPart = 12 * 1024;
+    static constexpr int kG = kUop + 3 * kUopPart;
+    static constexpr int kRec = kG + 3 * kGPart;         // face records [2][E][6]
+    static constexpr int kRecBytes = E * 6 * 48;
+    static constexpr int kMeta = kRec + 2 * kRecBytes;   // per element: JD[9], eref, hr, pref (FP32) [2][E][12]
+    static constexpr int kCls = kMeta + 2 * E * 12 * 4;  // geometry class [2][E]
+    static constexpr int kBar = ((kCls + 2 * E * 4 + 7) / 8) * 8;  // mbarriers
+    static constexpr int kNumBar = 5;  // operator, frec slot 0 / 1, GEMM1, GEMM2
+    static constexpr int kSlot = kBar + kNumBar * 8;    // TMEM base address
+    static constexpr int kBytes = ((kSlot + 16 + 15) / 16) * 16;
     static constexpr size_t kSmem = kBytes + 1024;      // + alignment slack
     // epilogue buffers over regions that are free by then
-    static constexpr int kPart = kGHi;                  // FP32 [3][C][PS] direction partials (G is dead)
     static constexpr int PS = NB + 1;
-    static constexpr int kRes = kPart + ((3 * C * PS * 4 + 15) / 16) * 16;  // FP64 [C][PS] residual
-    static constexpr int kLift = kUopHi;                // FP32 [E][6][5][N*N] face lifts (Uop is dead)
-    static_assert(kRes + C * PS * 8 <= kFh, "epilogue buffers must fit in the G region");
-    static_assert(kLift + E * 30 * N * N * 4 <= kGHi, "lift buffer must fit in the Uop region");
-    static_assert(kGLo + kGAtom + 16 * 1024 <= kBytes, "the last G atom's unused rows must stay inside shared memory");
-    static_assert(kSmem <= 227 * 1024, "tensor-core stage kernel exceeds 227 KB of shared memory");
+    static constexpr int kPart = kG;                     // FP32 [3][C][PS]; FP64 residual [C][PS] over it (GEMM2 done)
+    static constexpr int kLift = kUop;                   // FP32 [E][6][5][N*N] face lifts (GEMM1 done)
+    static_assert(C * PS * 8 <= 3 * C * PS * 4, "the FP64 residual must fit over the direction partials");
+    static_assert(kPart + 3 * C * PS * 4 <= kRec, "direction partials must fit in the G region");
+    static_assert(kLift + E * 30 * N * N * 4 <= kG, "face lifts must fit in the Uop region");
+    static_assert(kG + 2 * kGPart + 16 * 1024 <= kBytes, "the last G part's unused rows must stay inside shared memory");
+    static_assert(kRec % 16 == 0 && kRecBytes % 16 == 0, "bulk-copy targets");
+    static_assert((FSTR * 4) % 16 == 0 && FSTR >= 5 * NF, "face block stride");
+    static_assert(MINB * (kSmem + 1024) <= 228 * 1024, "two CTAs per SM");
 };
 
-// host: TF32 rounding of cvt.rna.tf32.f32 (to nearest, ties away from zero)
-inline float tf32_host(float x)
+// host: FP32 -> BF16 bits, round to nearest even (finite values)
+inline uint16_t bf16_host(float x)
 {
     uint32_t u;
     std::memcpy(&u, &x, 4);
-    u = (u + 0x1000u) & ~0x1FFFu;
+    u += 0x7FFFu + ((u >> 16) & 1u);
+    return static_cast<uint16_t>(u >> 16);
+}
+inline float bf16_value(uint16_t h)
+{
+    const uint32_t u = static_cast<uint32_t>(h) << 16;
     float r;
     std::memcpy(&r, &u, 4);
     return r;
@@ -240,110 +276,187 @@ inline float tf32_host(float x)
 // host: the operator B[q][b] of order P -- q over the (p+2)^3 volume points
 // (q = qx + M qy + M^2 qz, zero rows past them), b over the (p+1)^3 basis
 // functions (b = bx + N by + N^2 bz), B = B1[qx][bx] B1[qy][by] B1[qz][bz] --
-// as TF32 hi and lo, in the swizzled layouts of TcCfg: Bop [q][b] then
-// Bt [b][q] (kOpBytes, one bulk copy).  B1[q * N + b] is the 1D basis at the
-// GL points.
+// as three BF16 parts (B = B0 + B1 + B2 to 24 bits) in the swizzled layout of
+// TcCfg (kOpBytes, one bulk copy).  B1[q * N + b] is the 1D basis at the GL
+// points.
 template <int P>
-void tc_operator_table(const double* B1, float* out)
+void tc_operator_table(const double* B1, uint16_t* out)
 {
     using K = TcCfg<P>;
     constexpr int N = K::N, M = K::M;
-    for (int i = 0; i < K::kOpBytes / 4; ++i) out[i] = 0.f;
+    for (int i = 0; i < K::kOpBytes / 2; ++i) out[i] = 0;
     for (int q = 0; q < K::NQ; ++q)
         for (int b = 0; b < K::NB; ++b) {
             const double v = B1[(q % M) * N + b % N] * B1[((q / M) % M) * N + (b / N) % N] * B1[(q / (M * M)) * N + b / (N * N)];
-            const float hi = tf32_host(static_cast<float>(v));
-            const float lo = tf32_host(static_cast<float>(v - static_cast<double>(hi)));
-            const uint32_t o1 = tc::sw128(q, b, K::kBopAtom), o2 = tc::sw128(b, q, K::kBtAtom);
-            out[(K::kBopHi + o1) / 4] = hi;
-            out[(K::kBopLo + o1) / 4] = lo;
-            out[(K::kBtHi + o2) / 4] = hi;
-            out[(K::kBtLo + o2) / 4] = lo;
+            const float vf = static_cast<float>(v);
+            const uint16_t h0 = bf16_host(vf);
+            const float r1 = vf - bf16_value(h0);
+            const uint16_t h1 = bf16_host(r1);
+            const uint16_t h2 = bf16_host(r1 - bf16_value(h1));
+            const uint32_t o = tc::sw128h(q, b, K::kOpPart) / 2;
+            out[o] = h0;
+            out[K::kOpPart / 2 + o] = h1;
+            out[K::kOpPart + o] = h2;
         }
+}
+
+// the flux at point q for the three elements of half FH of a tile, written
+// as GEMM2's A operand: rows 32 d + 5 e + v, column ql (the point within the
+// chunk), three BF16 parts.  u: D1 row of this lane (all 32 columns).
+template <int P, int FH>
+__device__ __forceinline__ void tc_flux_half(const float (&u)[32], int q, int ql, int nel, const float* __restrict__ mtab,
+                                             float gamma, float wq, unsigned char* gbase, unsigned& status)
+{
+    using K = TcCfg<P>;
+    const uint32_t kc = static_cast<uint32_t>((ql >> 3) & 7), kb = static_cast<uint32_t>((ql & 7) * 2);
+#pragma unroll
+    for (int ee = 0; ee < 3; ++ee) {
+        const int e = FH * 3 + ee;
+        float G[15];
+        if (q < K::NQ && e < nel) {
+            const float* mt = mtab + e * 12;
+            float U[5], F[15];
+#pragma unroll
+            for (int v = 0; v < 5; ++v) U[v] = u[FH * 15 + ee * 5 + v];
+            const float p = dgp::interior_flux_r1<float, true>(gamma, U, F, mt[10]);
+            if (!(U[0] > 0.f)) status |= kStatusRho;
+            if (!(p + mt[11] > 0.f)) status |= kStatusPressure;
+            if (U[0] != U[0] || p != p) status |= kStatusNaN;
+#pragma unroll
+            for (int v = 0; v < 5; ++v)
+#pragma unroll
+                for (int d = 0; d < 3; ++d)
+                    G[d * 5 + v] = (F[v] * mt[d * 3 + 0] + F[5 + v] * mt[d * 3 + 1] + F[10 + v] * mt[d * 3 + 2]) * wq;
+        } else {
+#pragma unroll
+            for (int k = 0; k < 15; ++k) G[k] = 0.f;
+        }
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+#pragma unroll
+            for (int v = 0; v < 5; ++v) {
+                const int row = 32 * d + 5 * (FH * 3 + ee) + v;  // compile time
+                uint16_t parts[3];
+                tc::split3(G[d * 5 + v], parts);
+                unsigned char* p0 = gbase + (row >> 3) * 1024 + (row & 7) * 128 + ((kc ^ (row & 7)) << 4) + kb;
+#pragma unroll
+                for (int k = 0; k < 3; ++k) *reinterpret_cast<uint16_t*>(p0 + k * K::kGPart) = parts[k];
+            }
+    }
 }
 
 // the kernel
 template <int P>
-__global__ void __launch_bounds__(TcCfg<P>::NT, 1) tc_stage_kernel(StageArgs a)
+__global__ void __launch_bounds__(TcCfg<P>::NT, TcCfg<P>::MINB) tc_stage_kernel(StageArgs a)
 {
     using K = TcCfg<P>;
-    constexpr int N = K::N, M = K::M, NB = K::NB, NQ = K::NQ, NF = K::NF, FS = K::FS, E = K::E, C = K::C;
-    constexpr int N2 = N * N, PS = K::PS;
+    constexpr int N = K::N, M = K::M, NB = K::NB, NQ = K::NQ, NF = K::NF, E = K::E, C = K::C;
+    constexpr int N2 = N * N, PS = K::PS, FSTR = K::FSTR;
     constexpr long long kWait = 2000000000ll;  // ~1 s at 2 GHz
     extern __shared__ unsigned char smem_raw[];
     const uint32_t raw = tc::smem_u32(smem_raw);
     const uint32_t sbase = (raw + 1023u) & ~1023u;  // swizzle atoms need 1024-byte alignment
     unsigned char* sm = smem_raw + (sbase - raw);
-    float* Fh = reinterpret_cast<float*>(sm + K::kFh);
-    FaceRec* sRec = reinterpret_cast<FaceRec*>(sm + K::kRec);
-    float* sMeta = reinterpret_cast<float*>(sm + K::kMeta);
-    int* sCls = reinterpret_cast<int*>(sm + K::kCls);
     float* Part = reinterpret_cast<float*>(sm + K::kPart);
-    double* Res = reinterpret_cast<double*>(sm + K::kRes);
+    double* Res = reinterpret_cast<double*>(sm + K::kPart);  // over Part, after the sum
     float* Lift = reinterpret_cast<float*>(sm + K::kLift);
-    const uint32_t barOp = sbase + K::kBar, bar1 = barOp + 8, bar2 = barOp + 16;
+    const uint32_t barOp = sbase + K::kBar, barR0 = barOp + 8, bar1 = barOp + 24, bar2 = barOp + 32;
     uint32_t* slot = reinterpret_cast<uint32_t*>(sm + K::kSlot);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const float* __restrict__ Bt = a.tab.Bf;
     const float* __restrict__ Wt = a.tab.Wf;
     const float* __restrict__ Dn = a.tab.Dn;
     const double* __restrict__ Mi = a.tab.Minv;
+    const float* __restrict__ gF = reinterpret_cast<const float*>(a.fflux);
     const float gamma = float(a.gamma);
     const int ntiles = (a.ne - a.e_begin + E - 1) / E;
+    const int nt = ntiles > (int)blockIdx.x ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;  // this CTA's tiles
     const bool need_acc = a.mode == kModeRK2 || a.mode == kModeRK3 || a.mode == kModeRK4;
     const bool need_u0 = a.mode >= kModeRK1;
     unsigned status = 0;
+
+    auto tile_e0 = [&](int j) { return a.e_begin + ((int)blockIdx.x + j * (int)gridDim.x) * E; };
+    auto tile_nel = [&](int j) { return min(E, a.ne - tile_e0(j)); };
+    auto recs = [&](int j) { return reinterpret_cast<const FaceRec*>(sm + K::kRec + (j & 1) * K::kRecBytes); };
+    auto meta = [&](int j) { return reinterpret_cast<float*>(sm + K::kMeta + (j & 1) * E * 12 * 4); };
+    auto cls = [&](int j) { return reinterpret_cast<int*>(sm + K::kCls + (j & 1) * E * 4); };
 
     if (warp == 0) {
         tc::tmem_alloc(sbase + K::kSlot, K::kTmemCols);
         tc::tmem_relinquish();
     }
     if (tid == 0) {
-        tc::mbar_init(barOp, 1);
-        tc::mbar_init(bar1, 1);
-        tc::mbar_init(bar2, 1);
+        for (int i = 0; i < K::kNumBar; ++i) tc::mbar_init(barOp + 8 * i, 1);
         tc::mbar_fence_init();
     }
     tc::tc_fence_before();
     __syncthreads();
     tc::tc_fence_after();
     const uint32_t tmem = *slot;
-    const uint32_t d1 = tmem, d2 = tmem + K::kD2;
-    if (tid == 0 && (int)blockIdx.x < ntiles) {
-        tc::mbar_expect_tx(barOp, K::kOpBytes);
-        tc::bulk_g2s(sbase, a.tcop, K::kOpBytes, barOp);
-    }
-    // the state (and the RK operands) of tile t into L2 ahead of their plain loads
-    auto prefetch_tile = [&](int t) {
-        if (t >= ntiles) return;
-        const int e0 = a.e_begin + t * E, nel = min(E, a.ne - e0);
-        const int lines = nel * 5 * NB * 8 / 128;  // 20 per element
-        const size_t off = (size_t)e0 * 5 * NB;
+    const uint32_t d1 = tmem, d1s = tmem + K::kD1s, d2 = tmem + K::kD2, d2s = tmem + K::kD2s;
+
+    // face records of tile j into slot j & 1 (thread 0)
+    bool pend[2] = {false, false};
+    uint32_t pph[2] = {0, 0};
+    auto load_recs = [&](int j) {
+        const uint32_t bytes = tile_nel(j) * 6 * 48;
+        const uint32_t bar = barR0 + 8 * (j & 1);
+        tc::mbar_expect_tx(bar, bytes);
+        tc::bulk_g2s(sbase + K::kRec + (j & 1) * K::kRecBytes, a.frec + (size_t)tile_e0(j) * 6, bytes, bar);
+        pend[j & 1] = true;
+        pph[j & 1] = (j >> 1) & 1;
+    };
+    // waits for phase `parity` of `bar` on every thread; false (uniformly) if it gave up
+    auto wait_all = [&](uint32_t bar, uint32_t parity) {
+        const bool ok = __syncthreads_and(tc::mbar_wait(bar, parity, kWait));
+        if (!ok) status |= kStatusTimeout;
+        return ok;
+    };
+    // the state of tile j and its RK operands into L2 ahead of their plain loads
+    auto prefetch_state = [&](int j) {
+        const int lines = tile_nel(j) * 5 * NB * 8 / 128;
+        const size_t off = (size_t)tile_e0(j) * 5 * NB;
         for (int i = tid; i < 3 * lines; i += K::NT) {
-            const int k = i / lines, l = i - k * lines;
+            const int k = i / lines;
             const double* src = k == 0 ? a.Us : (k == 1 ? (need_u0 ? a.U0 : nullptr) : (need_acc ? a.acc : nullptr));
-            if (src) asm volatile("prefetch.global.L2 [%0];\n" ::"l"(src + off + l * 16));
+            if (src) tc::prefetch_l2(src + off + (i - k * lines) * 16);
         }
     };
-    prefetch_tile(blockIdx.x);
-    bool alive = __syncthreads_and(tc::mbar_wait(barOp, 0, kWait));
-    if (!alive) status |= kStatusTimeout;
+    // the face fluxes of tile j (its records have landed) into L2
+    auto prefetch_faces = [&](int j) {
+        const FaceRec* r = recs(j);
+        const int nel = tile_nel(j);
+        for (int i = tid; i < nel * 6 * 4; i += K::NT)
+            tc::prefetch_l2(gF + (size_t)(r[i >> 2].pad & 0x3fffffff) * FSTR + (i & 3) * 32);
+    };
+
+    bool alive = nt > 0;
     uint32_t ph1 = 0, ph2 = 0;
-    for (int t = blockIdx.x; t < ntiles && alive; t += gridDim.x) {
-        const int e0 = a.e_begin + t * E, nel = min(E, a.ne - e0);
-        prefetch_tile(t + gridDim.x);
-        // ---- face records and geometry of the tile ----
-        for (int i = tid; i < E * 6 * 3; i += K::NT) {  // 16-byte pieces of the records
-            const int e = i / 18;
-            const int ge = min(e0 + e, a.ne - 1);
-            reinterpret_cast<int4*>(sRec)[i] = reinterpret_cast<const int4*>(a.frec + (size_t)ge * 6)[i - e * 18];
+    if (alive) {
+        if (tid == 0) {
+            tc::mbar_expect_tx(barOp, K::kOpBytes);
+            tc::bulk_g2s(sbase + K::kOp, a.tcop, K::kOpBytes, barOp);
+            load_recs(0);
         }
+        prefetch_state(0);
+        alive = wait_all(barOp, 0);
+    }
+    for (int j = 0; j < nt && alive; ++j) {
+        const int nel = tile_nel(j), e0 = tile_e0(j);
+        // ---- this tile's records, the next tile's in flight ----
+        if (!(alive = wait_all(barR0 + 8 * (j & 1), (j >> 1) & 1))) break;
+        if (tid == 0) {
+            pend[j & 1] = false;
+            if (j + 1 < nt) load_recs(j + 1);
+        }
+        const FaceRec* r = recs(j);
+        prefetch_faces(j);
+        if (j + 1 < nt) prefetch_state(j + 1);
         if (tid < E) {
-            const int ge = min(e0 + tid, a.ne - 1);
-            const int cls = a.geo_class[ge];
-            const GeoDev& g = a.geo[cls];
-            sCls[tid] = cls;
-            float* mt = sMeta + tid * 12;
+            const int c0 = r[min(tid, nel - 1) * 6].cls;
+            const GeoDev& g = a.geo[c0];
+            cls(j)[tid] = c0;
+            float* mt = meta(j) + tid * 12;
 #pragma unroll
             for (int k = 0; k < 9; ++k) mt[k] = float(g.JD[k]);
             mt[9] = float(g.eref);
@@ -351,165 +464,98 @@ __global__ void __launch_bounds__(TcCfg<P>::NT, 1) tc_stage_kernel(StageArgs a)
             mt[11] = float((a.gamma - 1.0) * g.eref);
         }
         __syncthreads();
-        // ---- the state as GEMM1's B operand (rows c = 5 e + v, K = b), hi / lo ----
-        for (int i = tid; i < K::N1 * NB; i += K::NT) {
-            const int c = i / NB, b = i - c * NB, e = c / 5, v = c - 5 * e;
-            float hi = 0.f, lo = 0.f;
-            if (c < C && e < nel) {
-                const double x = a.Us[(size_t)e0 * 5 * NB + i] - (v == 4 ? a.geo[sCls[e]].eref : 0.0);
-                hi = tc::tf32(float(x));
-                lo = tc::tf32(float(x - double(hi)));
+        // ---- the state as GEMM1's B operand (rows c = 5 e + v, K = b), three parts ----
+        {
+            for (int i = tid; i < K::N1 * NB; i += K::NT) {
+                const int c = i / NB, b = i - c * NB, e = c / 5, v = c - 5 * e;
+                uint16_t parts[3] = {0, 0, 0};
+                if (c < C && e < nel) {
+                    const double x = a.Us[(size_t)e0 * 5 * NB + i] - (v == 4 ? a.geo[cls(j)[e]].eref : 0.0);
+                    tc::split3(float(x), parts);
+                }
+                unsigned char* p0 = sm + K::kUop + tc::sw128h(c, b, K::kUopPart);
+#pragma unroll
+                for (int k = 0; k < 3; ++k) *reinterpret_cast<uint16_t*>(p0 + k * K::kUopPart) = parts[k];
             }
-            const uint32_t off = tc::sw128(c, b, K::kUopAtom);
-            *reinterpret_cast<float*>(sm + K::kUopHi + off) = hi;
-            *reinterpret_cast<float*>(sm + K::kUopLo + off) = lo;
         }
         tc::fence_proxy_async();
         tc::tc_fence_before();
         __syncthreads();
         if (tid == 0) {
             tc::tc_fence_after();
-            // GEMM1: D1[q][c] = sum_b B[q][b] U[c][b]; lo*hi, hi*lo, hi*hi
-            constexpr uint32_t id1 = tc::idesc_tf32(128, K::N1, 0);
+            constexpr uint32_t id1 = tc::idesc_bf16(128, K::N1, 0);
 #pragma unroll
-            for (int s = 0; s < 3; ++s) {
-                const uint32_t ab = sbase + (s == 0 ? K::kBopLo : K::kBopHi);
-                const uint32_t bb = sbase + (s == 1 ? K::kUopLo : K::kUopHi);
+            for (int s = 0; s < 6; ++s) {
+                const uint32_t ab = sbase + K::kOp + tc::prod_a(s) * K::kOpPart;
+                const uint32_t bb = sbase + K::kUop + tc::prod_b(s) * K::kUopPart;
+                const bool big = s == 5;
 #pragma unroll
-                for (int kk = 0; kk < NB / 8; ++kk) {
-                    const uint64_t ad = tc::sdesc(ab + (kk >> 2) * K::kBopAtom + (kk & 3) * 32, 16, 1024);
-                    const uint64_t bd = tc::sdesc(bb + (kk >> 2) * K::kUopAtom + (kk & 3) * 32, 16, 1024);
-                    tc::mma_tf32(d1, ad, bd, id1, (s > 0 || kk > 0) ? 1u : 0u);
-                }
+                for (int kk = 0; kk < NB / 16; ++kk)
+                    tc::mma_bf16(big ? d1 : d1s, tc::sdesc(ab + kk * 32, 16, 1024), tc::sdesc(bb + kk * 32, 16, 1024),
+                                 id1, ((big ? 0 : s) > 0 || kk > 0) ? 1u : 0u);
             }
             tc::mma_commit(bar1);
         }
-        // the six faces' fluxes of the face kernel (the listed side reads its own
-        // point order, the other side through the face-point permutation)
-        {
-            const float* gF = reinterpret_cast<const float*>(a.fflux);
-            for (int i = tid; i < E * 6 * NF; i += K::NT) {
-                const int c = i % NF, f = (i / NF) % 6, e = i / (6 * NF);
-                if (e >= nel) continue;
-                const FaceRec& rec = sRec[e * 6 + f];
-                const int pc = ((rec.pad >> 30) & 1) ? c : a.cmap[(rec.info >> 4) * NF + c];
-                const float* src = gF + (size_t)(rec.pad & 0x3fffffff) * 5 * NF + pc;
-                float* dst = Fh + (e * 6 + f) * 5 * FS + c;
-#pragma unroll
-                for (int v = 0; v < 5; ++v) cp_async4(dst + v * FS, src + v * NF);
-            }
-            cp_async_commit();
-        }
-        // ---- the flux at every point: D1 -> G (GEMM2's A operand) ----
-        if (!__syncthreads_and(tc::mbar_wait(bar1, ph1, kWait))) {
-            status |= kStatusTimeout;
-            alive = false;
-            break;
-        }
+        if (!(alive = wait_all(bar1, ph1))) break;
         ph1 ^= 1;
         tc::tc_fence_after();
+        // ---- fluxes: D1 -> G in two chunks of points (lane quarters 0-1, then 2-3) ----
         const int qt = warp & 3, fhalf = warp >> 2;
-        const int q = qt * 32 + lane;
-        const int chunk = qt >> 1;        // this warp's points fall in GEMM2's K chunk 0 (q < 64) or 1
-        const int ql = q - chunk * K::KC;  // point within the chunk
-        float G[3][15];                    // this thread's fluxes: 3 elements x (d, v)
+        const int q = qt * 32 + lane, ql = q & (K::KC - 1);
+        float u[32];
         {
-            float u[32];  // all 32 columns (aligned loads); this half's elements start at column 15 fhalf
-            const uint32_t lrow = d1 + (static_cast<uint32_t>(qt * 32) << 16);
-            tc::tmem_ld16(lrow, u);
-            tc::tmem_ld16(lrow + 16, u + 16);
+            const uint32_t lrow = static_cast<uint32_t>(qt * 32) << 16;
+            float us[32];
+            tc::tmem_ld16(d1 + lrow, u);
+            tc::tmem_ld16(d1 + lrow + 16, u + 16);
+            tc::tmem_ld16(d1s + lrow, us);
+            tc::tmem_ld16(d1s + lrow + 16, us + 16);
             tc::tmem_wait_ld();
-            const int qx = q % M, qy = (q / M) % M, qz = q / (M * M);
-            const float wq = q < NQ ? Wt[qx] * Wt[qy] * Wt[qz] : 0.f;
 #pragma unroll
-            for (int ee = 0; ee < 3; ++ee) {
-                const int e = fhalf * 3 + ee;
-                if (q < NQ && e < nel) {
-                    const float* mt = sMeta + e * 12;
-                    float U[5], F[15];
-#pragma unroll
-                    for (int v = 0; v < 5; ++v) U[v] = fhalf ? u[15 + ee * 5 + v] : u[ee * 5 + v];
-                    const float p = dgp::interior_flux_r1<float, true>(gamma, U, F, mt[10]);
-                    if (!(U[0] > 0.f)) status |= kStatusRho;
-                    if (!(p + mt[11] > 0.f)) status |= kStatusPressure;
-                    if (U[0] != U[0] || p != p) status |= kStatusNaN;
-#pragma unroll
-                    for (int v = 0; v < 5; ++v)
-#pragma unroll
-                        for (int d = 0; d < 3; ++d)
-                            G[ee][d * 5 + v] = (F[v] * mt[d * 3 + 0] + F[5 + v] * mt[d * 3 + 1] + F[10 + v] * mt[d * 3 + 2]) * wq;
-                } else {
-#pragma unroll
-                    for (int k = 0; k < 15; ++k) G[ee][k] = 0.f;
-                }
-            }
+            for (int k = 0; k < 32; ++k) u[k] += us[k];
         }
-        // G of one chunk into the buffer: rows 32 d + 5 e + v, K = the point within the chunk
-        auto store_G = [&]() {
-#pragma unroll
-            for (int ee = 0; ee < 3; ++ee) {
-                const int e = fhalf * 3 + ee;
-#pragma unroll
-                for (int d = 0; d < 3; ++d)
-#pragma unroll
-                    for (int v = 0; v < 5; ++v) {
-                        const float g = G[ee][d * 5 + v];
-                        const float hi = tc::tf32(g), lo = tc::tf32(g - hi);
-                        const uint32_t off = tc::sw128(32 * d + 5 * e + v, ql, K::kGAtom);
-                        *reinterpret_cast<float*>(sm + K::kGHi + off) = hi;
-                        *reinterpret_cast<float*>(sm + K::kGLo + off) = lo;
-                    }
-            }
+        const int qx = q % M, qy = (q / M) % M, qz = q / (M * M);
+        const float wq = q < NQ ? Wt[qx] * Wt[qy] * Wt[qz] : 0.f;
+        auto flux = [&]() {
+            if (fhalf) tc_flux_half<P, 1>(u, q, ql, nel, meta(j), gamma, wq, sm + K::kG, status);
+            else tc_flux_half<P, 0>(u, q, ql, nel, meta(j), gamma, wq, sm + K::kG, status);
         };
-        // GEMM2 over chunk ch: H[r][b] += sum_{q in chunk} G[r][q] Bt[b][q]
-        auto issue_gemm2 = [&](int ch) {
-            constexpr uint32_t id2 = tc::idesc_tf32(128, NB, 0);
+        auto gemm2 = [&](int ch) {
+            // H[r][b] += sum_{q in chunk} G[r][q] B[q][b]: the operator read MN-major (b contiguous)
+            constexpr uint32_t id2 = tc::idesc_bf16(128, NB, 1);
 #pragma unroll
-            for (int s = 0; s < 3; ++s) {
-                const uint32_t ab = sbase + (s == 0 ? K::kGLo : K::kGHi);
-                const uint32_t bb = sbase + (s == 1 ? K::kBtLo : K::kBtHi);
+            for (int s = 0; s < 6; ++s) {
+                const uint32_t ab = sbase + K::kG + tc::prod_a(s) * K::kGPart;
+                const uint32_t bb = sbase + K::kOp + tc::prod_b(s) * K::kOpPart;
+                const bool big = s == 5;
 #pragma unroll
-                for (int kl = 0; kl < K::KC / 8; ++kl) {
-                    const int kk = ch * (K::KC / 8) + kl;
-                    const uint64_t ad = tc::sdesc(ab + (kl >> 2) * K::kGAtom + (kl & 3) * 32, 16, 1024);
-                    const uint64_t bd = tc::sdesc(bb + (kk >> 2) * K::kBtAtom + (kk & 3) * 32, 16, 1024);
-                    tc::mma_tf32(d2, ad, bd, id2, (ch > 0 || s > 0 || kl > 0) ? 1u : 0u);
-                }
+                for (int kl = 0; kl < K::KC / 16; ++kl)
+                    tc::mma_bf16(big ? d2 : d2s, tc::sdesc(ab + kl * 32, 16, 1024),
+                                 tc::sdesc(bb + (ch * (K::KC / 16) + kl) * 2048, K::kOpPart, 1024), id2,
+                                 (ch > 0 || (big ? 0 : s) > 0 || kl > 0) ? 1u : 0u);
             }
             tc::mma_commit(bar2);
         };
-        if (chunk == 0) store_G();
+        if (qt < 2) flux();
         tc::fence_proxy_async();
         tc::tc_fence_before();
         __syncthreads();
         if (tid == 0) {
             tc::tc_fence_after();
-            issue_gemm2(0);
+            gemm2(0);
         }
-        // the first chunk must be consumed before the second overwrites the buffer
-        if (!__syncthreads_and(tc::mbar_wait(bar2, ph2, kWait))) {
-            status |= kStatusTimeout;
-            alive = false;
-            break;
-        }
-        ph2 ^= 1;
-        tc::tc_fence_after();
-        if (chunk == 1) store_G();
-        tc::fence_proxy_async();
-        tc::tc_fence_before();
-        __syncthreads();
-        if (tid == 0) {
-            tc::tc_fence_after();
-            issue_gemm2(1);
-        }
-        // ---- face lifts (FP32) while GEMM2 runs, into the Uop region ----
-        cp_async_wait_all();
-        __syncthreads();
+        // ---- face lifts (FP32) while the first chunk multiplies (into the Uop region) ----
         for (int t2 = tid; t2 < E * 30; t2 += K::NT) {
             const int v = t2 % 5, f = (t2 / 5) % 6, e = t2 / 30;
             if (e >= nel) continue;
-            const float* Fq = Fh + ((e * 6 + f) * 5 + v) * FS;
-            const float sgn = ((sRec[e * 6 + f].info >> 3) & 1) ? -1.f : 1.f;
+            const FaceRec& rec = r[e * 6 + f];
+            const float* Fq = gF + (size_t)(rec.pad & 0x3fffffff) * FSTR + v * NF;
+            const bool own = (rec.pad >> 30) & 1;
+            const uint8_t* pm = a.cmap + (rec.info >> 4) * NF;
+            float fl[NF];
+#pragma unroll
+            for (int c = 0; c < NF; ++c) fl[c] = __ldg(Fq + (own ? c : __ldg(pm + c)));
+            const float sgn = ((rec.info >> 3) & 1) ? -1.f : 1.f;
             float tmp[M][N];
 #pragma unroll
             for (int t1 = 0; t1 < M; ++t1)
@@ -517,7 +563,7 @@ __global__ void __launch_bounds__(TcCfg<P>::NT, 1) tc_stage_kernel(StageArgs a)
                 for (int b0 = 0; b0 < N; ++b0) {
                     float s = 0.f;
 #pragma unroll
-                    for (int t0 = 0; t0 < M; ++t0) s += Bt[t0 * N + b0] * Fq[t1 * M + t0];
+                    for (int t0 = 0; t0 < M; ++t0) s += Bt[t0 * N + b0] * fl[t1 * M + t0];
                     tmp[t1][b0] = s;
                 }
             float* Lf = Lift + ((e * 6 + f) * 5 + v) * N2;
@@ -531,47 +577,56 @@ __global__ void __launch_bounds__(TcCfg<P>::NT, 1) tc_stage_kernel(StageArgs a)
                     Lf[b1 * N + b0] = sgn * s;
                 }
         }
-        // ---- Delta_d^T along each axis (FP32), one warp per direction and half ----
-        if (!__syncthreads_and(tc::mbar_wait(bar2, ph2, kWait))) {
-            status |= kStatusTimeout;
-            alive = false;
-            break;
-        }
+        // the first chunk has been read: the second overwrites it
+        if (!(alive = wait_all(bar2, ph2))) break;
         ph2 ^= 1;
         tc::tc_fence_after();
+        if (qt >= 2) flux();
+        tc::fence_proxy_async();
+        tc::tc_fence_before();
+        __syncthreads();
+        if (tid == 0) {
+            tc::tc_fence_after();
+            gemm2(1);
+        }
+        if (!(alive = wait_all(bar2, ph2))) break;
+        ph2 ^= 1;
+        tc::tc_fence_after();
+        // ---- Delta_d^T along each axis (FP32), one warp per direction and half ----
         {
             const int d = warp & 3, half = warp >> 2;
             if (d < 3) {
-                const uint32_t row = d2 + (static_cast<uint32_t>(d * 32) << 16);
-                float h[32];
+                const uint32_t lrow = static_cast<uint32_t>(d * 32) << 16;
+                float h[32], hs[32];
                 if (d < 2) {
-                    tc::tmem_ld16(row + half * 32, h);
-                    tc::tmem_ld16(row + half * 32 + 16, h + 16);
+                    tc::tmem_ld16(d2 + lrow + half * 32, h);
+                    tc::tmem_ld16(d2 + lrow + half * 32 + 16, h + 16);
+                    tc::tmem_ld16(d2s + lrow + half * 32, hs);
+                    tc::tmem_ld16(d2s + lrow + half * 32 + 16, hs + 16);
                 } else {
 #pragma unroll
                     for (int bz = 0; bz < 4; ++bz) {
-                        float r8[8];
-                        tc::tmem_ld8(row + bz * 16 + half * 8, r8);
-#pragma unroll
-                        for (int k = 0; k < 8; ++k) h[bz * 8 + k] = r8[k];
+                        tc::tmem_ld8(d2 + lrow + bz * 16 + half * 8, h + bz * 8);
+                        tc::tmem_ld8(d2s + lrow + bz * 16 + half * 8, hs + bz * 8);
                     }
                 }
                 tc::tmem_wait_ld();
+#pragma unroll
+                for (int k = 0; k < 32; ++k) h[k] += hs[k];
                 const int c = lane;
                 if (c < C && c / 5 < nel) {
                     float* out = Part + (d * C + c) * PS;
                     if (d == 0) {
                         // h[(bz - 2 half) * 16 + by * 4 + bx]
 #pragma unroll
-                        for (int j = 0; j < 8; ++j) {
+                        for (int jj = 0; jj < 8; ++jj)
 #pragma unroll
                             for (int bx = 0; bx < N; ++bx) {
                                 float s = 0.f;
 #pragma unroll
-                                for (int i = 0; i < N; ++i) s += Dn[i * N + bx] * h[j * 4 + i];
-                                out[half * 32 + j * 4 + bx] = s;
+                                for (int i = 0; i < N; ++i) s += Dn[i * N + bx] * h[jj * 4 + i];
+                                out[half * 32 + jj * 4 + bx] = s;
                             }
-                        }
                     } else if (d == 1) {
 #pragma unroll
                         for (int bzl = 0; bzl < 2; ++bzl)
@@ -601,8 +656,15 @@ __global__ void __launch_bounds__(TcCfg<P>::NT, 1) tc_stage_kernel(StageArgs a)
         }
         tc::tc_fence_before();
         __syncthreads();
-        // ---- residual (FP64): directions + face lifts ----
-        for (int i = tid; i < C * NB; i += K::NT) {
+        // ---- residual (FP64): the three directions and the face lifts, summed in
+        //      registers, then written over the partials ----
+        constexpr int kPer = (C * NB + K::NT - 1) / K::NT;
+        double rs[kPer];
+#pragma unroll
+        for (int k = 0; k < kPer; ++k) {
+            const int i = tid + k * K::NT;
+            rs[k] = 0.0;
+            if (i >= C * NB) continue;
             const int c = i / NB, b = i - c * NB, e = c / 5, v = c - 5 * e;
             if (e >= nel) continue;
             double s = double(Part[c * PS + b]) + double(Part[(C + c) * PS + b]) + double(Part[(2 * C + c) * PS + b]);
@@ -616,7 +678,13 @@ __global__ void __launch_bounds__(TcCfg<P>::NT, 1) tc_stage_kernel(StageArgs a)
                     s += double(Lift[((e * 6 + f) * 5 + v) * N2 + b1 * N + b0]);
                 }
             }
-            Res[c * PS + b] = s;
+            rs[k] = s;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < kPer; ++k) {
+            const int i = tid + k * K::NT;
+            if (i < C * NB) Res[(i / NB) * PS + i % NB] = rs[k];
         }
         __syncthreads();
         if (a.mode == kModeResidual) {
@@ -629,38 +697,38 @@ __global__ void __launch_bounds__(TcCfg<P>::NT, 1) tc_stage_kernel(StageArgs a)
         }
         // ---- inverse mass (FP64): x and y passes in place, z pass with the update ----
         for (int i = tid; i < nel * 5 * N2; i += K::NT) {
-            const int c = i / N2, r = i - c * N2;
-            double* rr = Res + c * PS + r * N;  // pencil along x at (by, bz) = r
+            const int c = i / N2, rr0 = i - c * N2;
+            double* rr = Res + c * PS + rr0 * N;  // pencil along x at (by, bz)
             double t4[N];
 #pragma unroll
             for (int k = 0; k < N; ++k) t4[k] = rr[k];
 #pragma unroll
-            for (int j = 0; j < N; ++j) {
+            for (int jj = 0; jj < N; ++jj) {
                 double s = 0.0;
 #pragma unroll
-                for (int k = 0; k < N; ++k) s += Mi[j * N + k] * t4[k];
-                rr[j] = s;
+                for (int k = 0; k < N; ++k) s += Mi[jj * N + k] * t4[k];
+                rr[jj] = s;
             }
         }
         __syncthreads();
         for (int i = tid; i < nel * 5 * N2; i += K::NT) {
-            const int c = i / N2, r = i - c * N2, bx = r % N, bz = r / N;
+            const int c = i / N2, rr0 = i - c * N2, bx = rr0 % N, bz = rr0 / N;
             double* rr = Res + c * PS + bz * N2 + bx;  // pencil along y
             double t4[N];
 #pragma unroll
             for (int k = 0; k < N; ++k) t4[k] = rr[k * N];
 #pragma unroll
-            for (int j = 0; j < N; ++j) {
+            for (int jj = 0; jj < N; ++jj) {
                 double s = 0.0;
 #pragma unroll
-                for (int k = 0; k < N; ++k) s += Mi[j * N + k] * t4[k];
-                rr[j * N] = s;
+                for (int k = 0; k < N; ++k) s += Mi[jj * N + k] * t4[k];
+                rr[jj * N] = s;
             }
         }
         __syncthreads();
         for (int i = tid; i < nel * 5 * N2; i += K::NT) {
             const int c = i / N2, bxy = i - c * N2, e = c / 5;
-            const GeoDev& gg = a.geo[sCls[e]];
+            const GeoDev& gg = a.geo[cls(j)[e]];
             const double scale = a.dt * gg.dtf * gg.inv_djac;
             const double* rr = Res + c * PS + bxy;  // pencil along z
             double t4[N];
@@ -668,12 +736,12 @@ __global__ void __launch_bounds__(TcCfg<P>::NT, 1) tc_stage_kernel(StageArgs a)
             for (int k = 0; k < N; ++k) t4[k] = rr[k * N2];
             const size_t gbase = (size_t)e0 * 5 * NB + (size_t)c * NB + bxy;
 #pragma unroll
-            for (int j = 0; j < N; ++j) {
+            for (int jj = 0; jj < N; ++jj) {
                 double s = 0.0;
 #pragma unroll
-                for (int k = 0; k < N; ++k) s += Mi[j * N + k] * t4[k];
+                for (int k = 0; k < N; ++k) s += Mi[jj * N + k] * t4[k];
                 const double kk = scale * s;
-                const size_t gi = gbase + (size_t)j * N2;
+                const size_t gi = gbase + (size_t)jj * N2;
                 switch (a.mode) {
                     case kModeMassInv: a.out[gi] = kk; break;
                     case kModeRK1: a.acc[gi] = kk; a.out[gi] = 0.5 * kk + a.U0[gi]; break;
@@ -686,10 +754,11 @@ __global__ void __launch_bounds__(TcCfg<P>::NT, 1) tc_stage_kernel(StageArgs a)
         }
         __syncthreads();
     }
-    // a CTA that gave up waiting for the operator may still have its copy in
-    // flight: wait for it (bounded) before the shared memory goes away
-    if (!alive && tid == 0) (void)tc::mbar_wait(barOp, 0, kWait);
-    cp_async_wait_all();
+    // a CTA that stopped early may have record copies in flight: wait for them
+    // (bounded) before the shared memory goes away
+    if (tid == 0)
+        for (int s2 = 0; s2 < 2; ++s2)
+            if (pend[s2]) (void)tc::mbar_wait(barR0 + 8 * s2, pph[s2], kWait);
     tc::tc_fence_before();
     __syncthreads();
     if (warp == 0) {

@@ -118,3 +118,66 @@ def test_precision_config_p5_500_steps(flux):
     # states are O(1), rho E ~ 3)
     assert np.all(np.abs(emx - e64) <= 3.0 * TOL), (emx, e64)
     assert mix.status() == 0 and f64.status() == 0
+
+
+def _tc_variant(case):
+    vs = case.stage_variants()
+    tc = [i for i, v in enumerate(vs) if "tc" in v[4].split("+")]
+    assert tc, "p = 3 compiles a tensor-core variant"
+    return tc[0]
+
+
+@pytest.mark.parametrize("n", [(7, 1, 1), (5, 3, 2), (3, 2, 3)])
+def test_tensor_core_residual_and_modes_match_fp64(n):
+    """The tensor-core kernel (split-BF16 volume GEMMs on tcgen05) on meshes whose
+    element count leaves a partial tile (7 = 6 + 1) or none, rotated elements:
+    residual, inverse-mass residual and RK4 steps against the FP64 path at the
+    FP32 residual's accuracy."""
+    mesh = dg_b200.periodic_box(n, (0, 0, 0), (10.0, 10.0, 10.0), rotate_seed=13)
+    f64 = dg_b200.Case(mesh, 3, gas_constant=1.0, precision="fp64")
+    tc = dg_b200.Case(mesh, 3, gas_constant=1.0, precision="mixed_fp32")
+    tc.stage_variant = _tc_variant(tc)
+    U = f64.project_ic("IsentropicVortexXY", VORTEX_XY)
+    tc.set_state(U)
+    R64, Rtc = f64.residual(), tc.residual()
+    scale = np.abs(R64).max()
+    assert np.abs(Rtc - R64).max() < 1e-5 * scale
+    dt = f64.cfl_time_step(U, 0.1)
+    M64, Mtc = f64.mass_inverse_residual(dt), tc.mass_inverse_residual(dt)
+    assert np.abs(Mtc - M64).max() < 1e-5 * np.abs(M64).max()
+    f64.rk4(dt, 10)
+    tc.rk4(dt, 10)
+    assert rel_l2(tc.get_state(), f64.get_state()).max() < TOL
+    assert tc.status() == 0
+
+
+@pytest.mark.parametrize("flux", ["LaxFriedrichs", "HLLC"])
+def test_tensor_core_stepping_within_bound(flux):
+    """60 RK4 steps of the 8^3 p = 3 vortex and 40 of low-Mach Taylor-Green on the
+    tensor-core kernel: within 1e-6 of FP64 per variable."""
+    mesh = dg_b200.periodic_box((8, 8, 8), (0, 0, 0), (10.0, 10.0, 10.0), rotate_seed=3)
+    f64 = dg_b200.Case(mesh, 3, flux=flux, gas_constant=1.0, precision="fp64")
+    tc = dg_b200.Case(mesh, 3, flux=flux, gas_constant=1.0, precision="mixed_fp32")
+    tc.stage_variant = _tc_variant(tc)
+    U0 = f64.project_ic("IsentropicVortexXY", VORTEX_XY)
+    dt = f64.cfl_time_step(U0, 0.1)
+    tc.set_state(U0)
+    f64.rk4(dt, 60)
+    tc.rk4(dt, 60)
+    d = rel_l2(tc.get_state(), f64.get_state())
+    print(f"tensor-core 8^3 p=3 vortex 60 steps {flux}: {d}")
+    assert d.max() < TOL, d
+    L = 2 * np.pi
+    mesh = dg_b200.periodic_box((8, 8, 8), (0, 0, 0), (L, L, L))
+    f64 = dg_b200.Case(mesh, 3, flux=flux, gas_constant=1.0, precision="fp64")
+    tc = dg_b200.Case(mesh, 3, flux=flux, gas_constant=1.0, precision="mixed_fp32")
+    tc.stage_variant = _tc_variant(tc)
+    U0 = f64.project_ic("TaylorGreen", [0.1])
+    dt = f64.cfl_time_step(U0, 0.1)
+    tc.set_state(U0)
+    f64.rk4(dt, 40)
+    tc.rk4(dt, 40)
+    d = rel_l2(tc.get_state(), f64.get_state())
+    print(f"tensor-core 8^3 p=3 Taylor-Green M=0.1 40 steps {flux}: {d}")
+    assert d.max() < TOL, d
+    assert tc.status() == 0
