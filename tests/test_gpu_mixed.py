@@ -136,15 +136,19 @@ def test_tensor_core_residual_and_modes_match_fp64(n):
     mesh = dg_b200.periodic_box(n, (0, 0, 0), (10.0, 10.0, 10.0), rotate_seed=13)
     f64 = dg_b200.Case(mesh, 3, gas_constant=1.0, precision="fp64")
     tc = dg_b200.Case(mesh, 3, gas_constant=1.0, precision="mixed_fp32")
+    f32 = dg_b200.Case(mesh, 3, gas_constant=1.0, precision="mixed_fp32")  # the CUDA-core FP32 residual
     tc.stage_variant = _tc_variant(tc)
     U = f64.project_ic("IsentropicVortexXY", VORTEX_XY)
     tc.set_state(U)
-    R64, Rtc = f64.residual(), tc.residual()
+    f32.set_state(U)
+    R64, Rtc, R32 = f64.residual(), tc.residual(), f32.residual()
     scale = np.abs(R64).max()
     assert np.abs(Rtc - R64).max() < 1e-5 * scale
     dt = f64.cfl_time_step(U, 0.1)
-    M64, Mtc = f64.mass_inverse_residual(dt), tc.mass_inverse_residual(dt)
-    assert np.abs(Mtc - M64).max() < 1e-5 * np.abs(M64).max()
+    M64, Mtc, M32 = f64.mass_inverse_residual(dt), tc.mass_inverse_residual(dt), f32.mass_inverse_residual(dt)
+    # the inverse mass amplifies FP32 rounding alike on both FP32 residuals
+    etc, e32 = np.abs(Mtc - M64).max(), np.abs(M32 - M64).max()
+    assert etc < 1e-4 * np.abs(M64).max() and etc < 4 * e32, (etc, e32)
     f64.rk4(dt, 10)
     tc.rk4(dt, 10)
     assert rel_l2(tc.get_state(), f64.get_state()).max() < TOL
