@@ -25,6 +25,7 @@
 
 #include "../host/case.h"
 #include "dg_ctx.cuh"
+#include "dg_ensemble.cuh"
 
 namespace {
 
@@ -36,6 +37,8 @@ struct BatchGroup {
     std::vector<int> cases;        // case ids, in element order
     std::vector<int> class_case;   // owning case of each geometry class
     dg_ctx* ctx = nullptr;
+    int own_variant = 0;           // the group's launch variant in per-group mode
+    int ens_variant = -1;          // the variant of the ensemble launch's configuration (-1: none)
 };
 
 struct BatchCase {
@@ -54,6 +57,8 @@ struct dg_batch {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     bool geo_dirty = true;               // time steps changed since the last upload
+    bool single = false;                 // one ensemble launch per RK stage (else one per group)
+    int* d_work = nullptr;               // ensemble launches' batch counters [8 launches][8 groups]
     unsigned status_accum = 0;
     std::string err;
 };
@@ -86,6 +91,7 @@ void release_batch(dg_batch* b)
     if (!b) return;
     cudaSetDevice(b->device);
     drop_graph(b);
+    cudaFree(b->d_work);
     for (cudaEvent_t e : b->events) cudaEventDestroy(e);
     if (b->stream) cudaStreamDestroy(b->stream);
     for (auto& g : b->groups) dgi::destroy_ctx(g.ctx);
@@ -110,9 +116,148 @@ int upload_time_steps(dg_batch* b)
     return DG_OK;
 }
 
+// relative cost per DOF and stage of the ensemble configuration of each order
+// (inverse of the measured rates of those variants), weighting the groups'
+// block ranges
+double ensemble_cost(int p, bool fp32)
+{
+    static const double r32[dgk::kMaxP + 1] = {5.2, 16.6, 28.4, 37.4, 40.3, 40.8};
+    static const double r64[dgk::kMaxP + 1] = {3.8, 11.3, 22.0, 29.7, 28.2, 31.2};
+    return 1.0 / (fp32 ? r32[p] : r64[p]);
+}
+
+// splits `total` blocks over the groups in proportion to w (at least one per
+// group with work, at most cap[g]) into boundaries blk[0..n]
+void split_blocks(const std::vector<double>& w, const std::vector<int>& cap, int total, int* blk)
+{
+    double W = 0.0;
+    for (double x : w) W += x;
+    blk[0] = 0;
+    for (size_t g = 0; g < w.size(); ++g) {
+        int n = cap[g] > 0 ? static_cast<int>(std::lround(total * (W > 0 ? w[g] / W : 0.0))) : 0;
+        n = std::min(std::max(n, cap[g] > 0 ? 1 : 0), cap[g]);
+        blk[g + 1] = blk[g] + n;
+    }
+}
+
+// the step graph with one face launch and one stage launch per RK stage for
+// all groups (dg_ensemble.cuh)
+int prepare_ensemble_graph(dg_batch* b)
+{
+    const bool fp32 = b->precision == DG_PREC_MIXED_FP32;
+    const dgk::EnsembleKernels K = dgk::ensemble_kernels(fp32);
+    const int ng = static_cast<int>(b->groups.size());
+    unsigned mask = 0;
+    for (auto& g : b->groups) mask |= 1u << g.order;
+    const size_t smem = K.stage_smem(mask), fsmem = K.face_smem(mask);
+    cudaError_t ce = cudaFuncSetAttribute(K.stage, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (ce == cudaSuccess) ce = cudaFuncSetAttribute(K.stage, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+    if (ce == cudaSuccess) ce = cudaFuncSetAttribute(K.face, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsmem);
+    int sms = 0, per_sm = 0, fper_sm = 0;
+    if (ce == cudaSuccess) ce = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
+    if (ce == cudaSuccess) ce = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, K.stage, dgk::kEnsThreads, smem);
+    if (ce == cudaSuccess) ce = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fper_sm, K.face, dgk::kFaceThreads, fsmem);
+    if (ce != cudaSuccess) return bfail(b, DG_ERR_CUDA, std::string("ensemble launch set-up: ") + cudaGetErrorString(ce));
+    if (per_sm < 1 || fper_sm < 1) return bfail(b, DG_ERR_UNSUPPORTED, "ensemble kernels do not fit on an SM");
+    // block ranges: stage blocks by DOF x cost, face blocks by face points
+    std::vector<double> ws(ng), wf(ng);
+    std::vector<int> cs(ng), cf(ng);
+    bool any_face = false;
+    for (int g = 0; g < ng; ++g) {
+        const BatchGroup& gr = b->groups[g];
+        int E = 1, fl = 0;
+        dgk::ensemble_config(gr.order, fp32, E, fl);
+        const double nb = gr.ctx->nb, m = gr.order + 2;
+        ws[g] = gr.ctx->ne * nb * ensemble_cost(gr.order, fp32);
+        cs[g] = (gr.ctx->ne + E - 1) / E;
+        const bool fx = (fl & dgk::kFX) != 0;
+        const int fb = dgk::face_batch_of(gr.order, fp32 ? 4 : 8);
+        wf[g] = fx ? gr.ctx->nface * m * m : 0.0;
+        cf[g] = fx ? (gr.ctx->nface + fb - 1) / fb : 0;
+        any_face = any_face || (fx && gr.ctx->nface > 0);
+    }
+    dgk::EnsembleArgs sa{}, fa{};
+    sa.ngroup = fa.ngroup = ng;
+    split_blocks(ws, cs, sms * per_sm, sa.blk);
+    split_blocks(wf, cf, sms * fper_sm, fa.blk);
+    for (int g = 0; g < ng; ++g) sa.order[g] = fa.order[g] = b->groups[g].order;
+    constexpr int kCounters = 8 * dgk::kEnsMaxGroups;  // [stage 0..3][face, stage][group]
+    if (!b->d_work && cudaMalloc((void**)&b->d_work, kCounters * sizeof(int)) != cudaSuccess) {
+        cudaGetLastError();
+        b->d_work = nullptr;
+        return bfail(b, DG_ERR_NOMEM, "ensemble work counters");
+    }
+    ce = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
+    if (ce != cudaSuccess) return bfail(b, DG_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+    ce = cudaMemsetAsync(b->d_work, 0, kCounters * sizeof(int), b->stream);  // every step starts at zero
+    const int modes[4] = {dgk::kModeRK1, dgk::kModeRK2, dgk::kModeRK3, dgk::kModeRK4};
+    for (int s = 0; s < 4 && ce == cudaSuccess; ++s) {
+        for (int g = 0; g < ng; ++g) {
+            dg_ctx* c = b->groups[g].ctx;
+            const double* in[4] = {c->d_U0, c->d_Ua, c->d_Ub, c->d_Ua};
+            double* out[4] = {c->d_Ua, c->d_Ub, c->d_Ua, c->d_U0};
+            dgi::stage_args(c, modes[s], in[s], c->d_U0, out[s], 1.0, 0, c->ne, sa.g[g]);
+            fa.g[g] = sa.g[g];
+            if (cf[g] == 0) fa.g[g].nface = 0;  // no face kernel in this group's configuration
+        }
+        fa.work = b->d_work + (2 * s) * dgk::kEnsMaxGroups;
+        sa.work = b->d_work + (2 * s + 1) * dgk::kEnsMaxGroups;
+        if (any_face) ce = K.launch_face(fa, fa.blk[ng], fsmem, b->stream);
+        if (ce == cudaSuccess) ce = K.launch_stage(sa, sa.blk[ng], smem, b->stream);
+    }
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ce_end = cudaStreamEndCapture(b->stream, &graph);
+    if (ce != cudaSuccess || ce_end != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        return bfail(b, DG_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce != cudaSuccess ? ce : ce_end));
+    }
+    b->graph = graph;
+    ce = cudaGraphInstantiate(&b->exec, b->graph, 0);
+    if (ce != cudaSuccess) {
+        drop_graph(b);
+        return bfail(b, DG_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
+    }
+    return DG_OK;
+}
+
+// the variant of group g's order with the ensemble launch's configuration, or -1
+int ensemble_variant(const BatchGroup& g)
+{
+    const dg_ctx* c = g.ctx;
+    if (c->p < 1 || c->pm.general) return -1;
+    int E = 1, fl = 0;
+    dgk::ensemble_config(c->p, c->precision == DG_PREC_MIXED_FP32, E, fl);
+    const dgk::StageVariant* vs = nullptr;
+    const int nv = dgk::stage_variants(c->p, &vs);
+    for (int v = 0; v < nv; ++v)
+        if (vs[v].E == E && vs[v].NT == dgk::kEnsThreads && vs[v].G == 1 && (vs[v].flags & 0xFF) == fl &&
+            dgi::variant_matches(c, v))
+            return v;
+    return -1;
+}
+
+// one ensemble launch per RK stage (on = true), or one launch per group
+int set_single_launch(dg_batch* b, bool on)
+{
+    if (on)
+        for (auto& g : b->groups)
+            if (g.ens_variant < 0)
+                return bfail(b, DG_ERR_UNSUPPORTED, "group of order " + std::to_string(g.order) +
+                                                        " has no launch variant for the ensemble launch (orders 1..5, affine meshes)");
+    for (auto& g : b->groups) {
+        const int v = on ? g.ens_variant : g.own_variant;
+        const int rc = dg_set_stage_variant(g.ctx, v);
+        if (rc) return gfail(b, rc, g);
+    }
+    if (on != b->single) drop_graph(b);
+    b->single = on;
+    return DG_OK;
+}
+
 int prepare_graph(dg_batch* b)
 {
     if (b->exec) return DG_OK;
+    if (b->single) return prepare_ensemble_graph(b);
     for (auto& g : b->groups) {
         const int rc = dgi::prepare_variant(g.ctx, g.ctx->variant);
         if (rc) return gfail(b, rc, g);
@@ -172,6 +317,38 @@ int check_groups(dg_batch* b)
         return bfail(b, DG_ERR_NONPHYSICAL, buf);
     }
     return DG_OK;
+}
+
+// device time of `reps` RK4 steps of the batch in its current launch mode;
+// every group's step-start state is saved before and restored after
+int time_steps(dg_batch* b, int reps, float* ms)
+{
+    int rc = upload_time_steps(b);
+    if (!rc) rc = prepare_graph(b);
+    if (rc) return rc;
+    cudaError_t ce = cudaSuccess;
+    for (auto& g : b->groups) {
+        const size_t bytes = static_cast<size_t>(g.ctx->ne_alloc) * g.ctx->nb * 5 * sizeof(double);
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(g.ctx->d_out, g.ctx->d_U0, bytes, cudaMemcpyDeviceToDevice, b->stream);
+    }
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    if (ce == cudaSuccess) ce = cudaEventCreate(&ev[0]);
+    if (ce == cudaSuccess) ce = cudaEventCreate(&ev[1]);
+    if (ce == cudaSuccess) ce = cudaGraphLaunch(b->exec, b->stream);  // warm-up step
+    if (ce == cudaSuccess) ce = cudaEventRecord(ev[0], b->stream);
+    for (int r = 0; r < reps && ce == cudaSuccess; ++r) ce = cudaGraphLaunch(b->exec, b->stream);
+    if (ce == cudaSuccess) ce = cudaEventRecord(ev[1], b->stream);
+    if (ce == cudaSuccess) ce = cudaEventSynchronize(ev[1]);
+    if (ce == cudaSuccess) ce = cudaEventElapsedTime(ms, ev[0], ev[1]);
+    for (auto& g : b->groups) {
+        const size_t bytes = static_cast<size_t>(g.ctx->ne_alloc) * g.ctx->nb * 5 * sizeof(double);
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(g.ctx->d_U0, g.ctx->d_out, bytes, cudaMemcpyDeviceToDevice, b->stream);
+    }
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(b->stream);
+    if (ev[0]) cudaEventDestroy(ev[0]);
+    if (ev[1]) cudaEventDestroy(ev[1]);
+    if (ce != cudaSuccess) return bfail(b, DG_ERR_CUDA, std::string("dg_batch_tune timing: ") + cudaGetErrorString(ce));
+    return check_groups(b);
 }
 
 }  // namespace
@@ -295,8 +472,19 @@ int dg_batch_create(int ncases, const dg_case_desc* cases, const dg_mesh_desc* m
     for (auto& e : b->events)
         if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
             return bail(DG_ERR_CUDA, "event creation failed");
-    const int rc = upload_time_steps(b);
+    int rc = upload_time_steps(b);
     if (rc) return bail(rc, b->err);
+    // one ensemble launch per RK stage when every group has its configuration
+    bool ens = true;
+    for (auto& g : b->groups) {
+        g.own_variant = g.ctx->variant;
+        g.ens_variant = ensemble_variant(g);
+        ens = ens && g.ens_variant >= 0;
+    }
+    // default: one launch per group (measured faster on the 256-case ensemble:
+    // the single launch runs every order at the largest order's occupancy);
+    // dg_batch_tune times both and keeps the faster
+    (void)ens;
     *out = b;
     return DG_OK;
 }
@@ -441,18 +629,40 @@ int dg_batch_rk4_steps_timed(dg_batch* b, int nsteps, double* device_ms)
 
 int dg_batch_rk4_steps(dg_batch* b, int nsteps) { return dg_batch_rk4_steps_timed(b, nsteps, nullptr); }
 
+int dg_batch_set_launch_mode(dg_batch* b, int single)
+{
+    if (!b) return DG_ERR_ARG;
+    if (cudaSetDevice(b->device) != cudaSuccess) return bfail(b, DG_ERR_CUDA, "cudaSetDevice failed");
+    return set_single_launch(b, single != 0);
+}
+
+int dg_batch_get_launch_mode(const dg_batch* b) { return b ? (b->single ? 1 : 0) : -1; }
+
 int dg_batch_tune(dg_batch* b, int reps)
 {
     dgi::NvtxRange nvtx_("dg_batch_tune");
     if (!b || reps < 1) return bfail(b, DG_ERR_ARG, "dg_batch_tune: bad argument");
+    if (cudaSetDevice(b->device) != cudaSuccess) return bfail(b, DG_ERR_CUDA, "cudaSetDevice failed");
+    // each group's fastest variant, in per-group mode
+    int rc = set_single_launch(b, false);
+    if (rc) return rc;
     for (auto& g : b->groups) {
         const int keep = g.ctx->variant;
         int best = keep;
-        const int rc = dg_tune_stage(g.ctx, reps, &best, nullptr);
+        rc = dg_tune_stage(g.ctx, reps, &best, nullptr);
         if (rc) return gfail(b, rc, g);
+        g.own_variant = best;
         if (best != keep) drop_graph(b);
     }
-    return DG_OK;
+    // then the launch mode: one launch per group against one launch per stage
+    bool ens = true;
+    for (auto& g : b->groups) ens = ens && g.ens_variant >= 0;
+    if (!ens) return DG_OK;
+    float ms_group = 0.f, ms_single = 0.f;
+    if ((rc = time_steps(b, reps, &ms_group)) != DG_OK) return rc;
+    if ((rc = set_single_launch(b, true)) != DG_OK) return rc;
+    if ((rc = time_steps(b, reps, &ms_single)) != DG_OK) return rc;
+    return ms_single < ms_group ? DG_OK : set_single_launch(b, false);
 }
 
 int dg_batch_l2_error(dg_batch* b, int c, int ic_type, const double* data, int ndata, double t, double* err)

@@ -157,12 +157,10 @@ int prepare_variant(dg_ctx* c, int v)
     return DG_OK;
 }
 
-int launch_stage(dg_ctx* c, int mode, const double* Us, const double* U0, double* out, double dt, int e_begin, int e_end)
+void stage_args(const dg_ctx* c, int mode, const double* Us, const double* U0, double* out, double dt, int e_begin,
+                int e_end, StageArgs& a)
 {
-    if (e_end < 0) e_end = c->ne;
-    if (e_begin < 0 || e_end > c->ne || e_begin > e_end) return fail(c, DG_ERR_ARG, "stage element range out of bounds");
-    if (e_begin == e_end) return DG_OK;
-    StageArgs a{};
+    a = StageArgs{};
     a.Us = Us;
     a.U0 = U0;
     a.acc = c->d_acc;
@@ -189,13 +187,24 @@ int launch_stage(dg_ctx* c, int mode, const double* Us, const double* U0, double
     a.gamma = c->gamma;
     a.dt = dt;
     a.tab = c->stage_tab;
+    const dgk::StageVariant* vs = nullptr;
+    dgk::stage_variants(c->p, &vs);
+    // the tensor-core kernel bulk-copies each face's fluxes: a 16-byte multiple per face
+    if (vs[c->variant].flags & dgk::kTC) a.fstride = dgk::tc_face_stride(c->p);
+}
+
+int launch_stage(dg_ctx* c, int mode, const double* Us, const double* U0, double* out, double dt, int e_begin, int e_end)
+{
+    if (e_end < 0) e_end = c->ne;
+    if (e_begin < 0 || e_end > c->ne || e_begin > e_end) return fail(c, DG_ERR_ARG, "stage element range out of bounds");
+    if (e_begin == e_end) return DG_OK;
+    StageArgs a;
+    stage_args(c, mode, Us, U0, out, dt, e_begin, e_end, a);
     int rc = prepare_variant(c, c->variant);
     if (rc) return rc;
     const dgk::StageVariant* vs = nullptr;
     dgk::stage_variants(c->p, &vs);
     const dgk::StageVariant& sv = vs[c->variant];
-    // the tensor-core kernel bulk-copies each face's fluxes: a 16-byte multiple per face
-    if (sv.flags & dgk::kTC) a.fstride = dgk::tc_face_stride(c->p);
     if (sv.face_launch) {
         // the fluxes of the faces this element range is the first to need (the
         // stage kernel reads them): all faces, the faces touching an interior

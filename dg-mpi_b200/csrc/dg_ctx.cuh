@@ -99,6 +99,9 @@ void destroy_ctx(dg_ctx* c);
 
 int prepare_variant(dg_ctx* c, int v);
 bool variant_matches(const dg_ctx* c, int v);
+// the stage kernels' arguments for elements [e_begin, e_end) with the context's variant
+void stage_args(const dg_ctx* c, int mode, const double* Us, const double* U0, double* out, double dt, int e_begin,
+                int e_end, dgk::StageArgs& a);
 // stage launch over the owned elements [e_begin, e_end) (e_end < 0: all)
 int launch_stage(dg_ctx* c, int mode, const double* Us, const double* U0, double* out, double dt, int e_begin = 0,
                  int e_end = -1);

@@ -437,8 +437,15 @@ __device__ __forceinline__ void interp2d(const T* __restrict__ Bt, const T (&s)[
         }
 }
 
+// bid / nblk: this block's index among the nblk blocks that share the
+// launch's element range (blockIdx.x / gridDim.x).  With a work counter
+// (work != nullptr, an ensemble launch) the batches are claimed instead:
+// batch k = atomicAdd(work, 1) starts at e_begin + k E, claimed one batch
+// ahead by thread 0 and passed on through the two shared slots `slots`, so
+// the next batch is known when its prefetch is issued.
 template <int P, int E, int NT, int G, typename T, int FL>
-__device__ __forceinline__ void stage_body(const StageArgs& a)
+__device__ __forceinline__ void stage_body(const StageArgs& a, int bid, int nblk, int* work = nullptr,
+                                           int* slots = nullptr)
 {
     using L = Lay<P, G, T, FL>;
     constexpr bool PZ = L::PZ, SB = L::SB;
@@ -472,8 +479,16 @@ __device__ __forceinline__ void stage_body(const StageArgs& a)
     // p = 5, 2 at the other orders (more points add registers); 1 with K1
     constexpr int kFluxPoints = L::K1 ? 1 : ((P == 2 || P == 5) ? 3 : 2);
     unsigned status = 0;
-    const int stride = gridDim.x * E;
-    const int e_first = a.e_begin + blockIdx.x * E;
+    const int stride = nblk * E;
+    int e_first = a.e_begin + bid * E;
+    if (work) {
+        if (tid == 0) {
+            slots[0] = a.e_begin + atomicAdd(work, 1) * E;
+            slots[1] = a.e_begin + atomicAdd(work, 1) * E;
+        }
+        __syncthreads();
+        e_first = slots[0];
+    }
 
     int buf = 0;
     if (e_first < a.ne) {
@@ -482,10 +497,17 @@ __device__ __forceinline__ void stage_body(const StageArgs& a)
     }
     cp_async_commit();
 
-    for (int e0 = e_first; e0 < a.ne; e0 += stride, buf ^= 1) {
+    int en = e_first, it = 0;  // the next batch
+    for (int e0 = e_first; e0 < a.ne; e0 = en, buf ^= 1, ++it) {
         double* sU = sUbuf + (SB ? 0 : buf) * E * ES;
         cp_async_wait_all();
         __syncthreads();
+        if (work) {
+            en = slots[(it + 1) & 1];
+            if (tid == 0) slots[it & 1] = a.e_begin + atomicAdd(work, 1) * E;  // read two iterations ago
+        } else {
+            en = e0 + stride;
+        }
         // stream in the neighbours' boundary slices (the periodic face gather)
         // for the face phase, then the next batch's coefficients; one task per
         // (element, face, variable), or per slice row when the CTA has threads
@@ -528,8 +550,8 @@ __device__ __forceinline__ void stage_body(const StageArgs& a)
             }
         }
         cp_async_commit();
-        if (!SB && e0 + stride < a.ne)
-            prefetch_batch<P, G, E, NT>(a.Us, a.ne, e0 + stride, sUbuf + (buf ^ 1) * E * ES, ES);
+        if (!SB && en < a.ne)
+            prefetch_batch<P, G, E, NT>(a.Us, a.ne, en, sUbuf + (buf ^ 1) * E * ES, ES);
         cp_async_commit();
 
         // ---- volume: interpolation passes x, y ----
@@ -565,7 +587,7 @@ __device__ __forceinline__ void stage_body(const StageArgs& a)
         // with FX the x pass was the coefficients' last reader: refill the
         // single buffer with the next batch now
         if constexpr (L::FX) {
-            if (e0 + stride < a.ne) prefetch_batch<P, G, E, NT>(a.Us, a.ne, e0 + stride, sU, ES);
+            if (en < a.ne) prefetch_batch<P, G, E, NT>(a.Us, a.ne, en, sU, ES);
             cp_async_commit();
         }
         for (int i = tid; i < E * 5 * N * M; i += NT) {
@@ -955,7 +977,7 @@ __device__ __forceinline__ void stage_body(const StageArgs& a)
             // with SB, the next batch's coefficients: the traces were their last reader)
             if (stage_u0) prefetch_batch<P, G, E, NT>(a.U0, a.ne, e0, sOps, OPS);
             if (need_u0_acc) prefetch_batch<P, G, E, NT>(a.acc, a.ne, e0, sOps + ES, OPS);
-            if (SB && e0 + stride < a.ne) prefetch_batch<P, G, E, NT>(a.Us, a.ne, e0 + stride, sU, ES);
+            if (SB && en < a.ne) prefetch_batch<P, G, E, NT>(a.Us, a.ne, en, sU, ES);
             cp_async_commit();
 
             // numerical flux at every face point, written over the own trace; two
@@ -1019,7 +1041,7 @@ __device__ __forceinline__ void stage_body(const StageArgs& a)
 
             // the face records have been read: queue the next batch's (they land
             // before the inverse-mass pass, which waits for all copies)
-            if (e0 + stride < a.ne) prefetch_recs<E, NT>(a.frec, a.ne, e0 + stride, sRec);
+            if (en < a.ne) prefetch_recs<E, NT>(a.frec, a.ne, en, sRec);
             cp_async_commit();
         } else {
             // the face fluxes have landed (the next batch's coefficients may
@@ -1096,7 +1118,7 @@ __device__ __forceinline__ void stage_body(const StageArgs& a)
             // batch's RK operands and the next batch's records
             if (stage_u0) prefetch_batch<P, G, E, NT>(a.U0, a.ne, e0, sOps, OPS);
             if (need_u0_acc) prefetch_batch<P, G, E, NT>(a.acc, a.ne, e0, sOps + ES, OPS);
-            if (e0 + stride < a.ne) prefetch_recs<E, NT>(a.frec, a.ne, e0 + stride, sRec);
+            if (en < a.ne) prefetch_recs<E, NT>(a.frec, a.ne, en, sRec);
             cp_async_commit();
         }
         // add the six face contributions to the (FP64) residual
@@ -1280,9 +1302,11 @@ constexpr size_t face_smem_bytes()
     return ((sizeof(T) * FB * 10 * L::FS + 15) / 16) * 16 + FB * sizeof(FaceRec) + 2 * FB * sizeof(int);
 }
 
-// GEO: general geometry, the left element's normal data per face point
+// GEO: general geometry, the left element's normal data per face point;
+// bid / nblk as for stage_body
 template <int P, typename T, bool GEO>
-__global__ void __launch_bounds__(kFaceThreads) face_flux_kernel(StageArgs a)
+__device__ __forceinline__ void face_flux_body(const StageArgs& a, int bid, int nblk, int* work = nullptr,
+                                               int* slots = nullptr)
 {
     using L = Lay<P, 1, T>;
     constexpr int FB = face_batch<P, T>(), NT = kFaceThreads;
@@ -1299,8 +1323,25 @@ __global__ void __launch_bounds__(kFaceThreads) face_flux_kernel(StageArgs a)
     T* out = reinterpret_cast<T*>(a.fflux);
     const int tid = threadIdx.x;
     unsigned status = 0;
-    for (int f0 = a.face_begin + blockIdx.x * FB; f0 < a.nface; f0 += gridDim.x * FB) {
+    // batches of faces: static (bid, nblk) or claimed one ahead (work, slots), as in stage_body
+    int f_first = a.face_begin + bid * FB;
+    if (work) {
+        if (tid == 0) {
+            slots[0] = a.face_begin + atomicAdd(work, 1) * FB;
+            slots[1] = a.face_begin + atomicAdd(work, 1) * FB;
+        }
         __syncthreads();
+        f_first = slots[0];
+    }
+    int fn = f_first, it = 0;
+    for (int f0 = f_first; f0 < a.nface; f0 = fn, ++it) {
+        __syncthreads();
+        if (work) {
+            fn = slots[(it + 1) & 1];
+            if (tid == 0) slots[it & 1] = a.face_begin + atomicAdd(work, 1) * FB;
+        } else {
+            fn = f0 + nblk * FB;
+        }
         for (int j = tid; j < FB; j += NT) {
             const int2 fe = a.faces[min(f0 + j, a.nface - 1)];
             sRecL[j] = a.frec[(size_t)fe.x * 6 + fe.y];
@@ -1372,17 +1413,23 @@ __global__ void __launch_bounds__(kFaceThreads) face_flux_kernel(StageArgs a)
     if (status) atomicOr(a.status, status);
 }
 
+template <int P, typename T, bool GEO>
+__global__ void __launch_bounds__(kFaceThreads) face_flux_kernel(StageArgs a)
+{
+    face_flux_body<P, T, GEO>(a, blockIdx.x, gridDim.x);
+}
+
 template <int P, int E, int NT, int G, typename T, int FL>
 __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a)
 {
-    stage_body<P, E, NT, G, T, FL>(a);
+    stage_body<P, E, NT, G, T, FL>(a, blockIdx.x, gridDim.x);
 }
 // the same with at least MB resident CTAs per SM asked of the compiler (it then
 // keeps the registers within 64K / (NT * MB) per thread)
 template <int P, int E, int NT, int G, typename T, int FL, int MB>
 __global__ void __launch_bounds__(NT, MB) stage_kernel_mb(StageArgs a)
 {
-    stage_body<P, E, NT, G, T, FL>(a);
+    stage_body<P, E, NT, G, T, FL>(a, blockIdx.x, gridDim.x);
 }
 
 template <int P, int E, int G, typename T, int FL = 0>

@@ -29,6 +29,9 @@ static const StageVariant kVariants2[] = {
     make_variant<2, 1, 32, 1, float, kUF | kGE>(),
     make_variant<2, 1, 32, 1, double, kUF | kSB | kGE | kFX>(),
     make_variant<2, 1, 32, 1, float, kUF | kSB | kGE | kFX>(),
+    // 128 threads per CTA (the ensemble launch's block size for every order)
+    make_variant<2, 4, 128, 1, double, kUF | kSB | kFX>(),
+    make_variant<2, 4, 128, 1, float, kUF | kSB | kFX>(),
 };
 
 int stage_variants_p2(const StageVariant** out)

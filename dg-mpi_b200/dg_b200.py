@@ -132,6 +132,8 @@ def library(path: str | None = None) -> ctypes.CDLL:
         "dg_batch_rk4_steps": (ctypes.c_int, [vp, ctypes.c_int]),
         "dg_batch_rk4_steps_timed": (ctypes.c_int, [vp, ctypes.c_int, dp]),
         "dg_batch_tune": (ctypes.c_int, [vp, ctypes.c_int]),
+        "dg_batch_set_launch_mode": (ctypes.c_int, [vp, ctypes.c_int]),
+        "dg_batch_get_launch_mode": (ctypes.c_int, [vp]),
         "dg_batch_l2_error": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, dp, ctypes.c_int, ctypes.c_double, dp]),
         "dg_batch_status": (ctypes.c_int, [vp, up]),
     }
@@ -561,6 +563,17 @@ class Batch:
 
     def tune(self, reps: int = 2):
         self._check(self._lib.dg_batch_tune(self._b, int(reps)))
+
+    @property
+    def single_launch(self) -> bool:
+        """True when each RK stage is one launch over all groups (possible when every
+        group has order 1..5 on affine elements), False for one launch per group (the
+        default; tune() keeps the faster of the two)."""
+        return self._lib.dg_batch_get_launch_mode(self._b) == 1
+
+    @single_launch.setter
+    def single_launch(self, on: bool):
+        self._check(self._lib.dg_batch_set_launch_mode(self._b, 1 if on else 0))
 
     def l2_error(self, c: int, name: str, data=(), t: float = 0.0) -> np.ndarray:
         d = np.ascontiguousarray(np.asarray(data, np.float64).reshape(-1))

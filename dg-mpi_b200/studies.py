@@ -129,16 +129,24 @@ def ensemble(scale: float, steps: int = 100, cfl: float = 0.1):
             dts.append(b.cfl_time_step(i, U, cfl))
             b.set_time_step(i, dts[-1])
         setup = time.perf_counter() - t0
-        b.tune(reps=1)
-        for i, (_, _, data) in enumerate(spec):   # the tuner left the state unchanged; restart anyway
-            b.project_ic(i, "IsentropicVortexXY", data)
+        # one launch per RK stage for all groups
+        b.single_launch = True
+        single = b.single_launch
         ms = b.rk4_timed(steps)
         errs = [b.l2_error(i, "IsentropicVortexXY", data, steps * dts[i]) for i, (_, _, data) in enumerate(spec)]
         finals[prec] = [b.get_state(i) for i in range(0, len(spec), 4)]  # host memory: every 4th case
         out[prec] = {"dof_stage_per_s": sum(dof) * 4 * steps / (ms / 1e3), "ms_total": ms, "setup_s": setup,
-                     "groups": b.groups(), "status": b.status(),
+                     "single_launch": single, "groups": b.groups(), "status": b.status(),
                      "max_l2_error_vs_exact": np.max(np.array(errs), axis=0).tolist(),
                      "median_l2_error_vs_exact": np.median(np.array(errs), axis=0).tolist()}
+        # one launch per group and stage, each group's variant tuned
+        b.single_launch = False
+        b.tune(reps=1)
+        for i, (_, _, data) in enumerate(spec):
+            b.project_ic(i, "IsentropicVortexXY", data)
+        ms_g = b.rk4_timed(steps)
+        out[prec]["per_group_tuned"] = {"dof_stage_per_s": sum(dof) * 4 * steps / (ms_g / 1e3), "ms_total": ms_g,
+                                        "groups": b.groups()}
         b.close()
     diffs = np.array([rel_l2(a, c) for a, c in zip(finals["mixed_fp32"], finals["fp64"])])
     out["max_rel_l2_mixed_vs_fp64_every_4th_case"] = diffs.max(axis=0).tolist()

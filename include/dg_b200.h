@@ -330,12 +330,18 @@ void* dg_stream(dg_ctx* ctx);
  * advanced together by the `dg_batch_*` entry points (the reference runs one
  * case per process, so there is no reference function they replace; each
  * case's arithmetic is exactly that of a dg_ctx on the same case).  Cases of the same (order, flux, gamma, gas
- * constant) share one group: their meshes are concatenated and one stage
- * launch per group and RK stage advances all of them, each element scaling its
- * update by its own case's dt.  dg_batch_rk4_steps replays a CUDA graph that
- * runs the groups' launches one group after another (each fills the GPU).  All cases must name
- * the same device and precision.  Results per case are bit-identical to a
- * dg_ctx of that case running the same stage variant. */
+ * constant) share one group: their meshes are concatenated, each element
+ * scaling its update by its own case's dt.  dg_batch_rk4_steps replays a CUDA
+ * graph of one RK4 step: by default each group's launches, one group after
+ * another; in single-launch mode (every group of order 1..5 on affine
+ * elements) each RK stage is ONE persistent launch over all groups, after one
+ * face-flux launch over all groups, whose blocks start on per-group ranges
+ * weighted by the groups' work and then claim element batches of any group
+ * from per-group counters until all are done (128 threads per block, each
+ * order's configuration one of its compiled variants).  dg_batch_tune keeps
+ * whichever form is faster on the batch.  All cases must name the same device
+ * and precision.  Results per case are bit-identical to a dg_ctx of that case
+ * running the same stage variant (dg_batch_group_info). */
 typedef struct dg_batch dg_batch;
 
 int dg_batch_create(int ncases, const dg_case_desc* cases, const dg_mesh_desc* meshes, dg_batch** out);
@@ -361,9 +367,17 @@ int dg_batch_set_time_step(dg_batch* b, int c, double dt);
 int dg_batch_rk4_steps(dg_batch* b, int nsteps);
 /* the same, device time of the graph launches in milliseconds */
 int dg_batch_rk4_steps_timed(dg_batch* b, int nsteps, double* device_ms);
-/* picks the fastest stage variant of every group (dg_tune_stage per group,
- * on the group's current state; the state is unchanged) */
+/* picks the fastest stage variant of every group (dg_tune_stage per group),
+ * then times `reps` RK4 steps in per-group mode and in single-launch mode (when
+ * every group can run it) and keeps the faster mode; the state is unchanged */
 int dg_batch_tune(dg_batch* b, int reps);
+/* single = 1: one launch per RK stage for all groups (DG_ERR_UNSUPPORTED when
+ * a group has order 0 or non-affine elements); 0: one launch per group and
+ * stage (each group back to its own variant).  No counterpart in the
+ * reference (one case per process). */
+int dg_batch_set_launch_mode(dg_batch* b, int single);
+/* 1 in single-launch mode, 0 in per-group mode */
+int dg_batch_get_launch_mode(const dg_batch* b);
 /* dg_l2_error for case c */
 int dg_batch_l2_error(dg_batch* b, int c, int ic_type, const double* data, int ndata, double t, double* err);
 /* status flags of all groups since the last call (bits as dg_status) */

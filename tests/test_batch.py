@@ -126,3 +126,87 @@ def test_batch_error_tuning_and_zero_time_step():
         e_s = case.l2_error("IsentropicVortexXY", vortex(i), 3 * dts[i])
         assert np.allclose(e_b, e_s, rtol=1e-12, atol=0)
     assert t > 0
+
+
+# ---------------------------------------------------------------- one launch per RK stage
+
+ENS = [c for c in CASES if c[2] > 0]  # orders 1..5: the ensemble launch takes every group
+
+
+def setup_ensemble(precision):
+    ms = [dg_b200.periodic_box(n, (0, 0, 0), (10.0, 10.0, 10.0), rotate_seed=s) for n, s, _ in ENS]
+    batch = dg_b200.Batch([(m, p) for m, (_, _, p) in zip(ms, ENS)], gas_constant=1.0, precision=precision)
+    singles, dts = [], []
+    for i, (m, (_, _, p)) in enumerate(zip(ms, ENS)):
+        case = dg_b200.Case(m, p, gas_constant=1.0, precision=precision)
+        U = case.project_ic("IsentropicVortexXY", vortex(i))
+        Ub = batch.project_ic(i, "IsentropicVortexXY", vortex(i))
+        dt = batch.cfl_time_step(i, Ub, 0.1)
+        batch.set_time_step(i, dt)
+        singles.append(case)
+        dts.append(dt)
+    return batch, singles, dts
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "mixed_fp32"])
+def test_single_launch_batch_bit_identical_to_single_contexts(precision):
+    """Orders 1..5 in one launch per RK stage (plus one face launch): every case
+    bit-identical to a single context running its group's variant (a compiled
+    128-thread variant of the order), then the same after switching the batch
+    to one launch per group."""
+    batch, singles, dts = setup_ensemble(precision)
+    assert not batch.single_launch  # the default: one launch per group
+    batch.single_launch = True
+    variant = {g[0]: g[3] for g in batch.groups()}
+    for i, case in enumerate(singles):
+        case.stage_variant = variant[ENS[i][2]]
+        assert case.stage_variants()[variant[ENS[i][2]]][1] == 128
+    batch.rk4(3)
+    for i, case in enumerate(singles):
+        case.rk4(dts[i], 3)
+        assert np.array_equal(batch.get_state(i), case.get_state()), i
+    assert batch.status() == 0
+    # back to one launch per group: each group's own (default) variant
+    batch.single_launch = False
+    assert not batch.single_launch
+    variant = {g[0]: g[3] for g in batch.groups()}
+    batch.rk4(2)
+    for i, case in enumerate(singles):
+        case.stage_variant = variant[ENS[i][2]]
+        case.rk4(dts[i], 2)
+        assert np.array_equal(batch.get_state(i), case.get_state()), i
+
+
+@pytest.mark.gpu
+def test_single_launch_batch_matches_oracle_and_rejects_order_zero():
+    batch, singles, dts = setup_ensemble("fp64")
+    batch.single_launch = True
+    U0 = [s.get_state() for s in singles]
+    batch.rk4(4)
+    for i in (0, 3):  # p = 2 on a rotated mesh, p = 5
+        n, seed, p = ENS[i]
+        mesh = dg_b200.periodic_box(n, (0, 0, 0), (10.0, 10.0, 10.0), rotate_seed=seed)
+        orc = pyoracle.OracleCase.from_mesh(mesh, p, gas_constant=1.0)
+        assert rel_l2(batch.get_state(i), orc.rk4(U0[i], dts[i], 4)).max() < 1e-12
+    # a batch with an order-0 group runs one launch per group and refuses the single launch
+    full, _, _, _ = setup_pair()
+    assert not full.single_launch
+    with pytest.raises(dg_b200.DGError) as ei:
+        full.single_launch = True
+    assert ei.value.code == 5
+
+
+@pytest.mark.gpu
+def test_batch_tuner_keeps_the_faster_launch_mode_and_the_state():
+    batch, singles, dts = setup_ensemble("mixed_fp32")
+    before = [batch.get_state(i) for i in range(len(ENS))]
+    batch.tune(reps=1)
+    assert all(np.array_equal(batch.get_state(i), u) for i, u in enumerate(before))
+    mode = batch.single_launch
+    variant = {g[0]: g[3] for g in batch.groups()}
+    batch.rk4(2)
+    for i, case in enumerate(singles):
+        case.stage_variant = variant[ENS[i][2]]
+        case.rk4(dts[i], 2)
+        assert np.array_equal(batch.get_state(i), case.get_state()), (i, mode)
