@@ -1299,7 +1299,9 @@ constexpr size_t face_smem_bytes()
 {
     using L = Lay<P, 1, T>;
     constexpr int FB = face_batch<P, T>();
-    return ((sizeof(T) * FB * 10 * L::FS + 15) / 16) * 16 + FB * sizeof(FaceRec) + 2 * FB * sizeof(int);
+    // traces, then two buffers of the batch's face records (the next batch's are
+    // fetched while this one computes) and listed elements / faces
+    return ((sizeof(T) * FB * 10 * L::FS + 15) / 16) * 16 + 2 * FB * sizeof(FaceRec) + 4 * FB * sizeof(int);
 }
 
 // GEO: general geometry, the left element's normal data per face point;
@@ -1315,9 +1317,9 @@ __device__ __forceinline__ void face_flux_body(const StageArgs& a, int bid, int 
     extern __shared__ double fsm[];
     T* sTr = reinterpret_cast<T*>(fsm);                                             // [FB][2][5][FS]
     unsigned char* tail = reinterpret_cast<unsigned char*>(sTr) + ((sizeof(T) * FB * 10 * FS + 15) / 16) * 16;
-    FaceRec* sRecL = reinterpret_cast<FaceRec*>(tail);                              // [FB] listed side's record
-    int* sEL = reinterpret_cast<int*>(sRecL + FB);                                  // [FB] listed element
-    int* sFL = sEL + FB;                                                            // [FB] listed face
+    FaceRec* sRecBuf = reinterpret_cast<FaceRec*>(tail);                            // [2][FB] listed side's records
+    int* sELBuf = reinterpret_cast<int*>(sRecBuf + 2 * FB);                         // [2][FB] listed elements
+    int* sFLBuf = sELBuf + 2 * FB;                                                  // [2][FB] listed faces
     const T* __restrict__ Bt = TabSel<T>::B(a.tab);
     const T* __restrict__ Wt = TabSel<T>::W(a.tab);
     T* out = reinterpret_cast<T*>(a.fflux);
@@ -1333,8 +1335,28 @@ __device__ __forceinline__ void face_flux_body(const StageArgs& a, int bid, int 
         __syncthreads();
         f_first = slots[0];
     }
+    // the records of batch f into buffer rb: listed (element, face), then the
+    // listed side's face record by cp.async (waited for at the next batch's top)
+    auto fetch_records = [&](int f, int rb, int2 fe) {
+        if (tid < FB && f < a.nface) {
+            sELBuf[rb * FB + tid] = fe.x;
+            sFLBuf[rb * FB + tid] = fe.y;
+            const double* src = reinterpret_cast<const double*>(a.frec + (size_t)fe.x * 6 + fe.y);
+            double* dst = reinterpret_cast<double*>(sRecBuf + rb * FB + tid);
+#pragma unroll
+            for (int w = 0; w < 6; ++w) cp_async8(dst + w, src + w);
+        }
+        cp_async_commit();
+    };
     int fn = f_first, it = 0;
+    if (f_first < a.nface)
+        fetch_records(f_first, 0, tid < FB ? a.faces[min(f_first + tid, a.nface - 1)] : make_int2(0, 0));
     for (int f0 = f_first; f0 < a.nface; f0 = fn, ++it) {
+        const int rb = it & 1;
+        FaceRec* sRecL = sRecBuf + rb * FB;
+        const int* sEL = sELBuf + rb * FB;
+        const int* sFL = sFLBuf + rb * FB;
+        cp_async_wait_all();
         __syncthreads();
         if (work) {
             fn = slots[(it + 1) & 1];
@@ -1342,13 +1364,8 @@ __device__ __forceinline__ void face_flux_body(const StageArgs& a, int bid, int 
         } else {
             fn = f0 + nblk * FB;
         }
-        for (int j = tid; j < FB; j += NT) {
-            const int2 fe = a.faces[min(f0 + j, a.nface - 1)];
-            sRecL[j] = a.frec[(size_t)fe.x * 6 + fe.y];
-            sEL[j] = fe.x;
-            sFL[j] = fe.y;
-        }
-        __syncthreads();
+        // the next batch's face list entries, in flight during the traces
+        const int2 fe_next = tid < FB && fn < a.nface ? a.faces[min(fn + tid, a.nface - 1)] : make_int2(0, 0);
         // traces of both sides, in the left element's energy frame: one task per
         // (face, side, variable) gathers its boundary slice from the state into
         // registers (entry (b0, b1) at coefficient o0 + b0 s0 + b1 s1)
@@ -1374,6 +1391,8 @@ __device__ __forceinline__ void face_flux_body(const StageArgs& a, int bid, int 
                 for (int b0 = 0; b0 < N; ++b0) sl[b1][b0] = kShift ? T(x[b1][b0] - sh) : T(x[b1][b0]);
             interp2d<N, M, T>(Bt, sl, sTr + (sj * 5 + v) * FS);
         }
+        // the next batch's records stream in while this batch's fluxes compute
+        fetch_records(fn, rb ^ 1, fe_next);
         __syncthreads();
         // the flux at the listed side's face points
         for (int i = tid; i < FB * NF; i += NT) {
@@ -1410,6 +1429,7 @@ __device__ __forceinline__ void face_flux_body(const StageArgs& a, int bid, int 
             for (int v = 0; v < 5; ++v) o[v * NF] = Fo[v] * w;
         }
     }
+    cp_async_wait_all();
     if (status) atomicOr(a.status, status);
 }
 
