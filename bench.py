@@ -181,11 +181,68 @@ def mixed_leg(local, mesh, U0, dt, K, W, dist, world, ref_case, fixed_variant=No
     ref_case.set_state(U0)
     ref_case.rk4(dt, nacc)
     diff = rel_l2_per_variable(case.get_state(), ref_case.get_state())
+    # the tensor-core kernel (split-BF16 volume GEMMs on tcgen05) on the same workload
+    tc = None
+    tcv = [i for i, v in enumerate(case.stage_variants()) if "tc" in v[4].split("+")]
+    if tcv:
+        case.stage_variant = tcv[0]
+        case.set_state(U0)
+        case.rk4(dt, W)
+        torch.cuda.synchronize()
+        ms_tc = case.rk4_timed(dt, K)
+        if dist:
+            t = torch.tensor([ms_tc], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms_tc = float(t.item())
+        case.set_state(U0)
+        case.rk4(dt, nacc)
+        tc = {"value": world * dof * 4 * K / (ms_tc / 1e3), "unit": UNIT, "ms_per_step": ms_tc / K,
+              "stage_variant": case.stage_variants()[tcv[0]],
+              "rel_l2_vs_fp64_after_%d_steps" % nacc: rel_l2_per_variable(case.get_state(), ref_case.get_state()),
+              "arithmetic": "volume GEMMs as six BF16 split products on tcgen05 (FP32 accumulation in TMEM); "
+                            "flux, lift in FP32; FP64 state, inverse mass and update"}
     case.close()
     return {"value": world * dof * 4 * K / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / K,
             "stage_variant": variant, "rel_l2_vs_fp64_after_%d_steps" % nacc: diff,
             "arithmetic": "FP32 traces, fluxes and contractions; FP64 state, residual accumulation, "
-                          "inverse mass, geometry and RK update"}
+                          "inverse mass, geometry and RK update", "tensor_core_kernel": tc}
+
+
+def ensemble_leg(local, steps):
+    """The batching configuration: 256 seeded x-y vortex cases (N in {8,12,16,24,32},
+    p in 1..5, per-case CFL 0.1 time steps), mixed precision, one graph per RK4 step:
+    rates with one launch per group (tuned variants) and with one launch per RK
+    stage for all groups, and of the same cases one context at a time."""
+    import studies
+    spec = studies.ensemble_cases(256)
+    box = {n: __import__("dg_b200").periodic_box((n, n, n), (0, 0, 0), (10.0, 10.0, 10.0)) for n in {c[0] for c in spec}}
+    cases = [(box[n], p) for n, p, _ in spec]
+    dof = sum(box[n].nelem * (p + 1) ** 3 * 5 for n, p, _ in spec)
+    import dg_b200
+    b = dg_b200.Batch(cases, gas_constant=1.0, precision="mixed_fp32", device=local)
+    for i, (_, _, data) in enumerate(spec):
+        U = b.project_ic(i, "IsentropicVortexXY", data)
+        b.set_time_step(i, b.cfl_time_step(i, U, CFL))
+    out = {"cases": len(spec), "dof": dof, "steps": steps, "precision": "mixed_fp32"}
+    for single in (False, True):
+        b.single_launch = single
+        if not single:
+            b.tune(reps=1)
+            b.single_launch = False
+        b.rk4(1)
+        ms = b.rk4_timed(steps)
+        out["one_launch_per_stage" if single else "one_launch_per_group_tuned"] = {
+            "value": dof * 4 * steps / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / steps}
+    out["status"] = b.status()
+    b.close()
+    ms_seq = 0.0
+    for i, (mesh, p) in enumerate(cases):
+        c = dg_b200.Case(mesh, p, gas_constant=1.0, precision="mixed_fp32", device=local)
+        U = c.project_ic("IsentropicVortexXY", spec[i][2])
+        ms_seq += c.rk4_timed(c.cfl_time_step(U, CFL), steps)
+        c.close()
+    out["one_context_at_a_time"] = {"value": dof * 4 * steps / (ms_seq / 1e3), "unit": UNIT}
+    return out
 
 
 def cpu_oracle_rate(warmup: int, steps: int | None, budget_s: float = 12.0):
@@ -349,6 +406,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--nel", type=int, default=NEL, help="elements per direction (profiling on a smaller box)")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision leg")
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the 256-case ensemble leg")
     ap.add_argument("--variant", type=int, default=None, help="fixed FP64 launch variant instead of the tuner's pick")
     ap.add_argument("--mixed-variant", type=int, default=None, help="fixed mixed-precision launch variant")
     ap.add_argument("--replicas", action="store_true", help="N > 1: independent replicas instead of the slab decomposition")
@@ -438,6 +496,7 @@ def main():
             raise RuntimeError("non-finite state after the e2e run")
 
     mixed = None if args.no_mixed else mixed_leg(local, mesh, U0, dt, K, W, dist, world, case, args.mixed_variant)
+    ens = None if (args.no_ensemble or world > 1) else ensemble_leg(local, max(5, K // 4))
 
     if rank == 0:
         peaks, peak_kind = measured_peaks()
@@ -482,6 +541,8 @@ def main():
         }
         if mixed is not None:
             line["mixed_fp32"] = mixed
+        if ens is not None:
+            line["ensemble"] = ens
         if world == 1 and not args.no_cpu_baseline:
             rate, steps, sec, threads = cpu_oracle_rate(1, None)
             line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
