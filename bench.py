@@ -12,7 +12,10 @@ graph).  Metric: DOF-stage updates/s = DOF x 4 x steps / time.
 
 value    : device time (CUDA events on the kernels' stream), state resident in HBM
 e2e      : the same steps through the C ABI from pinned host buffers:
-           dg_set_state (H2D), K x dg_rk4_steps(dt, 1), dg_get_state (D2H)
+           dg_set_state (H2D), K x dg_rk4_steps(dt, 1), dg_get_state (D2H) --
+           the resident-state use of the drop-in (one upload and one download
+           around the K steps), so the per-step copy bytes, and the e2e rate,
+           depend on K: 671 MB / K each way
 roofline : one RK stage (the face-flux kernel + the stage kernel when the tuner
            picks a face-flux variant, else the stage kernel alone: the only
            kernels of the timed region), per stage

@@ -136,6 +136,11 @@ def library(path: str | None = None) -> ctypes.CDLL:
         "dg_batch_get_launch_mode": (ctypes.c_int, [vp]),
         "dg_batch_l2_error": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, dp, ctypes.c_int, ctypes.c_double, dp]),
         "dg_batch_status": (ctypes.c_int, [vp, up]),
+        "dg_mesh_read_h5": (ctypes.c_int, [ctypes.c_char_p, ip, ip, ip, ip, dp, ip, up, ip, up]),
+        "dg_mesh_write_h5": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(_MeshDesc)]),
+        "dg_solution_write_h5": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(_MeshDesc), ctypes.c_int, dp,
+                                                ctypes.c_double]),
+        "dg_solution_read_h5": (ctypes.c_int, [ctypes.c_char_p, ip, ip, ip, dp, dp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -156,10 +161,14 @@ def _uptr(a: np.ndarray):
 
 @dataclass
 class Mesh:
-    """Hex mesh in the reference's in-memory form (src/mesh/mesh.h)."""
-    node_coords: np.ndarray      # [nnode][3] float64
-    elem_to_node_ids: np.ndarray  # [nelem][8] uint32
+    """Hex mesh in the reference's in-memory form (src/mesh/mesh.h).  A mesh
+    read from a file may have another dimension or element type (dim, the
+    file's QOrder); contexts take dim 3, qorder 1, 8-node hexahedra."""
+    node_coords: np.ndarray      # [nnode][dim] float64
+    elem_to_node_ids: np.ndarray  # [nelem][nodes per element] uint32
     interior_faces: np.ndarray    # [nface][8] uint32
+    dim: int = 3
+    qorder: int = 1
 
     @property
     def nelem(self) -> int:
@@ -239,10 +248,77 @@ def partition_periodic_box(n, x0, length, nparts: int, part: int, axis: int = 2,
     return Mesh(coords, e2n, faces), Partition(part, no.value, ni.value, gr, ge, gl)
 
 
+def _path(path) -> bytes:
+    return os.fsencode(os.fspath(path))
+
+
+def read_mesh_h5(path) -> Mesh:
+    """A mesh file of the reference's format (Mesh::read_mesh,
+    src/mesh/mesh.cpp:79-204) through dg_mesh_read_h5."""
+    lib = library()
+    d, q, npe, nn, ne, nf = (ctypes.c_int() for _ in range(6))
+    args = [ctypes.byref(v) for v in (d, q, npe, nn)]
+    rc = lib.dg_mesh_read_h5(_path(path), *args, None, ctypes.byref(ne), None, ctypes.byref(nf), None)
+    if rc:
+        raise DGError(rc, lib.dg_last_error(None).decode())
+    coords = np.zeros((nn.value, d.value), np.float64)
+    e2n = np.zeros((ne.value, npe.value), np.uint32)
+    faces = np.zeros((nf.value, 8), np.uint32)
+    rc = lib.dg_mesh_read_h5(_path(path), *args, _dptr(coords), ctypes.byref(ne), _uptr(e2n), ctypes.byref(nf),
+                             _uptr(faces))
+    if rc:
+        raise DGError(rc, lib.dg_last_error(None).decode())
+    return Mesh(coords, e2n, faces, d.value, q.value)
+
+
+def write_mesh_h5(path, mesh: Mesh):
+    """Writes a hexahedral mesh in the reference's mesh-file format (dg_mesh_write_h5)."""
+    lib = library()
+    keep = []
+    md = _mesh_desc(mesh, 0, keep)
+    rc = lib.dg_mesh_write_h5(_path(path), ctypes.byref(md))
+    if rc:
+        raise DGError(rc, lib.dg_last_error(None).decode())
+
+
+def write_solution_h5(path, mesh: Mesh, order: int, Uc: np.ndarray, time: float = 0.0):
+    """Writes Uc[ne][nb][5] in the reference writer's data.h5 schema
+    (Writer::write, src/io/writer.cpp:10-64) through dg_solution_write_h5."""
+    lib = library()
+    keep = []
+    md = _mesh_desc(mesh, 0, keep)
+    U = np.ascontiguousarray(Uc, np.float64)
+    if U.size != mesh.nelem * (order + 1) ** 3 * 5:
+        raise ValueError("Uc does not hold a state of this mesh and order")
+    rc = lib.dg_solution_write_h5(_path(path), ctypes.byref(md), int(order), _dptr(U), float(time))
+    if rc:
+        raise DGError(rc, lib.dg_last_error(None).decode())
+
+
+def read_solution_h5(path):
+    """(Uc [ne][nb][ns], time) from a data.h5 of the reference writer's schema
+    (Solver::read_in_coefficients, src/solver/base.cpp:234-279)."""
+    lib = library()
+    ne, nb, ns, t = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+    rc = lib.dg_solution_read_h5(_path(path), ctypes.byref(ne), ctypes.byref(nb), ctypes.byref(ns), ctypes.byref(t),
+                                 None)
+    if rc:
+        raise DGError(rc, lib.dg_last_error(None).decode())
+    U = np.zeros((ne.value, nb.value, ns.value), np.float64)
+    rc = lib.dg_solution_read_h5(_path(path), ctypes.byref(ne), ctypes.byref(nb), ctypes.byref(ns), ctypes.byref(t),
+                                 _dptr(U))
+    if rc:
+        raise DGError(rc, lib.dg_last_error(None).decode())
+    return U, t.value
+
+
 def _mesh_desc(mesh: Mesh, rank: int, keep: list) -> _MeshDesc:
     c = np.ascontiguousarray(mesh.node_coords, np.float64)
     e = np.ascontiguousarray(mesh.elem_to_node_ids, np.uint32)
     f = np.ascontiguousarray(mesh.interior_faces, np.uint32)
+    if c.ndim != 2 or c.shape[1] != 3 or e.ndim != 2 or e.shape[1] != 8 or f.ndim != 2 or f.shape[1] != 8:
+        raise ValueError("the C ABI takes 3D meshes of 8-node hexahedra (node_coords [n][3], "
+                         "elem_to_node_ids [ne][8], interior_faces [nf][8])")
     keep += [c, e, f]
     return _MeshDesc(c.shape[0], _dptr(c), e.shape[0], _uptr(e), f.shape[0], _uptr(f), rank)
 

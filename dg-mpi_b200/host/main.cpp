@@ -7,8 +7,13 @@
 //
 // Deck keys (as in the reference, src/exec/main.cpp:52-119,
 // src/solver/base.cpp:20-67, src/physics/base/base.cpp:25-32):
-//   [Mesh]     file = "...cube_<N>.h5"  -> periodic N^3 box on [0,1]^3 (the
-//              reference's cube meshes; no HDF5 reader in this build), or
+//   [Mesh]     file = "mesh.h5": a mesh file of the reference's format
+//              (Mesh::read_mesh, src/mesh/mesh.cpp:79-204; read by
+//              dg_mesh_read_h5; a relative path is taken from the working
+//              directory, as the reference opens it);
+//              when no such file exists and the name is the reference's
+//              "...cube_<N>.h5", the periodic N^3 box on [0,1]^3 that file
+//              holds is generated instead; or
 //              periodic_box = [nx, ny, nz], origin = [..], length = [..]
 //   [Numerics] order, basis = "LagrangeHex"
 //   [Stepper]  type = "FE" | "RK4" (default "FE"), timestep, end;
@@ -16,12 +21,17 @@
 //   [Physics]  name = "Euler", dim = 3, gamma = 1.4, GasConstant = 287.05,
 //              convective_flux_fcn = "LaxFriedrichs" | "HLLC"
 //   [InitialCondition] name, data
-//   [Output]   (extensions) print_every = N; state_file = "path" (binary
-//              checkpoint at the end: int64 ne, nb, 5, double time, then
-//              Uc [ne][nb][5]); restart_file = "path" (start from such a
-//              checkpoint instead of the initial condition; with `end` the
-//              run stops at that time, with `steps` it takes that many more);
-//              json = true (one JSON line of run metrics at the end)
+//   [Output]   as the reference (src/exec/main.cpp:105-112), the final state
+//              is written to data.h5 in the writer's schema
+//              (dg_solution_write_h5); disable_all_outputs = true skips it;
+//              (extensions) solution_file = "path" (instead of data.h5);
+//              print_every = N; state_file = "path" (binary checkpoint at
+//              the end: int64 ne, nb, 5, double time, then Uc [ne][nb][5]);
+//              restart_file = "path" (start from such a checkpoint, or from a
+//              *.h5 solution file of the writer's schema, instead of the
+//              initial condition; with `end` the run stops at that time, with
+//              `steps` it takes that many more); json = true (one JSON line
+//              of run metrics at the end)
 #include <cfloat>
 #include <chrono>
 #include <cstdio>
@@ -102,11 +112,23 @@ int ic_code(const std::string& name)
     throw std::runtime_error("unknown [InitialCondition] name " + name);
 }
 
+bool file_exists(const std::string& path)
+{
+    std::ifstream f(path, std::ios::binary);
+    return static_cast<bool>(f);
+}
+
+bool ends_with(const std::string& s, const std::string& tail)
+{
+    return s.size() >= tail.size() && s.compare(s.size() - tail.size(), tail.size(), tail) == 0;
+}
+
 int run(const dgh::Toml& deck, bool check_only)
 {
     // ---- mesh ----
     int n[3] = {0, 0, 0};
     double x0[3] = {0, 0, 0}, len[3] = {1, 1, 1};
+    std::string mesh_file;
     if (deck.has("Mesh", "periodic_box")) {
         const auto b = deck.nums("Mesh", "periodic_box");
         if (b.size() != 3) throw std::runtime_error("[Mesh] periodic_box needs 3 entries");
@@ -115,11 +137,15 @@ int run(const dgh::Toml& deck, bool check_only)
         if (deck.has("Mesh", "length")) { auto l = deck.nums("Mesh", "length"); for (int i = 0; i < 3; ++i) len[i] = l.at(i); }
     } else {
         const std::string file = deck.str("Mesh", "file");
+        const std::string& path = file;
         std::smatch m;
-        if (!std::regex_search(file, m, std::regex("cube_([0-9]+)\\.h5$")))
-            throw std::runtime_error("[Mesh] file " + file + ": only the reference's periodic cube_<N>.h5 meshes are "
-                                     "generated in memory (no HDF5 reader); use periodic_box");
-        n[0] = n[1] = n[2] = std::stoi(m[1]);
+        if (file_exists(path)) {
+            mesh_file = path;
+        } else if (std::regex_search(file, m, std::regex("cube_([0-9]+)\\.h5$"))) {
+            n[0] = n[1] = n[2] = std::stoi(m[1]);
+        } else {
+            throw std::runtime_error("[Mesh] file " + path + " not found");
+        }
     }
     // ---- numerics / physics ----
     const int order = static_cast<int>(deck.num("Numerics", "order"));
@@ -141,15 +167,39 @@ int run(const dgh::Toml& deck, bool check_only)
     const std::string stype = deck.str_or("Stepper", "type", "FE");
     if (stype != "FE" && stype != "RK4") throw std::runtime_error("[Stepper] type must be FE or RK4");
 
-    std::printf("case: %dx%dx%d periodic hex, p=%d, %s flux, %s, IC %s\n", n[0], n[1], n[2], order, flux_name.c_str(),
-                stype.c_str(), ic_name.c_str());
+    int nn = 0, ne = 0, nf = 0;
+    std::vector<double> coords;
+    std::vector<unsigned> e2n, faces;
+    if (!mesh_file.empty()) {
+        int dim = 0, qorder = 0, npe = 0;
+        if (dg_mesh_read_h5(mesh_file.c_str(), &dim, &qorder, &npe, &nn, nullptr, &ne, nullptr, &nf, nullptr))
+            throw std::runtime_error(dg_last_error(nullptr));
+        if (dim != 3 || qorder != 1 || npe != 8)
+            throw std::runtime_error("[Mesh] file " + mesh_file + ": dimension " + std::to_string(dim) + ", QOrder " +
+                                     std::to_string(qorder) + ", " + std::to_string(npe) +
+                                     " nodes per element; the device path takes linear hexahedra (3, 1, 8)");
+        coords.resize(static_cast<size_t>(nn) * 3);
+        e2n.resize(static_cast<size_t>(ne) * 8);
+        faces.resize(static_cast<size_t>(nf) * 8);
+        if (dg_mesh_read_h5(mesh_file.c_str(), &dim, &qorder, &npe, &nn, coords.data(), &ne, e2n.data(), &nf,
+                            faces.data()))
+            throw std::runtime_error(dg_last_error(nullptr));
+        std::printf("case: %s (%d hex elements, %d interior faces), p=%d, %s flux, %s, IC %s\n", mesh_file.c_str(), ne,
+                    nf, order, flux_name.c_str(), stype.c_str(), ic_name.c_str());
+    } else {
+        std::printf("case: %dx%dx%d periodic hex, p=%d, %s flux, %s, IC %s\n", n[0], n[1], n[2], order,
+                    flux_name.c_str(), stype.c_str(), ic_name.c_str());
+    }
     if (check_only) return 0;
 
-    int nn = 0, ne = 0, nf = 0;
-    if (dg_mesh_periodic_box(n, x0, len, 0, &nn, nullptr, &ne, nullptr, &nf, nullptr)) throw std::runtime_error("bad box");
-    std::vector<double> coords(static_cast<size_t>(nn) * 3);
-    std::vector<unsigned> e2n(static_cast<size_t>(ne) * 8), faces(static_cast<size_t>(nf) * 8);
-    dg_mesh_periodic_box(n, x0, len, 0, &nn, coords.data(), &ne, e2n.data(), &nf, faces.data());
+    if (mesh_file.empty()) {
+        if (dg_mesh_periodic_box(n, x0, len, 0, &nn, nullptr, &ne, nullptr, &nf, nullptr))
+            throw std::runtime_error("bad box");
+        coords.resize(static_cast<size_t>(nn) * 3);
+        e2n.resize(static_cast<size_t>(ne) * 8);
+        faces.resize(static_cast<size_t>(nf) * 8);
+        dg_mesh_periodic_box(n, x0, len, 0, &nn, coords.data(), &ne, e2n.data(), &nf, faces.data());
+    }
     dg_mesh_desc md{nn, coords.data(), ne, e2n.data(), nf, faces.data(), 0};
     dg_case_desc cd{order, flux, gamma, R, DG_PREC_FP64, 0};
 
@@ -165,16 +215,27 @@ int run(const dgh::Toml& deck, bool check_only)
         // the time step still comes from the deck (or the CFL on the initial
         // condition), so a resumed run takes the same steps as an unbroken one
         const std::string path = deck.str("Output", "restart_file");
-        std::ifstream f(path, std::ios::binary);
-        long long hdr[3] = {0, 0, 0};
-        double t = 0.0;
-        f.read(reinterpret_cast<char*>(hdr), sizeof(hdr));
-        f.read(reinterpret_cast<char*>(&t), sizeof(double));
-        if (!f || hdr[0] != ne || hdr[1] != nb || hdr[2] != 5)
-            throw std::runtime_error("restart_file " + path + " does not hold a state of this mesh and order");
         std::vector<double> U0(Uc.size());
-        f.read(reinterpret_cast<char*>(U0.data()), static_cast<std::streamsize>(U0.size() * sizeof(double)));
-        if (!f) throw std::runtime_error("restart_file " + path + " is truncated");
+        double t = 0.0;
+        if (ends_with(path, ".h5")) {
+            // a solution file of the writer's schema (Solver::read_in_coefficients, base.cpp:234-279)
+            int fne = 0, fnb = 0, fns = 0;
+            if (dg_solution_read_h5(path.c_str(), &fne, &fnb, &fns, &t, nullptr))
+                throw std::runtime_error(dg_last_error(nullptr));
+            if (fne != ne || fnb != nb || fns != 5)
+                throw std::runtime_error("restart_file " + path + " does not hold a state of this mesh and order");
+            if (dg_solution_read_h5(path.c_str(), &fne, &fnb, &fns, &t, U0.data()))
+                throw std::runtime_error(dg_last_error(nullptr));
+        } else {
+            std::ifstream f(path, std::ios::binary);
+            long long hdr[3] = {0, 0, 0};
+            f.read(reinterpret_cast<char*>(hdr), sizeof(hdr));
+            f.read(reinterpret_cast<char*>(&t), sizeof(double));
+            if (!f || hdr[0] != ne || hdr[1] != nb || hdr[2] != 5)
+                throw std::runtime_error("restart_file " + path + " does not hold a state of this mesh and order");
+            f.read(reinterpret_cast<char*>(U0.data()), static_cast<std::streamsize>(U0.size() * sizeof(double)));
+            if (!f) throw std::runtime_error("restart_file " + path + " is truncated");
+        }
         solver.time = t;
         solver.restart_state = std::move(U0);
     }
@@ -239,8 +300,16 @@ int run(const dgh::Toml& deck, bool check_only)
         json += "]";
     }
     if (deck.has("Output", "json") && deck.boolean("Output", "json")) std::printf("%s}\n", json.c_str());
+    const bool outputs = !(deck.has("Output", "disable_all_outputs") && deck.boolean("Output", "disable_all_outputs"));
+    if (outputs || deck.has("Output", "state_file")) dg_get_state(solver.ctx, Uc.data());
+    if (outputs) {
+        // Writer("data.h5", ...) after the solve, src/exec/main.cpp:105-112
+        const std::string out = deck.has("Output", "solution_file") ? deck.str("Output", "solution_file") : "data.h5";
+        if (dg_solution_write_h5(out.c_str(), &md, order, Uc.data(), solver.time))
+            throw std::runtime_error(dg_last_error(nullptr));
+        std::printf("solution written to %s\n", out.c_str());
+    }
     if (deck.has("Output", "state_file")) {
-        dg_get_state(solver.ctx, Uc.data());
         std::ofstream f(deck.str("Output", "state_file"), std::ios::binary);
         const long long hdr[3] = {ne, nb, 5};
         f.write(reinterpret_cast<const char*>(hdr), sizeof(hdr));

@@ -399,6 +399,45 @@ int dg_mesh_periodic_box(const int n[3], const double x0[3], const double len[3]
                          int* nelem, unsigned* elem_to_node_ids,
                          int* nface, unsigned* interior_faces);
 
+/* ---- mesh and solution files in the reference's HDF5 schemas (host only,
+ * no GPU; a self-contained reader/writer of the HDF5 subset these files use:
+ * version 0 superblock, symbol-table groups, version 1 object headers,
+ * contiguous or compact integer / IEEE float datasets; other HDF5 files are
+ * refused with DG_ERR_ARG and a message, never guessed) ---- */
+
+/* Replaces Mesh::read_mesh (src/mesh/mesh.cpp:79-204): reads Dimension,
+ * QOrder, nElem, nNode, nIFace, nNodePerElem, NodeCoords, Elem2Nodes and
+ * IFaceData.  node_coords is [nnode][dim], elem_to_node_ids
+ * [nelem][nnode_per_elem] (the file's gbasis node order), interior_faces
+ * [nface][8] in the dg_mesh_desc row form with both rank entries 0.  Sizes
+ * first: with all three arrays NULL only the counts are returned.  Any
+ * dimension and element type is read; dg_create takes dim 3, qorder 1,
+ * nnode_per_elem 8 meshes whose faces are all interior (periodic). */
+int dg_mesh_read_h5(const char* path, int* dim, int* qorder, int* nnode_per_elem, int* nnode, double* node_coords,
+                    int* nelem, unsigned* elem_to_node_ids, int* nface, unsigned* interior_faces);
+
+/* Writes a hexahedral mesh in that format (Dimension 3, QOrder 1,
+ * nNodePerElem 8, nNodePerFace 4, nBFaceGroup 0, 64-bit integers as the
+ * reference's mesh files store them); dg_mesh_read_h5 reads it back exactly. */
+int dg_mesh_write_h5(const char* path, const dg_mesh_desc* md);
+
+/* Replaces Writer::write (src/io/writer.cpp:10-64) for one rank: the
+ * attributes Number of Ranks / Dimensions / Elements / Nodes / Nodes Per
+ * Element / Basis Functions / State Variables, Solver Final Time and Stored
+ * Layout (1: row-major), the dataset Number of Elements per Partition, and the
+ * parallel datasets Node Coordinates, Local to Global Node ID, Element Global
+ * Node IDs, Local to Global Element IDs and Solution Coefficients (each with
+ * its _offsets and _dims, src/io/HDF5Wrapper.h:775-880).  Uc is [nelem][nb][5]
+ * with nb = (order+1)^3. */
+int dg_solution_write_h5(const char* path, const dg_mesh_desc* md, int order, const double* Uc, double time);
+
+/* Replaces Solver::read_in_coefficients (src/solver/base.cpp:234-279) and
+ * Reader's serialisation (src/io/reader.h:28-80): reads Solution Coefficients
+ * of every rank block, in either stored layout, into Uc[nelem][nb][ns] in
+ * global element order (Local to Global Element IDs).  Sizes first: with Uc
+ * NULL only nelem, nb, ns and the file's Solver Final Time are returned. */
+int dg_solution_read_h5(const char* path, int* nelem, int* nb, int* ns, double* time, double* Uc);
+
 /* Host-side time step from a CFL number on a given state (the reference has
  * none; [Stepper] timestep is used as is): dt = cfl * h_min /
  * ((2p+1) * max over element nodes of (|u| + c)). */

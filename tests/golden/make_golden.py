@@ -10,15 +10,21 @@ executed) and records the numbers its tests and tables pin:
     src/numerics/quadrature/segment.cpp, keyed by quadrature order;
   * the p = 1 LagrangeHex gradient expectations at xi = (-1,-1,-1)
     (test/numerics/basis/test_basis.cpp:264-272) and the equidistant-node
-    expectations (test/numerics/test_nodes.cpp, test/numerics/basis/test_tools.cpp).
+    expectations (test/numerics/test_nodes.cpp, test/numerics/basis/test_tools.cpp);
+  * the reference's own HDF5 mesh files (examples/quad_1x1/quad_1x1.h5,
+    examples/quad_2x2/quad_2x2.h5, test/mpi_enabled_tests/mesh/quad_2x2.h5),
+    copied byte for byte into tests/golden/meshes/ as reader inputs, with
+    their SHA-256 in the JSON.
 
 Usage: python tests/golden/make_golden.py <reference root>
 """
 from __future__ import annotations
 
+import hashlib
 import json
 import os
 import re
+import shutil
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -82,6 +88,16 @@ def main(root):
         "cases": [[0.0, 10.0, 1, [0.0]], [0.0, 10.0, 2, [0.0, 10.0]], [-1.0, 1.0, 3, [-1.0, 0.0, 1.0]]],
     }
     g["tolerance"] = {"source": "test/numerics/basis/test_basis.cpp:8", "double": 1e-13}
+    meshes = {}
+    os.makedirs(os.path.join(HERE, "meshes"), exist_ok=True)
+    for rel, name in (("examples/quad_1x1/quad_1x1.h5", "quad_1x1.h5"),
+                      ("examples/quad_2x2/quad_2x2.h5", "quad_2x2.h5"),
+                      ("test/mpi_enabled_tests/mesh/quad_2x2.h5", "mpi_test_mesh.h5")):
+        dst = os.path.join(HERE, "meshes", name)
+        shutil.copyfile(os.path.join(root, rel), dst)
+        with open(dst, "rb") as f:
+            meshes[name] = {"source": rel, "sha256": hashlib.sha256(f.read()).hexdigest()}
+    g["mesh_files"] = meshes
     with open(os.path.join(HERE, "reference_vectors.json"), "w") as f:
         json.dump(g, f, indent=1)
     print("wrote", len(gl), "Gauss-Legendre orders")

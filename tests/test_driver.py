@@ -9,6 +9,7 @@ import numpy as np
 import pytest
 
 from conftest import PKG
+import dg_b200
 
 SOLVE = os.path.join(PKG, "_build", "dg_solve")
 EXAMPLES = os.path.join(PKG, "examples")
@@ -40,15 +41,46 @@ def test_driver_rejects_unsupported_input(tmp_path, bad, msg):
     assert r.returncode == 2 and msg in r.stderr
 
 
-@pytest.mark.gpu
-def test_driver_reproduces_reference_regression(golden):
-    r = run(["-input", os.path.join(EXAMPLES, "vortex3d_regression.toml")], timeout=300)
+def _check_regression(r, golden):
     assert r.returncode == 0, r.stderr
     err = {int(m.group(1)): float(m.group(2)) for m in re.finditer(r"norm_total_error\((\d)\)=(\S+)", r.stdout)}
     ref = np.array(golden["vortex3d_regression"]["l2_errors"])
     assert "number of iterations = 1000" in r.stdout
     for s in (0, 1, 3, 4):
         assert abs(err[s] - ref[s]) <= 1e-12 * ref[s], (s, err[s], ref[s])
+
+
+@pytest.mark.gpu
+def test_driver_reproduces_reference_regression(golden, tmp_path):
+    """No meshes/cube_4.h5 exists: the driver generates the periodic box that
+    file holds; the final state goes to data.h5 as the reference writes it."""
+    r = run(["-input", os.path.join(EXAMPLES, "vortex3d_regression.toml")], timeout=300, cwd=str(tmp_path))
+    _check_regression(r, golden)
+    assert "periodic hex" in r.stdout
+    U, t = dg_b200.read_solution_h5(str(tmp_path / "data.h5"))
+    assert U.shape == (64, 64, 5) and t == pytest.approx(1.0, abs=1e-12)
+
+
+@pytest.mark.gpu
+def test_driver_runs_reference_regression_from_a_mesh_file(golden, tmp_path):
+    """The same deck on a cube_4.h5 mesh file of the reference's format (the
+    4^3 box with rotated element numberings written by dg_mesh_write_h5):
+    read through dg_mesh_read_h5, same published errors."""
+    (tmp_path / "meshes").mkdir()
+    dg_b200.write_mesh_h5(str(tmp_path / "meshes" / "cube_4.h5"),
+                          dg_b200.periodic_box((4, 4, 4), (0, 0, 0), (1, 1, 1), rotate_seed=3))
+    r = run(["-input", os.path.join(EXAMPLES, "vortex3d_regression.toml")], timeout=300, cwd=str(tmp_path))
+    _check_regression(r, golden)
+    assert "cube_4.h5 (64 hex elements, 192 interior faces)" in r.stdout
+
+
+def test_driver_refuses_a_two_dimensional_mesh_file(tmp_path):
+    text = open(os.path.join(EXAMPLES, "vortex3d_regression.toml")).read()
+    quad = os.path.join(os.path.dirname(__file__), "golden", "meshes", "quad_2x2.h5")
+    deck = tmp_path / "deck.toml"
+    deck.write_text(re.sub(r"^file\s*=.*$", 'file = "%s"' % quad, text, flags=re.M))
+    r = run(["-input", str(deck), "-check"])
+    assert r.returncode == 2 and "takes linear hexahedra" in r.stderr
 
 
 def _deck(tmp_path, name, steps, output):
@@ -68,7 +100,7 @@ def test_driver_deck_with_output_extensions_parses(tmp_path):
 def test_driver_rejects_a_restart_file_of_another_mesh(tmp_path):
     bad = tmp_path / "other.state"
     np.array([7, 27, 5], np.int64).tofile(str(bad))
-    r = run(["-input", _deck(tmp_path, "d.toml", 5, 'restart_file = "%s"' % bad)])
+    r = run(["-input", _deck(tmp_path, "d.toml", 5, 'restart_file = "%s"' % bad)], cwd=str(tmp_path))
     assert r.returncode == 2 and "does not hold a state of this mesh" in r.stderr
 
 
@@ -79,14 +111,15 @@ def test_driver_checkpoint_resume_matches_unbroken_run(tmp_path):
     reports the run."""
     import json
     full, part, rest = tmp_path / "full.state", tmp_path / "part.state", tmp_path / "rest.state"
-    r = run(["-input", _deck(tmp_path, "a.toml", 20, 'state_file = "%s"\njson = true' % full)])
+    r = run(["-input", _deck(tmp_path, "a.toml", 20, 'state_file = "%s"\njson = true' % full)], cwd=str(tmp_path))
     assert r.returncode == 0, r.stderr
     metrics = json.loads(r.stdout.strip().splitlines()[-1])
     assert metrics["steps"] == 20 and metrics["stages_per_step"] == 4 and metrics["dof"] == 512 * 27 * 5
     assert len(metrics["l2_error"]) == 5 and metrics["dof_stage_per_s"] > 0
-    r = run(["-input", _deck(tmp_path, "b.toml", 12, 'state_file = "%s"' % part)])
+    r = run(["-input", _deck(tmp_path, "b.toml", 12, 'state_file = "%s"' % part)], cwd=str(tmp_path))
     assert r.returncode == 0, r.stderr
-    r = run(["-input", _deck(tmp_path, "c.toml", 8, 'restart_file = "%s"\nstate_file = "%s"' % (part, rest))])
+    r = run(["-input", _deck(tmp_path, "c.toml", 8, 'restart_file = "%s"\nstate_file = "%s"' % (part, rest))],
+            cwd=str(tmp_path))
     assert r.returncode == 0, r.stderr
 
     def load(path):
@@ -99,3 +132,19 @@ def test_driver_checkpoint_resume_matches_unbroken_run(tmp_path):
     assert list(h1) == list(h2) == [512, 27, 5]
     assert t1 == t2 == metrics["time"]
     assert np.array_equal(u1, u2)
+
+
+@pytest.mark.gpu
+def test_driver_resumes_from_its_data_h5(tmp_path):
+    """12 steps written to data.h5 (the writer's schema), then 8 more from that
+    file, against 20 unbroken steps: bit for bit the same state and time."""
+    r = run(["-input", _deck(tmp_path, "a.toml", 20, 'solution_file = "full.h5"')], cwd=str(tmp_path))
+    assert r.returncode == 0, r.stderr
+    r = run(["-input", _deck(tmp_path, "b.toml", 12, "")], cwd=str(tmp_path))
+    assert r.returncode == 0, r.stderr
+    r = run(["-input", _deck(tmp_path, "c.toml", 8, 'restart_file = "data.h5"\nsolution_file = "rest.h5"')],
+            cwd=str(tmp_path))
+    assert r.returncode == 0, r.stderr
+    u1, t1 = dg_b200.read_solution_h5(str(tmp_path / "full.h5"))
+    u2, t2 = dg_b200.read_solution_h5(str(tmp_path / "rest.h5"))
+    assert t1 == t2 and np.array_equal(u1, u2)
