@@ -299,7 +299,6 @@ int run(const dgh::Toml& deck, bool check_only)
         }
         json += "]";
     }
-    if (deck.has("Output", "json") && deck.boolean("Output", "json")) std::printf("%s}\n", json.c_str());
     const bool outputs = !(deck.has("Output", "disable_all_outputs") && deck.boolean("Output", "disable_all_outputs"));
     if (outputs || deck.has("Output", "state_file")) dg_get_state(solver.ctx, Uc.data());
     if (outputs) {
@@ -316,6 +315,7 @@ int run(const dgh::Toml& deck, bool check_only)
         f.write(reinterpret_cast<const char*>(&solver.time), sizeof(double));
         f.write(reinterpret_cast<const char*>(Uc.data()), static_cast<std::streamsize>(Uc.size() * sizeof(double)));
     }
+    if (deck.has("Output", "json") && deck.boolean("Output", "json")) std::printf("%s}\n", json.c_str());
     dg_destroy(solver.ctx);
     return 0;
 }
