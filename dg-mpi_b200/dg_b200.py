@@ -30,6 +30,9 @@ FLUX = {"LaxFriedrichs": 0, "HLLC": 1}
 PRECISION = {"fp64": 0, "mixed_fp32": 1}
 # [InitialCondition] name -> DG_IC_* (include/dg_b200.h)
 IC = {"Uniform": 0, "IsentropicVortex": 1, "Sphere": 2, "IsentropicVortexXY": 3, "TaylorGreen": 4}
+# the 2D path's families: the reference's 2D vortex (data rho, u, v, p, strength),
+# the x-y vortex at (x, y, 0), a uniform state of four conserved values
+IC2D = {"Uniform": 0, "IsentropicVortex": 5, "IsentropicVortexXY": 3}
 
 
 class DGError(RuntimeError):
@@ -141,6 +144,22 @@ def library(path: str | None = None) -> ctypes.CDLL:
         "dg_solution_write_h5": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(_MeshDesc), ctypes.c_int, dp,
                                                 ctypes.c_double]),
         "dg_solution_read_h5": (ctypes.c_int, [ctypes.c_char_p, ip, ip, ip, dp, dp]),
+        "dg2d_create": (ctypes.c_int, [ctypes.POINTER(_CaseDesc), ctypes.POINTER(_MeshDesc), ctypes.POINTER(vp)]),
+        "dg2d_destroy": (None, [vp]),
+        "dg2d_last_error": (ctypes.c_char_p, [vp]),
+        "dg2d_num_basis": (ctypes.c_int, [vp]),
+        "dg2d_set_state": (ctypes.c_int, [vp, dp]),
+        "dg2d_get_state": (ctypes.c_int, [vp, dp]),
+        "dg2d_residual": (ctypes.c_int, [vp, dp]),
+        "dg2d_rk4_steps": (ctypes.c_int, [vp, ctypes.c_double, ctypes.c_int]),
+        "dg2d_rk4_steps_timed": (ctypes.c_int, [vp, ctypes.c_double, ctypes.c_int, dp]),
+        "dg2d_fe_steps": (ctypes.c_int, [vp, ctypes.c_double, ctypes.c_int]),
+        "dg2d_project_ic": (ctypes.c_int, [vp, ctypes.c_int, dp, ctypes.c_int, ctypes.c_double, dp]),
+        "dg2d_l2_error": (ctypes.c_int, [vp, ctypes.c_int, dp, ctypes.c_int, ctypes.c_double, dp]),
+        "dg2d_status": (ctypes.c_int, [vp, up]),
+        "dg_mesh2d_periodic_box": (ctypes.c_int, [ip, dp, dp, ctypes.c_uint, ip, dp, ip, up, ip, up]),
+        "dg2d_solution_write_h5": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(_MeshDesc), ctypes.c_int, dp,
+                                                  ctypes.c_double]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -702,3 +721,133 @@ def kinetic_energy_noalloc(order: int, nelem: int, d_state: int, d_djac: int, d_
                                        ctypes.c_void_p(d_ke), ctypes.c_void_p(stream))
     if rc:
         raise DGError(rc, lib.dg_last_error(None).decode())
+
+
+# ---------------------------------------------------------------------------
+# 2D quadrilaterals (dg2d_*)
+# ---------------------------------------------------------------------------
+
+def periodic_box_2d(n, x0=(0.0, 0.0), length=(1.0, 1.0), rotate_seed: int = 0) -> Mesh:
+    """Periodic quadrilateral box from dg_mesh2d_periodic_box (a Mesh with dim 2)."""
+    lib = library()
+    n_arr = (ctypes.c_int * 2)(*[int(v) for v in n])
+    x_arr = (ctypes.c_double * 2)(*[float(v) for v in x0])
+    l_arr = (ctypes.c_double * 2)(*[float(v) for v in length])
+    nn, ne, nf = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    rc = lib.dg_mesh2d_periodic_box(n_arr, x_arr, l_arr, ctypes.c_uint(rotate_seed), ctypes.byref(nn), None,
+                                    ctypes.byref(ne), None, ctypes.byref(nf), None)
+    if rc:
+        raise DGError(rc, "dg_mesh2d_periodic_box: bad box")
+    coords = np.zeros((nn.value, 2), np.float64)
+    e2n = np.zeros((ne.value, 4), np.uint32)
+    faces = np.zeros((nf.value, 8), np.uint32)
+    rc = lib.dg_mesh2d_periodic_box(n_arr, x_arr, l_arr, ctypes.c_uint(rotate_seed), ctypes.byref(nn), _dptr(coords),
+                                    ctypes.byref(ne), _uptr(e2n), ctypes.byref(nf), _uptr(faces))
+    if rc:
+        raise DGError(rc, "dg_mesh2d_periodic_box failed")
+    return Mesh(coords, e2n, faces, 2, 1)
+
+
+def _mesh2d_desc(mesh: Mesh, keep: list) -> _MeshDesc:
+    c = np.ascontiguousarray(mesh.node_coords, np.float64)
+    e = np.ascontiguousarray(mesh.elem_to_node_ids, np.uint32)
+    f = np.ascontiguousarray(mesh.interior_faces, np.uint32)
+    if c.ndim != 2 or c.shape[1] != 2 or e.ndim != 2 or e.shape[1] != 4 or f.ndim != 2 or f.shape[1] != 8:
+        raise ValueError("the 2D path takes quadrilateral meshes (node_coords [n][2], elem_to_node_ids [ne][4], "
+                         "interior_faces [nf][8])")
+    keep += [c, e, f]
+    return _MeshDesc(c.shape[0], _dptr(c), e.shape[0], _uptr(e), f.shape[0], _uptr(f), 0)
+
+
+def write_solution_h5_2d(path, mesh: Mesh, order: int, Uc: np.ndarray, time: float = 0.0):
+    """Uc[ne][nb][4] in the writer's data.h5 schema (dg2d_solution_write_h5)."""
+    lib = library()
+    keep = []
+    md = _mesh2d_desc(mesh, keep)
+    U = np.ascontiguousarray(Uc, np.float64)
+    if U.size != mesh.nelem * (order + 1) ** 2 * 4:
+        raise ValueError("Uc does not hold a 2D state of this mesh and order")
+    rc = lib.dg2d_solution_write_h5(_path(path), ctypes.byref(md), int(order), _dptr(U), float(time))
+    if rc:
+        raise DGError(rc, lib.dg_last_error(None).decode())
+
+
+class Case2D:
+    """One 2D case (Solver<2> with LagrangeQuad) on the device: states
+    Uc[ne][nb][4], nb = (p+1)^2, FP64."""
+
+    def __init__(self, mesh: Mesh, order: int, flux: str = "LaxFriedrichs", gamma: float = 1.4,
+                 gas_constant: float = 287.05, device: int = 0):
+        self._lib = library()
+        keep = []
+        md = _mesh2d_desc(mesh, keep)
+        cd = _CaseDesc(order, FLUX[flux], gamma, gas_constant, PRECISION["fp64"], device)
+        h = ctypes.c_void_p()
+        rc = self._lib.dg2d_create(ctypes.byref(cd), ctypes.byref(md), ctypes.byref(h))
+        if rc:
+            raise DGError(rc, self._lib.dg_last_error(None).decode())
+        self._h = h
+        self.order = order
+        self.ne = mesh.nelem
+        self.nb = self._lib.dg2d_num_basis(self._h)
+
+    def _check(self, rc):
+        if rc:
+            raise DGError(rc, self._lib.dg2d_last_error(self._h).decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.dg2d_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_state(self, Uc: np.ndarray):
+        U = np.ascontiguousarray(Uc, np.float64)
+        if U.size != self.ne * self.nb * 4:
+            raise ValueError("state size")
+        self._check(self._lib.dg2d_set_state(self._h, _dptr(U)))
+
+    def get_state(self) -> np.ndarray:
+        U = np.zeros((self.ne, self.nb, 4))
+        self._check(self._lib.dg2d_get_state(self._h, _dptr(U)))
+        return U
+
+    def residual(self) -> np.ndarray:
+        R = np.zeros((self.ne, self.nb, 4))
+        self._check(self._lib.dg2d_residual(self._h, _dptr(R)))
+        return R
+
+    def rk4(self, dt: float, nsteps: int):
+        self._check(self._lib.dg2d_rk4_steps(self._h, dt, int(nsteps)))
+
+    def rk4_timed(self, dt: float, nsteps: int) -> float:
+        ms = ctypes.c_double()
+        self._check(self._lib.dg2d_rk4_steps_timed(self._h, dt, int(nsteps), ctypes.byref(ms)))
+        return ms.value
+
+    def fe(self, dt: float, nsteps: int):
+        self._check(self._lib.dg2d_fe_steps(self._h, dt, int(nsteps)))
+
+    def project_ic(self, name: str, data=(), t: float = 0.0) -> np.ndarray:
+        d = np.ascontiguousarray(np.asarray(data, np.float64).reshape(-1))
+        U = np.zeros((self.ne, self.nb, 4))
+        self._check(self._lib.dg2d_project_ic(self._h, IC2D[name], _dptr(d) if d.size else None, d.size, t,
+                                              _dptr(U)))
+        return U
+
+    def l2_error(self, name: str, data=(), t: float = 0.0) -> np.ndarray:
+        d = np.ascontiguousarray(np.asarray(data, np.float64).reshape(-1))
+        err = np.zeros(4)
+        self._check(self._lib.dg2d_l2_error(self._h, IC2D[name], _dptr(d) if d.size else None, d.size, t,
+                                            _dptr(err)))
+        return err
+
+    def status(self) -> int:
+        f = ctypes.c_uint()
+        self._lib.dg2d_status(self._h, ctypes.byref(f))
+        return f.value

@@ -198,15 +198,15 @@ int dg_mesh_write_h5_impl(const char* path, const dg_mesh_desc* md)
     return DG_OK;
 }
 
-int dg_solution_write_h5_impl(const char* path, const dg_mesh_desc* md, int order, const double* Uc, double time)
+// Writer::write for one rank: dim-D mesh of npe-node elements, ns variables
+int solution_write(const char* fn, const char* path, int dim, int npe, int ns, int nnode, const double* coords,
+                   int nelem, const unsigned* e2n_in, int nb, const double* Uc, double time)
 {
-    if (!path || !md || !md->node_coords || !md->elem_to_node_ids || !Uc || md->nnode < 1 || md->nelem < 1 ||
-        order < 0 || order > 5)
-        return ferr(DG_ERR_ARG, "dg_solution_write_h5: bad argument");
-    const uint64_t ne = md->nelem, nn = md->nnode, nb = (order + 1) * (order + 1) * (order + 1), ns = 5;
+    const uint64_t ne = nelem, nn = nnode;
     h5::Writer w;
-    const uint32_t u_ranks = 1, u_dim = 3, u_ne = static_cast<uint32_t>(ne), u_nn = static_cast<uint32_t>(nn), u_npe = 8,
-                   u_nb = static_cast<uint32_t>(nb), u_ns = 5;
+    const uint32_t u_ranks = 1, u_dim = static_cast<uint32_t>(dim), u_ne = static_cast<uint32_t>(ne),
+                   u_nn = static_cast<uint32_t>(nn), u_npe = static_cast<uint32_t>(npe), u_nb = static_cast<uint32_t>(nb),
+                   u_ns = static_cast<uint32_t>(ns);
     const int32_t row_major = 1;  // "Stored Layout": LayoutRight, written as an int (HDF5Wrapper.h:212-215)
     w.attribute("", "Number of Ranks", h5::Type::u32(), &u_ranks);
     w.attribute("", "Number of Dimensions", h5::Type::u32(), &u_dim);
@@ -218,18 +218,38 @@ int dg_solution_write_h5_impl(const char* path, const dg_mesh_desc* md, int orde
     w.attribute("", "Solver Final Time", h5::Type::f64(), &time);
     w.attribute("", "Stored Layout", h5::Type::i32(), &row_major);
     w.dataset("Number of Elements per Partition", {1}, h5::Type::u32(), &u_ne);
-    std::vector<uint32_t> l2g_node(nn), l2g_elem(ne), e2n(ne * 8);
+    std::vector<uint32_t> l2g_node(nn), l2g_elem(ne), e2n(ne * npe);
     for (uint64_t i = 0; i < nn; ++i) l2g_node[i] = static_cast<uint32_t>(i);
     for (uint64_t i = 0; i < ne; ++i) l2g_elem[i] = static_cast<uint32_t>(i);
-    for (uint64_t i = 0; i < ne * 8; ++i) e2n[i] = md->elem_to_node_ids[i];
-    write_parallel(w, "Node Coordinates", {nn, 3}, h5::Type::f64(), md->node_coords);
+    for (uint64_t i = 0; i < ne * npe; ++i) e2n[i] = e2n_in[i];
+    write_parallel(w, "Node Coordinates", {nn, static_cast<uint64_t>(dim)}, h5::Type::f64(), coords);
     write_parallel(w, "Local to Global Node ID", {nn}, h5::Type::u32(), l2g_node.data());
-    write_parallel(w, "Element Global Node IDs", {ne, 8}, h5::Type::u32(), e2n.data());
+    write_parallel(w, "Element Global Node IDs", {ne, static_cast<uint64_t>(npe)}, h5::Type::u32(), e2n.data());
     write_parallel(w, "Local to Global Element IDs", {ne}, h5::Type::u32(), l2g_elem.data());
-    write_parallel(w, "Solution Coefficients", {ne, nb, ns}, h5::Type::f64(), Uc);
+    write_parallel(w, "Solution Coefficients", {ne, static_cast<uint64_t>(nb), static_cast<uint64_t>(ns)}, h5::Type::f64(), Uc);
     std::string err;
-    if (!w.write(path, err)) return ferr(DG_ERR_ARG, "dg_solution_write_h5: " + err);
+    if (!w.write(path, err)) return ferr(DG_ERR_ARG, std::string(fn) + ": " + err);
     return DG_OK;
+}
+
+int dg_solution_write_h5_impl(const char* path, const dg_mesh_desc* md, int order, const double* Uc, double time)
+{
+    if (!path || !md || !md->node_coords || !md->elem_to_node_ids || !Uc || md->nnode < 1 || md->nelem < 1 ||
+        order < 0 || order > 5)
+        return ferr(DG_ERR_ARG, "dg_solution_write_h5: bad argument");
+    const int nb = (order + 1) * (order + 1) * (order + 1);
+    return solution_write("dg_solution_write_h5", path, 3, 8, 5, md->nnode, md->node_coords, md->nelem,
+                          md->elem_to_node_ids, nb, Uc, time);
+}
+
+int dg2d_solution_write_h5_impl(const char* path, const dg_mesh2d_desc* md, int order, const double* Uc, double time)
+{
+    if (!path || !md || !md->node_coords || !md->elem_to_node_ids || !Uc || md->nnode < 1 || md->nelem < 1 ||
+        order < 0 || order > 5)
+        return ferr(DG_ERR_ARG, "dg2d_solution_write_h5: bad argument");
+    const int nb = (order + 1) * (order + 1);
+    return solution_write("dg2d_solution_write_h5", path, 2, 4, 4, md->nnode, md->node_coords, md->nelem,
+                          md->elem_to_node_ids, nb, Uc, time);
 }
 
 int dg_solution_read_h5_impl(const char* path, int* nelem, int* nb, int* ns, double* time, double* Uc)
@@ -323,6 +343,11 @@ int dg_solution_write_h5(const char* path, const dg_mesh_desc* md, int order, co
 int dg_solution_read_h5(const char* path, int* nelem, int* nb, int* ns, double* time, double* Uc)
 {
     return guarded("dg_solution_read_h5", [&] { return dg_solution_read_h5_impl(path, nelem, nb, ns, time, Uc); });
+}
+
+int dg2d_solution_write_h5(const char* path, const dg_mesh2d_desc* md, int order, const double* Uc, double time)
+{
+    return guarded("dg2d_solution_write_h5", [&] { return dg2d_solution_write_h5_impl(path, md, order, Uc, time); });
 }
 
 }  // extern "C"

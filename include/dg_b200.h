@@ -62,6 +62,7 @@ extern "C" {
 #define DG_IC_SPHERE 2         /* "Sphere" */
 #define DG_IC_VORTEX_XY 3      /* "IsentropicVortexXY": data = rho,u,v,p,beta,xc,yc,Lx,Ly */
 #define DG_IC_TAYLOR_GREEN 4   /* "TaylorGreen": data = Mach */
+#define DG_IC_VORTEX_2D 5      /* 2D "IsentropicVortex": data = rho,u,v,p,strength (dg2d_* only) */
 
 typedef struct dg_ctx dg_ctx;
 
@@ -460,6 +461,77 @@ int dg_face_orientation_order(int orient, int npts, int* order);
  * inverse 1D mass matrix Minv[n][n] (n = p+1); the 3D operators of
  * src/solver/helpers.cpp:5-100 are their tensor products. */
 int dg_basis_tables(int p, double* B, double* D, double* Minv);
+
+/* ======================================================================
+ * 2D quadrilaterals (Solver<2> with LagrangeQuad, src/solver/base.cpp
+ * instantiated for dim 2): a separate context type, FP64.
+ *
+ * The same residual and RK stage as the 3D path on periodic meshes of
+ * parallelograms, with the reference's 2D rules: (p+2)^2 Gauss points per
+ * element (quadrature/quadrilateral.cpp:36-41), p+1 Gauss points per edge
+ * (segment quadrature of order 2p+1, segment.cpp:424-426, helpers.cpp:225),
+ * edge points ordered by the two orientations of
+ * get_face_pts_order_wrt_orient0_quadrilateral (shape.cpp:43-66), normals
+ * (dy/ds, -dx/ds) of the left element's edge (shape.cpp:154-210).
+ * Host state layout Uc[ne][nb][4] (rho, rho u, rho v, rho E), nb = (p+1)^2,
+ * basis index j(p+1)+i.
+ * ====================================================================== */
+
+/* A quadrilateral mesh: node_coords [nnode][2], elem_to_node_ids [nelem][4]
+ * (gbasis node order, x fastest), interior_faces [nface][8] rows (rankL,
+ * elemL, faceL, orientL, rankR, elemR, faceR, orientR) with local faces
+ * 0..3 (get_local_nodes_on_face_quadrilateral, shape.cpp:125-152) and
+ * orientations 0 / 1; every face interior, every element a parallelogram. */
+typedef struct dg_mesh2d_desc {
+    int nnode;
+    const double* node_coords;
+    int nelem;
+    const unsigned* elem_to_node_ids;
+    int nface;
+    const unsigned* interior_faces;
+    int rank;
+} dg_mesh2d_desc;
+
+typedef struct dg_ctx2d dg_ctx2d;
+
+/* Solver<2>::Solver + precompute_matrix_helpers: tables, connectivity,
+ * geometry, device buffers.  cd->precision must be DG_PREC_FP64;
+ * DG_ERR_UNSUPPORTED for non-parallelogram elements.  Errors of a failed
+ * create: dg_last_error(NULL). */
+int dg2d_create(const dg_case_desc* cd, const dg_mesh2d_desc* md, dg_ctx2d** out);
+void dg2d_destroy(dg_ctx2d* ctx);
+const char* dg2d_last_error(const dg_ctx2d* ctx);
+int dg2d_num_basis(const dg_ctx2d* ctx);
+int dg2d_set_state(dg_ctx2d* ctx, const double* Uc);
+int dg2d_get_state(dg_ctx2d* ctx, double* Uc);
+/* R(U) of the current state (Solver<2>::get_residual, base.cpp:401-561) */
+int dg2d_residual(dg_ctx2d* ctx, double* res);
+/* RK4 / FE steps on the device state (stepper.cpp:23-142) */
+int dg2d_rk4_steps(dg_ctx2d* ctx, double dt, int nsteps);
+int dg2d_rk4_steps_timed(dg_ctx2d* ctx, double dt, int nsteps, double* device_ms);
+int dg2d_fe_steps(dg_ctx2d* ctx, double dt, int nsteps);
+/* L2 projection of an initial condition (init_state_from_fcn,
+ * base.cpp:113-223) into Uc (may be NULL) and the device state; ic_type
+ * DG_IC_UNIFORM (data = 4 conserved values), DG_IC_VORTEX_2D, or
+ * DG_IC_VORTEX_XY (evaluated at (x, y, 0)) */
+int dg2d_project_ic(dg_ctx2d* ctx, int ic_type, const double* data, int ndata, double t, double* Uc);
+/* volume-normalised L2 error of the device state against the same
+ * families at time t (get_error, src/post/main.cpp:30-201); err[4] */
+int dg2d_l2_error(dg_ctx2d* ctx, int ic_type, const double* data, int ndata, double t, double* err);
+/* the device status word (the 3D bits); DG_ERR_NONPHYSICAL when set */
+int dg2d_status(dg_ctx2d* ctx, unsigned* flags);
+
+/* Periodic box [x0,x0+L0]x[x1,x1+L1] of n0*n1 quadrilaterals, element id
+ * i + n0 j; faces (right, top) of each element in element order; with
+ * rotate_seed != 0 every element's local numbering is rotated by a seeded
+ * multiple of 90 degrees.  Sizes first (NULL arrays). */
+int dg_mesh2d_periodic_box(const int n[2], const double x0[2], const double len[2], unsigned rotate_seed,
+                           int* nnode, double* node_coords, int* nelem, unsigned* elem_to_node_ids, int* nface,
+                           unsigned* interior_faces);
+
+/* Writer::write for a 2D state (Uc[ne][nb][4]; Number of Dimensions 2,
+ * Number of Nodes Per Element 4, Number of State Variables 4) */
+int dg2d_solution_write_h5(const char* path, const dg_mesh2d_desc* md, int order, const double* Uc, double time);
 
 #ifdef __cplusplus
 }

@@ -608,6 +608,8 @@ static void inv_lu(int n, double* a, double* ia)
     }
 }
 
+void orc_inv_lu(int n, double* a, double* ia) { inv_lu(n, a, ia); }
+
 /* ------------------------------------------------------------------------ */
 /* the case                                                                  */
 /* ------------------------------------------------------------------------ */

@@ -69,6 +69,9 @@ void orc_lagrange_hex_grad(int p, int nq, const double* xq, double* grad);
 void orc_face_pts_order(int orient, int npts, int* order);
 void orc_points_on_face(int face, int orient, int np, const double* fpts, double* epts);
 void orc_local_nodes_on_face(int face, int gorder, int* lfnodes);
+/* Math::invA for n > 3 (linear_algebra.cpp:123-131): unpivoted LU inverse;
+ * a[n][n] is overwritten */
+void orc_inv_lu(int n, double* a, double* ia);
 
 /* ---- pointwise physics ---- */
 double orc_pressure(double gamma, const double* U);
