@@ -15,10 +15,13 @@
 //              "...cube_<N>.h5", the periodic N^3 box on [0,1]^3 that file
 //              holds is generated instead; or
 //              periodic_box = [nx, ny, nz], origin = [..], length = [..]
-//   [Numerics] order, basis = "LagrangeHex"
+//              2D ([Physics] dim = 2): a quadrilateral mesh file, a missing
+//              "...box_<N>x<M>.h5" (the periodic N x M box on [-5, 5]^2 of the
+//              reference's 2D vortex study), or periodic_box = [nx, ny]
+//   [Numerics] order, basis = "LagrangeHex" (2D: "LagrangeQuad")
 //   [Stepper]  type = "FE" | "RK4" (default "FE"), timestep, end;
 //              extensions: cfl (derive timestep from the IC), steps (count)
-//   [Physics]  name = "Euler", dim = 3, gamma = 1.4, GasConstant = 287.05,
+//   [Physics]  name = "Euler", dim = 3 or 2, gamma = 1.4, GasConstant = 287.05,
 //              convective_flux_fcn = "LaxFriedrichs" | "HLLC"
 //   [InitialCondition] name, data
 //   [Output]   as the reference (src/exec/main.cpp:105-112), the final state
@@ -63,6 +66,7 @@ struct StepperBase {
 
 struct Solver {
     dg_ctx* ctx = nullptr;
+    dg_ctx2d* ctx2 = nullptr;  // a 2D case (Solver<2>) instead
     double time = 0.0;
     std::vector<double> restart_state;  // [ne][nb][5] from a checkpoint, else empty
     long num_iterations = 0;
@@ -87,7 +91,7 @@ struct Solver {
 struct RK4Gpu : StepperBase {
     int take_time_step(Solver& s) override
     {
-        const int rc = dg_rk4_steps(s.ctx, dt, 1);
+        const int rc = s.ctx2 ? dg2d_rk4_steps(s.ctx2, dt, 1) : dg_rk4_steps(s.ctx, dt, 1);
         s.time += dt;  // stage times t, t+dt/2, t+dt/2, t+dt (stepper.cpp:98,125)
         return rc;
     }
@@ -96,7 +100,7 @@ struct RK4Gpu : StepperBase {
 struct FEGpu : StepperBase {
     int take_time_step(Solver& s) override
     {
-        const int rc = dg_fe_steps(s.ctx, dt, 1);
+        const int rc = s.ctx2 ? dg2d_fe_steps(s.ctx2, dt, 1) : dg_fe_steps(s.ctx, dt, 1);
         s.time += dt;
         return rc;
     }
@@ -123,8 +127,11 @@ bool ends_with(const std::string& s, const std::string& tail)
     return s.size() >= tail.size() && s.compare(s.size() - tail.size(), tail.size(), tail) == 0;
 }
 
+int run2d(const dgh::Toml& deck, bool check_only);
+
 int run(const dgh::Toml& deck, bool check_only)
 {
+    if (static_cast<int>(deck.num_or("Physics", "dim", 3)) == 2) return run2d(deck, check_only);
     // ---- mesh ----
     int n[3] = {0, 0, 0};
     double x0[3] = {0, 0, 0}, len[3] = {1, 1, 1};
@@ -152,7 +159,7 @@ int run(const dgh::Toml& deck, bool check_only)
     const std::string basis = deck.str_or("Numerics", "basis", "LagrangeHex");
     if (basis != "LagrangeHex") throw std::runtime_error("[Numerics] basis " + basis + " is not on the device path");
     if (deck.str_or("Physics", "name", "Euler") != "Euler") throw std::runtime_error("[Physics] name must be Euler");
-    if (static_cast<int>(deck.num_or("Physics", "dim", 3)) != 3) throw std::runtime_error("[Physics] dim must be 3");
+    if (static_cast<int>(deck.num_or("Physics", "dim", 3)) != 3) throw std::runtime_error("[Physics] dim must be 2 or 3");
     const double gamma = deck.num_or("Physics", "gamma", 1.4);
     const double R = deck.num_or("Physics", "GasConstant", 287.05);
     const std::string flux_name = deck.str_or("Physics", "convective_flux_fcn", "LaxFriedrichs");
@@ -317,6 +324,154 @@ int run(const dgh::Toml& deck, bool check_only)
     }
     if (deck.has("Output", "json") && deck.boolean("Output", "json")) std::printf("%s}\n", json.c_str());
     dg_destroy(solver.ctx);
+    return 0;
+}
+
+// the 2D case (run_solver<2>, src/exec/main.cpp:52-119): quadrilateral
+// meshes, LagrangeQuad, the dg2d_* entry points
+int run2d(const dgh::Toml& deck, bool check_only)
+{
+    int n[2] = {0, 0};
+    double x0[2] = {-5.0, -5.0}, len[2] = {10.0, 10.0};
+    std::string mesh_file;
+    if (deck.has("Mesh", "periodic_box")) {
+        const auto b = deck.nums("Mesh", "periodic_box");
+        if (b.size() != 2) throw std::runtime_error("[Mesh] periodic_box needs 2 entries in 2D");
+        for (int i = 0; i < 2; ++i) n[i] = static_cast<int>(b[i]);
+        if (deck.has("Mesh", "origin")) { auto o = deck.nums("Mesh", "origin"); for (int i = 0; i < 2; ++i) x0[i] = o.at(i); }
+        if (deck.has("Mesh", "length")) { auto l = deck.nums("Mesh", "length"); for (int i = 0; i < 2; ++i) len[i] = l.at(i); }
+    } else {
+        const std::string file = deck.str("Mesh", "file");
+        std::smatch m;
+        if (file_exists(file)) {
+            mesh_file = file;
+        } else if (std::regex_search(file, m, std::regex("box_([0-9]+)x([0-9]+)\\.h5$"))) {
+            // the reference's 2D vortex boxes: periodic on [-5, 5]^2
+            n[0] = std::stoi(m[1]);
+            n[1] = std::stoi(m[2]);
+        } else {
+            throw std::runtime_error("[Mesh] file " + file + " not found");
+        }
+    }
+    const int order = static_cast<int>(deck.num("Numerics", "order"));
+    const std::string basis = deck.str_or("Numerics", "basis", "LagrangeQuad");
+    if (basis != "LagrangeQuad") throw std::runtime_error("[Numerics] basis " + basis + " is not on the device path (2D: LagrangeQuad)");
+    if (deck.str_or("Physics", "name", "Euler") != "Euler") throw std::runtime_error("[Physics] name must be Euler");
+    const double gamma = deck.num_or("Physics", "gamma", 1.4);
+    const double R = deck.num_or("Physics", "GasConstant", 287.05);
+    const std::string flux_name = deck.str_or("Physics", "convective_flux_fcn", "LaxFriedrichs");
+    int flux = DG_FLUX_LAX_FRIEDRICHS;
+    if (flux_name == "HLLC") flux = DG_FLUX_HLLC;
+    else if (flux_name != "LaxFriedrichs") throw std::runtime_error("unknown convective_flux_fcn " + flux_name);
+    const std::string ic_name = deck.str("InitialCondition", "name");
+    int ic = DG_IC_VORTEX_2D;
+    if (ic_name == "Uniform") ic = DG_IC_UNIFORM;
+    else if (ic_name == "IsentropicVortexXY") ic = DG_IC_VORTEX_XY;
+    else if (ic_name != "IsentropicVortex") throw std::runtime_error("[InitialCondition] name " + ic_name + " has no 2D form");
+    std::vector<double> ic_data = deck.has("InitialCondition", "data") ? deck.nums("InitialCondition", "data")
+                                                                          : std::vector<double>();
+    const std::string stype = deck.str_or("Stepper", "type", "FE");
+    if (stype != "FE" && stype != "RK4") throw std::runtime_error("[Stepper] type must be FE or RK4");
+    if (deck.has("Stepper", "cfl")) throw std::runtime_error("[Stepper] cfl: the 2D path takes timestep");
+
+    int nn = 0, ne = 0, nf = 0;
+    std::vector<double> coords;
+    std::vector<unsigned> e2n, faces;
+    if (!mesh_file.empty()) {
+        int dim = 0, qorder = 0, npe = 0;
+        if (dg_mesh_read_h5(mesh_file.c_str(), &dim, &qorder, &npe, &nn, nullptr, &ne, nullptr, &nf, nullptr))
+            throw std::runtime_error(dg_last_error(nullptr));
+        if (dim != 2 || qorder != 1 || npe != 4)
+            throw std::runtime_error("[Mesh] file " + mesh_file + ": dimension " + std::to_string(dim) + ", QOrder " +
+                                     std::to_string(qorder) + ", " + std::to_string(npe) +
+                                     " nodes per element; the 2D path takes linear quadrilaterals (2, 1, 4)");
+        coords.resize(static_cast<size_t>(nn) * 2);
+        e2n.resize(static_cast<size_t>(ne) * 4);
+        faces.resize(static_cast<size_t>(nf) * 8);
+        if (dg_mesh_read_h5(mesh_file.c_str(), &dim, &qorder, &npe, &nn, coords.data(), &ne, e2n.data(), &nf,
+                            faces.data()))
+            throw std::runtime_error(dg_last_error(nullptr));
+        std::printf("case: %s (%d quadrilaterals, %d interior faces), p=%d, %s flux, %s, IC %s\n", mesh_file.c_str(),
+                    ne, nf, order, flux_name.c_str(), stype.c_str(), ic_name.c_str());
+    } else {
+        std::printf("case: %dx%d periodic quad, p=%d, %s flux, %s, IC %s\n", n[0], n[1], order, flux_name.c_str(),
+                    stype.c_str(), ic_name.c_str());
+    }
+    if (check_only) return 0;
+    if (mesh_file.empty()) {
+        if (dg_mesh2d_periodic_box(n, x0, len, 0, &nn, nullptr, &ne, nullptr, &nf, nullptr)) throw std::runtime_error("bad box");
+        coords.resize(static_cast<size_t>(nn) * 2);
+        e2n.resize(static_cast<size_t>(ne) * 4);
+        faces.resize(static_cast<size_t>(nf) * 8);
+        dg_mesh2d_periodic_box(n, x0, len, 0, &nn, coords.data(), &ne, e2n.data(), &nf, faces.data());
+    }
+    dg_mesh2d_desc md{nn, coords.data(), ne, e2n.data(), nf, faces.data(), 0};
+    dg_case_desc cd{order, flux, gamma, R, DG_PREC_FP64, 0};
+    Solver solver;
+    if (dg2d_create(&cd, &md, &solver.ctx2)) throw std::runtime_error(std::string("dg2d_create: ") + dg_last_error(nullptr));
+    const int nb = dg2d_num_basis(solver.ctx2);
+    std::vector<double> Uc(static_cast<size_t>(ne) * nb * 4);
+    if (dg2d_project_ic(solver.ctx2, ic, ic_data.data(), static_cast<int>(ic_data.size()), 0.0, Uc.data()))
+        throw std::runtime_error(std::string("dg2d_project_ic: ") + dg2d_last_error(solver.ctx2));
+    const bool restart = deck.has("Output", "restart_file");
+    if (restart) {
+        const std::string path = deck.str("Output", "restart_file");
+        int fne = 0, fnb = 0, fns = 0;
+        double t = 0.0;
+        if (!ends_with(path, ".h5")) throw std::runtime_error("restart_file: the 2D path resumes from *.h5 solution files");
+        if (dg_solution_read_h5(path.c_str(), &fne, &fnb, &fns, &t, nullptr)) throw std::runtime_error(dg_last_error(nullptr));
+        if (fne != ne || fnb != nb || fns != 4)
+            throw std::runtime_error("restart_file " + path + " does not hold a state of this mesh and order");
+        if (dg_solution_read_h5(path.c_str(), &fne, &fnb, &fns, &t, Uc.data())) throw std::runtime_error(dg_last_error(nullptr));
+        if (dg2d_set_state(solver.ctx2, Uc.data())) throw std::runtime_error(dg2d_last_error(solver.ctx2));
+        solver.time = t;
+    }
+    const double dt = deck.num_or("Stepper", "timestep", 0.0);
+    if (!(dt > 0.0)) throw std::runtime_error("[Stepper] needs timestep > 0");
+    if (deck.has("Stepper", "steps")) {
+        solver.num_iterations = static_cast<long>(deck.num("Stepper", "steps"));
+    } else {
+        const double end = deck.num("Stepper", "end");
+        solver.num_iterations = static_cast<int>(end / dt) - (restart ? static_cast<long>(solver.time / dt + 0.5) : 0);
+        if (solver.num_iterations < 0) solver.num_iterations = 0;
+    }
+    if (stype == "RK4") solver.stepper = std::make_unique<RK4Gpu>();
+    else solver.stepper = std::make_unique<FEGpu>();
+    solver.stepper->set_time_step(dt);
+    solver.stepper->set_final_time(dt * solver.num_iterations);
+    solver.print_every = static_cast<int>(deck.num_or("Output", "print_every", 0));
+    std::printf("timestep = %.17g, number of iterations = %ld, DOF = %lld\n", dt, solver.num_iterations,
+                static_cast<long long>(ne) * nb * 4);
+    const auto t0 = std::chrono::steady_clock::now();
+    if (solver.solve()) throw std::runtime_error(std::string("solve: ") + dg2d_last_error(solver.ctx2));
+    const double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    double err[4] = {0, 0, 0, 0};
+    if (ic != DG_IC_UNIFORM || ic_data.size() >= 4) {
+        if (dg2d_l2_error(solver.ctx2, ic, ic_data.data(), static_cast<int>(ic_data.size()), solver.time, err))
+            throw std::runtime_error(std::string("l2 error: ") + dg2d_last_error(solver.ctx2));
+        for (int s = 0; s < 4; ++s) std::printf("norm_total_error(%d)=%.*e\n", s, DECIMAL_DIG, err[s]);
+    }
+    const bool outputs = !(deck.has("Output", "disable_all_outputs") && deck.boolean("Output", "disable_all_outputs"));
+    if (outputs) {
+        if (dg2d_get_state(solver.ctx2, Uc.data())) throw std::runtime_error(dg2d_last_error(solver.ctx2));
+        const std::string out = deck.has("Output", "solution_file") ? deck.str("Output", "solution_file") : "data.h5";
+        if (dg2d_solution_write_h5(out.c_str(), &md, order, Uc.data(), solver.time))
+            throw std::runtime_error(dg_last_error(nullptr));
+        std::printf("solution written to %s\n", out.c_str());
+    }
+    if (deck.has("Output", "json") && deck.boolean("Output", "json")) {
+        char buf[512];
+        const int stages = stype == "RK4" ? 4 : 1;
+        const double dof = static_cast<double>(ne) * nb * 4;
+        std::snprintf(buf, sizeof(buf),
+                      "{\"dim\": 2, \"dof\": %lld, \"order\": %d, \"steps\": %ld, \"stages_per_step\": %d, \"wall_s\": %.6f, "
+                      "\"dof_stage_per_s\": %.6g, \"time\": %.17g, \"l2_error\": [%.17g, %.17g, %.17g, %.17g]}",
+                      static_cast<long long>(dof), order, solver.num_iterations, stages, wall,
+                      wall > 0 ? dof * stages * solver.num_iterations / wall : 0.0, solver.time, err[0], err[1], err[2],
+                      err[3]);
+        std::printf("%s\n", buf);
+    }
+    dg2d_destroy(solver.ctx2);
     return 0;
 }
 

@@ -6,6 +6,7 @@
   python dg-mpi_b200/studies.py ensemble     # 256 seeded vortex cases, p=1..5, 8^3..32^3, 100 steps
   python dg-mpi_b200/studies.py <name> --scale 0.25  # smaller mesh (fewer cases), same orders
   python dg-mpi_b200/studies.py general       # bent (non-affine) periodic boxes: 48^3 p=3, 24^3 p=5
+  python dg-mpi_b200/studies.py convergence2d # the reference's 2D convergence table, N = 2..256, p = 1..3
   python dg-mpi_b200/studies.py stage --nel 40 --order 3 --precision fp64 --variant 0
                                              # one launch variant, 2 RK4 steps, no tuner (ncu captures)
 
@@ -221,9 +222,54 @@ def stage(nel: int, order: int, precision_: str, variant: int, steps: int):
     return out
 
 
+# the reference's published 2D convergence table: density L2 error of the 2D
+# isentropic vortex, HLLC, LagrangeQuad, RK4 dt = 1e-3 to t = 1, N x N boxes
+# (examples/isentropic_vortex/convergence.py:51-86; entries marked "HOLD FOR
+# NOW" there repeat the previous value and are left out)
+TABLE_2D = {
+    1: {2: 4.057487237640151206408e-02, 4: 3.659091741930729779764e-02, 8: 1.399040502291195101070e-02,
+        16: 3.736915003326653998000e-03, 32: 9.128245919612695130629e-04, 64: 2.230394344260663451376e-04,
+        128: 5.552798642178519519276e-05, 256: 1.390242977018099767455e-05},
+    2: {2: 3.932754850914681188367e-02, 4: 1.414430149472130186783e-02, 8: 3.248199949411992391163e-03,
+        16: 3.915751398100587301818e-04, 32: 4.874570751994351309371e-05, 64: 5.808150680654376531750e-06,
+        128: 7.102447210422075577049e-07},
+    3: {2: 2.911726700453628677301e-02, 4: 6.747203591607888774340e-03, 8: 5.564165617240108456867e-04,
+        16: 3.771907882313834693960e-05, 32: 2.369398862192326906355e-06, 64: 1.424882779046236941575e-07,
+        128: 9.074300168426849006228e-09},
+}
+
+
+def convergence2d(scale: float):
+    """The reference's 2D convergence study on the 2D path (dg2d_*): periodic
+    N x N boxes on [-5, 5]^2, the 2D vortex, 1000 RK4 steps of 1e-3; the
+    density error against the published table and the device-timed rate."""
+    rows = []
+    nmax = max(2, int(256 * scale))
+    for p in (1, 2, 3):
+        prev = None
+        for N in (2, 4, 8, 16, 32, 64, 128, 256):
+            if N > nmax:
+                break
+            mesh = dg_b200.periodic_box_2d((N, N), (-5.0, -5.0), (10.0, 10.0))
+            case = dg_b200.Case2D(mesh, p, flux="HLLC", gas_constant=1.0)
+            case.project_ic("IsentropicVortex", VORTEX[:5])
+            ms = case.rk4_timed(1e-3, 1000)
+            err = float(case.l2_error("IsentropicVortex", VORTEX[:5], 1.0)[0])
+            ref = TABLE_2D[p].get(N)
+            dof = N * N * (p + 1) ** 2 * 4
+            rows.append({"p": p, "N": N, "rho_l2_error": err, "reference": ref,
+                         "rel_diff": None if ref is None else err / ref - 1.0,
+                         "order": None if prev is None else math.log(prev / err) / math.log(2.0),
+                         "dof_stage_per_s": dof * 4 * 1000 / (ms / 1e3), "ms_per_step": ms / 1000,
+                         "status": case.status()})
+            prev = err
+            case.close()
+    return {"rows": rows, "max_abs_rel_diff": max(abs(r["rel_diff"]) for r in rows if r["rel_diff"] is not None)}
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("study", choices=["precision", "taylor_green", "ensemble", "general", "stage"])
+    ap.add_argument("study", choices=["precision", "taylor_green", "ensemble", "general", "stage", "convergence2d"])
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--nel", type=int, default=40, help="stage: elements per direction")
     ap.add_argument("--order", type=int, default=3, help="stage: polynomial order")
@@ -234,7 +280,8 @@ def main():
     if args.study == "stage":
         res = stage(args.nel, args.order, args.precision, args.variant, args.steps)
     else:
-        run = {"precision": precision, "taylor_green": taylor_green, "ensemble": ensemble, "general": general}[args.study]
+        run = {"precision": precision, "taylor_green": taylor_green, "ensemble": ensemble, "general": general,
+               "convergence2d": convergence2d}[args.study]
         res = run(args.scale)
     res["study"] = args.study
     print(json.dumps(res), flush=True)

@@ -148,3 +148,28 @@ def test_driver_resumes_from_its_data_h5(tmp_path):
     u1, t1 = dg_b200.read_solution_h5(str(tmp_path / "full.h5"))
     u2, t2 = dg_b200.read_solution_h5(str(tmp_path / "rest.h5"))
     assert t1 == t2 and np.array_equal(u1, u2)
+
+
+def test_2d_deck_with_a_quad_mesh_file_parses(tmp_path):
+    quad = os.path.join(os.path.dirname(__file__), "golden", "meshes", "quad_1x1.h5")
+    text = open(os.path.join(EXAMPLES, "vortex2d_box8_p2.toml")).read()
+    deck = tmp_path / "deck.toml"
+    deck.write_text(re.sub(r"^file\s*=.*$", 'file = "%s"' % quad, text, flags=re.M))
+    r = run(["-input", str(deck), "-check"])
+    assert r.returncode == 0, r.stderr
+    assert "(1 quadrilaterals, 2 interior faces)" in r.stdout
+
+
+@pytest.mark.gpu
+def test_driver_2d_deck_reproduces_reference_convergence_entry(golden, tmp_path):
+    """The reference's 2D vortex deck on the 8x8 box (p = 2): its density
+    error against the convergence table to the 2D pin, and data.h5 in the
+    writer's schema with four state variables."""
+    from test_oracle2d import TABLE, PIN_RTOL
+    r = run(["-input", os.path.join(EXAMPLES, "vortex2d_box8_p2.toml")], timeout=300, cwd=str(tmp_path))
+    assert r.returncode == 0, r.stderr
+    err = {int(m.group(1)): float(m.group(2)) for m in re.finditer(r"norm_total_error\((\d)\)=(\S+)", r.stdout)}
+    assert "number of iterations = 1000" in r.stdout
+    assert abs(err[0] / TABLE[2][2] - 1.0) < PIN_RTOL, err[0]
+    U, t = dg_b200.read_solution_h5(str(tmp_path / "data.h5"))
+    assert U.shape == (64, 9, 4) and t == pytest.approx(1.0, abs=1e-12)
