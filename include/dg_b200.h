@@ -1,6 +1,7 @@
 /*
  * dg_b200.h -- C ABI of the B200-native residual + RK-stage path for
- * IhmeGroup/DG-MPI's 3D Euler solver on periodic hexahedral meshes.
+ * IhmeGroup/DG-MPI's 3D Euler solver on periodic hexahedral meshes (and its
+ * 2D form on quadrilaterals, the dg2d_* entry points at the end).
  *
  * One library, libdg_b200.so, exports everything below.  Plain C types only
  * (no CUDA or torch types), so a C++ stepper inside the reference, ctypes, or
