@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -825,6 +826,9 @@ void release(dg_ctx* c)
     cudaFree(c->d_gjd); cudaFree(c->d_gnrm); cudaFree(c->d_gimm); cudaFree(c->d_gnodes); cudaFree(c->d_gfsd);
     cudaFree(c->d_faces); cudaFree(c->d_fflux); cudaFree(c->d_tcop);
     cudaFree(c->d_halo_send); cudaFree(c->d_halo_recv);
+    for (cudaEvent_t e : c->chunk_ev) cudaEventDestroy(e);
+    c->chunk_ev.clear();
+    if (c->stream2) cudaStreamDestroy(c->stream2);
     if (c->stream) cudaStreamDestroy(c->stream);
 }
 
@@ -1076,11 +1080,29 @@ int dgi::create_ctx(const dg_case_desc* cd, const dg_mesh_desc* md, const int* e
                 if (r.nbr < c->ne && ((r.info >> 3) & 1) && (e < c->ninterior || r.nbr < c->ninterior)) listed(e, f);
             }
         c->nface_inner = static_cast<int>(faces.size());
-        for (int e = 0; e < c->ne; ++e)
-            for (int f = 0; f < 6; ++f) {
-                const dgk::FaceRec& r = rec(e, f);
-                if (r.nbr >= c->ne || (((r.info >> 3) & 1) && e >= c->ninterior && r.nbr >= c->ninterior)) listed(e, f);
+        if (c->ninterior == 0 && c->ne_alloc == c->ne) {
+            // no ghosts: every face by its left side, ordered by the lower of
+            // its two elements (stable in the left element and face)
+            std::vector<std::array<int, 3>> order;
+            for (int e = 0; e < c->ne; ++e)
+                for (int f = 0; f < 6; ++f) {
+                    const dgk::FaceRec& r = rec(e, f);
+                    if (r.nbr < c->ne && ((r.info >> 3) & 1)) order.push_back({std::min(e, r.nbr), e, f});
+                }
+            std::stable_sort(order.begin(), order.end(),
+                             [](const std::array<int, 3>& x, const std::array<int, 3>& y) { return x[0] < y[0]; });
+            c->face_key.clear();
+            for (const auto& o : order) {
+                listed(o[1], o[2]);
+                c->face_key.push_back(o[0]);
             }
+        } else {
+            for (int e = 0; e < c->ne; ++e)
+                for (int f = 0; f < 6; ++f) {
+                    const dgk::FaceRec& r = rec(e, f);
+                    if (r.nbr >= c->ne || (((r.info >> 3) & 1) && e >= c->ninterior && r.nbr >= c->ninterior)) listed(e, f);
+                }
+        }
         for (int e = 0; e < c->ne; ++e)
             for (int f = 0; f < 6; ++f) {
                 dgk::FaceRec& r = rec(e, f);
@@ -1382,6 +1404,47 @@ int dg_mass_inverse_residual(dg_ctx* c, double dt, double* dU)
 
 namespace {
 
+// one RK stage as c->chunks element chunks (contexts without ghosts, a
+// face-kernel variant): the face launches of the chunks on the second stream
+// (they read only the stage input), each chunk's stage launch on the main
+// stream after its face launch, so a chunk's face kernel runs beside the
+// previous chunk's stage kernel and its fluxes are read soon after they are
+// written.  `stage` (0..3) picks the stage's events.
+int launch_stage_chunked(dg_ctx* c, int stage, int mode, const double* Us, const double* U0, double* out, double dt)
+{
+    const dgk::StageVariant* vs = nullptr;
+    dgk::stage_variants(c->p, &vs);
+    const dgk::StageVariant& sv = vs[c->variant];
+    const int C = c->chunks;
+    if (!sv.face_launch || C <= 1 || c->face_key.size() != static_cast<size_t>(c->nface) ||
+        c->chunk_ev.size() < static_cast<size_t>(4 * (C + 1)))
+        return launch_stage(c, mode, Us, U0, out, dt);
+    cudaEvent_t* ev = c->chunk_ev.data() + stage * (C + 1);
+    StageArgs a;
+    stage_args(c, mode, Us, U0, out, dt, 0, c->ne, a);
+    DG_CUDA(c, cudaEventRecord(ev[0], c->stream));
+    DG_CUDA(c, cudaStreamWaitEvent(c->stream2, ev[0], 0));
+    std::vector<int> e_at(C + 1);
+    for (int k = 0; k <= C; ++k) e_at[k] = static_cast<int>(static_cast<long long>(c->ne) * k / C);
+    const int fb = sv.face_batch;
+    for (int k = 0; k < C; ++k) {
+        const int f0 = static_cast<int>(std::lower_bound(c->face_key.begin(), c->face_key.end(), e_at[k]) - c->face_key.begin());
+        const int f1 = static_cast<int>(std::lower_bound(c->face_key.begin(), c->face_key.end(), e_at[k + 1]) - c->face_key.begin());
+        a.face_begin = f0;
+        a.nface = f1;
+        if (f1 > f0) DG_CUDA(c, sv.face_launch(a, std::min(c->variant_face_grid[c->variant], (f1 - f0 + fb - 1) / fb), c->stream2));
+        DG_CUDA(c, cudaEventRecord(ev[k + 1], c->stream2));
+    }
+    for (int k = 0; k < C; ++k) {
+        DG_CUDA(c, cudaStreamWaitEvent(c->stream, ev[k + 1], 0));
+        a.e_begin = e_at[k];
+        a.ne = e_at[k + 1];
+        const int batches = (e_at[k + 1] - e_at[k] + sv.E - 1) / sv.E;
+        if (batches > 0) DG_CUDA(c, sv.launch(a, std::min(c->variant_grid[c->variant], batches), c->stream));
+    }
+    return DG_OK;
+}
+
 int prepare_rk4_graph(dg_ctx* c, double dt)
 {
     if (c->graph_exec && c->graph_dt == dt) return DG_OK;
@@ -1391,10 +1454,17 @@ int prepare_rk4_graph(dg_ctx* c, double dt)
     int rc = prepare_variant(c, c->variant);
     if (rc) return rc;
     DG_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    rc = launch_stage(c, dgk::kModeRK1, c->d_U0, c->d_U0, c->d_Ua, dt);
-    if (!rc) rc = launch_stage(c, dgk::kModeRK2, c->d_Ua, c->d_U0, c->d_Ub, dt);
-    if (!rc) rc = launch_stage(c, dgk::kModeRK3, c->d_Ub, c->d_U0, c->d_Ua, dt);
-    if (!rc) rc = launch_stage(c, dgk::kModeRK4, c->d_Ua, c->d_U0, c->d_U0, dt);
+    if (c->chunks > 1) {
+        rc = launch_stage_chunked(c, 0, dgk::kModeRK1, c->d_U0, c->d_U0, c->d_Ua, dt);
+        if (!rc) rc = launch_stage_chunked(c, 1, dgk::kModeRK2, c->d_Ua, c->d_U0, c->d_Ub, dt);
+        if (!rc) rc = launch_stage_chunked(c, 2, dgk::kModeRK3, c->d_Ub, c->d_U0, c->d_Ua, dt);
+        if (!rc) rc = launch_stage_chunked(c, 3, dgk::kModeRK4, c->d_Ua, c->d_U0, c->d_U0, dt);
+    } else {
+        rc = launch_stage(c, dgk::kModeRK1, c->d_U0, c->d_U0, c->d_Ua, dt);
+        if (!rc) rc = launch_stage(c, dgk::kModeRK2, c->d_Ua, c->d_U0, c->d_Ub, dt);
+        if (!rc) rc = launch_stage(c, dgk::kModeRK3, c->d_Ub, c->d_U0, c->d_Ua, dt);
+        if (!rc) rc = launch_stage(c, dgk::kModeRK4, c->d_Ua, c->d_U0, c->d_U0, dt);
+    }
     cudaGraph_t g = nullptr;
     cudaError_t ce = cudaStreamEndCapture(c->stream, &g);
     if (rc) { if (g) cudaGraphDestroy(g); return rc; }
@@ -1472,6 +1542,30 @@ int dg_set_stage_variant(dg_ctx* c, int v)
 }
 
 int dg_get_stage_variant(const dg_ctx* c) { return c ? c->variant : -1; }
+
+int dg_set_stage_chunks(dg_ctx* c, int chunks)
+{
+    if (!c || chunks < 1 || chunks > 64) return fail(c, DG_ERR_ARG, "dg_set_stage_chunks: chunks must be 1..64");
+    if (chunks > 1 && (c->face_key.size() != static_cast<size_t>(c->nface) || !c->d_fflux))
+        return fail(c, DG_ERR_UNSUPPORTED, "dg_set_stage_chunks: contexts with ghosts or without a face list");
+    DG_CUDA(c, cudaSetDevice(c->device));
+    DG_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (chunks > 1 && !c->stream2) DG_CUDA(c, cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking));
+    while (c->chunk_ev.size() < static_cast<size_t>(4 * (chunks + 1))) {
+        cudaEvent_t e;
+        DG_CUDA(c, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        c->chunk_ev.push_back(e);
+    }
+    if (c->chunks != chunks) {
+        c->chunks = chunks;
+        // the RK4 graph holds the launch sequence
+        if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }
+        if (c->graph) { cudaGraphDestroy(c->graph); c->graph = nullptr; }
+    }
+    return DG_OK;
+}
+
+int dg_get_stage_chunks(const dg_ctx* c) { return c ? c->chunks : -1; }
 
 int dg_tune_stage(dg_ctx* c, int reps, int* best, double* ms_per_variant)
 {

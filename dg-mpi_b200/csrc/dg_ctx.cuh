@@ -56,6 +56,16 @@ struct dg_ctx {
     int nface = 0, nface_inner = 0;
     int2* d_faces = nullptr;
     double* d_fflux = nullptr;
+    // contexts without ghosts list their faces by their lower element
+    // (face_key[i] = min(elemL, elemR) of face i, ascending), so that element
+    // chunks [e0, e1) first need the contiguous faces with key in [e0, e1):
+    // the RK4 graph may then run each stage as `chunks` face launches on a
+    // second stream, each followed on the main stream by the stage launch of
+    // its element chunk (dg_set_stage_chunks)
+    std::vector<int> face_key;
+    int chunks = 1;
+    cudaStream_t stream2 = nullptr;
+    std::vector<cudaEvent_t> chunk_ev;  // 4 stages x (chunks + 1)
     // tensor-core variants (kTC): the basis operator in its shared-memory layout
     uint16_t* d_tcop = nullptr;
     int variant_face_grid[dgi::kMaxVariants] = {};  // face kernel grid per FX variant

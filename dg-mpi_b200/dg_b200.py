@@ -105,6 +105,8 @@ def library(path: str | None = None) -> ctypes.CDLL:
         "dg_stage_variant_info": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ip, ip, ip, ip]),
         "dg_stage_variant_flags": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ip]),
         "dg_set_stage_variant": (ctypes.c_int, [vp, ctypes.c_int]),
+        "dg_set_stage_chunks": (ctypes.c_int, [vp, ctypes.c_int]),
+        "dg_get_stage_chunks": (ctypes.c_int, [vp]),
         "dg_get_stage_variant": (ctypes.c_int, [vp]),
         "dg_tune_stage": (ctypes.c_int, [vp, ctypes.c_int, ip, dp]),
         "dg_create_partitioned": (ctypes.c_int, [ctypes.POINTER(_CaseDesc), ctypes.POINTER(_MeshDesc),
@@ -551,6 +553,15 @@ class Case:
     @stage_variant.setter
     def stage_variant(self, v: int):
         self._check(self._lib.dg_set_stage_variant(self._ctx, int(v)))
+
+    @property
+    def stage_chunks(self) -> int:
+        """Element chunks per RK stage of the RK4 graph (dg_set_stage_chunks)."""
+        return self._lib.dg_get_stage_chunks(self._ctx)
+
+    @stage_chunks.setter
+    def stage_chunks(self, n: int):
+        self._check(self._lib.dg_set_stage_chunks(self._ctx, int(n)))
 
     def tune_stage(self, reps: int = 3):
         """Times every variant on this case (state unchanged), selects the fastest.

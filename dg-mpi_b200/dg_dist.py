@@ -121,6 +121,27 @@ class DistributedCase:
         dist.all_reduce(dt, op=dist.ReduceOp.MIN, group=self.group)
         return float(dt.item())
 
+    def _sum_over_ranks(self, values) -> np.ndarray:
+        dev = torch.device("cuda", self.device) if self.exchange.transport == "device" else "cpu"
+        t = torch.tensor(list(values), dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM, group=self.group)
+        return t.cpu().numpy()
+
+    def l2_error(self, name: str, data=(), t: float = 0.0) -> np.ndarray:
+        """Volume-normalised L2 error over the whole decomposed mesh: each
+        rank's sum of squares over its owned elements and its volume, summed
+        over the ranks (get_error with its MPI_Allreduce, src/post/main.cpp:30-201)."""
+        e = self.case.l2_error(name, data, t)
+        v = self.case.total_volume()
+        s = self._sum_over_ranks([*(e * e * v), v])
+        return np.sqrt(s[:5] / s[5])
+
+    def kinetic_energy(self) -> float:
+        """Volume-averaged kinetic energy over the whole decomposed mesh."""
+        v = self.case.total_volume()
+        s = self._sum_over_ranks([self.case.kinetic_energy() * v, v])
+        return float(s[0] / s[1])
+
     def stage(self, s: int, dt: float):
         buf = dg_b200.STAGE_INPUT[s]
         if not self.exchange.peers:

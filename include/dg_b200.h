@@ -174,6 +174,16 @@ int dg_stage_variant_info(int order, int variant, int* elems_per_cta, int* threa
 int dg_stage_variant_flags(int order, int variant, int* flags);
 int dg_set_stage_variant(dg_ctx* ctx, int variant);
 int dg_get_stage_variant(const dg_ctx* ctx);
+/* RK4 steps of a face-kernel variant on a context without ghosts as `chunks`
+ * (1..64) element chunks per stage: the chunks' face-flux launches on a
+ * second stream of the context, each chunk's stage launch after its face
+ * launch, so a chunk's face kernel runs beside the previous chunk's stage
+ * kernel.  The arithmetic is unchanged (bit-identical states); 1 (the
+ * default) is one face launch and one stage launch per stage.
+ * DG_ERR_UNSUPPORTED for partitioned contexts and contexts without a face
+ * list. */
+int dg_set_stage_chunks(dg_ctx* ctx, int chunks);
+int dg_get_stage_chunks(const dg_ctx* ctx);
 int dg_tune_stage(dg_ctx* ctx, int reps, int* best_variant, double* ms_per_variant);
 
 /* Forward Euler, replaces FE<3>::take_time_step (stepper.cpp:23-55). */

@@ -253,3 +253,31 @@ def test_every_stage_variant_matches_oracle(p, flux):
             assert rel_l2(case.get_state(), ref).max() < tol, (precision, v, info)
             assert case.status() == 0
         case.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed_fp32"])
+def test_chunked_stages_are_bit_identical(precision):
+    """RK4 steps with each stage split into element chunks (face launches on a
+    second stream beside the previous chunk's stage launch) give the same bits
+    as one face and one stage launch per stage, for chunk counts that do and
+    do not divide the mesh, on a mesh with rotated elements."""
+    mesh = dg_b200.periodic_box((7, 6, 5), (0, 0, 0), (10.0, 10.0, 10.0), rotate_seed=9)
+    case = dg_b200.Case(mesh, 3, flux="HLLC", gas_constant=1.0, precision=precision)
+    fx = [i for i, v in enumerate(case.stage_variants()) if v[3] == precision and "fx" in v[4].split("+")]
+    assert fx
+    case.stage_variant = fx[0]
+    U0 = case.project_ic("IsentropicVortexXY", [1, 1, 1, 1, 5, 5, 5, 10, 10])
+    dt = case.cfl_time_step(U0, 0.1)
+    case.rk4(dt, 3)
+    ref = case.get_state()
+    for chunks in (2, 3, 7, 64):
+        case.stage_chunks = chunks
+        assert case.stage_chunks == chunks
+        case.set_state(U0)
+        case.rk4(dt, 3)
+        assert np.array_equal(case.get_state(), ref), chunks
+    case.stage_chunks = 1
+    case.set_state(U0)
+    case.rk4(dt, 3)
+    assert np.array_equal(case.get_state(), ref)
+    assert case.status() == 0

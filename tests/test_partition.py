@@ -253,6 +253,10 @@ def _host_transport_worker(rank, world, port, order, flux, errq):
         assert d < 1e-13, (rank, d)
         assert dc.case.status() == 0
         assert dc.exchange.peers, "every rank of a periodic slab decomposition has peers"
+        # the error and kinetic energy summed over the ranks are the whole mesh's
+        np.testing.assert_allclose(dc.l2_error("IsentropicVortexXY", VORTEX_XY, 3 * dt),
+                                   full.l2_error("IsentropicVortexXY", VORTEX_XY, 3 * dt), rtol=1e-11, atol=1e-14)
+        assert abs(dc.kinetic_energy() / full.kinetic_energy() - 1.0) < 1e-12
         dc.close()
         full.close()
         dist.barrier()
