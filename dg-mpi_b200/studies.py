@@ -7,6 +7,7 @@
   python dg-mpi_b200/studies.py <name> --scale 0.25  # smaller mesh (fewer cases), same orders
   python dg-mpi_b200/studies.py general       # bent (non-affine) periodic boxes: 48^3 p=3, 24^3 p=5
   python dg-mpi_b200/studies.py convergence2d # the reference's 2D convergence table, N = 2..256, p = 1..3
+  python dg-mpi_b200/studies.py stage2d --nel 512 --order 3 --steps 2   # one 2D case (ncu captures)
   python dg-mpi_b200/studies.py stage --nel 40 --order 3 --precision fp64 --variant 0
                                              # one launch variant, 2 RK4 steps, no tuner (ncu captures)
 
@@ -267,9 +268,23 @@ def convergence2d(scale: float):
     return {"rows": rows, "max_abs_rel_diff": max(abs(r["rel_diff"]) for r in rows if r["rel_diff"] is not None)}
 
 
+def stage2d(nel: int, order: int, steps: int):
+    """The 2D vortex on an nel x nel box of [-5, 5]^2: projection, then `steps`
+    RK4 steps (four stage2d_kernel launches each) for profiling captures."""
+    mesh = dg_b200.periodic_box_2d((nel, nel), (-5.0, -5.0), (10.0, 10.0))
+    case = dg_b200.Case2D(mesh, order, flux="HLLC", gas_constant=1.0)
+    case.project_ic("IsentropicVortex", VORTEX[:5])
+    dt = 1e-3 * min(1.0, 256.0 / nel)  # the convergence study's CFL at its finest mesh
+    ms = case.rk4_timed(dt, steps)
+    out = {"nel": nel, "order": order, "steps": steps, "dt": dt, "ms_per_step": ms / max(steps, 1),
+           "dof_stage_per_s": nel * nel * (order + 1) ** 2 * 4 * 4 * steps / (ms / 1e3), "status": case.status()}
+    case.close()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("study", choices=["precision", "taylor_green", "ensemble", "general", "stage", "convergence2d"])
+    ap.add_argument("study", choices=["precision", "taylor_green", "ensemble", "general", "stage", "convergence2d", "stage2d"])
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--nel", type=int, default=40, help="stage: elements per direction")
     ap.add_argument("--order", type=int, default=3, help="stage: polynomial order")
@@ -279,6 +294,8 @@ def main():
     args = ap.parse_args()
     if args.study == "stage":
         res = stage(args.nel, args.order, args.precision, args.variant, args.steps)
+    elif args.study == "stage2d":
+        res = stage2d(args.nel, args.order, args.steps)
     else:
         run = {"precision": precision, "taylor_green": taylor_green, "ensemble": ensemble, "general": general,
                "convergence2d": convergence2d}[args.study]
