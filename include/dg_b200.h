@@ -492,7 +492,11 @@ int dg_basis_tables(int p, double* B, double* D, double* Minv);
  * (gbasis node order, x fastest), interior_faces [nface][8] rows (rankL,
  * elemL, faceL, orientL, rankR, elemR, faceR, orientR) with local faces
  * 0..3 (get_local_nodes_on_face_quadrilateral, shape.cpp:125-152) and
- * orientations 0 / 1; every face interior, every element a parallelogram. */
+ * orientations 0 / 1; every element a parallelogram (to 1e-9 of its size:
+ * the Jacobian is taken at the element's centre).  Element edges that
+ * are no interior face (the boundary edges of a non-periodic mesh) add
+ * nothing to the residual, as in the reference, whose residual loops over the
+ * interior faces only (src/solver/base.cpp:470-561). */
 typedef struct dg_mesh2d_desc {
     int nnode;
     const double* node_coords;

@@ -108,3 +108,21 @@ def test_nonphysical_state_is_reported_2d():
     gpu.set_state(U)
     with pytest.raises(dg_b200.DGError, match="NONPHYSICAL"):
         gpu.rk4(1e-3, 1)
+
+
+@pytest.mark.parametrize("flux", ["LaxFriedrichs", "HLLC"])
+def test_reference_quad_2x2_mesh_with_boundary_edges(flux):
+    """The reference's non-periodic 2x2 example mesh (its boundary edges carry
+    no interior face): the residual adds nothing on those edges, as the
+    reference's residual loops over the interior faces only; GPU against the
+    oracle on a vortex state, and FE steps."""
+    m = dg_b200.read_mesh_h5(os.path.join(os.path.dirname(__file__), "golden", "meshes", "quad_2x2.h5"))
+    assert m.interior_faces.shape[0] == 4 and m.elem_to_node_ids.shape[0] == 4
+    gpu = dg_b200.Case2D(m, 2, flux=flux, gas_constant=1.0)
+    orc = pyoracle.OracleCase2D.from_mesh(m, 2, flux=flux, gas_constant=1.0)
+    data = [1.0, 0.3, 0.2, 1.0, 5.0, 0.4, 0.6, 1e30, 1e30]
+    U = orc.project_ic("IsentropicVortexXY", data)
+    assert rel_l2(gpu.project_ic("IsentropicVortexXY", data), U).max() < 1e-13
+    assert rel_l2(gpu.residual(), orc.residual(U)).max() < 1e-11
+    gpu.fe(1e-3, 2)
+    assert rel_l2(gpu.get_state(), orc.fe(U, 1e-3, 2)).max() < 1e-12
