@@ -1293,6 +1293,14 @@ __host__ __device__ constexpr int face_batch_of(int p, int bytes) { return p <= 
 template <int P, typename T>
 __host__ __device__ constexpr int face_batch() { return face_batch_of(P, sizeof(T)); }
 constexpr int kFaceThreads = 128;
+// threads of the standalone face kernel: one round of the batch's gather tasks
+// (faces x 2 sides x 5 variables), at least 128
+template <int P, typename T>
+__host__ __device__ constexpr int face_threads()
+{
+    return (face_batch<P, T>() * 10 + 31) / 32 * 32 > kFaceThreads ? (face_batch<P, T>() * 10 + 31) / 32 * 32
+                                                                    : kFaceThreads;
+}
 
 template <int P, typename T>
 constexpr size_t face_smem_bytes()
@@ -1306,12 +1314,12 @@ constexpr size_t face_smem_bytes()
 
 // GEO: general geometry, the left element's normal data per face point;
 // bid / nblk as for stage_body
-template <int P, typename T, bool GEO>
+template <int P, typename T, bool GEO, int NTF = kFaceThreads>
 __device__ __forceinline__ void face_flux_body(const StageArgs& a, int bid, int nblk, int* work = nullptr,
                                                int* slots = nullptr)
 {
     using L = Lay<P, 1, T>;
-    constexpr int FB = face_batch<P, T>(), NT = kFaceThreads;
+    constexpr int FB = face_batch<P, T>(), NT = NTF;
     constexpr int N = L::N, M = L::M, NB = L::NB, NF = L::NF, N2 = L::N2, FS = L::FS;
     constexpr bool kShift = sizeof(T) == 4;
     extern __shared__ double fsm[];
@@ -1434,9 +1442,9 @@ __device__ __forceinline__ void face_flux_body(const StageArgs& a, int bid, int 
 }
 
 template <int P, typename T, bool GEO>
-__global__ void __launch_bounds__(kFaceThreads) face_flux_kernel(StageArgs a)
+__global__ void __launch_bounds__(face_threads<P, T>()) face_flux_kernel(StageArgs a)
 {
-    face_flux_body<P, T, GEO>(a, blockIdx.x, gridDim.x);
+    face_flux_body<P, T, GEO, face_threads<P, T>()>(a, blockIdx.x, gridDim.x);
 }
 
 template <int P, int E, int NT, int G, typename T, int FL>
@@ -1483,7 +1491,7 @@ struct StageVariant {
 template <int P, typename T, bool GEO>
 cudaError_t launch_face_kernel(const StageArgs& a, int grid, cudaStream_t s)
 {
-    face_flux_kernel<P, T, GEO><<<grid, kFaceThreads, face_smem_bytes<P, T>(), s>>>(a);
+    face_flux_kernel<P, T, GEO><<<grid, face_threads<P, T>(), face_smem_bytes<P, T>(), s>>>(a);
     return cudaGetLastError();
 }
 
@@ -1523,7 +1531,7 @@ StageVariant make_variant()
         constexpr bool geo = (FL & 32) != 0;
         v.face_func = (const void*)face_flux_kernel<P, T, geo>;
         v.face_smem = face_smem_bytes<P, T>();
-        v.face_threads = kFaceThreads;
+        v.face_threads = face_threads<P, T>();
         v.face_launch = launch_face_kernel<P, T, geo>;
         v.face_batch = face_batch<P, T>();
     }

@@ -784,7 +784,7 @@ StageVariant make_tc_variant()
     using K = TcCfg<P>;
     StageVariant v{K::E, K::NT, 1, 1, kUF | kSB | kFX | kTC, K::kSmem, (const void*)tc_stage_kernel<P>,
                    launch_tc_stage<P>, (const void*)face_flux_kernel<P, float, false>, face_smem_bytes<P, float>(),
-                   kFaceThreads, launch_face_kernel<P, float, false>, face_batch<P, float>()};
+                   face_threads<P, float>(), launch_face_kernel<P, float, false>, face_batch<P, float>()};
     return v;
 }
 
