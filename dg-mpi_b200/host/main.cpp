@@ -4,6 +4,9 @@
 // L2 error, and calls libdg_b200.so through the C ABI for the hot path.
 //
 //   dg_solve [-input input.toml] [-check]     (default deck: input.toml)
+//   dg_solve [-input input.toml] -post [data.h5]
+//            the reference's post tool (src/post/main.cpp:204-253): the case of
+//            the deck, the state and time of a solution file, its L2 errors
 //
 // Deck keys (as in the reference, src/exec/main.cpp:52-119,
 // src/solver/base.cpp:20-67, src/physics/base/base.cpp:25-32):
@@ -127,11 +130,11 @@ bool ends_with(const std::string& s, const std::string& tail)
     return s.size() >= tail.size() && s.compare(s.size() - tail.size(), tail.size(), tail) == 0;
 }
 
-int run2d(const dgh::Toml& deck, bool check_only);
+int run2d(const dgh::Toml& deck, bool check_only, const char* post);
 
-int run(const dgh::Toml& deck, bool check_only)
+int run(const dgh::Toml& deck, bool check_only, const char* post)
 {
-    if (static_cast<int>(deck.num_or("Physics", "dim", 3)) == 2) return run2d(deck, check_only);
+    if (static_cast<int>(deck.num_or("Physics", "dim", 3)) == 2) return run2d(deck, check_only, post);
     // ---- mesh ----
     int n[3] = {0, 0, 0};
     double x0[3] = {0, 0, 0}, len[3] = {1, 1, 1};
@@ -214,6 +217,24 @@ int run(const dgh::Toml& deck, bool check_only)
     if (dg_create(&cd, &md, &solver.ctx)) throw std::runtime_error(std::string("dg_create: ") + dg_last_error(nullptr));
     const int nb = dg_num_basis(solver.ctx);
     std::vector<double> Uc(static_cast<size_t>(ne) * nb * 5);
+    if (post) {
+        // run_post (src/post/main.cpp:204-253): the solution file's state and
+        // time, then get_error
+        int fne = 0, fnb = 0, fns = 0;
+        double t = 0.0;
+        if (dg_solution_read_h5(post, &fne, &fnb, &fns, &t, nullptr)) throw std::runtime_error(dg_last_error(nullptr));
+        if (fne != ne || fnb != nb || fns != 5)
+            throw std::runtime_error(std::string(post) + " does not hold a state of this mesh and order");
+        if (dg_solution_read_h5(post, &fne, &fnb, &fns, &t, Uc.data())) throw std::runtime_error(dg_last_error(nullptr));
+        if (dg_set_state(solver.ctx, Uc.data())) throw std::runtime_error(dg_last_error(solver.ctx));
+        std::printf("time=%.17g\n", t);
+        double err[5];
+        if (dg_l2_error(solver.ctx, ic, ic_data.data(), static_cast<int>(ic_data.size()), t, err))
+            throw std::runtime_error(std::string("l2 error: ") + dg_last_error(solver.ctx));
+        for (int k = 0; k < 5; ++k) std::printf("norm_total_error(%d)=%.*e\n", k, DECIMAL_DIG, err[k]);
+        dg_destroy(solver.ctx);
+        return 0;
+    }
     // Solver::init_state_from_fcn (L2 projection), base.cpp:113-223
     if (dg_project_ic(solver.ctx, ic, ic_data.data(), static_cast<int>(ic_data.size()), 0.0, Uc.data()))
         throw std::runtime_error(std::string("dg_project_ic: ") + dg_last_error(solver.ctx));
@@ -329,7 +350,7 @@ int run(const dgh::Toml& deck, bool check_only)
 
 // the 2D case (run_solver<2>, src/exec/main.cpp:52-119): quadrilateral
 // meshes, LagrangeQuad, the dg2d_* entry points
-int run2d(const dgh::Toml& deck, bool check_only)
+int run2d(const dgh::Toml& deck, bool check_only, const char* post)
 {
     int n[2] = {0, 0};
     double x0[2] = {-5.0, -5.0}, len[2] = {10.0, 10.0};
@@ -411,6 +432,22 @@ int run2d(const dgh::Toml& deck, bool check_only)
     if (dg2d_create(&cd, &md, &solver.ctx2)) throw std::runtime_error(std::string("dg2d_create: ") + dg_last_error(nullptr));
     const int nb = dg2d_num_basis(solver.ctx2);
     std::vector<double> Uc(static_cast<size_t>(ne) * nb * 4);
+    if (post) {
+        int fne = 0, fnb = 0, fns = 0;
+        double t = 0.0;
+        if (dg_solution_read_h5(post, &fne, &fnb, &fns, &t, nullptr)) throw std::runtime_error(dg_last_error(nullptr));
+        if (fne != ne || fnb != nb || fns != 4)
+            throw std::runtime_error(std::string(post) + " does not hold a 2D state of this mesh and order");
+        if (dg_solution_read_h5(post, &fne, &fnb, &fns, &t, Uc.data())) throw std::runtime_error(dg_last_error(nullptr));
+        if (dg2d_set_state(solver.ctx2, Uc.data())) throw std::runtime_error(dg2d_last_error(solver.ctx2));
+        std::printf("time=%.17g\n", t);
+        double err[4];
+        if (dg2d_l2_error(solver.ctx2, ic, ic_data.data(), static_cast<int>(ic_data.size()), t, err))
+            throw std::runtime_error(std::string("l2 error: ") + dg2d_last_error(solver.ctx2));
+        for (int k = 0; k < 4; ++k) std::printf("norm_total_error(%d)=%.*e\n", k, DECIMAL_DIG, err[k]);
+        dg2d_destroy(solver.ctx2);
+        return 0;
+    }
     if (dg2d_project_ic(solver.ctx2, ic, ic_data.data(), static_cast<int>(ic_data.size()), 0.0, Uc.data()))
         throw std::runtime_error(std::string("dg2d_project_ic: ") + dg2d_last_error(solver.ctx2));
     const bool restart = deck.has("Output", "restart_file");
@@ -479,14 +516,18 @@ int run2d(const dgh::Toml& deck, bool check_only)
 
 int main(int argc, char* argv[])
 {
-    std::string deck_path = "input.toml";
-    bool check_only = false;
+    std::string deck_path = "input.toml", post_file;
+    bool check_only = false, post = false;
     for (int i = 1; i < argc; ++i) {
         if (!std::strcmp(argv[i], "-input") && i + 1 < argc) deck_path = argv[++i];
         else if (!std::strcmp(argv[i], "-check")) check_only = true;
+        else if (!std::strcmp(argv[i], "-post")) {
+            post = true;
+            post_file = i + 1 < argc && argv[i + 1][0] != '-' ? argv[++i] : "data.h5";
+        }
     }
     try {
-        return run(dgh::Toml::parse_file(deck_path), check_only);
+        return run(dgh::Toml::parse_file(deck_path), check_only, post ? post_file.c_str() : nullptr);
     } catch (const std::exception& ex) {
         std::fprintf(stderr, "dg_solve: %s\n", ex.what());
         return 2;

@@ -173,3 +173,26 @@ def test_driver_2d_deck_reproduces_reference_convergence_entry(golden, tmp_path)
     assert abs(err[0] / TABLE[2][2] - 1.0) < PIN_RTOL, err[0]
     U, t = dg_b200.read_solution_h5(str(tmp_path / "data.h5"))
     assert U.shape == (64, 9, 4) and t == pytest.approx(1.0, abs=1e-12)
+
+
+@pytest.mark.gpu
+def test_driver_post_mode_recomputes_the_errors_of_a_run(tmp_path):
+    """dg_solve -post (the reference's post tool, src/post/main.cpp:204-253):
+    the deck's case, data.h5's state and time, the same L2 errors the run
+    printed; 3D and 2D decks."""
+    def errors(out):
+        return {int(m.group(1)): m.group(2) for m in re.finditer(r"norm_total_error\((\d)\)=(\S+)", out)}
+    deck3 = _deck(tmp_path, "a.toml", 7, "")
+    r = run(["-input", deck3], cwd=str(tmp_path))
+    assert r.returncode == 0, r.stderr
+    p = run(["-input", deck3, "-post", "data.h5"], cwd=str(tmp_path))
+    assert p.returncode == 0, p.stderr
+    assert errors(p.stdout) == errors(r.stdout) and len(errors(p.stdout)) == 5
+    assert re.search(r"^time=", p.stdout, re.M)
+    deck2 = os.path.join(EXAMPLES, "vortex2d_box8_p2.toml")
+    (tmp_path / "two").mkdir()
+    r = run(["-input", deck2], cwd=str(tmp_path / "two"), timeout=300)
+    assert r.returncode == 0, r.stderr
+    p = run(["-input", deck2, "-post"], cwd=str(tmp_path / "two"))
+    assert p.returncode == 0, p.stderr
+    assert errors(p.stdout) == errors(r.stdout) and len(errors(p.stdout)) == 4
