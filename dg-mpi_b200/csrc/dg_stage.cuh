@@ -194,6 +194,7 @@ struct TaskOrd {
     static constexpr int gather = P == 4 ? 1 : 0;                                               // (b, v)
     static constexpr int minvx = P >= 2 ? 1 : 0;                                                // (v, byz)
     static constexpr int minvy = P == 2 || P == 4 ? 11 : P == 3 || P == 5 ? 7 : 21;             // (v, bx, bz)
+    static constexpr int minvxg = P == 5 && W8 ? 0 : 1;                                         // (v, byz), MG
 };
 template <int O, int n0, int n1>
 __device__ __forceinline__ void task2(int r, int& c0, int& c1)
@@ -238,12 +239,16 @@ __device__ __forceinline__ void task3(int r, int& c0, int& c1, int& c2)
 // memory (requires UF); flag 64 (FX) -- face fluxes from the face kernel:
 // every interior face's flux is computed once (face_flux_kernel, launched
 // before the stage kernel) and each element stages its six faces' fluxes
-// instead of computing traces and fluxes (requires SB)
+// instead of computing traces and fluxes (requires SB); flag 4096 (MG) -- the
+// six faces' lifted fluxes added to the residual inside the inverse mass's x
+// pass instead of a separate pass over the residual (affine geometry)
 template <int P, int G, typename T = double, int FL = 0>
 struct Lay {
     static constexpr bool PZ = FL & 1, SB = FL & 2, UF = FL & 4, RS = FL & 8, K1 = FL & 16, GE = FL & 32, FX = FL & 64;
+    static constexpr bool MG = FL & 4096;
     static_assert(!GE || UF, "general geometry needs the unfused volume");
     static_assert(!FX || SB, "face fluxes from the face kernel need the single buffer");
+    static_assert(!MG || !GE, "the folded lift gather needs the Kronecker inverse mass");
     static constexpr int N = P + 1, M = P + 2, NB = N * N * N, NF = M * M, N2 = N * N;
     static constexpr int GV = G == 1 ? 5 : (G == 2 ? 3 : 2);  // variables per group (max)
     static constexpr int GA = PZ ? 5 : GV;       // variables of the z-contraction buffers
@@ -1121,8 +1126,10 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int bid, int nblk
             if (en < a.ne) prefetch_recs<E, NT>(a.frec, a.ne, en, sRec);
             cp_async_commit();
         }
-        // add the six face contributions to the (FP64) residual
-        for (int i = tid; i < E * 5 * NB; i += NT) {
+        // add the six face contributions to the (FP64) residual (with MG, in
+        // the inverse mass's x pass, except for the residual output)
+        const bool fold_lifts = L::MG && a.mode != kModeResidual;
+        for (int i = tid; i < (fold_lifts ? 0 : E * 5 * NB); i += NT) {
             const int e = i / (5 * NB);
             int b, v;
             task2<TO::gather, NB, 5>(i - e * 5 * NB, b, v);
@@ -1144,7 +1151,7 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int bid, int nblk
             }
             sRes[e * ES + v * VS + L::cw(bc[0], bc[1], bc[2])] += s;
         }
-        __syncthreads();
+        if (!fold_lifts) __syncthreads();
 
         if (a.mode == kModeResidual) {
             for (int i = tid; i < E * 5 * NB; i += NT) {
@@ -1201,12 +1208,32 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int bid, int nblk
             for (int i = tid; i < E * 5 * N2; i += NT) {
                 const int e = i / (5 * N2);
                 int v, byz;
-                task2<TO::minvx, 5, N2>(i - e * 5 * N2, v, byz);
+                task2<(L::MG ? TO::minvxg : TO::minvx), 5, N2>(i - e * 5 * N2, v, byz);
                 const int by = byz % N, bz = byz / N;
                 double* r = sRes + e * ES + v * VS;  // pencil along x
                 double t[N];
 #pragma unroll
                 for (int k = 0; k < N; ++k) t[k] = r[L::cw(k, by, bz)];
+                if constexpr (L::MG) {
+                    // the face contributions of the pencil's coefficients, summed
+                    // in face order and added as the separate pass adds them
+                    const T* Lf = sW + e * W + 30 * FS + v * FS;
+#pragma unroll
+                    for (int k = 0; k < N; ++k) {
+                        const int bc[3] = {k, by, bz};
+                        double s = 0.0;
+#pragma unroll
+                        for (int f = 0; f < 6; ++f) {
+                            const int ax = face_axis(f), sidx = face_side(f) ? N - 1 : 0;
+                            if (bc[ax] == sidx) {
+                                const int b0 = ax == 0 ? bc[1] : bc[0];
+                                const int b1 = ax == 2 ? bc[1] : bc[2];
+                                s += double(Lf[f * 5 * FS + b1 * N + b0]);
+                            }
+                        }
+                        t[k] += s;
+                    }
+                }
 #pragma unroll
                 for (int j = 0; j < N; ++j) {
                     double s = 0.0;
@@ -1512,7 +1539,7 @@ cudaError_t launch_stage_variant(const StageArgs& a, int grid, cudaStream_t s)
 // parallel tasks and registers (high orders); general geometry is a property
 // of the mesh, not a tuning choice: contexts on non-affine meshes run GE
 // variants only, the others never do
-constexpr int kPZ = 1, kSB = 2, kUF = 4, kRS = 8, kK1 = 16, kGE = 32, kFX = 64;
+constexpr int kPZ = 1, kSB = 2, kUF = 4, kRS = 8, kK1 = 16, kGE = 32, kFX = 64, kMG = 4096;
 // the tensor-core stage kernel (dg_tc.cuh): a kernel of its own, not an option of stage_kernel
 constexpr int kTC = 128;
 // MB > 0: at least MB resident CTAs per SM asked of the compiler (a register cap)

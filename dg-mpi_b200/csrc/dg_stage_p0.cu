@@ -1,8 +1,9 @@
 // dg_stage_p0.cu -- compiled launch variants of the stage kernel for order p = 0
 // (elements per CTA, threads per CTA, variable groups, residual arithmetic; then the
 // optional flags: all groups' pencils in one phase, single coefficient buffer, unfused
-// volume, row-split traces and lifts, one face-flux point per thread; then the minimum of
-// resident CTAs per SM asked of the compiler).  Contexts on non-affine meshes use the
+// volume, row-split traces and lifts, one face-flux point per thread, face fluxes from
+// the face kernel, face lifts added in the inverse mass's first pass; then the minimum
+// of resident CTAs per SM asked of the compiler).  Contexts on non-affine meshes use the
 // general-geometry (kGE) entries only, the others never do.  The
 // first variant of each precision is the default (the measured best); dg_tune_stage may pick another.
 #include "dg_stage.cuh"

@@ -532,7 +532,8 @@ class Case:
         "k1" (one face-flux point per thread), "ge" (general trilinear geometry: the variants that
         non-affine meshes run), "fx" (each face's flux once, from a face kernel launched before the
         stage kernel), "tc" (the tensor-core kernel: split products on tcgen05 for the volume
-        integral), and "mb<n>" when the variant asks the compiler for n resident CTAs per SM."""
+        integral), "mg" (the face lifts added inside the inverse mass's first pass), and "mb<n>"
+        when the variant asks the compiler for n resident CTAs per SM."""
         out = []
         for v in range(self._lib.dg_num_stage_variants(self.order)):
             E, NT, G, pr, fl = (ctypes.c_int() for _ in range(5))
@@ -540,9 +541,9 @@ class Case:
                                             ctypes.byref(pr))
             self._lib.dg_stage_variant_flags(self.order, v, ctypes.byref(fl))
             opts = "+".join(n for b, n in ((1, "pz"), (2, "sb"), (4, "uf"), (8, "rs"), (16, "k1"), (32, "ge"), (64, "fx"),
-                                           (128, "tc")) if fl.value & b)
-            if fl.value >> 8:
-                opts += ("+" if opts else "") + "mb%d" % (fl.value >> 8)
+                                           (128, "tc"), (4096, "mg")) if fl.value & b)
+            if (fl.value >> 8) & 15:
+                opts += ("+" if opts else "") + "mb%d" % ((fl.value >> 8) & 15)
             out.append((E.value, NT.value, G.value, "mixed_fp32" if pr.value == 1 else "fp64", opts))
         return out
 

@@ -170,7 +170,8 @@ int dg_stage_variant_info(int order, int variant, int* elems_per_cta, int* threa
  * flux computed once by a face kernel launched before the stage kernel (the
  * elements read their six faces' fluxes);
  * bits 8..11 -- the minimum of resident CTAs per SM the kernel was compiled
- * for (0: none; a register cap). */
+ * for (0: none; a register cap); bit 12 -- the six faces' lifted fluxes
+ * added inside the inverse mass's first pass instead of a pass of their own. */
 int dg_stage_variant_flags(int order, int variant, int* flags);
 int dg_set_stage_variant(dg_ctx* ctx, int variant);
 int dg_get_stage_variant(const dg_ctx* ctx);

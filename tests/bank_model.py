@@ -20,7 +20,8 @@ Passes modelled (per element, E = 1; the face-flux variant, non-row-split
 lift): x interpolation (coefficients -> X1), y interpolation (X1 -> X2), z
 interpolation in place, pointwise flux (5 rows -> 15 rows), z / y / x
 contractions, lift, lift gather into the residual, inverse-mass x and y
-passes and the update (z pencils).
+passes and the update (z pencils); with the launch option MG the lift gather
+and the inverse-mass x pass are one pass (minvxg).
 
     python tests/bank_model.py 3 8      # p = 3, FP64 work area
     python tests/bank_model.py 5 4 --search
@@ -117,11 +118,13 @@ def task_orders(p, nbytes):
     gather = 1 if p == 4 else 0
     minvx = 1 if p >= 2 else 0
     minvy = {2: 11, 3: 7, 4: 11, 5: 7}.get(p, 21)
+    minvxg = 0 if p == 5 and w8 else 1
     return {
         "x": order2(x, ("v", "byz")), "y": order3(y, ("v", "qx", "bz")), "z": order2(z, ("qxy", "v")),
         "zc": order2(zc, ("qxy", "v")), "yc": order3(yc, ("v", "qx", "bz")), "xc": order2(xc, ("v", "byz")),
         "gather": order2(gather, ("b", "v")), "minvx": order2(minvx, ("v", "byz")),
         "minvy": order3(minvy, ("v", "bx", "bz")), "upd": ("bxy", "v"), "lift": ("v", "f"), "flux": ("q",),
+        "minvxg": order2(minvxg, ("v", "byz")),
     }
 
 
@@ -185,6 +188,19 @@ def passes(p, W, VS, X1S, QS, FS, cw):
         (lambda t: [t["v"] * VS + cw(t["b"] % N, (t["b"] // N) % N, t["b"] // N2)] * 2, 8)])
     out["minvx"] = (dict(v=5, byz=N2), [
         (lambda t: [t["v"] * VS + cw(k, t["byz"] % N, t["byz"] // N) for k in range(N)] * 2, 8)])
+
+    def minvx_lifts(t):
+        # launch option MG: the x pencil, the lifted face fluxes on it (x faces at
+        # its ends, y / z faces along it when the pencil lies on them), the pencil
+        v, by, bz = t["v"], t["byz"] % N, t["byz"] // N
+        lift = lambda f, b0, b1: 30 * FS + f * 5 * FS + v * FS + b1 * N + b0
+        rows = [v * VS + cw(k, by, bz) for k in range(N)] + [lift(4, by, bz), lift(2, by, bz)]
+        for f, c, sidx in ((1, by, 0), (3, by, N - 1), (0, bz, 0), (5, bz, N - 1)):
+            other = bz if f in (1, 3) else by
+            rows += [lift(f, k, other) if c == sidx else None for k in range(N)]
+        return rows + [v * VS + cw(k, by, bz) for k in range(N)]
+
+    out["minvxg"] = (dict(v=5, byz=N2), [(minvx_lifts, W)])
     out["minvy"] = (dict(v=5, bx=N, bz=N), [
         (lambda t: [t["v"] * VS + cw(t["bx"], k, t["bz"]) for k in range(N)] * 2, 8)])
     out["upd"] = (dict(bxy=N2, v=5), [
@@ -192,13 +208,20 @@ def passes(p, W, VS, X1S, QS, FS, cw):
     return out
 
 
-def count(p, nbytes, QS=None, orders=None, rotated=True):
+def kernel_passes(ps, mg=False):
+    """the passes one stage runs: with the launch option MG the lift gather and
+    the inverse mass's x pass are one pass (minvxg)"""
+    drop = ("gather", "minvx") if mg else ("minvxg",)
+    return {k: v for k, v in ps.items() if k not in drop}
+
+
+def count(p, nbytes, QS=None, orders=None, rotated=True, mg=False):
     """per-pass (wavefronts, ideal) with the given stride and orders."""
     N, M = p + 1, p + 2
     VS, X1S, FS = (N ** 3) | 1, (N * N * M) | 1, (M * M) | 1
     QS = QS if QS is not None else qs_stride(p, nbytes)
     orders = orders or task_orders(p, nbytes)
-    ps = passes(p, nbytes, VS, X1S, QS, FS, coef_word(p, rotated))
+    ps = kernel_passes(passes(p, nbytes, VS, X1S, QS, FS, coef_word(p, rotated)), mg)
     return {name: pass_cost(dims, orders[name], acc) for name, (dims, acc) in ps.items()}
 
 
@@ -209,7 +232,7 @@ def search(p, nbytes, rotated=True):
     VS, X1S, FS = (N ** 3) | 1, (N * N * M) | 1, (M * M) | 1
     best = None
     for QS in range(M ** 3, M ** 3 + 17):
-        ps = passes(p, nbytes, VS, X1S, QS, FS, coef_word(p, rotated))
+        ps = kernel_passes(passes(p, nbytes, VS, X1S, QS, FS, coef_word(p, rotated)))
         total, chosen = 0, {}
         for name, (dims, acc) in ps.items():
             cands = [("bxy", "v")] if name == "upd" else list(itertools.permutations(dims))
@@ -236,6 +259,9 @@ def main():
         print(f"  {name:7s} {cur[name][0]:6d} {plain[name][0]:6d} {cur[name][1]:6d}")
     print(f"  {'total':7s} {sum(c[0] for c in cur.values()):6d} {sum(c[0] for c in plain.values()):6d} "
           f"{sum(c[1] for c in cur.values()):6d}")
+    mg = count(args.order, args.width, mg=True)
+    print(f"  with the lifts added in the inverse mass's x pass (MG): minvxg {mg['minvxg'][0]} "
+          f"(gather + minvx {cur['gather'][0] + cur['minvx'][0]}), total {sum(c[0] for c in mg.values())}")
     if args.search:
         total, QS, chosen = search(args.order, args.width)
         print(f"search: total {total} with QS = {QS}; orders {chosen}")

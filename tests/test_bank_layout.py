@@ -22,8 +22,9 @@ PROBE = r"""
 template <int P, int B> void orders() {
     using O = dgk::TaskOrd<P, B>;
     std::printf("{\"p\": %d, \"bytes\": %d, \"qs\": %d, \"x\": %d, \"y\": %d, \"z\": %d, \"zc\": %d, "
-                "\"yc\": %d, \"xc\": %d, \"gather\": %d, \"minvx\": %d, \"minvy\": %d}\n",
-                P, B, dgk::qs_stride(P, B), O::x, O::y, O::z, O::zc, O::yc, O::xc, O::gather, O::minvx, O::minvy);
+                "\"yc\": %d, \"xc\": %d, \"gather\": %d, \"minvx\": %d, \"minvy\": %d, \"minvxg\": %d}\n",
+                P, B, dgk::qs_stride(P, B), O::x, O::y, O::z, O::zc, O::yc, O::xc, O::gather, O::minvx, O::minvy,
+                O::minvxg);
 }
 int main() {
     orders<2, 8>(); orders<2, 4>(); orders<3, 8>(); orders<3, 4>();
@@ -69,6 +70,7 @@ def test_model_tables_are_the_headers(header, p, w):
     assert o["gather"] == bm.order2(h["gather"], ("b", "v"))
     assert o["minvx"] == bm.order2(h["minvx"], ("v", "byz"))
     assert o["minvy"] == bm.order3(h["minvy"], ("v", "bx", "bz"))
+    assert o["minvxg"] == bm.order2(h["minvxg"], ("v", "byz"))
 
 
 def test_rotated_rows_are_the_headers(header):
@@ -85,12 +87,28 @@ def test_committed_layout_is_the_model_optimum(p, w):
     assert committed == best
 
 
+@pytest.mark.parametrize("p,w", CASES)
+def test_folded_lift_gather_order_is_the_model_optimum(p, w):
+    """Launch option MG: the inverse mass's x pass with the lift gather in it
+    takes the model's best task order, and has fewer wavefronts than the two
+    passes it replaces."""
+    N, M = p + 1, p + 2
+    VS, X1S, FS = (N ** 3) | 1, (N * N * M) | 1, (M * M) | 1
+    ps = bm.passes(p, w, VS, X1S, bm.qs_stride(p, w), FS, bm.coef_word(p, True))
+    dims, acc = ps["minvxg"]
+    committed = bm.pass_cost(dims, bm.task_orders(p, w)["minvxg"], acc)[0]
+    assert committed == min(bm.pass_cost(dims, o, acc)[0] for o in (("v", "byz"), ("byz", "v")))
+    cur = bm.count(p, w)
+    assert committed < cur["gather"][0] + cur["minvx"][0]
+
+
 def test_p3_fp64_wavefront_counts():
     cur = bm.count(3, 8)
     plain = bm.count(3, 8, QS=125, orders=bm.task_orders(0, 8), rotated=False)
     assert sum(c[0] for c in cur.values()) == 1324
     assert sum(c[0] for c in plain.values()) == 1734
     assert sum(c[1] for c in cur.values()) == 1139
+    assert sum(c[0] for c in bm.count(3, 8, mg=True).values()) == 1284
     # the rotated rows make every coefficient-block pencil pass conflict-free
     for name in ("minvx", "minvy", "upd"):
         assert cur[name][0] == cur[name][1]
