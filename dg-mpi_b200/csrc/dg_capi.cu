@@ -1700,6 +1700,66 @@ int dg_kinetic_energy(dg_ctx* c, double* ke)
     return DG_OK;
 }
 
+namespace {
+
+// The bounded mbarrier wait of the tensor-core kernel (tc::mbar_wait) on a
+// barrier that nothing completes, or that thread 0 completes first: the wait
+// gives up after `limit` SM cycles and the kernel reports kStatusTimeout and
+// returns. No asynchronous copy is attached to the barrier, so a wait that
+// gives up leaves nothing in flight.
+__global__ void bounded_wait_probe_kernel(long long limit, int arrive, unsigned* status, long long* cycles)
+{
+    __shared__ alignas(8) unsigned long long bar;
+    const uint32_t b = dgk::tc::smem_u32(&bar);
+    if (threadIdx.x == 0) {
+        dgk::tc::mbar_init(b, 1);
+        dgk::tc::mbar_fence_init();
+    }
+    __syncthreads();
+    if (arrive && threadIdx.x == 0) dgk::tc::mbar_arrive(b);
+    const long long t0 = clock64();
+    const bool ok = __syncthreads_and(dgk::tc::mbar_wait(b, 0, limit));
+    if (threadIdx.x == 0) {
+        cycles[0] = clock64() - t0;
+        status[0] = ok ? 0u : dgk::kStatusTimeout;
+        dgk::tc::mbar_inval(b);
+    }
+}
+
+}  // namespace
+
+int dg_probe_bounded_wait(int device, long long limit_cycles, int arrive, long long* waited_cycles)
+{
+    g_create_error.clear();
+    if (limit_cycles < 0 || limit_cycles > 4000000000LL)
+        return fail(nullptr, DG_ERR_ARG, "dg_probe_bounded_wait: limit must be 0 .. 4e9 SM cycles (about 2 s)");
+    int prev = 0;
+    cudaError_t ce = cudaGetDevice(&prev);
+    if (ce == cudaSuccess) ce = cudaSetDevice(device);
+    if (ce != cudaSuccess) return fail(nullptr, DG_ERR_CUDA, std::string("dg_probe_bounded_wait: ") + cudaGetErrorString(ce));
+    void* buf = nullptr;
+    unsigned st = 0;
+    long long cyc = 0;
+    ce = cudaMalloc(&buf, 16);
+    if (ce == cudaSuccess) {
+        long long* d_cycles = static_cast<long long*>(buf);
+        unsigned* d_status = reinterpret_cast<unsigned*>(d_cycles + 1);
+        bounded_wait_probe_kernel<<<1, 32>>>(limit_cycles, arrive ? 1 : 0, d_status, d_cycles);
+        ce = cudaGetLastError();
+        if (ce == cudaSuccess) ce = cudaMemcpy(&st, d_status, sizeof(st), cudaMemcpyDeviceToHost);
+        if (ce == cudaSuccess) ce = cudaMemcpy(&cyc, d_cycles, sizeof(cyc), cudaMemcpyDeviceToHost);
+        const cudaError_t fe = cudaFree(buf);
+        if (ce == cudaSuccess) ce = fe;
+    }
+    (void)cudaSetDevice(prev);
+    if (ce != cudaSuccess) return fail(nullptr, DG_ERR_CUDA, std::string("dg_probe_bounded_wait: ") + cudaGetErrorString(ce));
+    if (waited_cycles) *waited_cycles = cyc;
+    if (st & dgk::kStatusTimeout)
+        return fail(nullptr, DG_ERR_TIMEOUT,
+                    "dg_probe_bounded_wait: the bounded wait gave up after " + std::to_string(cyc) + " SM cycles");
+    return DG_OK;
+}
+
 int dg_kinetic_energy_noalloc(int order, int nelem, const double* d_state, const double* d_djac, double* d_ke,
                               void* stream)
 {

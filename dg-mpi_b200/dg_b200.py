@@ -23,6 +23,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "_build", "libdg_b200.so")
 
 DG_OK = 0
+DG_ERR_TIMEOUT = 4
 ERROR_NAMES = {1: "DG_ERR_ARG", 2: "DG_ERR_CUDA", 3: "DG_ERR_NONPHYSICAL", 4: "DG_ERR_TIMEOUT",
                5: "DG_ERR_UNSUPPORTED", 6: "DG_ERR_NOMEM"}
 
@@ -95,6 +96,8 @@ def library(path: str | None = None) -> ctypes.CDLL:
         "dg_total_volume": (ctypes.c_int, [vp, dp]),
         "dg_status": (ctypes.c_int, [vp, up]),
         "dg_sync": (ctypes.c_int, [vp]),
+        "dg_probe_bounded_wait": (ctypes.c_int, [ctypes.c_int, ctypes.c_longlong, ctypes.c_int,
+                                                 ctypes.POINTER(ctypes.c_longlong)]),
         "dg_device_state": (vp, [vp]),
         "dg_mesh_periodic_box": (ctypes.c_int, [ip, dp, dp, ctypes.c_uint, ip, dp, ip, up, ip, up]),
         "dg_cfl_time_step": (ctypes.c_int, [vp, dp, ctypes.c_double, dp]),
@@ -733,6 +736,18 @@ def kinetic_energy_noalloc(order: int, nelem: int, d_state: int, d_djac: int, d_
                                        ctypes.c_void_p(d_ke), ctypes.c_void_p(stream))
     if rc:
         raise DGError(rc, lib.dg_last_error(None).decode())
+
+
+def probe_bounded_wait(device: int, limit_cycles: int, arrive: bool) -> tuple[int, int]:
+    """The failure-detection probe of the bounded device waits
+    (dg_probe_bounded_wait): (return code, SM cycles the wait took); the code
+    is DG_ERR_TIMEOUT when the wait gave up, 0 when the barrier completed."""
+    lib = library()
+    cyc = ctypes.c_longlong()
+    rc = lib.dg_probe_bounded_wait(int(device), int(limit_cycles), 1 if arrive else 0, ctypes.byref(cyc))
+    if rc not in (DG_OK, DG_ERR_TIMEOUT):
+        raise DGError(rc, lib.dg_last_error(None).decode())
+    return rc, cyc.value
 
 
 # ---------------------------------------------------------------------------

@@ -257,6 +257,16 @@ int dg_status(dg_ctx* ctx, unsigned* flags);
 /* Waits for all work of ctx. */
 int dg_sync(dg_ctx* ctx);
 
+/* Failure-detection probe of the bounded device waits: one CTA on `device`
+ * waits, through the same bounded mbarrier wait the tensor-core kernel's
+ * waits use, on a barrier that nothing completes (arrive = 0) or that one of
+ * its threads completes first (arrive = 1).  The first gives up after about
+ * limit_cycles SM cycles (0 .. 4e9) and returns DG_ERR_TIMEOUT, the second
+ * returns DG_OK; *waited_cycles (may be NULL) receives the cycles the wait
+ * took.  The kernel returns normally either way and leaves nothing in flight,
+ * so the device stays usable.  Error text: dg_last_error(NULL). */
+int dg_probe_bounded_wait(int device, long long limit_cycles, int arrive, long long* waited_cycles);
+
 /* Raw device pointers for callers that keep data resident (benchmarks,
  * multi-GPU exchange).  Layout of the device state: [ne][5][nb]. */
 void* dg_device_state(dg_ctx* ctx);

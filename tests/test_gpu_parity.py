@@ -317,3 +317,24 @@ def test_folded_lift_gather_is_bit_identical(p, precision):
             got.append((R, case.get_state()))
         assert np.array_equal(got[0][0], got[1][0]) and np.array_equal(got[0][1], got[1][1]), (vs[i], vs[j])
     assert case.status() == 0
+
+
+def test_bounded_wait_gives_up_and_the_device_stays_usable():
+    """Failure detection without a fault: a bounded device wait on a barrier
+    that nothing completes gives up after its limit and reports
+    DG_ERR_TIMEOUT; the same wait on a completed barrier returns at once; a
+    context created afterwards computes as before."""
+    limit = 2_000_000  # SM cycles, about 1 ms
+    rc, cycles = dg_b200.probe_bounded_wait(0, limit, arrive=False)
+    assert rc == dg_b200.DG_ERR_TIMEOUT and cycles >= limit, (rc, cycles)
+    assert "gave up" in dg_b200.library().dg_last_error(None).decode()
+    rc, cycles = dg_b200.probe_bounded_wait(0, limit, arrive=True)
+    assert rc == dg_b200.DG_OK and cycles < limit, (rc, cycles)
+    mesh = dg_b200.periodic_box((3, 2, 3), (0.0, 0.0, 0.0), (10.0, 10.0, 10.0), rotate_seed=7)
+    orc = pyoracle.OracleCase.from_mesh(mesh, 2, flux="HLLC", gas_constant=1.0)
+    U = orc.project_ic("IsentropicVortexXY", VORTEX_XY)
+    case = dg_b200.Case(mesh, 2, flux="HLLC", gas_constant=1.0)
+    case.set_state(U)
+    assert rel_l2(case.residual(), orc.residual(U)).max() < 1e-11
+    assert case.status() == 0
+    case.close()

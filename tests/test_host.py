@@ -36,6 +36,14 @@ def test_binding_covers_every_declared_symbol():
         assert getattr(lib, n).argtypes is not None, n
 
 
+def test_bounded_wait_probe_rejects_limits_out_of_range():
+    """dg_probe_bounded_wait checks its limit before any device work."""
+    lib = dg_b200.library()
+    for limit in (-1, 4_000_000_001):
+        assert lib.dg_probe_bounded_wait(0, limit, 0, None) == 1  # DG_ERR_ARG
+        assert b"limit" in lib.dg_last_error(None)
+
+
 @pytest.mark.parametrize("n", range(1, 13))
 def test_gauss_legendre_matches_oracle(n):
     x, w = dg_b200.gauss_legendre(n)
