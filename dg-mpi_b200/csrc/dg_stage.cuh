@@ -747,6 +747,9 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int bid, int nblk
 #pragma unroll
                 for (int bx = 0; bx < N; ++bx) res[L::cw(bx, byz % N, byz / N)] = double(r[bx]);
             }
+            // with FX the face fluxes must have landed before the lift: their copies
+            // are waited for here, so this barrier serves both
+            if constexpr (L::FX) cp_async_wait_older();
             __syncthreads();
         } else {
             // ---- fused: z interpolation, Euler flux, contravariant transform and
@@ -1048,9 +1051,10 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int bid, int nblk
             // before the inverse-mass pass, which waits for all copies)
             if (en < a.ne) prefetch_recs<E, NT>(a.frec, a.ne, en, sRec);
             cp_async_commit();
-        } else {
+        } else if constexpr (!L::UF) {
             // the face fluxes have landed (the next batch's coefficients may
-            // still be in flight)
+            // still be in flight; the unfused volume waited for them before
+            // its last barrier)
             cp_async_wait_older();
             __syncthreads();
         }
