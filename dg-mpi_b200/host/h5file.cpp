@@ -311,9 +311,13 @@ bool Reader::heap_data(uint64_t addr, std::vector<uint8_t>& data, std::string& e
     return rd(le(h + 24, 8), data.data(), data.size(), err);
 }
 
-bool Reader::group_btree(uint64_t btree, const std::vector<uint8_t>& heap, int depth, std::string& err)
+bool Reader::group_btree(uint64_t btree, const std::vector<uint8_t>& heap, int level_expected, long& budget,
+                         std::string& err)
 {
-    if (depth > 32) { err = "group B-tree too deep"; return false; }
+    // every node is visited at most once per budget unit, and a child sits one
+    // level below its parent: a corrupt tree (a cycle, a node shared by many
+    // parents) ends in an error instead of an endless or exponential walk
+    if (--budget < 0) { err = "group B-tree has too many nodes"; return false; }
     uint8_t h[24];
     if (!rd(btree, h, 24, err)) return false;
     if (std::memcmp(h, "TREE", 4) != 0 || h[4] != 0) {
@@ -321,13 +325,17 @@ bool Reader::group_btree(uint64_t btree, const std::vector<uint8_t>& heap, int d
         return false;
     }
     const int level = h[5];
+    if (level_expected >= 0 && level != level_expected) {
+        err = "group B-tree child is not one level below its parent";
+        return false;
+    }
     const uint64_t used = le(h + 6, 2);
     std::vector<uint8_t> kc(8 + 16 * used);
     if (!rd(btree + 24, kc.data(), kc.size(), err)) return false;
     for (uint64_t i = 0; i < used; ++i) {
         const uint64_t child = le(&kc[8 + 16 * i], 8);
         if (level > 0) {
-            if (!group_btree(child, heap, depth + 1, err)) return false;
+            if (!group_btree(child, heap, level - 1, budget, err)) return false;
             continue;
         }
         uint8_t s[8];
@@ -392,7 +400,8 @@ bool Reader::open(const std::string& path, std::string& err)
             if (m.data.size() < 16) { err = "short symbol table message"; return false; }
             std::vector<uint8_t> heap;
             if (!heap_data(le(m.data.data() + 8, 8), heap, err)) return false;
-            if (!group_btree(le(m.data.data(), 8), heap, 0, err)) return false;
+            long budget = 1 << 16;
+            if (!group_btree(le(m.data.data(), 8), heap, -1, budget, err)) return false;
             found = true;
         } else if (m.type == kMsgLinkInfo) {
             if (m.data.size() >= 10 && le(m.data.data() + 2 + ((m.data[1] & 1) ? 8 : 0), 8) != kUndef) {
@@ -407,7 +416,10 @@ bool Reader::open(const std::string& path, std::string& err)
             const uint8_t fl = p[1];
             size_t pos = 2;
             int ltype = 0;
-            if (fl & 8) ltype = p[pos++];
+            if (fl & 8) {
+                if (pos >= n) { err = "short link message"; return false; }
+                ltype = p[pos++];
+            }
             if (fl & 4) pos += 8;
             if (fl & 16) pos += 1;
             const int lsz = 1 << (fl & 3);
@@ -415,7 +427,7 @@ bool Reader::open(const std::string& path, std::string& err)
             const uint64_t nlen = le(p + pos, lsz);
             pos += lsz;
             if (ltype != 0) { err = "soft or external link"; return false; }
-            if (pos + nlen + 8 > n) { err = "short link message"; return false; }
+            if (nlen > n || pos + nlen + 8 > n) { err = "short link message"; return false; }
             names_.emplace_back(reinterpret_cast<const char*>(p + pos), nlen);
             addrs_.push_back(le(p + pos + nlen, 8));
             found = true;

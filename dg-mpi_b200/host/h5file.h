@@ -86,7 +86,8 @@ private:
     };
     bool rd(uint64_t addr, void* dst, uint64_t n, std::string& err);
     bool header(uint64_t addr, std::vector<Msg>& msgs, std::string& err);
-    bool group_btree(uint64_t btree, const std::vector<uint8_t>& heap, int depth, std::string& err);
+    bool group_btree(uint64_t btree, const std::vector<uint8_t>& heap, int level_expected, long& budget,
+                     std::string& err);
     bool heap_data(uint64_t addr, std::vector<uint8_t>& data, std::string& err);
     bool object(const std::string& name, uint64_t& addr, std::string& err) const;
     bool dataset(const std::string& name, Dset& d, std::string& err);

@@ -212,6 +212,22 @@ def test_corrupt_files_fail_cleanly(tmp_path):
         dg_b200.read_mesh_h5(str(tmp_path / "missing.h5"))
 
 
+def test_cyclic_group_btree_fails_cleanly(tmp_path):
+    """A group B-tree node turned into an internal node whose child is itself
+    (a cycle) is refused, not walked forever."""
+    b = bytearray(open(os.path.join(MESHES, "quad_2x2.h5"), "rb").read())
+    root = int.from_bytes(b[64:72], "little")
+    stab = [m for t, m in h5_subset._messages(bytes(b), root) if t == 0x11][0]
+    btree = int.from_bytes(stab[0:8], "little")
+    assert b[btree:btree + 4] == b"TREE"
+    b[btree + 5] = 1                                        # level 1: children are B-tree nodes
+    b[btree + 32:btree + 40] = btree.to_bytes(8, "little")  # first child: the node itself
+    bad = tmp_path / "cyclic.h5"
+    bad.write_bytes(bytes(b))
+    with pytest.raises(dg_b200.DGError, match="B-tree"):
+        dg_b200.read_mesh_h5(str(bad))
+
+
 def test_two_dimensional_mesh_is_refused_by_the_context_boundary():
     m = dg_b200.read_mesh_h5(os.path.join(MESHES, "quad_2x2.h5"))
     with pytest.raises(ValueError, match="3D meshes"):
