@@ -60,7 +60,8 @@ bool read_parallel(h5::Reader& r, const std::string& name, bool integer, Paralle
     if (!r.attr_int(name + "_offsets", "nDims", nd, err) || !r.attr_int(name + "_offsets", "nRanks", nr, err))
         return false;
     if (!r.read_int(name + "_offsets", offs, nullptr, err) || !r.read_int(name + "_dims", dall, nullptr, err)) return false;
-    if (nd < 1 || nr < 1 || static_cast<int64_t>(offs.size()) != nr || static_cast<int64_t>(dall.size()) != nd * nr) {
+    if (nd < 1 || nr < 1 || nd > 16 || nr > (1 << 24) || static_cast<int64_t>(offs.size()) != nr ||
+        static_cast<int64_t>(dall.size()) != nd * nr) {
         err = name + ": inconsistent _offsets / _dims";
         return false;
     }
