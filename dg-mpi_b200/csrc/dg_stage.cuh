@@ -1318,9 +1318,10 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int bid, int nblk
 // the listed side's canonical point order.  The same operations as the stage kernel's own face
 // phase (flux_functors_impl.h:168-264), done once per face instead of once per
 // side.
-// faces per batch (measured best: 16 up to p = 3; above, 12 for the FP64
-// kernel and 8 for the FP32 one) and threads of the face kernel
-__host__ __device__ constexpr int face_batch_of(int p, int bytes) { return p <= 3 ? 16 : (bytes == 8 ? 12 : 8); }
+// faces per batch (measured best: 12 for the FP64 kernel at every order, one
+// round of 120 gather tasks on 128 threads; for the FP32 one 16 up to p = 3
+// and 8 above) and threads of the face kernel
+__host__ __device__ constexpr int face_batch_of(int p, int bytes) { return bytes == 8 ? 12 : (p <= 3 ? 16 : 8); }
 template <int P, typename T>
 __host__ __device__ constexpr int face_batch() { return face_batch_of(P, sizeof(T)); }
 constexpr int kFaceThreads = 128;
