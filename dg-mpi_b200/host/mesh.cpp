@@ -325,8 +325,11 @@ std::string prepare_mesh(const MeshView& mv, int m, PreparedMesh& out)
         double X[24];
         for (int l = 0; l < 8; ++l) {
             const unsigned nid = mv.e2n[static_cast<size_t>(e) * 8 + l];
-            if (static_cast<int>(nid) >= mv.nnode) return "element node id out of range";
-            for (int a = 0; a < 3; ++a) X[l * 3 + a] = mv.coords[static_cast<size_t>(nid) * 3 + a];
+            if (nid >= static_cast<unsigned>(mv.nnode)) return "element node id out of range";
+            for (int a = 0; a < 3; ++a) {
+                X[l * 3 + a] = mv.coords[static_cast<size_t>(nid) * 3 + a];
+                if (!std::isfinite(X[l * 3 + a])) return "element " + std::to_string(e) + " has a non-finite node coordinate";
+            }
         }
         double* J = &Jall[static_cast<size_t>(e) * 9];
         for (int i = 0; i < 3; ++i) {
@@ -471,9 +474,12 @@ std::string prepare_mesh(const MeshView& mv, int m, PreparedMesh& out)
         if (mv.elem_rank[e] != mv.rank) return "owned element " + std::to_string(e) + " has another rank";
     for (int i = 0; i < mv.nface; ++i) {
         const unsigned* r = &mv.faces[static_cast<size_t>(i) * 8];
-        const int eL = r[1], fL = r[2], oL = r[3], eR = r[5], fR = r[6], oR = r[7];
-        if (eL >= ne || eR >= ne || fL > 5 || fR > 5 || oL > 7 || oR > 7)
+        // the entries are unsigned: compared as such, a negative value written
+        // into the table is a huge one, not a small one
+        if (r[1] >= static_cast<unsigned>(ne) || r[5] >= static_cast<unsigned>(ne) || r[2] > 5u || r[6] > 5u ||
+            r[3] > 7u || r[7] > 7u)
             return "face " + std::to_string(i) + " has an out-of-range entry";
+        const int eL = r[1], fL = r[2], oL = r[3], eR = r[5], fR = r[6], oR = r[7];
         if (!mv.elem_rank) {
             if (static_cast<int>(r[0]) != mv.rank || static_cast<int>(r[4]) != mv.rank)
                 return "unsupported: face " + std::to_string(i) + " crosses ranks (single-GPU build)";

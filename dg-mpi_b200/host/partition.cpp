@@ -109,9 +109,12 @@ std::string make_halo_plan(const MeshView& mv, const int* ghost_elem, HaloPlan& 
     std::vector<Slice> s;
     for (int i = 0; i < mv.nface; ++i) {
         const unsigned* r = &mv.faces[static_cast<size_t>(i) * 8];
+        // unsigned comparisons: a negative entry is a huge one, not a small one
+        if (r[1] >= static_cast<unsigned>(mv.nelem) || r[5] >= static_cast<unsigned>(mv.nelem) || r[2] > 5u ||
+            r[6] > 5u)
+            return "face " + std::to_string(i) + " has an out-of-range entry";
         const int eL = static_cast<int>(r[1]), fL = static_cast<int>(r[2]);
         const int eR = static_cast<int>(r[5]), fR = static_cast<int>(r[6]);
-        if (eL >= mv.nelem || eR >= mv.nelem) return "face " + std::to_string(i) + " has an out-of-range element";
         const bool gL = eL >= nowned, gR = eR >= nowned;
         if (gL == gR) continue;  // owned-owned (local) or ghost-ghost (not ours)
         const int ghost = gL ? eL : eR, own = gL ? eR : eL;

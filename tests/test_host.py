@@ -178,3 +178,79 @@ def test_create_without_gpu_fails_cleanly():
     with pytest.raises(dg_b200.DGError) as ei:
         dg_b200.Case(mesh, 1)
     assert ei.value.code == 2
+
+
+FUZZ_CHILD = r"""
+import sys
+import numpy as np
+sys.path.insert(0, sys.argv[1])
+import dg_b200
+rng = np.random.default_rng(int(sys.argv[2]))
+mesh = dg_b200.periodic_box((2, 3, 2), rotate_seed=3)
+codes = {}
+for it in range(int(sys.argv[3])):
+    faces = mesh.interior_faces.copy()
+    e2n = mesh.elem_to_node_ids.copy()
+    coords = mesh.node_coords.copy()
+    for _ in range(int(rng.integers(1, 4))):
+        kind = int(rng.integers(0, 3))
+        if kind == 0:
+            i, j = int(rng.integers(0, faces.shape[0])), int(rng.integers(0, 8))
+            faces[i, j] = int(rng.choice([0, 1, 5, 7, 8, 23, 2**31 - 1, 2**32 - 1]))
+        elif kind == 1:
+            i, j = int(rng.integers(0, e2n.shape[0])), int(rng.integers(0, 8))
+            e2n[i, j] = int(rng.choice([0, coords.shape[0] - 1, coords.shape[0], 2**32 - 1]))
+        else:
+            coords[int(rng.integers(0, coords.shape[0])), int(rng.integers(0, 3))] = float(
+                rng.choice([np.nan, np.inf, -1e300, 0.0]))
+    try:
+        c = dg_b200.Case(dg_b200.Mesh(coords, e2n, faces), int(rng.integers(0, 4)))
+        c.close()
+        codes[0] = codes.get(0, 0) + 1
+    except dg_b200.DGError as e:
+        codes[e.code] = codes.get(e.code, 0) + 1
+# the halo plan of a slab partition and the 2D context take the same tables
+pm, part = dg_b200.partition_periodic_box((2, 2, 4), (0, 0, 0), (1, 1, 1), 2, 0)
+m2 = dg_b200.periodic_box_2d((3, 2), rotate_seed=4)
+for it in range(int(sys.argv[3])):
+    faces = pm.interior_faces.copy()
+    i, j = int(rng.integers(0, faces.shape[0])), int(rng.choice([1, 2, 5, 6]))
+    faces[i, j] = int(rng.choice([5, 6, 2**31 - 1, 2**32 - 1]))
+    try:
+        dg_b200.halo_plan(dg_b200.Mesh(pm.node_coords, pm.elem_to_node_ids, faces), part)
+        codes[0] = codes.get(0, 0) + 1
+    except dg_b200.DGError as e:
+        codes[e.code] = codes.get(e.code, 0) + 1
+    faces2, e2n2 = m2.interior_faces.copy(), m2.elem_to_node_ids.copy()
+    if rng.integers(0, 2):
+        faces2[int(rng.integers(0, faces2.shape[0])), int(rng.integers(0, 8))] = int(rng.choice([2, 4, 2**32 - 1]))
+    else:
+        e2n2[int(rng.integers(0, e2n2.shape[0])), int(rng.integers(0, 4))] = int(rng.choice([12, 2**32 - 1]))
+    try:
+        c = dg_b200.Case2D(dg_b200.Mesh(m2.node_coords, e2n2, faces2), 1)
+        c.close()
+        codes[0] = codes.get(0, 0) + 1
+    except dg_b200.DGError as e:
+        codes[e.code] = codes.get(e.code, 0) + 1
+print(sorted(codes.items()))
+"""
+
+
+def test_corrupt_mesh_tables_fail_cleanly(tmp_path):
+    """Random corruptions of the face table (element, face, orientation and
+    rank entries, negative values included, which the unsigned table holds
+    as huge ones), the element-to-node table and the node coordinates (NaN,
+    infinities) end in an error code from the host-side validation (or, where
+    the corruption leaves a valid mesh, in a context or the no-GPU error),
+    never in a crash -- for 3D contexts, the halo plan of a partition and 2D
+    contexts; run in a child process so that a fault would fail this test."""
+    import subprocess
+    import sys
+    script = tmp_path / "fuzz.py"
+    script.write_text(FUZZ_CHILD)
+    r = subprocess.run([sys.executable, str(script), os.path.join(ROOT, "dg-mpi_b200"), "11", "300"],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    counts = dict(eval(r.stdout.strip()))
+    assert set(counts) <= {0, 1, 2, 5}, counts
+    assert counts.get(1, 0) + counts.get(5, 0) > 400, counts
