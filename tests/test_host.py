@@ -232,6 +232,15 @@ for it in range(int(sys.argv[3])):
         codes[0] = codes.get(0, 0) + 1
     except dg_b200.DGError as e:
         codes[e.code] = codes.get(e.code, 0) + 1
+    # a batch with one corrupt case among valid ones
+    bad = dg_b200.Mesh(mesh.node_coords, mesh.elem_to_node_ids, mesh.interior_faces.copy())
+    bad.interior_faces[int(rng.integers(0, bad.interior_faces.shape[0])), int(rng.choice([1, 5]))] = 2**32 - 1
+    try:
+        b = dg_b200.Batch([(mesh, 2), (bad, 3)])
+        b.close()
+        codes[0] = codes.get(0, 0) + 1
+    except dg_b200.DGError as e:
+        codes[e.code] = codes.get(e.code, 0) + 1
 print(sorted(codes.items()))
 """
 
@@ -242,8 +251,9 @@ def test_corrupt_mesh_tables_fail_cleanly(tmp_path):
     as huge ones), the element-to-node table and the node coordinates (NaN,
     infinities) end in an error code from the host-side validation (or, where
     the corruption leaves a valid mesh, in a context or the no-GPU error),
-    never in a crash -- for 3D contexts, the halo plan of a partition and 2D
-    contexts; run in a child process so that a fault would fail this test."""
+    never in a crash -- for 3D contexts, the halo plan of a partition, 2D
+    contexts and batches; run in a child process so that a fault would fail
+    this test."""
     import subprocess
     import sys
     script = tmp_path / "fuzz.py"
