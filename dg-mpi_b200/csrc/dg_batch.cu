@@ -669,7 +669,8 @@ int dg_batch_l2_error(dg_batch* b, int c, int ic_type, const double* data, int n
 {
     if (!case_ok(b, c) || !err) return bfail(b, DG_ERR_ARG, "dg_batch_l2_error: bad argument");
     if (ic_type < DG_IC_UNIFORM || ic_type > DG_IC_TAYLOR_GREEN) return bfail(b, DG_ERR_ARG, "unknown exact solution");
-    if (ndata > 0 && !data) return bfail(b, DG_ERR_ARG, "dg_batch_l2_error: null data");
+    const int need[] = {5, 0, 0, 9, 1};
+    if (ndata < need[ic_type] || (ndata > 0 && !data)) return bfail(b, DG_ERR_ARG, "exact solution needs more data values");
     const BatchCase& k = b->cases[c];
     BatchGroup& g = b->groups[k.group];
     if (cudaSetDevice(b->device) != cudaSuccess) return bfail(b, DG_ERR_CUDA, "cudaSetDevice failed");

@@ -1187,6 +1187,12 @@ void dgi::destroy_ctx(dg_ctx* c)
 }
 
 // ===========================================================================
+namespace {
+// data values each initial condition / exact solution family reads (DG_IC_*)
+constexpr int kIcData[] = {5, 0, 0, 9, 1};
+
+}  // namespace
+
 extern "C" {
 
 int dg_create(const dg_case_desc* cd, const dg_mesh_desc* md, dg_ctx** out)
@@ -1651,10 +1657,10 @@ int dg_project_ic(dg_ctx* c, int ic_type, const double* data, int ndata, double 
     dgi::NvtxRange nvtx_("dg_project_ic");
     if (!c) return fail(c, DG_ERR_ARG, "dg_project_ic: null context");
     if (ic_type < DG_IC_UNIFORM || ic_type > DG_IC_TAYLOR_GREEN) return fail(c, DG_ERR_ARG, "unknown initial condition");
+    if (ndata < kIcData[ic_type] || (ndata > 0 && !data))
+        return fail(c, DG_ERR_ARG, "initial condition needs more data values");
     double d[16] = {0};
     for (int i = 0; i < ndata && i < 16; ++i) d[i] = data[i];
-    const int need[] = {5, 0, 0, 9, 1};
-    if (ndata < need[ic_type]) return fail(c, DG_ERR_ARG, "initial condition needs more data values");
     DG_CUDA(c, cudaSetDevice(c->device));
     int rc = project_ic_device(c, ic_type, d, 16, t, c->gamma, c->R, 0, c->ne);
     if (rc) return rc;
@@ -1680,6 +1686,8 @@ int dg_l2_error(dg_ctx* c, int ic_type, const double* data, int ndata, double t,
     dgi::NvtxRange nvtx_("dg_l2_error");
     if (!c || !err) return fail(c, DG_ERR_ARG, "dg_l2_error: null argument");
     if (ic_type < DG_IC_UNIFORM || ic_type > DG_IC_TAYLOR_GREEN) return fail(c, DG_ERR_ARG, "unknown exact solution");
+    if (ndata < kIcData[ic_type] || (ndata > 0 && !data))
+        return fail(c, DG_ERR_ARG, "exact solution needs more data values");
     DG_CUDA(c, cudaSetDevice(c->device));
     double sums[5];
     int rc = run_reduce(c, 0, ic_type, data, ndata, t, sums, 0, c->ne, c->gamma, c->R);
