@@ -264,3 +264,33 @@ def test_corrupt_mesh_tables_fail_cleanly(tmp_path):
     counts = dict(eval(r.stdout.strip()))
     assert set(counts) <= {0, 1, 2, 5}, counts
     assert counts.get(1, 0) + counts.get(5, 0) > 400, counts
+
+
+NULL_CHILD = r"""
+import ctypes, re, sys
+sys.path.insert(0, sys.argv[1])
+import dg_b200
+lib = dg_b200.library()
+text = re.sub(r"/\*.*?\*/", "", open(sys.argv[2]).read(), flags=re.S)
+for n in sorted(set(re.findall(r"\b(dg[a-z0-9_]*)\s*\(", text))):
+    f = getattr(lib, n)
+    args = [0 if t in (ctypes.c_int, ctypes.c_uint, ctypes.c_longlong) else 0.0 if t is ctypes.c_double else None
+            for t in f.argtypes]
+    f(*args)
+print("survived")
+"""
+
+
+def test_every_entry_point_survives_null_and_zero_arguments(tmp_path):
+    """Every function of include/dg_b200.h called with NULL pointers and zero
+    sizes (a null context, no mesh, no buffers) returns an error code (or, for
+    the destroy calls and pointer getters, nothing) instead of dereferencing
+    them; run in a child process so that a fault would fail this test."""
+    import subprocess
+    import sys
+    script = tmp_path / "nulls.py"
+    script.write_text(NULL_CHILD)
+    r = subprocess.run([sys.executable, str(script), os.path.join(ROOT, "dg-mpi_b200"),
+                        os.path.join(ROOT, "include", "dg_b200.h")], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert r.stdout.strip().endswith("survived")
