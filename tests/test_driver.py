@@ -41,6 +41,44 @@ def test_driver_rejects_unsupported_input(tmp_path, bad, msg):
     assert r.returncode == 2 and msg in r.stderr
 
 
+def test_mutated_decks_are_refused_or_parsed_never_crash(tmp_path):
+    """Seeded mutations of the example decks (deleted, truncated, shuffled and
+    garbage lines, out-of-range values, unterminated strings and arrays)
+    end in a clean parse (exit 0) or a refusal with a message (exit 2),
+    never in a signal."""
+    import random
+    rng = random.Random(7)
+    decks = [open(os.path.join(EXAMPLES, f)).read() for f in sorted(os.listdir(EXAMPLES)) if f.endswith(".toml")]
+    junk = ['"', "]", "[", "=", " = 1e999", " = -5", ",", "\\"]
+    inserts = ["[Numerics]", "order = 99", "order = -1", "data = []", "timestep = 0", "end = -1",
+               'file = "nonexistent.h5"', 'type = "Bogus"', 'x = "unterminated']
+    values = ['"a"', "[1,2", "1.5.5", "true", "-0", "99999999999999999999"]
+    outcomes = {0: 0, 2: 0}
+    for it in range(150):
+        lines = rng.choice(decks).splitlines()
+        for _ in range(rng.randint(1, 3)):
+            k = rng.randrange(len(lines))
+            op = rng.randrange(6)
+            if op == 0:
+                del lines[k]
+            elif op == 1:
+                lines[k] = lines[k][:rng.randrange(len(lines[k]) + 1)]
+            elif op == 2:
+                lines[k] += rng.choice(junk)
+            elif op == 3:
+                lines.insert(k, rng.choice(inserts))
+            elif op == 4 and "=" in lines[k]:
+                lines[k] = lines[k].split("=")[0] + "= " + rng.choice(values)
+            else:
+                lines[k] = "".join(rng.sample(lines[k], len(lines[k])))
+        deck = tmp_path / f"d{it}.toml"
+        deck.write_text("\n".join(lines) + "\n")
+        r = run(["-input", str(deck), "-check"], cwd=str(tmp_path))
+        assert r.returncode in (0, 2), (it, r.returncode, deck.read_text(), r.stderr[-500:])
+        outcomes[r.returncode] += 1
+    assert outcomes[2] > 50 and outcomes[0] > 10, outcomes
+
+
 def _check_regression(r, golden):
     assert r.returncode == 0, r.stderr
     err = {int(m.group(1)): float(m.group(2)) for m in re.finditer(r"norm_total_error\((\d)\)=(\S+)", r.stdout)}
