@@ -267,6 +267,18 @@ int dg_solution_read_h5_impl(const char* path, int* nelem, int* nb, int* ns, dou
         return ferr(DG_ERR_ARG, std::string("dg_solution_read_h5: ") + path + ": " + err);
     if (ne < 1 || b < 1 || s < 1 || ne > (1LL << 30) || b > 4096 || s > 64)
         return ferr(DG_ERR_ARG, "dg_solution_read_h5: sizes out of range");
+    // the sizes must be those of the stored coefficients (a caller allocates
+    // from them before the data is read)
+    {
+        std::vector<uint64_t> dims;
+        h5::Type ty;
+        if (!r.shape("Solution Coefficients", dims, ty, err))
+            return ferr(DG_ERR_ARG, std::string("dg_solution_read_h5: ") + path + ": " + err);
+        uint64_t total = 1;
+        for (uint64_t d : dims) total = d > 0 && total > (1ULL << 62) / d ? 0 : total * d;
+        if (dims.empty() || total != static_cast<uint64_t>(ne) * static_cast<uint64_t>(b) * static_cast<uint64_t>(s))
+            return ferr(DG_ERR_ARG, "dg_solution_read_h5: element, basis and variable counts disagree with the stored coefficients");
+    }
     *nelem = static_cast<int>(ne);
     *nb = static_cast<int>(b);
     *ns = static_cast<int>(s);

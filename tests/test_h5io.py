@@ -212,6 +212,28 @@ def test_corrupt_files_fail_cleanly(tmp_path):
         dg_b200.read_mesh_h5(str(tmp_path / "missing.h5"))
 
 
+def test_solution_sizes_must_match_the_stored_coefficients(tmp_path):
+    """The sizes query of a solution file checks the element, basis and
+    variable counts against the stored coefficients, so a caller never
+    allocates from a corrupt count."""
+    m = dg_b200.periodic_box((2, 2, 2))
+    U = np.random.default_rng(0).standard_normal((8, 27, 5))
+    good = tmp_path / "sol.h5"
+    dg_b200.write_solution_h5(str(good), m, 2, U, 0.5)
+    data = bytearray(good.read_bytes())
+    import struct
+    # the root attribute "Number of Elements" holds 8 as an 8-byte integer right after its name
+    at = data.find(b"Number of Elements")
+    assert at > 0
+    pos = data.find(struct.pack("<q", 8), at)
+    assert pos > 0
+    data[pos:pos + 8] = struct.pack("<q", 486539272)
+    bad = tmp_path / "bad.h5"
+    bad.write_bytes(bytes(data))
+    with pytest.raises(dg_b200.DGError, match="disagree with the stored coefficients"):
+        dg_b200.read_solution_h5(str(bad))
+
+
 def test_cyclic_group_btree_fails_cleanly(tmp_path):
     """A group B-tree node turned into an internal node whose child is itself
     (a cycle) is refused, not walked forever."""
