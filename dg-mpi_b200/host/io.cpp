@@ -127,6 +127,19 @@ int dg_mesh_read_h5_impl(const char* path, int* dim, int* qorder, int* nnode_per
     if (d < 1 || d > 3 || q < 1 || ne < 1 || nn < 1 || nf < 0 || npe < 2 || ne > (1LL << 30) || nn > (1LL << 31) - 1 ||
         nf > (1LL << 31) - 1 || ne * npe > (1LL << 34))
         return ferr(DG_ERR_ARG, std::string("dg_mesh_read_h5: ") + path + ": sizes out of range");
+    // the counts must be those of the stored arrays (a caller allocates from
+    // them before the data is read)
+    const std::pair<const char*, int64_t> stored[3] = {{"NodeCoords", nn * d}, {"Elem2Nodes", ne * npe},
+                                                       {"IFaceData", nf * 6}};
+    for (const auto& [name, want] : stored) {
+        std::vector<uint64_t> dims;
+        h5::Type ty;
+        if (!r.shape(name, dims, ty, err)) return ferr(DG_ERR_ARG, std::string("dg_mesh_read_h5: ") + path + ": " + err);
+        uint64_t total = 1;
+        for (uint64_t n : dims) total = n > 0 && total > (1ULL << 62) / n ? 0 : total * n;
+        if (total != static_cast<uint64_t>(want))
+            return ferr(DG_ERR_ARG, std::string("dg_mesh_read_h5: ") + path + ": array sizes disagree with the counts");
+    }
     *dim = static_cast<int>(d);
     *qorder = static_cast<int>(q);
     *nnode_per_elem = static_cast<int>(npe);

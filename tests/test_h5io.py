@@ -234,6 +234,26 @@ def test_solution_sizes_must_match_the_stored_coefficients(tmp_path):
         dg_b200.read_solution_h5(str(bad))
 
 
+def test_mesh_counts_must_match_the_stored_arrays(tmp_path):
+    """The sizes query of a mesh file checks nNode, nElem and nIFace against
+    the stored arrays before a caller allocates from them (a file written by
+    the test-side encoder with every array intact and one count wrong)."""
+    mesh = dg_b200.periodic_box((2, 2, 2))
+    good = tmp_path / "mesh.h5"
+    dg_b200.write_mesh_h5(str(good), mesh)
+    ds = h5_subset.read(str(good))["datasets"]
+    for key in ("nElem", "nNode", "nIFace"):
+        bad_ds = dict(ds)
+        bad_ds[key] = np.array(1 << 29, dtype=np.int64)
+        bad = tmp_path / f"bad_{key}.h5"
+        h5_subset.write(str(bad), bad_ds)
+        with pytest.raises(dg_b200.DGError, match="disagree with the counts"):
+            dg_b200.read_mesh_h5(str(bad))
+    ok = tmp_path / "ok.h5"
+    h5_subset.write(str(ok), ds)
+    assert dg_b200.read_mesh_h5(str(ok)).elem_to_node_ids.shape == (8, 8)
+
+
 def test_cyclic_group_btree_fails_cleanly(tmp_path):
     """A group B-tree node turned into an internal node whose child is itself
     (a cycle) is refused, not walked forever."""
