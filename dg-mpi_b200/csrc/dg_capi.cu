@@ -1328,7 +1328,8 @@ int dg_halo_unpack(dg_ctx* c, int buf, const double* d_recv, void* stream)
 int dg_rk4_stage(dg_ctx* c, int stage, double dt, int range)
 {
     dgi::NvtxRange nvtx_("dg_rk4_stage");
-    if (!c || stage < 1 || stage > 4 || range < 0 || range > 2) return fail(c, DG_ERR_ARG, "dg_rk4_stage: bad argument");
+    if (!c || stage < 1 || stage > 4 || range < 0 || range > 2 || !std::isfinite(dt))
+        return fail(c, DG_ERR_ARG, "dg_rk4_stage: bad argument");
     DG_CUDA(c, cudaSetDevice(c->device));
     const int e0 = range == 2 ? c->ninterior : 0, e1 = range == 1 ? c->ninterior : c->ne;
     switch (stage) {
@@ -1399,7 +1400,7 @@ int dg_residual(dg_ctx* c, double* res)
 int dg_mass_inverse_residual(dg_ctx* c, double dt, double* dU)
 {
     dgi::NvtxRange nvtx_("dg_mass_inverse_residual");
-    if (!c || !dU) return fail(c, DG_ERR_ARG, "dg_mass_inverse_residual: null argument");
+    if (!c || !dU || !std::isfinite(dt)) return fail(c, DG_ERR_ARG, "dg_mass_inverse_residual: bad argument");
     DG_CUDA(c, cudaSetDevice(c->device));
     int rc = launch_stage(c, dgk::kModeMassInv, c->d_U0, c->d_U0, c->d_acc, dt);
     if (rc) return rc;
@@ -1486,7 +1487,7 @@ int prepare_rk4_graph(dg_ctx* c, double dt)
 int dg_rk4_steps_timed(dg_ctx* c, double dt, int nsteps, double* device_ms)
 {
     dgi::NvtxRange nvtx_("dg_rk4_steps_timed");
-    if (!c || nsteps < 0 || !device_ms) return fail(c, DG_ERR_ARG, "dg_rk4_steps_timed: bad argument");
+    if (!c || nsteps < 0 || !device_ms || !std::isfinite(dt)) return fail(c, DG_ERR_ARG, "dg_rk4_steps_timed: bad argument");
     DG_CUDA(c, cudaSetDevice(c->device));
     int rc = prepare_rk4_graph(c, dt);
     if (rc) return rc;
@@ -1621,7 +1622,7 @@ int dg_tune_stage(dg_ctx* c, int reps, int* best, double* ms_per_variant)
 int dg_rk4_steps(dg_ctx* c, double dt, int nsteps)
 {
     dgi::NvtxRange nvtx_("dg_rk4_steps");
-    if (!c || nsteps < 0) return fail(c, DG_ERR_ARG, "dg_rk4_steps: bad argument");
+    if (!c || nsteps < 0 || !std::isfinite(dt)) return fail(c, DG_ERR_ARG, "dg_rk4_steps: bad argument");
     if (nsteps == 0) return DG_OK;
     DG_CUDA(c, cudaSetDevice(c->device));
     int rc = prepare_rk4_graph(c, dt);
@@ -1634,7 +1635,7 @@ int dg_rk4_steps(dg_ctx* c, double dt, int nsteps)
 int dg_fe_steps(dg_ctx* c, double dt, int nsteps)
 {
     dgi::NvtxRange nvtx_("dg_fe_steps");
-    if (!c || nsteps < 0) return fail(c, DG_ERR_ARG, "dg_fe_steps: bad argument");
+    if (!c || nsteps < 0 || !std::isfinite(dt)) return fail(c, DG_ERR_ARG, "dg_fe_steps: bad argument");
     DG_CUDA(c, cudaSetDevice(c->device));
     for (int s = 0; s < nsteps; ++s) {
         int rc = launch_stage(c, dgk::kModeFE, c->d_U0, c->d_U0, c->d_Ua, dt);
