@@ -216,6 +216,36 @@ def test_nonphysical_state_is_reported_not_faulted():
     assert gpu.status() == 0
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed_fp32"])
+@pytest.mark.parametrize("flux", ["LaxFriedrichs", "HLLC"])
+def test_garbage_states_are_reported_by_every_default_variant(flux, precision):
+    """States no physical flow has (NaN, infinities, negative density or
+    energy, huge values) stepped by the default variant of p = 1 .. 5 end in
+    DG_ERR_NONPHYSICAL with the status word set, and a valid state steps
+    again afterwards: the kernels' arithmetic on garbage reports, it never
+    faults or hangs (no index depends on a state value)."""
+    rng = np.random.default_rng(23)
+    mesh = dg_b200.periodic_box((3, 2, 2), (0, 0, 0), (10.0, 10.0, 10.0), rotate_seed=2)
+    for p in range(1, 6):
+        case = dg_b200.Case(mesh, p, flux=flux, gas_constant=1.0, precision=precision)
+        good = case.project_ic("IsentropicVortexXY", VORTEX_XY)
+        dt = case.cfl_time_step(good, 0.1)
+        for garbage in (np.nan, np.inf, -1.0, 1e300):
+            U = good.copy()
+            idx = rng.integers(0, U.size, 7)
+            U.reshape(-1)[idx] = garbage
+            U[0, :, 0] = garbage if garbage != 1e300 else -1.0  # always one bad density
+            case.set_state(U)
+            with pytest.raises(dg_b200.DGError) as ei:
+                case.rk4(dt, 1)
+            assert ei.value.code == 3, (p, garbage, ei.value)
+            assert case.status() != 0
+        case.set_state(good)
+        case.rk4(dt, 2)
+        assert case.status() == 0
+        case.close()
+
+
 def test_time_step_change_rebuilds_graph():
     _, gpu, orc = make_pair((2, 2, 2), 2)
     U = orc.project_ic("IsentropicVortexXY", VORTEX_XY)
